@@ -1,0 +1,216 @@
+"""ctypes view of the C-ABI in include/pale_b200.h.
+
+The renderer lives in ``libpale_b200.so`` next to this file (built by
+``__graft_entry__.build()`` or ``python -m differentiablepointrendering_b200.build``).
+There is no fallback: importing the product without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+from .scene import POINT_FIELDS, SceneArrays, as_points
+
+LIB_NAME = "libpale_b200.so"
+
+f32p = C.POINTER(C.c_float)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+
+
+class PaleSettings(C.Structure):
+    _fields_ = [("photons_per_launch", C.c_uint32), ("max_bounces", C.c_uint32),
+                ("forward_passes", C.c_uint32), ("gather_passes", C.c_uint32),
+                ("adjoint_bounces", C.c_uint32), ("adjoint_passes", C.c_uint32),
+                ("seed", C.c_uint64), ("random_number", C.c_uint32), ("rr_start", C.c_uint32),
+                ("q_null", C.c_float), ("q_reflect", C.c_float), ("q_transmit", C.c_float),
+                ("gather_radius", C.c_float), ("leaf_size", C.c_uint32), ("rng_mode", C.c_uint32),
+                ("debug_images", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float)]
+
+
+class PalePoints(C.Structure):
+    _fields_ = [("count", C.c_uint32)] + [(k, f32p) for k in POINT_FIELDS]
+
+
+class PaleSceneDesc(C.Structure):
+    _fields_ = [("num_vertices", C.c_uint32), ("vertices", f32p),
+                ("num_triangles", C.c_uint32), ("triangles", u32p),
+                ("num_meshes", C.c_uint32), ("mesh_ranges", u32p),
+                ("num_materials", C.c_uint32), ("materials", f32p),
+                ("num_instances", C.c_uint32), ("instance_mesh", u32p), ("instance_material", u32p),
+                ("instance_object_to_world", f32p), ("instance_world_to_object", f32p),
+                ("num_cameras", C.c_uint32), ("camera_inv_view", f32p), ("camera_forward", f32p),
+                ("camera_fovy_deg", f32p), ("camera_size", u32p), ("camera_names", C.c_char_p),
+                ("points", PalePoints)]
+
+
+class PaleStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in (
+        "photon_segments", "gather_segments", "adjoint_segments", "photons_stored", "gradient_events",
+        "gather_queries", "node_visits", "surfel_tests", "photons_scanned")] + \
+        [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms")]
+
+    def as_dict(self) -> Dict[str, float]:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Settings-dict keys of the reference (pale_bindings.cpp:123-139) plus the
+# ones this build exposes that the reference hard-codes.
+SETTINGS_KEYS = {
+    "photons": "photons_per_launch", "bounces": "max_bounces", "forward_passes": "forward_passes",
+    "gather_passes": "gather_passes", "adjoint_bounces": "adjoint_bounces",
+    "adjoint_passes": "adjoint_passes", "seed": "seed", "random_number": "random_number",
+    "rr_start": "rr_start", "q_null": "q_null", "q_reflect": "q_reflect", "q_transmit": "q_transmit",
+    "gather_radius": "gather_radius", "leaf_size": "leaf_size", "debug_images": "debug_images",
+    "exposure": "exposure", "gamma": "gamma",
+}
+IGNORED_KEYS = ("logging", "depth_distort_weight", "normal_consistency_weight")
+
+
+def default_settings(lib=None) -> PaleSettings:
+    s = PaleSettings()
+    s.photons_per_launch, s.max_bounces, s.forward_passes, s.gather_passes = 1000000, 6, 6, 6
+    s.adjoint_bounces, s.adjoint_passes, s.seed, s.random_number, s.rr_start = 6, 6, 42, 42, 6
+    s.q_null, s.q_reflect, s.q_transmit, s.gather_radius = 0.5, 0.5, 0.0, 0.01
+    s.leaf_size, s.rng_mode, s.debug_images, s.exposure, s.gamma = 4, 0, 0, 1.0, 2.2
+    return s
+
+
+def settings_from_dict(d: Optional[dict]) -> PaleSettings:
+    s = default_settings()
+    for k, v in (d or {}).items():
+        if k in IGNORED_KEYS:
+            continue
+        if k == "rng_mode":
+            s.rng_mode = {"reference": 0, "decorrelated": 1}.get(v, v) if isinstance(v, str) else int(v)
+            continue
+        if k not in SETTINGS_KEYS:
+            raise KeyError(f"unknown renderer setting '{k}'")
+        field = SETTINGS_KEYS[k]
+        cur = getattr(s, field)
+        setattr(s, field, float(v) if isinstance(cur, float) else int(v))
+    return s
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+class PointsHolder:
+    """Keeps contiguous float32 arrays alive behind a PalePoints struct."""
+
+    def __init__(self, pts: Optional[Dict[str, np.ndarray]] = None, n: int = 0, alloc: bool = False):
+        if pts is None:
+            from .scene import empty_points
+            pts = empty_points(n)
+        self.arrays = as_points(pts) if not alloc else pts
+        self.struct = PalePoints()
+        self.struct.count = int(self.arrays["position"].shape[0])
+        for k in POINT_FIELDS:
+            setattr(self.struct, k, _ptr(self.arrays[k], f32p))
+
+
+class SceneDescHolder:
+    """Builds a PaleSceneDesc from SceneArrays and keeps its buffers alive."""
+
+    def __init__(self, sc: SceneArrays, struct_cls=PaleSceneDesc, points_cls=PalePoints):
+        c = lambda a, dt: np.ascontiguousarray(a, dt)
+        self.v = c(sc.vertices, np.float32)
+        self.t = c(sc.triangles, np.uint32)
+        self.mr = c(sc.mesh_ranges, np.uint32)
+        self.mat = c(sc.materials, np.float32)
+        self.im = c(sc.instance_mesh, np.uint32)
+        self.imat = c(sc.instance_material, np.uint32)
+        self.o2w = c(sc.object_to_world, np.float32)
+        self.w2o = c(sc.world_to_object, np.float32)
+        self.civ = c(sc.camera_inv_view, np.float32)
+        self.cf = c(sc.camera_forward, np.float32)
+        self.fov = c(sc.camera_fovy, np.float32)
+        self.csz = c(sc.camera_size, np.uint32)
+        names = b"".join(n.encode()[:15].ljust(16, b"\0") for n in sc.camera_names)
+        self.names = C.create_string_buffer(names, max(1, len(names)))
+        self.points = PointsHolder(sc.points)
+        d = struct_cls()
+        d.num_vertices, d.vertices = self.v.shape[0], _ptr(self.v, f32p)
+        d.num_triangles, d.triangles = self.t.shape[0], _ptr(self.t, u32p)
+        d.num_meshes, d.mesh_ranges = self.mr.shape[0], _ptr(self.mr, u32p)
+        d.num_materials, d.materials = self.mat.shape[0], _ptr(self.mat, f32p)
+        d.num_instances = self.im.shape[0]
+        d.instance_mesh, d.instance_material = _ptr(self.im, u32p), _ptr(self.imat, u32p)
+        d.instance_object_to_world, d.instance_world_to_object = _ptr(self.o2w, f32p), _ptr(self.w2o, f32p)
+        d.num_cameras = self.civ.shape[0]
+        d.camera_inv_view, d.camera_forward = _ptr(self.civ, f32p), _ptr(self.cf, f32p)
+        d.camera_fovy_deg, d.camera_size = _ptr(self.fov, f32p), _ptr(self.csz, u32p)
+        d.camera_names = C.cast(self.names, C.c_char_p)
+        p = points_cls()
+        p.count = self.points.struct.count
+        for k in POINT_FIELDS:
+            setattr(p, k, getattr(self.points.struct, k))
+        d.points = p
+        self.struct = d
+
+
+_LIB = None
+
+
+def library_path() -> str:
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+
+
+def load_library() -> C.CDLL:
+    """Loads the CUDA library; raises if it was not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.isfile(path):
+        raise RuntimeError(f"{LIB_NAME} is missing at {path}; build it with "
+                           "`python -m differentiablepointrendering_b200.build`")
+    lib = C.CDLL(path)
+    H = C.c_void_p
+    sig = {
+        "pale_default_settings": (None, [C.POINTER(PaleSettings)]),
+        "pale_version": (C.c_char_p, []),
+        "pale_last_error": (C.c_char_p, [H]),
+        "pale_create": (C.c_int, [C.POINTER(PaleSceneDesc), C.POINTER(PaleSettings), C.POINTER(H)]),
+        "pale_destroy": (C.c_int, [H]),
+        "pale_point_count": (C.c_int, [H, u32p]),
+        "pale_camera_count": (C.c_int, [H, u32p]),
+        "pale_camera_info": (C.c_int, [H, C.c_uint32, C.c_char_p, u32p, u32p]),
+        "pale_render_forward": (C.c_int, [H, C.c_uint32, u32p, f32p, f32p]),
+        "pale_render_forward_device": (C.c_int, [H, C.c_uint32, u32p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "pale_render_backward": (C.c_int, [H, C.c_uint32, u32p, f32p, C.POINTER(PalePoints), f32p]),
+        "pale_render_backward_device": (C.c_int, [H, C.c_uint32, u32p, C.c_void_p, C.POINTER(PalePoints),
+                                                  C.c_void_p]),
+        "pale_get_points": (C.c_int, [H, C.POINTER(PalePoints)]),
+        "pale_get_order": (C.c_int, [H, u32p]),
+        "pale_apply_points": (C.c_int, [H, C.POINTER(PalePoints)]),
+        "pale_rebuild": (C.c_int, [H, C.POINTER(PalePoints)]),
+        "pale_trace_rays": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, i32p, f32p, f32p, f32p]),
+        "pale_gather_irradiance": (C.c_int, [H, C.c_uint32, f32p, f32p, f32p]),
+        "pale_load_photons": (C.c_int, [H, C.c_uint32, f32p, f32p, f32p]),
+        "pale_get_photons": (C.c_int, [H, u32p, f32p, f32p, f32p, u32p, u32p, f32p]),
+        "pale_get_bvh": (C.c_int, [H, u32p, u32p, f32p, C.c_uint32]),
+        "pale_get_stats": (C.c_int, [H, C.POINTER(PaleStats)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_create", "pale_destroy",
+            "pale_point_count", "pale_camera_count", "pale_camera_info", "pale_render_forward",
+            "pale_render_forward_device", "pale_render_backward", "pale_render_backward_device",
+            "pale_get_points", "pale_get_order", "pale_apply_points", "pale_rebuild", "pale_trace_rays",
+            "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
+            "pale_get_stats")
+
+
+def cams_array(idx: Sequence[int]) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(list(idx), np.uint32))

@@ -1,0 +1,1044 @@
+// api.cu -- host implementation of the C-ABI in include/pale_b200.h.
+//
+// A pale_handle owns every device buffer of one renderer: meshes, cameras,
+// the surfel parameters in BVH order with their derived arrays and LBVH,
+// the photon store and grid, the ray queues and the adjoint state.  Each
+// entry point runs on the handle's own stream and returns a status code;
+// nothing throws across the boundary.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pale_b200.h"
+#include "kernels.h"
+
+using namespace pale;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define CK(x)                                                                                       \
+  do {                                                                                              \
+    cudaError_t e_ = (x);                                                                           \
+    if (e_ != cudaSuccess)                                                                          \
+      throw CudaError(std::string(#x) + " failed: " + cudaGetErrorString(e_) + " (" __FILE__ ":" + \
+                      std::to_string(__LINE__) + ")");                                              \
+  } while (0)
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    if (count == 0) count = 1;
+    CK(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void ensure(size_t count) {
+    if (count > n || !p) alloc(count);
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+struct PointsBufs {
+  DBuf<float> pos, tu, tv, sc, alb, op, beta, shape;
+  void alloc(uint32_t n) {
+    pos.ensure(3 * (size_t)n); tu.ensure(3 * (size_t)n); tv.ensure(3 * (size_t)n); sc.ensure(2 * (size_t)n);
+    alb.ensure(3 * (size_t)n); op.ensure(n); beta.ensure(n); shape.ensure(n);
+  }
+  PointsDev view() const { return PointsDev{pos.p, tu.p, tv.p, sc.p, alb.p, op.p, beta.p, shape.p}; }
+};
+
+uint32_t next_pow2(uint32_t v) {
+  uint32_t c = 1;
+  while (c < v) c <<= 1;
+  return c;
+}
+
+}  // namespace
+
+struct pale_handle {
+  pale_settings st{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // meshes
+  uint32_t n_inst = 0, n_tris = 0;
+  DBuf<float> o2w, w2o;
+  DBuf<float4> inst_box, tri, materials;
+  DBuf<uint2> tri_range;
+  DBuf<uint32_t> inst_mat;
+  std::vector<float> h_inst_box;   // lo.xyz hi.xyz per instance
+  // lights
+  uint32_t n_lights = 0;
+  DBuf<uint4> light_rec;
+  DBuf<float4> light_col;
+  DBuf<float> light_area, light_cdf;
+  DBuf<uint32_t> light_tri;
+  float light0_area = 0.f;
+  // cameras
+  std::vector<CameraRec> cams;
+  std::vector<std::string> cam_names;
+  DBuf<CameraRec> d_cams;
+  // surfels
+  uint32_t np = 0;
+  PointsBufs asset, collected, params;
+  DBuf<float4> sf_pe, sf_n, sf_u, sf_v, sf_cn, sf_alb;
+  DBuf<float> aabb_lo, aabb_hi, bounds_part, bounds;
+  DBuf<uint32_t> codes, order, codes_tmp, order_tmp, sort_temp, rfirst, rlast, parent, leaf_parent, visits, d_n;
+  DBuf<int32_t> lc, rc;
+  DBuf<float> box;
+  DBuf<BvhNode> nodes;
+  uint32_t node_count = 0, top = 0;
+  float pc_lo[3] = {0, 0, 0}, pc_hi[3] = {0, 0, 0};
+  // photon grid
+  float radius = 0.01f, origin[3] = {0, 0, 0}, cell = 0.005f;
+  int res[3] = {1, 1, 1};
+  uint32_t cells = 1;
+  int key_bits = 8;
+  uint64_t photon_cap = 0;
+  DBuf<float4> ph_a, ph_b, ph_sa, ph_sb, g_pa, g_pb;
+  DBuf<float> ph_c, ph_sc, g_pc;
+  DBuf<uint32_t> g_cell_id, g_sorted, g_keys, g_vals_tmp, g_sort_temp, g_cell_count, g_cell_off, g_scan_temp,
+      g_stored, g_attempts;
+  // queues
+  uint32_t qcap = 0;
+  DBuf<RayRec> q0, q1, qstage;
+  DBuf<uint8_t> qflags;
+  DBuf<uint2> tile_counts, tile_offsets;
+  DBuf<float4> pend_a, pend_b;
+  DBuf<uint4> pend_c;
+  DBuf<EventRec> ev_stage, ev_list;
+  // run state, seeds, images, gradients
+  DBuf<RunState> run;
+  DBuf<uint32_t> seeds_fwd, seeds_adj;
+  DBuf<float> img_raw, img_ldr, dldi, dbg;
+  PointsBufs grads;
+  pale_stats stats{};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+
+  ~pale_handle() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (ev2) cudaEventDestroy(ev2);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  SceneView view() const {
+    SceneView s{};
+    s.mesh.o2w = o2w.p;
+    s.mesh.w2o = w2o.p;
+    s.mesh.box = inst_box.p;
+    s.mesh.tri_range = tri_range.p;
+    s.mesh.tri = tri.p;
+    s.mesh.material = inst_mat.p;
+    s.mesh.materials = materials.p;
+    s.mesh.instances = n_inst;
+    s.sf = SurfelView{sf_pe.p, sf_n.p, sf_u.p, sf_v.p, sf_cn.p, sf_alb.p, np};
+    s.nodes = nodes.p;
+    s.node_count = np ? node_count : 0;
+    s.top_nodes = np ? std::min(top, node_count) : 0;
+    s.pc_lo = v3(pc_lo[0], pc_lo[1], pc_lo[2]);
+    s.pc_hi = v3(pc_hi[0], pc_hi[1], pc_hi[2]);
+    s.has_pc = np > 0;
+    s.lights = LightView{n_lights, light_rec.p, light_col.p, light_area.p, light_cdf.p, light_tri.p};
+    GridView& g = s.grid;
+    g.radius = radius;
+    g.origin = v3(origin[0], origin[1], origin[2]);
+    g.cell = v3(cell, cell, cell);
+    g.res[0] = res[0]; g.res[1] = res[1]; g.res[2] = res[2];
+    g.cells = cells;
+    g.cell_off = g_cell_off.p;
+    g.pa = g_pa.p;
+    g.pb = g_pb.p;
+    g.pc = g_pc.p;
+    g.attempts = g_attempts.p;
+    g.capacity = photon_cap;
+    return s;
+  }
+};
+
+namespace {
+
+void check_points(const pale_points* p, const char* what) {
+  if (!p) throw ArgError(std::string(what) + ": null point block");
+  if (p->count && (!p->position || !p->tangent_u || !p->tangent_v || !p->scale || !p->albedo || !p->opacity ||
+                   !p->beta))
+    throw ArgError(std::string(what) + ": missing point field");
+}
+
+void upload_points(pale_handle* h, const pale_points* p, PointsBufs& dst, cudaStream_t s) {
+  const uint32_t n = p->count;
+  dst.alloc(n);
+  if (!n) return;
+  CK(cudaMemcpyAsync(dst.pos.p, p->position, 12ull * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dst.tu.p, p->tangent_u, 12ull * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dst.tv.p, p->tangent_v, 12ull * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dst.sc.p, p->scale, 8ull * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dst.alb.p, p->albedo, 12ull * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dst.op.p, p->opacity, 4ull * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dst.beta.p, p->beta, 4ull * n, cudaMemcpyHostToDevice, s));
+  if (p->shape) CK(cudaMemcpyAsync(dst.shape.p, p->shape, 4ull * n, cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(dst.shape.p, 0, 4ull * n, s));
+  (void)h;
+}
+
+// Builds the LBVH and surfel arrays from asset-order points.
+void build_surfels(pale_handle* h, const pale_points* asset) {
+  cudaStream_t s = h->stream;
+  const uint32_t n = asset->count;
+  h->np = n;
+  upload_points(h, asset, h->asset, s);
+  h->collected.alloc(n);
+  h->params.alloc(n);
+  h->sf_pe.ensure(n); h->sf_n.ensure(n); h->sf_u.ensure(n); h->sf_v.ensure(n); h->sf_cn.ensure(n);
+  h->sf_alb.ensure(n);
+  h->grads.alloc(n);
+  if (n == 0) {
+    h->node_count = 0;
+    return;
+  }
+  h->aabb_lo.ensure(3 * (size_t)n); h->aabb_hi.ensure(3 * (size_t)n);
+  h->bounds_part.ensure(12 * 148 * 4); h->bounds.ensure(12);
+  h->codes.ensure(n); h->order.ensure(n); h->codes_tmp.ensure(n); h->order_tmp.ensure(n);
+  h->sort_temp.ensure(radix_temp_words(n));
+  h->lc.ensure(n); h->rc.ensure(n); h->rfirst.ensure(n); h->rlast.ensure(n); h->parent.ensure(n);
+  h->leaf_parent.ensure(n); h->visits.ensure(n); h->box.ensure(6 * (size_t)n);
+  h->d_n.ensure(1);
+  const uint32_t leaf = std::max(1u, std::min(8u, h->st.leaf_size ? h->st.leaf_size : 4u));
+  h->top = 256;
+  h->node_count = (n <= leaf) ? 1 : h->top + (n - 1);
+  if (n <= leaf) h->top = 0;
+  h->nodes.ensure(h->node_count);
+  CK(cudaMemcpyAsync(h->d_n.p, &n, 4, cudaMemcpyHostToDevice, s));
+  LbvhArgs A{};
+  A.n = n;
+  A.d_n = h->d_n.p;
+  A.leaf_size = leaf;
+  A.top = h->top;
+  A.asset = h->asset.view();
+  A.collected = h->collected.view();
+  A.params = h->params.view();
+  A.derived = SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p};
+  A.lo = h->aabb_lo.p; A.hi = h->aabb_hi.p;
+  A.bounds_part = h->bounds_part.p; A.bounds = h->bounds.p;
+  A.codes = h->codes.p; A.order = h->order.p; A.codes_tmp = h->codes_tmp.p; A.order_tmp = h->order_tmp.p;
+  A.sort_temp = h->sort_temp.p;
+  A.lc = h->lc.p; A.rc = h->rc.p; A.rfirst = h->rfirst.p; A.rlast = h->rlast.p; A.parent = h->parent.p;
+  A.leaf_parent = h->leaf_parent.p; A.visits = h->visits.p; A.box = h->box.p;
+  A.nodes = h->nodes.p;
+  lbvh_build(A, s);
+  CK(cudaGetLastError());
+  float b[12];
+  CK(cudaMemcpyAsync(b, h->bounds.p, sizeof(b), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int k = 0; k < 3; ++k) {
+    h->pc_lo[k] = b[6 + k];
+    h->pc_hi[k] = b[9 + k];
+  }
+}
+
+// Host restatement of toWorldPoint with the device's operation order.
+V3 host_xform_point(const float* M, V3 p) { return xform_point(M, p); }
+
+void setup_scene(pale_handle* h, const pale_scene_desc* d) {
+  cudaStream_t s = h->stream;
+  // ---- meshes: per instance transforms, world boxes, triangles
+  h->n_inst = d->num_instances;
+  h->n_tris = d->num_triangles;
+  for (uint32_t i = 0; i < d->num_instances; ++i) {
+    if (d->instance_mesh[i] >= d->num_meshes) throw ArgError("instance mesh index out of range");
+    if (d->instance_material[i] >= d->num_materials) throw ArgError("instance material index out of range");
+  }
+  for (uint32_t t = 0; t < 3 * d->num_triangles; ++t)
+    if (d->triangles[t] >= d->num_vertices) throw ArgError("triangle vertex index out of range");
+  for (uint32_t m = 0; m < d->num_meshes; ++m)
+    if ((uint64_t)d->mesh_ranges[2 * m] + d->mesh_ranges[2 * m + 1] > d->num_triangles)
+      throw ArgError("mesh range out of range");
+  std::vector<float4> tri(3 * (size_t)std::max(1u, d->num_triangles));
+  for (uint32_t t = 0; t < d->num_triangles; ++t)
+    for (int c = 0; c < 3; ++c) {
+      const float* v = d->vertices + 3 * d->triangles[3 * t + c];
+      tri[3 * t + c] = make_float4(v[0], v[1], v[2], 0.f);
+    }
+  std::vector<uint2> rng(std::max(1u, h->n_inst));
+  std::vector<float4> box(2 * (size_t)std::max(1u, h->n_inst));
+  h->h_inst_box.assign(6 * (size_t)h->n_inst, 0.f);
+  for (uint32_t i = 0; i < h->n_inst; ++i) {
+    uint32_t m = d->instance_mesh[i];
+    uint32_t first = d->mesh_ranges[2 * m], cnt = d->mesh_ranges[2 * m + 1];
+    rng[i] = make_uint2(first, cnt);
+    V3 bl = v3(INFINITY, INFINITY, INFINITY), bh = v3(-INFINITY, -INFINITY, -INFINITY);
+    for (uint32_t k = 0; k < cnt; ++k)
+      for (int c = 0; c < 3; ++c) {
+        const float* v = d->vertices + 3 * d->triangles[3 * (first + k) + c];
+        bl = vmin(bl, v3(v[0], v[1], v[2]));
+        bh = vmax(bh, v3(v[0], v[1], v[2]));
+      }
+    // buildTLAS world box: the 8 transformed corners (SceneBuild.cpp:562-581)
+    V3 wl = v3(3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f);
+    V3 wh = v3(-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f);
+    for (int c = 0; c < 8; ++c) {
+      V3 p = v3((c & 4) ? bh.x : bl.x, (c & 2) ? bh.y : bl.y, (c & 1) ? bh.z : bl.z);
+      V3 pw = host_xform_point(d->instance_object_to_world + 16 * i, p);
+      wl = vmin(wl, pw);
+      wh = vmax(wh, pw);
+    }
+    box[2 * i] = make_float4(wl.x, wl.y, wl.z, 0.f);
+    box[2 * i + 1] = make_float4(wh.x, wh.y, wh.z, 0.f);
+    float* hb = &h->h_inst_box[6 * i];
+    hb[0] = wl.x; hb[1] = wl.y; hb[2] = wl.z; hb[3] = wh.x; hb[4] = wh.y; hb[5] = wh.z;
+  }
+  h->o2w.alloc(16 * (size_t)std::max(1u, h->n_inst));
+  h->w2o.alloc(16 * (size_t)std::max(1u, h->n_inst));
+  h->inst_box.alloc(box.size());
+  h->tri_range.alloc(rng.size());
+  h->tri.alloc(tri.size());
+  h->inst_mat.alloc(std::max(1u, h->n_inst));
+  h->materials.alloc(std::max(1u, d->num_materials));
+  if (h->n_inst) {
+    CK(cudaMemcpyAsync(h->o2w.p, d->instance_object_to_world, 64ull * h->n_inst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->w2o.p, d->instance_world_to_object, 64ull * h->n_inst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->inst_mat.p, d->instance_material, 4ull * h->n_inst, cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemcpyAsync(h->inst_box.p, box.data(), box.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->tri_range.p, rng.data(), rng.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->tri.p, tri.data(), tri.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+  std::vector<float4> mats(std::max(1u, d->num_materials));
+  for (uint32_t k = 0; k < d->num_materials; ++k)
+    mats[k] = make_float4(d->materials[4 * k], d->materials[4 * k + 1], d->materials[4 * k + 2], d->materials[4 * k + 3]);
+  CK(cudaMemcpyAsync(h->materials.p, mats.data(), mats.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+
+  // ---- lights: world-area CDF per emissive instance (SceneBuild.cpp:263-343)
+  std::vector<uint4> lrec;
+  std::vector<float4> lcol;
+  std::vector<float> larea, lcdf;
+  std::vector<uint32_t> ltri;
+  for (uint32_t i = 0; i < h->n_inst; ++i) {
+    const float* mat = d->materials + 4 * d->instance_material[i];
+    if (!(mat[3] > 0.f)) continue;
+    uint32_t m = d->instance_mesh[i];
+    uint32_t first = d->mesh_ranges[2 * m], cnt = d->mesh_ranges[2 * m + 1];
+    if (cnt == 0) continue;
+    const float* O2W = d->instance_object_to_world + 16 * i;
+    std::vector<float> areas(cnt);
+    float total = 0.f;
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const uint32_t* tr = d->triangles + 3 * (first + k);
+      auto P = [&](int c) { const float* v = d->vertices + 3 * tr[c]; return host_xform_point(O2W, v3(v[0], v[1], v[2])); };
+      V3 w0 = P(0), w1 = P(1), w2 = P(2);
+      areas[k] = 0.5f * length(cross(w1 - w0, w2 - w0));
+      total += areas[k];
+    }
+    if (total <= 0.f) continue;
+    uint32_t off = (uint32_t)lcdf.size();
+    float run = 0.f;
+    for (uint32_t k = 0; k < cnt; ++k) {
+      run += areas[k];
+      lcdf.push_back(run / total);
+      ltri.push_back(first + k);
+    }
+    lcdf[off + cnt - 1] = 1.0f;
+    lrec.push_back(make_uint4(i, off, cnt, 0));
+    lcol.push_back(make_float4(mat[0], mat[1], mat[2], mat[3]));
+    larea.push_back(total);
+  }
+  h->n_lights = (uint32_t)lrec.size();
+  h->light0_area = h->n_lights ? larea[0] : 0.f;
+  h->light_rec.alloc(std::max<size_t>(1, lrec.size()));
+  h->light_col.alloc(std::max<size_t>(1, lcol.size()));
+  h->light_area.alloc(std::max<size_t>(1, larea.size()));
+  h->light_cdf.alloc(std::max<size_t>(1, lcdf.size()));
+  h->light_tri.alloc(std::max<size_t>(1, ltri.size()));
+  if (h->n_lights) {
+    CK(cudaMemcpyAsync(h->light_rec.p, lrec.data(), lrec.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->light_col.p, lcol.data(), lcol.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->light_area.p, larea.data(), larea.size() * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->light_cdf.p, lcdf.data(), lcdf.size() * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->light_tri.p, ltri.data(), ltri.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+
+  // ---- cameras (makePrimaryRayFromPixelJitteredFov constants)
+  h->cams.resize(d->num_cameras);
+  h->cam_names.resize(d->num_cameras);
+  uint32_t max_pix = 0;
+  for (uint32_t c = 0; c < d->num_cameras; ++c) {
+    CameraRec& C = h->cams[c];
+    std::memset(&C, 0, sizeof(C));
+    std::memcpy(C.inv_view, d->camera_inv_view + 16 * c, 64);
+    C.w = d->camera_size[2 * c];
+    C.h = d->camera_size[2 * c + 1];
+    if (C.w == 0 || C.h == 0) throw ArgError("camera with zero size");
+    C.width = (float)C.w;
+    C.height = (float)C.h;
+    C.half_w = 0.5f * C.width;
+    C.half_h = 0.5f * C.height;
+    C.fy = 0.5f * C.height / std::tan(0.5f * (d->camera_fovy_deg[c] * 0.01745329251994329576923690768489f));
+    C.fx = C.fy * (C.width / C.height);
+    max_pix = std::max(max_pix, C.w * C.h);
+    char nm[17];
+    std::memset(nm, 0, sizeof(nm));
+    if (d->camera_names) std::memcpy(nm, d->camera_names + 16 * c, 16);
+    h->cam_names[c] = nm;
+  }
+  h->d_cams.alloc(std::max<size_t>(1, d->num_cameras));
+
+  // ---- surfels + LBVH
+  build_surfels(h, &d->points);
+
+  // ---- photon grid from the scene box (configurePhotonGrid, PathTracer.cpp:184-221)
+  V3 lo = v3(INFINITY, INFINITY, INFINITY), hi = v3(-INFINITY, -INFINITY, -INFINITY);
+  for (uint32_t i = 0; i < h->n_inst; ++i) {
+    const float* b = &h->h_inst_box[6 * i];
+    lo = vmin(lo, v3(b[0], b[1], b[2]));
+    hi = vmax(hi, v3(b[3], b[4], b[5]));
+  }
+  if (h->np) {
+    lo = vmin(lo, v3(h->pc_lo[0], h->pc_lo[1], h->pc_lo[2]));
+    hi = vmax(hi, v3(h->pc_hi[0], h->pc_hi[1], h->pc_hi[2]));
+  }
+  if (!(lo.x <= hi.x)) throw ArgError("scene is empty");
+  h->radius = h->st.gather_radius;
+  const float cs = 0.5f * h->radius;
+  h->cell = cs;
+  V3 pad = v3(h->radius, h->radius, h->radius);
+  V3 org = lo - pad, gmax = hi + pad, ext = gmax - org;
+  h->origin[0] = org.x; h->origin[1] = org.y; h->origin[2] = org.z;
+  const float safe = std::fmax(cs, 1e-6f);
+  h->res[0] = (int)std::ceil(ext.x / safe);
+  h->res[1] = (int)std::ceil(ext.y / safe);
+  h->res[2] = (int)std::ceil(ext.z / safe);
+  uint64_t tot = (uint64_t)h->res[0] * h->res[1] * h->res[2];
+  // the cell-offset scan handles up to 2^28 cells
+  if (tot == 0 || tot >= (1ull << 28)) throw ArgError("Photon grid resolution too high; increase r or tighten AABB.");
+  h->cells = (uint32_t)tot;
+  h->key_bits = 1;
+  while (h->key_bits < 32 && ((uint64_t)1 << h->key_bits) < tot) ++h->key_bits;
+
+  // ---- photon store (PathTracer.cpp:123-144): photons x passes x bounces,
+  // clamped to 10 GiB of the reference's 64-byte records
+  const pale_settings& st = h->st;
+  uint64_t req = (uint64_t)st.photons_per_launch * st.forward_passes * st.max_bounces;
+  uint64_t mx = (10ull << 30) / 64ull;
+  h->photon_cap = std::max<uint64_t>(1, std::min(req, mx));
+  const size_t pc = (size_t)h->photon_cap;
+  h->ph_a.alloc(pc); h->ph_b.alloc(pc); h->ph_c.alloc(pc);
+  h->g_pa.alloc(pc); h->g_pb.alloc(pc); h->g_pc.alloc(pc);
+  h->g_cell_id.alloc(pc); h->g_sorted.alloc(pc); h->g_keys.alloc(2 * pc); h->g_vals_tmp.alloc(pc);
+  h->g_sort_temp.alloc(radix_temp_words((uint32_t)pc));
+  h->g_cell_count.alloc((size_t)h->cells + 1);
+  h->g_cell_off.alloc((size_t)h->cells + 1);
+  h->g_scan_temp.alloc(scan_temp_words(h->cells + 1));
+  h->g_stored.alloc(1);
+  h->g_attempts.alloc(1);
+  CK(cudaMemsetAsync(h->g_stored.p, 0, 4, s));
+  CK(cudaMemsetAsync(h->g_attempts.p, 0, 4, s));
+  CK(cudaMemsetAsync(h->g_cell_off.p, 0, ((size_t)h->cells + 1) * 4, s));
+
+  // ---- queues: next power of two >= max(photons per launch, pixels)
+  h->qcap = next_pow2(std::max(std::max(st.photons_per_launch, max_pix), 256u));
+  const size_t qc = h->qcap;
+  h->q0.alloc(qc); h->q1.alloc(qc); h->qstage.alloc(qc); h->qflags.alloc(qc);
+  h->tile_counts.alloc(qc / kBlock + 1); h->tile_offsets.alloc(qc / kBlock + 1);
+  h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
+  h->pend_a.alloc(qc); h->pend_b.alloc(qc); h->pend_c.alloc(qc);
+  h->ev_stage.alloc(qc); h->ev_list.alloc(qc);
+  h->run.alloc(1);
+  CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+  CK(cudaStreamSynchronize(s));
+}
+
+std::vector<uint32_t> mt_table(uint64_t seed, size_t n) {
+  std::mt19937_64 g(seed);
+  std::vector<uint32_t> t(n);
+  for (size_t i = 0; i < n; ++i) t[i] = (uint32_t)g();
+  return t;
+}
+
+int fail(pale_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+template <typename F>
+int guarded(pale_handle* h, F&& f) {
+  try {
+    return f();
+  } catch (const ArgError& e) {
+    return fail(h, PALE_ERR_ARGUMENT, e.what());
+  } catch (const CudaError& e) {
+    return fail(h, PALE_ERR_CUDA, e.what());
+  } catch (const std::exception& e) {
+    return fail(h, PALE_ERR_STATE, e.what());
+  }
+}
+
+void copy_stats(pale_handle* h) {
+  RunState rs;
+  CK(cudaMemcpyAsync(&rs, h->run.p, sizeof(rs), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->stats.photon_segments = rs.photon_segments;
+  h->stats.gather_segments = rs.gather_segments;
+  h->stats.adjoint_segments = rs.adjoint_segments;
+  h->stats.photons_stored = std::min<uint64_t>(rs.photon_attempts, h->photon_cap);
+  h->stats.gradient_events = rs.gradient_events;
+  h->stats.gather_queries = rs.gather_queries;
+  h->stats.node_visits = rs.node_visits;
+  h->stats.surfel_tests = rs.surfel_tests;
+  h->stats.photons_scanned = rs.photons_scanned;
+  if (rs.error) {
+    char buf[128];
+    std::snprintf(buf, sizeof(buf), "device error flags 0x%x (1 stack, 2 layer cap, 4 photon capacity, 8 bounds, 16 queue)",
+                  rs.error);
+    throw std::runtime_error(buf);
+  }
+}
+
+void validate_cams(pale_handle* h, uint32_t nsel, const uint32_t* idx) {
+  if (nsel && !idx) throw ArgError("camera index list is null");
+  for (uint32_t i = 0; i < nsel; ++i)
+    if (idx[i] >= h->cams.size()) throw ArgError("camera index out of range");
+}
+
+// Forward render into the handle's packed device images.
+uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr) {
+  cudaStream_t s = h->stream;
+  const pale_settings& st = h->st;
+  validate_cams(h, nsel, idx);
+  std::vector<CameraRec> sel(nsel);
+  uint32_t total = 0;
+  for (uint32_t i = 0; i < nsel; ++i) {
+    sel[i] = h->cams[idx[i]];
+    sel[i].pixel_offset = total;
+    sel[i].seed_slot = i;
+    total += sel[i].w * sel[i].h;
+  }
+  h->d_cams.ensure(std::max<size_t>(1, nsel));
+  if (nsel) CK(cudaMemcpyAsync(h->d_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
+  // seed stream of submitPhotonMappingKernel: passes x (1 + bounces) + cameras
+  std::vector<uint32_t> seeds = mt_table(st.seed, (size_t)st.forward_passes * (1 + st.max_bounces) + nsel + 1);
+  h->seeds_fwd.ensure(seeds.size());
+  CK(cudaMemcpyAsync(h->seeds_fwd.p, seeds.data(), seeds.size() * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+  CK(cudaEventRecord(h->ev0, s));
+  SceneView sv = h->view();
+  PhotonArgs P{};
+  P.scene = sv;
+  P.st = h->run.p;
+  P.seeds = h->seeds_fwd.p;
+  P.qb = QueueBufs{{h->q0.p, h->q1.p}, h->qstage.p, h->qflags.p, h->tile_counts.p, h->tile_offsets.p, h->qcap};
+  P.ps = PhotonStore{h->ph_a.p, h->ph_b.p, h->ph_c.p, h->ph_sa.p, h->ph_sb.p, h->ph_sc.p, h->photon_cap};
+  P.photons_per_launch = st.photons_per_launch;
+  P.inv_emitted = 1.0f / (float)(st.photons_per_launch * st.forward_passes);
+  P.rr_start = st.rr_start;
+  P.q_null = st.q_null;
+  P.q_reflect = st.q_reflect;
+  P.q_transmit = st.q_transmit;
+  if (st.photons_per_launch > h->qcap) throw ArgError("photons per launch exceed the queue capacity");
+  for (uint32_t pass = 0; pass < st.forward_passes; ++pass) {
+    photon_emit(P, s);
+    for (uint32_t b = 0; b < st.max_bounces; ++b) photon_bounce(P, b & 1u, s);
+  }
+  GridBufs G{};
+  G.cell_id = h->g_cell_id.p;
+  G.sorted = h->g_sorted.p;
+  G.keys_tmp = h->g_keys.p;
+  G.vals_tmp = h->g_vals_tmp.p;
+  G.sort_temp = h->g_sort_temp.p;
+  G.cell_count = h->g_cell_count.p;
+  G.cell_off = h->g_cell_off.p;
+  G.scan_temp = h->g_scan_temp.p;
+  G.pa = h->g_pa.p;
+  G.pb = h->g_pb.p;
+  G.pc = h->g_pc.p;
+  G.d_stored = h->g_stored.p;
+  G.d_attempts = h->g_attempts.p;
+  grid_build(sv, h->run.p, P.ps, G, h->cells, h->key_bits, s);
+  CK(cudaEventRecord(h->ev1, s));
+  FrameArgs F{};
+  F.scene = sv;
+  F.st = h->run.p;
+  F.seeds = h->seeds_fwd.p;
+  F.cams = h->d_cams.p;
+  F.ncams = nsel;
+  F.total_pixels = total;
+  F.raw = d_raw;
+  F.ldr = d_ldr;
+  F.gather_passes = st.gather_passes;
+  F.rng_mode = st.rng_mode;
+  F.exposure = st.exposure;
+  F.gamma = st.gamma;
+  camera_gather(F, s);
+  CK(cudaEventRecord(h->ev2, s));
+  CK(cudaGetLastError());
+  copy_stats(h);
+  float a = 0.f, b = 0.f;
+  CK(cudaEventElapsedTime(&a, h->ev0, h->ev1));
+  CK(cudaEventElapsedTime(&b, h->ev1, h->ev2));
+  h->stats.photon_ms = a;
+  h->stats.gather_ms = b;
+  h->stats.forward_ms = a + b;
+  return total;
+}
+
+void zero_grads(pale_handle* h, cudaStream_t s) {
+  const size_t n = h->np ? h->np : 1;
+  PointsBufs& g = h->grads;
+  CK(cudaMemsetAsync(g.pos.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(g.tu.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(g.tv.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(g.sc.p, 0, 8 * n, s));
+  CK(cudaMemsetAsync(g.alb.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(g.op.p, 0, 4 * n, s));
+  CK(cudaMemsetAsync(g.beta.p, 0, 4 * n, s));
+  CK(cudaMemsetAsync(g.shape.p, 0, 4 * n, s));
+}
+
+// Adjoint pass reading packed dL/dI at d_dldi (device).
+void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi, float* d_dbg) {
+  cudaStream_t s = h->stream;
+  const pale_settings& st = h->st;
+  validate_cams(h, nsel, idx);
+  std::vector<uint32_t> seeds =
+      mt_table(st.rng_mode == PALE_RNG_DECORRELATED ? st.seed : 42ull,
+               (size_t)nsel * st.adjoint_passes * (1 + st.adjoint_bounces) + 1);
+  h->seeds_adj.ensure(seeds.size());
+  CK(cudaMemcpyAsync(h->seeds_adj.p, seeds.data(), seeds.size() * 4, cudaMemcpyHostToDevice, s));
+  zero_grads(h, s);
+  CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+  CK(cudaEventRecord(h->ev0, s));
+  AdjointArgs A{};
+  A.scene = h->view();
+  A.st = h->run.p;
+  A.seeds = h->seeds_adj.p;
+  A.qb = QueueBufs{{h->q0.p, h->q1.p}, h->qstage.p, h->qflags.p, h->tile_counts.p, h->tile_offsets.p, h->qcap};
+  A.pend = PendingBufs{h->pend_a.p, h->pend_b.p, h->pend_c.p};
+  A.ev = EventBufs{h->ev_stage.p, h->ev_list.p};
+  A.dldi = d_dldi;
+  A.grad_opacity = h->grads.op.p;
+  A.debug_opacity = d_dbg;
+  A.rr_start = st.rr_start;
+  A.q_null = st.q_null;
+  A.q_reflect = st.q_reflect;
+  A.q_transmit = st.q_transmit;
+  A.inv_spp = 1.0f / (float)st.adjoint_passes;
+  A.fixed_seed = st.random_number;
+  A.rng_mode = st.rng_mode;
+  A.light0_valid = h->n_lights > 0;
+  A.light0_area = h->light0_area;
+  uint32_t offset = 0;
+  for (uint32_t i = 0; i < nsel; ++i) {
+    A.cam = h->cams[idx[i]];
+    A.cam.pixel_offset = offset;
+    if (A.cam.w * A.cam.h > h->qcap) throw ArgError("camera larger than the queue capacity");
+    for (uint32_t spp = 0; spp < st.adjoint_passes; ++spp) {
+      adjoint_raygen(A, s);
+      for (uint32_t b = 0; b < st.adjoint_bounces; ++b) adjoint_bounce(A, b, s);
+    }
+    offset += A.cam.w * A.cam.h;
+  }
+  CK(cudaEventRecord(h->ev1, s));
+  CK(cudaGetLastError());
+  copy_stats(h);
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->stats.backward_ms = ms;
+}
+
+void download_points(pale_handle* h, const PointsBufs& src, pale_points* out) {
+  cudaStream_t s = h->stream;
+  const size_t n = h->np;
+  if (!n) return;
+  if (out->position) CK(cudaMemcpyAsync(out->position, src.pos.p, 12 * n, cudaMemcpyDeviceToHost, s));
+  if (out->tangent_u) CK(cudaMemcpyAsync(out->tangent_u, src.tu.p, 12 * n, cudaMemcpyDeviceToHost, s));
+  if (out->tangent_v) CK(cudaMemcpyAsync(out->tangent_v, src.tv.p, 12 * n, cudaMemcpyDeviceToHost, s));
+  if (out->scale) CK(cudaMemcpyAsync(out->scale, src.sc.p, 8 * n, cudaMemcpyDeviceToHost, s));
+  if (out->albedo) CK(cudaMemcpyAsync(out->albedo, src.alb.p, 12 * n, cudaMemcpyDeviceToHost, s));
+  if (out->opacity) CK(cudaMemcpyAsync(out->opacity, src.op.p, 4 * n, cudaMemcpyDeviceToHost, s));
+  if (out->beta) CK(cudaMemcpyAsync(out->beta, src.beta.p, 4 * n, cudaMemcpyDeviceToHost, s));
+  if (out->shape) CK(cudaMemcpyAsync(out->shape, src.shape.p, 4 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+
+// ===================================================================== ABI
+extern "C" {
+
+void pale_default_settings(pale_settings* s) {
+  if (!s) return;
+  std::memset(s, 0, sizeof(*s));
+  s->photons_per_launch = 1000000u;
+  s->max_bounces = 6;
+  s->forward_passes = 6;
+  s->gather_passes = 6;
+  s->adjoint_bounces = 6;
+  s->adjoint_passes = 6;
+  s->seed = 42;
+  s->random_number = 42;
+  s->rr_start = 6;
+  s->q_null = 0.5f;
+  s->q_reflect = 0.5f;
+  s->q_transmit = 0.0f;
+  s->gather_radius = 0.01f;
+  s->leaf_size = 4;
+  s->rng_mode = PALE_RNG_REFERENCE;
+  s->debug_images = 0;
+  s->exposure = 1.0f;
+  s->gamma = 2.2f;
+}
+
+const char* pale_version(void) { return "pale_b200 0.1 (sm_100a)"; }
+
+const char* pale_last_error(const pale_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale_handle** out) {
+  if (!desc || !settings || !out) return fail(nullptr, PALE_ERR_ARGUMENT, "pale_create: null argument");
+  *out = nullptr;
+  pale_handle* h = new pale_handle();
+  int rc = guarded(nullptr, [&]() {
+    h->st = *settings;
+    if (h->st.forward_passes == 0 || h->st.photons_per_launch == 0) throw ArgError("photons and forward passes must be > 0");
+    if (h->st.gather_passes == 0 || h->st.adjoint_passes == 0) throw ArgError("gather and adjoint passes must be > 0");
+    if (!(h->st.gather_radius > 0.f)) throw ArgError("gather radius must be > 0");
+    check_points(&desc->points, "pale_create");
+    if (desc->points.count >= (1u << 28)) throw ArgError("at most 2^28 surfels are supported");
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    CK(cudaEventCreate(&h->ev2));
+    setup_scene(h, desc);
+    return PALE_OK;
+  });
+  if (rc != PALE_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return PALE_OK;
+}
+
+int pale_destroy(pale_handle* h) {
+  if (!h) return PALE_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  delete h;
+  return PALE_OK;
+}
+
+int pale_point_count(const pale_handle* h, uint32_t* count) {
+  if (!h || !count) return PALE_ERR_ARGUMENT;
+  *count = h->np;
+  return PALE_OK;
+}
+
+int pale_camera_count(const pale_handle* h, uint32_t* count) {
+  if (!h || !count) return PALE_ERR_ARGUMENT;
+  *count = (uint32_t)h->cams.size();
+  return PALE_OK;
+}
+
+int pale_camera_info(const pale_handle* h, uint32_t index, char name[16], uint32_t* width, uint32_t* height) {
+  if (!h || index >= h->cams.size()) return PALE_ERR_ARGUMENT;
+  if (name) {
+    std::memset(name, 0, 16);
+    std::strncpy(name, h->cam_names[index].c_str(), 15);
+  }
+  if (width) *width = h->cams[index].w;
+  if (height) *height = h->cams[index].h;
+  return PALE_OK;
+}
+
+int pale_render_forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* ldr, float* raw) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    validate_cams(h, nsel, idx);
+    size_t pix = 0;
+    for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    h->img_raw.ensure(4 * std::max<size_t>(1, pix));
+    h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
+    forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p);
+    if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+    if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PALE_OK;
+  });
+}
+
+int pale_render_forward_device(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ldr, float* d_raw,
+                               void* stream) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    validate_cams(h, nsel, idx);
+    size_t pix = 0;
+    for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    if (stream) {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      CK(cudaEventRecord(e, (cudaStream_t)stream));
+      CK(cudaStreamWaitEvent(h->stream, e, 0));
+      CK(cudaEventDestroy(e));
+    }
+    h->img_raw.ensure(4 * std::max<size_t>(1, pix));
+    forward(h, nsel, idx, d_raw ? d_raw : h->img_raw.p, d_ldr);
+    return PALE_OK;
+  });
+}
+
+int pale_render_backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* dldi, pale_points* grads,
+                         float* debug_opacity) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    validate_cams(h, nsel, idx);
+    if (!dldi && nsel) throw ArgError("dL/dI is null");
+    size_t pix = 0;
+    for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    h->dldi.ensure(4 * std::max<size_t>(1, pix));
+    if (pix) CK(cudaMemcpyAsync(h->dldi.p, dldi, 16 * pix, cudaMemcpyHostToDevice, h->stream));
+    float* dbg = nullptr;
+    if (debug_opacity && h->st.debug_images) {
+      h->dbg.ensure(4 * std::max<size_t>(1, pix));
+      CK(cudaMemsetAsync(h->dbg.p, 0, 16 * pix, h->stream));
+      dbg = h->dbg.p;
+    }
+    backward(h, nsel, idx, h->dldi.p, dbg);
+    if (grads) download_points(h, h->grads, grads);
+    if (debug_opacity) {
+      if (dbg) CK(cudaMemcpyAsync(debug_opacity, dbg, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+      else std::memset(debug_opacity, 0, 16 * pix);
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return PALE_OK;
+  });
+}
+
+int pale_render_backward_device(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi,
+                                pale_points* d_grads, void* stream) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    validate_cams(h, nsel, idx);
+    if (stream) {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      CK(cudaEventRecord(e, (cudaStream_t)stream));
+      CK(cudaStreamWaitEvent(h->stream, e, 0));
+      CK(cudaEventDestroy(e));
+    }
+    backward(h, nsel, idx, d_dldi, nullptr);
+    if (d_grads) {
+      const size_t n = h->np;
+      cudaStream_t s = h->stream;
+      auto cp = [&](float* dst, const float* src, size_t bytes) {
+        if (dst && n) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+      };
+      cp(d_grads->position, h->grads.pos.p, 12 * n);
+      cp(d_grads->tangent_u, h->grads.tu.p, 12 * n);
+      cp(d_grads->tangent_v, h->grads.tv.p, 12 * n);
+      cp(d_grads->scale, h->grads.sc.p, 8 * n);
+      cp(d_grads->albedo, h->grads.alb.p, 12 * n);
+      cp(d_grads->opacity, h->grads.op.p, 4 * n);
+      cp(d_grads->beta, h->grads.beta.p, 4 * n);
+      cp(d_grads->shape, h->grads.shape.p, 4 * n);
+      CK(cudaStreamSynchronize(s));
+    }
+    return PALE_OK;
+  });
+}
+
+int pale_get_points(pale_handle* h, pale_points* out) {
+  if (!h || !out) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    download_points(h, h->params, out);
+    return PALE_OK;
+  });
+}
+
+int pale_get_order(pale_handle* h, uint32_t* order) {
+  if (!h || !order) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    if (h->np) CK(cudaMemcpyAsync(order, h->order.p, 4ull * h->np, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PALE_OK;
+  });
+}
+
+int pale_apply_points(pale_handle* h, const pale_points* p) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    check_points(p, "pale_apply_points");
+    if (p->count != h->np) throw ArgError("apply_point_optimization expects consistent point count");
+    cudaStream_t s = h->stream;
+    const size_t n = h->np;
+    if (!n) return PALE_OK;
+    PointsBufs& d = h->params;
+    CK(cudaMemcpyAsync(d.pos.p, p->position, 12 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d.tu.p, p->tangent_u, 12 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d.tv.p, p->tangent_v, 12 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d.sc.p, p->scale, 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d.alb.p, p->albedo, 12 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d.op.p, p->opacity, 4 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d.beta.p, p->beta, 4 * n, cudaMemcpyHostToDevice, s));
+    derive_surfels(d.view(), h->np, SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p},
+                   s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return PALE_OK;
+  });
+}
+
+int pale_rebuild(pale_handle* h, const pale_points* asset) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    check_points(asset, "pale_rebuild");
+    if (asset->count >= (1u << 28)) throw ArgError("at most 2^28 surfels are supported");
+    build_surfels(h, asset);
+    return PALE_OK;
+  });
+}
+
+int pale_trace_rays(pale_handle* h, uint32_t n, const float* o, const float* d, int32_t* inst, int32_t* prim,
+                    float* t, float* alpha, float* pos) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    if (n && (!o || !d || !inst || !prim || !t || !alpha)) throw ArgError("pale_trace_rays: null array");
+    if (!n) return PALE_OK;
+    cudaStream_t s = h->stream;
+    DBuf<float> dO, dD, dT, dA, dP;
+    DBuf<int32_t> dI, dR;
+    dO.alloc(3ull * n); dD.alloc(3ull * n); dT.alloc(n); dA.alloc(n); dP.alloc(3ull * n); dI.alloc(n); dR.alloc(n);
+    CK(cudaMemcpyAsync(dO.p, o, 12ull * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dD.p, d, 12ull * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+    trace_rays(h->view(), h->run.p, n, dO.p, dD.p, dI.p, dR.p, dT.p, dA.p, dP.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(inst, dI.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(prim, dR.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(t, dT.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(alpha, dA.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    if (pos) CK(cudaMemcpyAsync(pos, dP.p, 12ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return PALE_OK;
+  });
+}
+
+int pale_gather_irradiance(pale_handle* h, uint32_t n, const float* pts, const float* nrm, float* E) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    if (n && (!pts || !nrm || !E)) throw ArgError("pale_gather_irradiance: null array");
+    if (!n) return PALE_OK;
+    cudaStream_t s = h->stream;
+    DBuf<float> dP, dN, dE;
+    dP.alloc(3ull * n); dN.alloc(3ull * n); dE.alloc(3ull * n);
+    CK(cudaMemcpyAsync(dP.p, pts, 12ull * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dN.p, nrm, 12ull * n, cudaMemcpyHostToDevice, s));
+    gather_points(h->view(), n, dP.p, dN.p, dE.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(E, dE.p, 12ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return PALE_OK;
+  });
+}
+
+int pale_load_photons(pale_handle* h, uint32_t n, const float* pos, const float* pw, const float* dir) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    if (n && (!pos || !pw || !dir)) throw ArgError("pale_load_photons: null array");
+    if (n > h->photon_cap) throw ArgError("more photons than the photon store holds");
+    cudaStream_t s = h->stream;
+    DBuf<float> dP, dW, dD;
+    dP.alloc(3ull * n); dW.alloc(3ull * n); dD.alloc(3ull * n);
+    if (n) {
+      CK(cudaMemcpyAsync(dP.p, pos, 12ull * n, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(dW.p, pw, 12ull * n, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(dD.p, dir, 12ull * n, cudaMemcpyHostToDevice, s));
+    }
+    PhotonStore ps{h->ph_a.p, h->ph_b.p, h->ph_c.p, h->ph_sa.p, h->ph_sb.p, h->ph_sc.p, h->photon_cap};
+    load_photon_arrays(n, dP.p, dW.p, dD.p, ps, s);
+    CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+    CK(cudaMemcpyAsync(&h->run.p->photon_attempts, &n, 4, cudaMemcpyHostToDevice, s));
+    GridBufs G{};
+    G.cell_id = h->g_cell_id.p; G.sorted = h->g_sorted.p; G.keys_tmp = h->g_keys.p; G.vals_tmp = h->g_vals_tmp.p;
+    G.sort_temp = h->g_sort_temp.p; G.cell_count = h->g_cell_count.p; G.cell_off = h->g_cell_off.p;
+    G.scan_temp = h->g_scan_temp.p; G.pa = h->g_pa.p; G.pb = h->g_pb.p; G.pc = h->g_pc.p; G.d_stored = h->g_stored.p;
+    G.d_attempts = h->g_attempts.p;
+    grid_build(h->view(), h->run.p, ps, G, h->cells, h->key_bits, s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return PALE_OK;
+  });
+}
+
+int pale_get_photons(pale_handle* h, uint32_t* count, float* position, float* power, float* direction,
+                     uint32_t* cell_id, uint32_t* sorted, float* grid_info) {
+  if (!h || !count) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    cudaStream_t s = h->stream;
+    uint32_t n = 0;
+    CK(cudaMemcpyAsync(&n, h->g_stored.p, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *count = n;
+    if (n && (position || power || direction)) {
+      std::vector<float4> a(n), b(n);
+      std::vector<float> c(n);
+      CK(cudaMemcpyAsync(a.data(), h->ph_a.p, 16ull * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(b.data(), h->ph_b.p, 16ull * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(c.data(), h->ph_c.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (uint32_t i = 0; i < n; ++i) {
+        if (position) { position[3 * i] = a[i].x; position[3 * i + 1] = a[i].y; position[3 * i + 2] = a[i].z; }
+        if (power) { power[3 * i] = a[i].w; power[3 * i + 1] = b[i].w; power[3 * i + 2] = c[i]; }
+        if (direction) { direction[3 * i] = b[i].x; direction[3 * i + 1] = b[i].y; direction[3 * i + 2] = b[i].z; }
+      }
+    }
+    if (n && cell_id) CK(cudaMemcpyAsync(cell_id, h->g_cell_id.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    if (n && sorted) CK(cudaMemcpyAsync(sorted, h->g_sorted.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (grid_info) {
+      grid_info[0] = h->origin[0]; grid_info[1] = h->origin[1]; grid_info[2] = h->origin[2];
+      grid_info[3] = h->cell;
+      grid_info[4] = (float)h->res[0]; grid_info[5] = (float)h->res[1]; grid_info[6] = (float)h->res[2];
+    }
+    return PALE_OK;
+  });
+}
+
+int pale_get_bvh(pale_handle* h, uint32_t* codes, uint32_t* node_count, float* nodes, uint32_t max_nodes) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    cudaStream_t s = h->stream;
+    if (node_count) *node_count = h->np ? h->node_count : 0;
+    if (codes && h->np) CK(cudaMemcpyAsync(codes, h->codes.p, 4ull * h->np, cudaMemcpyDeviceToHost, s));
+    if (nodes && h->np) {
+      uint32_t k = std::min(max_nodes, h->node_count);
+      CK(cudaMemcpyAsync(nodes, h->nodes.p, 64ull * k, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return PALE_OK;
+  });
+}
+
+int pale_get_stats(pale_handle* h, pale_stats* out) {
+  if (!h || !out) return PALE_ERR_ARGUMENT;
+  *out = h->stats;
+  return PALE_OK;
+}
+
+}  // extern "C"

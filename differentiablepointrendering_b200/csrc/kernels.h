@@ -1,0 +1,169 @@
+// kernels.h -- launch wrappers shared by the build, render and API units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pale {
+
+// Per-point parameter arrays on the device (structure of arrays).
+struct PointsDev {
+  float* position;
+  float* tangent_u;
+  float* tangent_v;
+  float* scale;
+  float* albedo;
+  float* opacity;
+  float* beta;
+  float* shape;
+};
+
+struct SurfelArrays {
+  float4 *pe, *n, *u, *v, *cn, *alb;
+};
+
+struct LbvhArgs {
+  uint32_t n;
+  const uint32_t* d_n;      // device copy of n (radix sort)
+  uint32_t leaf_size;
+  uint32_t top;
+  PointsDev asset;          // asset-order input
+  PointsDev collected;      // asset-order collected
+  PointsDev params;         // BVH-order output
+  SurfelArrays derived;
+  float *lo, *hi;           // asset-order boxes
+  float *bounds_part, *bounds;   // bounds[0..5] centroid lo/hi, [6..11] box lo/hi
+  uint32_t *codes, *order, *codes_tmp, *order_tmp, *sort_temp;
+  int32_t *lc, *rc;
+  uint32_t *rfirst, *rlast, *parent, *leaf_parent, *visits;
+  float* box;
+  BvhNode* nodes;
+};
+
+size_t scan_temp_words(uint32_t n);
+void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* temp, uint32_t* total,
+                    cudaStream_t s);
+size_t radix_temp_words(uint32_t n_max);
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp, const uint32_t* d_n,
+                      uint32_t n_max, int bits, uint32_t* temp, cudaStream_t s);
+void lbvh_build(const LbvhArgs& a, cudaStream_t s);
+void derive_surfels(const PointsDev& p, uint32_t n, const SurfelArrays& d, cudaStream_t s);
+
+// ------------------------------------------------------------ rendering
+struct QueueBufs {
+  RayRec* q[2];           // ping-pong ray queues
+  RayRec* stage;          // per-slot staging of the next ray
+  uint8_t* flags;         // per-slot: 1 alive, 2 deposit / event
+  uint2* tile_counts;     // per 256-slot tile: (alive, deposit|event)
+  uint2* tile_offsets;
+  uint32_t capacity;
+};
+
+struct PhotonStore {
+  float4* a;              // deposit order: position, power.r
+  float4* b;              // incoming direction, power.g
+  float* c;               // power.b
+  float4 *sa, *sb;        // staging per slot
+  float* sc;
+  uint64_t capacity;
+};
+
+struct GridBufs {
+  uint32_t* cell_id;      // per stored photon (deposit order)
+  uint32_t* sorted;       // sorted position -> deposit index
+  uint32_t *keys_tmp, *vals_tmp, *sort_temp;
+  uint32_t* cell_count;   // cells + 1
+  uint32_t* cell_off;     // cells + 1
+  uint32_t* scan_temp;
+  float4 *pa, *pb;        // sorted photons
+  float* pc;
+  uint32_t* d_stored;     // photons stored (device)
+  uint32_t* d_attempts;   // deposits attempted, read by the lookups
+};
+
+// Adjoint pending interaction per path (PendingAdjointState,
+// GPUDataStructures.h:319-336): (position, alpha) (throughput, kind)
+// (primitive, instance, pixel, -).
+struct PendingBufs {
+  float4* a;
+  float4* b;
+  uint4* c;
+};
+
+// Completed gradient event (CompletedGradientEvent, :338-369), reduced to
+// what the transport step needs.
+struct EventRec {
+  float4 a;   // gather position, alpha (alpha_geom or endpoint alpha_geom)
+  float4 b;   // gather normal, endpoint pdf or endpoint cosine
+  float4 c;   // path throughput, -
+  uint4 d;    // kind, target surfel, material, pixel
+};
+
+struct EventBufs {
+  EventRec* stage;        // per slot
+  EventRec* list;         // compacted, slot order
+};
+
+struct FrameArgs {
+  SceneView scene;
+  RunState* st;
+  const uint32_t* seeds;
+  const CameraRec* cams;
+  uint32_t ncams;
+  uint32_t total_pixels;
+  float* raw;             // packed H*W*4 per camera
+  float* ldr;
+  uint32_t gather_passes;
+  uint32_t rng_mode;
+  float exposure, gamma;
+};
+
+struct PhotonArgs {
+  SceneView scene;
+  RunState* st;
+  const uint32_t* seeds;
+  QueueBufs qb;
+  PhotonStore ps;
+  uint32_t photons_per_launch;
+  float inv_emitted;
+  uint32_t rr_start;
+  float q_null, q_reflect, q_transmit;
+};
+
+struct AdjointArgs {
+  SceneView scene;
+  RunState* st;
+  const uint32_t* seeds;
+  QueueBufs qb;
+  PendingBufs pend;
+  EventBufs ev;
+  const float* dldi;       // packed H*W*4 per camera
+  float* grad_opacity;
+  float* debug_opacity;    // packed H*W*4 per camera or null
+  CameraRec cam;
+  uint32_t rr_start;
+  float q_null, q_reflect, q_transmit;
+  float inv_spp;
+  uint32_t fixed_seed;     // reference mode: settings.random.number
+  uint32_t rng_mode;
+  uint32_t light0_valid;
+  float light0_area;
+};
+
+void photon_emit(const PhotonArgs& a, cudaStream_t s);
+void photon_bounce(const PhotonArgs& a, uint32_t parity, cudaStream_t s);
+void grid_build(const SceneView& sv, RunState* st, const PhotonStore& ps, const GridBufs& g, uint32_t cells,
+                int key_bits, cudaStream_t s);
+void camera_gather(const FrameArgs& a, cudaStream_t s);
+void adjoint_raygen(const AdjointArgs& a, cudaStream_t s);
+void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, cudaStream_t s);
+
+// Component queries.
+void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d, int32_t* inst,
+                int32_t* prim, float* t, float* alpha, float* pos, cudaStream_t s);
+void gather_points(const SceneView& sv, uint32_t n, const float* p, const float* nrm, float* E, cudaStream_t s);
+void load_photon_arrays(uint32_t n, const float* pos, const float* pw, const float* dir, const PhotonStore& ps,
+                        cudaStream_t s);
+
+}  // namespace pale

@@ -1,0 +1,725 @@
+// render.cu -- photon wavefront, photon grid, camera gather and adjoint pass.
+//
+// Work queues.  The reference appends survivors of a bounce with an atomic
+// counter and seeds each item's RNG with its queue slot
+// (PrimalKernels.cpp:80-82, AdjointKernels.cpp:99-101).  Here every bounce
+// kernel writes its result to a staging record at the input slot and counts
+// survivors per 256-slot tile; a one-block scan turns the tile counts into
+// offsets and a scatter kernel compacts the staging records in slot order.
+// A survivor's new slot is therefore its rank among the survivors -- the
+// slot a sequential run of the reference assigns -- so the RNG stream, the
+// photon deposit order and the images are deterministic.
+//
+// Seeds.  The host expands the reference's std::mt19937_64 seed stream
+// (SyclBridge.cpp:83-146, 170-227) into a table; RunState::seed_cursor
+// walks it on the device, advancing only for bounces that had work, as
+// the host loop `for (bounce...; activeCount > 0; ...)` does.
+#include "kernels.h"
+#include "trace.cuh"
+
+namespace pale {
+
+static inline uint32_t blocks_for(uint64_t n, int b = kBlock) { return (uint32_t)((n + b - 1) / b); }
+
+__device__ __forceinline__ void stage_top_nodes(const SceneView& S, BvhNode* smem) {
+  for (uint32_t i = threadIdx.x; i < S.top_nodes; i += blockDim.x) smem[i] = S.nodes[i];
+  __syncthreads();
+}
+
+__device__ __forceinline__ RayRec make_ray(V3 o, V3 d, V3 thr, uint32_t path, uint32_t bounce, uint32_t pixel) {
+  RayRec r;
+  r.o = make_float4(o.x, o.y, o.z, __uint_as_float(path));
+  r.d = make_float4(d.x, d.y, d.z, __uint_as_float(bounce));
+  r.t = make_float4(thr.x, thr.y, thr.z, __uint_as_float(pixel));
+  return r;
+}
+
+// ---------------------------------------------------------- compaction
+// One block: exclusive scan of the per-tile (alive, deposit/event) counts
+// of `n_in` slots; updates queue length, deposit/event bases and seeds.
+__global__ void k_queue_scan(RunState* st, const uint2* __restrict__ counts, uint2* __restrict__ offsets,
+                             uint32_t parity, int emission, uint32_t emission_n, int events, uint64_t photon_cap) {
+  __shared__ uint32_t s_wx[32], s_wy[32];
+  __shared__ uint32_t s_carry[2];
+  const uint32_t n_in = emission ? emission_n : st->active[parity];
+  const uint32_t tiles = (n_in + kBlock - 1) / kBlock;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) { s_carry[0] = 0; s_carry[1] = 0; }
+  __syncthreads();
+  for (uint32_t base = 0; base < tiles; base += blockDim.x) {
+    uint32_t t = base + threadIdx.x;
+    uint2 c = t < tiles ? counts[t] : make_uint2(0u, 0u);
+    uint32_t x = c.x, y = c.y;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t ax = __shfl_up_sync(0xffffffffu, x, o), ay = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) { x += ax; y += ay; }
+    }
+    if (lane == 31) { s_wx[wid] = x; s_wy[wid] = y; }
+    __syncthreads();
+    if (wid == 0) {
+      const int nw = blockDim.x >> 5;
+      uint32_t wx = lane < nw ? s_wx[lane] : 0u, wy = lane < nw ? s_wy[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t ax = __shfl_up_sync(0xffffffffu, wx, o), ay = __shfl_up_sync(0xffffffffu, wy, o);
+        if (lane >= o) { wx += ax; wy += ay; }
+      }
+      if (lane < nw) { s_wx[lane] = wx; s_wy[lane] = wy; }
+    }
+    __syncthreads();
+    uint32_t px = (wid > 0 ? s_wx[wid - 1] : 0u) + x - c.x;
+    uint32_t py = (wid > 0 ? s_wy[wid - 1] : 0u) + y - c.y;
+    if (t < tiles) offsets[t] = make_uint2(s_carry[0] + px, s_carry[1] + py);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_carry[0] += s_wx[(blockDim.x >> 5) - 1];
+      s_carry[1] += s_wy[(blockDim.x >> 5) - 1];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    st->active[emission ? 0u : (parity ^ 1u)] = s_carry[0];
+    if (events) {
+      st->event_count = s_carry[1];
+    } else {
+      st->photon_base = st->photon_attempts;
+      st->photon_attempts += s_carry[1];
+      if ((uint64_t)st->photon_base + s_carry[1] > photon_cap) atomicOr(&st->error, kErrPhotonCapacity);
+    }
+    st->seed_cursor += (emission || n_in > 0) ? 1u : 0u;
+  }
+}
+
+// Compacts staged rays (and deposits or events) of the `n_in` input slots.
+template <int kMode>  // 0 photons, 1 adjoint events
+__global__ void k_queue_scatter(RunState* st, QueueBufs qb, uint32_t parity, int emission, uint32_t emission_n,
+                                PhotonStore ps, EventBufs ev) {
+  __shared__ uint32_t s_wx[kBlock / 32], s_wy[kBlock / 32];
+  const uint32_t n_in = emission ? emission_n : st->active[parity];
+  const uint32_t tile = blockIdx.x;
+  if ((uint64_t)tile * kBlock >= n_in) return;
+  const uint32_t slot = tile * kBlock + threadIdx.x;
+  const bool in = slot < n_in;
+  const uint8_t f = in ? qb.flags[slot] : 0;
+  const bool alive = f & 1, side = f & 2;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned ba = __ballot_sync(0xffffffffu, alive), bs = __ballot_sync(0xffffffffu, side);
+  unsigned lt = (1u << lane) - 1u;
+  if (lane == 0) { s_wx[wid] = __popc(ba); s_wy[wid] = __popc(bs); }
+  __syncthreads();
+  uint32_t ra = __popc(ba & lt), rs = __popc(bs & lt);
+  for (int w = 0; w < wid; ++w) { ra += s_wx[w]; rs += s_wy[w]; }
+  const uint2 off = qb.tile_offsets[tile];
+  RayRec* out = qb.q[emission ? 0u : (parity ^ 1u)];
+  if (alive) {
+    uint32_t dst = off.x + ra;
+    if (dst < qb.capacity) out[dst] = qb.stage[slot];
+    else flag_error(st, kErrQueueCapacity);
+  }
+  if (side) {
+    if (kMode == 0) {
+      uint64_t dst = (uint64_t)st->photon_base + off.y + rs;
+      if (dst < ps.capacity) {
+        ps.a[dst] = ps.sa[slot];
+        ps.b[dst] = ps.sb[slot];
+        ps.c[dst] = ps.sc[slot];
+      }
+    } else {
+      ev.list[off.y + rs] = ev.stage[slot];
+    }
+  }
+}
+
+__global__ void k_advance(RunState* st, uint32_t by) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) st->seed_cursor += by;
+}
+
+// --------------------------------------------------------------- photons
+// launchRayGenEmitterKernel (PrimalKernels.cpp:13-62).
+__global__ void k_photon_emit(PhotonArgs A) {
+  const uint32_t g = blockIdx.x * kBlock + threadIdx.x;
+  bool alive = false;
+  if (g < A.photons_per_launch) {
+    const uint64_t base = A.seeds[A.st->seed_cursor];
+    Rng r(per_item_seed(base, g));
+    V3 pos, nrm, dir, pw;
+    if (A.scene.lights.count > 0 && sample_light(A.scene, r, pos, nrm, dir, pw)) {
+      V3 thr = scale(scale(pw, (float)A.scene.lights.count), A.inv_emitted);
+      A.qb.stage[g] = make_ray(pos, dir, thr, g, 0u, 0u);
+      alive = true;
+    }
+    A.qb.flags[g] = alive ? 1 : 0;
+  }
+  uint32_t c = __syncthreads_count(alive);
+  if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(c, 0u);
+}
+
+// launchIntersectKernel for the photon pass (PrimalKernels.cpp:65-321).
+__global__ void __launch_bounds__(kBlock) k_photon_bounce(PhotonArgs A, uint32_t parity) {
+  extern __shared__ BvhNode s_top[];
+  const uint32_t n_in = A.st->active[parity];
+  if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
+  stage_top_nodes(A.scene, s_top);
+  const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
+  bool alive = false, dep = false;
+  TraceCounters ctr{0, 0};
+  if (slot < n_in) {
+    const SceneView& S = A.scene;
+    const uint64_t base = A.seeds[A.st->seed_cursor];
+    Rng r(per_item_seed(base, slot));
+    const RayRec ry = A.qb.q[parity][slot];
+    const V3 o = xyz(ry.o), d = xyz(ry.d), thr = xyz(ry.t);
+    const uint32_t path = __float_as_uint(ry.o.w), bounce = __float_as_uint(ry.d.w) + 1u;
+    Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
+    if (h.inst >= 0) {
+      V3 no, nd, nt;
+      if (h.inst < (int)S.mesh.instances) {
+        V3 nrm = hit_normal(S, h);
+        // depositPhotonSurface (KernelHelpers.h:1688-1727)
+        dep = true;
+        A.ps.sa[slot] = f4(h.pos, thr.x);
+        A.ps.sb[slot] = f4(d, thr.y);
+        A.ps.sc[slot] = thr.z;
+        const float4 mat = __ldg(&S.mesh.materials[__ldg(&S.mesh.material[h.inst])]);
+        float pdf;
+        sample_cosine(r, nrm, nd, pdf);
+        no = h.pos + scale(nrm, 1e-6f);
+        nt = mul(thr, xyz(mat));
+        alive = russian_roulette(r, bounce, nt, A.rr_start);
+      } else {
+        const float4 cn4 = __ldg(&S.sf.cn[h.prim]);
+        const float4 n4 = __ldg(&S.sf.n[h.prim]);
+        const float opacity = n4.w;
+        float u = r.next_float();
+        if (u < A.q_null) {
+          float att = 1.0f - h.alpha * opacity;
+          float w = att / A.q_null;
+          no = h.pos + scale(d, 1e-5f);
+          nd = d;
+          nt = scale(thr, w);
+          alive = russian_roulette(r, bounce, nt, A.rr_start);
+        } else if (u < A.q_null + A.q_reflect) {
+          V3 cn = xyz(cn4);
+          float sc = dot(cn, -d);
+          V3 on = scale(cn, (float)(sc >= 0.0f ? 1 : -1));
+          dep = true;
+          V3 pw = divs(thr, A.q_reflect);
+          A.ps.sa[slot] = f4(h.pos, pw.x);
+          A.ps.sb[slot] = f4(d, pw.y);
+          A.ps.sc[slot] = pw.z;
+          float pdf;
+          sample_uniform_hemi(r, on, nd, pdf);
+          float ct = fmaxf(0.0f, dot(nd, on));
+          const float4 al = __ldg(&S.sf.alb[h.prim]);
+          V3 fs = scale(scale(xyz(al), al.w), kInvPi);
+          float alpha = h.alpha * opacity;
+          V3 w = divs(scale(scale(fs, alpha / A.q_reflect), ct), pdf);
+          no = h.pos + scale(on, 1e-5f);
+          nt = mul(thr, w);
+          alive = russian_roulette(r, bounce, nt, A.rr_start);
+        } else if (u < A.q_null + A.q_reflect + A.q_transmit) {
+          V3 cn = xyz(cn4);
+          float sc = dot(cn, -d);
+          V3 on = scale(cn, (float)(sc >= 0.0f ? 1 : -1));
+          float pdf;
+          sample_uniform_hemi(r, on, nd, pdf);
+          float ct = fmaxf(0.0f, dot(nd, on));
+          const float4 al = __ldg(&S.sf.alb[h.prim]);
+          V3 fs = scale(scale(xyz(al), 0.0f), kInvPi);   // alpha_t = 0
+          float alpha = h.alpha * opacity;
+          V3 w = divs(scale(scale(fs, alpha / A.q_reflect), ct), pdf);
+          no = h.pos + scale(-on, 1e-5f);
+          nt = mul(thr, w);
+          alive = russian_roulette(r, bounce, nt, A.rr_start);
+        }
+      }
+      if (alive) A.qb.stage[slot] = make_ray(no, nd, nt, path, bounce, 0u);
+    }
+    A.qb.flags[slot] = (alive ? 1 : 0) | (dep ? 2 : 0);
+  }
+  warp_count(&A.st->photon_segments, slot < n_in ? 1u : 0u);
+  warp_count(&A.st->node_visits, ctr.nodes);
+  warp_count(&A.st->surfel_tests, ctr.tests);
+  uint32_t ca = __syncthreads_count(alive), cd = __syncthreads_count(dep);
+  if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, cd);
+}
+
+static size_t top_smem(const SceneView& s) { return (size_t)s.top_nodes * sizeof(BvhNode); }
+
+void photon_emit(const PhotonArgs& a, cudaStream_t s) {
+  const uint32_t nb = blocks_for(a.photons_per_launch);
+  if (nb == 0) return;
+  k_photon_emit<<<nb, kBlock, 0, s>>>(a);
+  k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, 0, 1, a.photons_per_launch, 0,
+                                  a.ps.capacity);
+  k_queue_scatter<0><<<nb, kBlock, 0, s>>>(a.st, a.qb, 0, 1, a.photons_per_launch, a.ps, EventBufs{});
+}
+
+void photon_bounce(const PhotonArgs& a, uint32_t parity, cudaStream_t s) {
+  const uint32_t nb = blocks_for(a.qb.capacity);
+  k_photon_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity);
+  k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 0, a.ps.capacity);
+  k_queue_scatter<0><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, a.ps, EventBufs{});
+}
+
+// ------------------------------------------------------------ photon grid
+__global__ void k_stored(RunState* st, uint64_t cap, uint32_t* d_stored, uint32_t* d_attempts) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    uint64_t a = st->photon_attempts;
+    *d_stored = (uint32_t)(a < cap ? a : cap);
+    *d_attempts = (uint32_t)a;
+  }
+}
+
+// computePhotonCellIdsAndPermutation + countPhotonsPerCell
+// (PrimalKernels.cpp:796-855).
+__global__ void k_cell_ids(GridView G, const float4* __restrict__ pa, const uint32_t* __restrict__ d_stored,
+                           uint32_t* __restrict__ cell_id, uint32_t* __restrict__ sort_keys,
+                           uint32_t* __restrict__ sorted, uint32_t* __restrict__ cell_count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *d_stored) return;
+  int c[3];
+  world_to_cell(G, xyz(pa[i]), c);
+  uint32_t id = (uint32_t)((c[2] * G.res[1] + c[1]) * G.res[0] + c[0]);
+  cell_id[i] = id;
+  sort_keys[i] = id;
+  sorted[i] = i;
+  atomicAdd(&cell_count[id], 1u);
+}
+
+__global__ void k_gather_sorted(const uint32_t* __restrict__ sorted, const uint32_t* __restrict__ d_stored,
+                                const float4* __restrict__ a, const float4* __restrict__ b,
+                                const float* __restrict__ c, float4* __restrict__ sa, float4* __restrict__ sb,
+                                float* __restrict__ sc) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *d_stored) return;
+  uint32_t j = sorted[i];
+  sa[i] = a[j];
+  sb[i] = b[j];
+  sc[i] = c[j];
+}
+
+void grid_build(const SceneView& sv, RunState* st, const PhotonStore& ps, const GridBufs& g, uint32_t cells,
+                int key_bits, cudaStream_t s) {
+  const uint32_t cap = (uint32_t)ps.capacity;
+  k_stored<<<1, 32, 0, s>>>(st, ps.capacity, g.d_stored, g.d_attempts);
+  cudaMemsetAsync(g.cell_count, 0, ((size_t)cells + 1) * 4, s);
+  uint32_t* sort_keys = g.keys_tmp;            // first half: keys, second: ping-pong
+  uint32_t* sort_keys_tmp = g.keys_tmp + cap;
+  k_cell_ids<<<blocks_for(cap), kBlock, 0, s>>>(sv.grid, ps.a, g.d_stored, g.cell_id, sort_keys, g.sorted,
+                                                g.cell_count);
+  exclusive_scan(g.cell_count, g.cell_off, cells + 1, g.scan_temp, nullptr, s);
+  radix_sort_pairs(sort_keys, g.sorted, sort_keys_tmp, g.vals_tmp, g.d_stored, cap, key_bits, g.sort_temp, s);
+  k_gather_sorted<<<blocks_for(cap), kBlock, 0, s>>>(g.sorted, g.d_stored, ps.a, ps.b, ps.c, g.pa, g.pb, g.pc);
+}
+
+// ---------------------------------------------------------- primary rays
+// makePrimaryRayFromPixelJitteredFov (KernelHelpers.h:764-796).
+__device__ __forceinline__ void primary_ray(const CameraRec& C, float px, float py, float jx, float jy, V3& o,
+                                            V3& d) {
+  float u = (px + 0.5f + jx);
+  float v = (py + 0.5f + jy);
+  float vf = C.height - v;
+  float ndcX = (2.0f * u / C.width - 1.0f);
+  float ndcY = (2.0f * vf / C.height - 1.0f);
+  V3 dc = normalize(v3(ndcX * C.half_w / C.fx, ndcY * C.half_h / C.fy, -1.0f));
+  d = xform_dir(C.inv_view, dc);
+  float h[4];
+  m4mul(C.inv_view, 0.f, 0.f, 0.f, 1.f, h);
+  float invW = 1.f / h[3];
+  o = v3(h[0] * invW, h[1] * invW, h[2] * invW);
+}
+
+// -------------------------------------------------------- camera gather
+// launchCameraGatherKernel (PrimalKernels.cpp:500-653) fused with
+// launchPostProcessKernel (PostprocessKernel.cpp:11-106).  One thread per
+// pixel of all cameras; the gather passes run in order inside the thread so
+// the framebuffer sum has the reference's order.
+__global__ void __launch_bounds__(kBlock) k_camera_gather(FrameArgs A) {
+  extern __shared__ BvhNode s_top[];
+  stage_top_nodes(A.scene, s_top);
+  const uint32_t gp = blockIdx.x * kBlock + threadIdx.x;
+  TraceCounters ctr{0, 0};
+  uint32_t segs = 0, queries = 0, scanned = 0;
+  if (gp < A.total_pixels) {
+    uint32_t ci = 0;
+    while (ci + 1 < A.ncams && A.cams[ci + 1].pixel_offset <= gp) ++ci;
+    const CameraRec& C = A.cams[ci];
+    const uint32_t pix = gp - C.pixel_offset;
+    const uint32_t px = pix % C.w, py = pix / C.w;
+    const SceneView& S = A.scene;
+    const uint64_t cseed = A.seeds[A.st->seed_cursor + C.seed_slot];
+    const float spp = (float)A.gather_passes;
+    float fb[4] = {0.f, 0.f, 0.f, 0.f};
+    for (uint32_t pass = 0; pass < A.gather_passes; ++pass) {
+      const uint64_t base = A.rng_mode == 1 ? per_item_seed(cseed, pass) : cseed;
+      Rng r(per_item_seed(base, pix));
+      float jx = r.next_float() - 0.5f, jy = r.next_float() - 0.5f;
+      V3 o, d;
+      primary_ray(C, (float)px, (float)py, jx, jy, o, d);
+      V3 acc = v3(0.f, 0.f, 0.f);
+      float T = 1.0f;
+      int layer = 0;
+      for (; layer < kMaxLayers; ++layer) {
+        ++segs;
+        Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
+        if (h.inst < 0) break;
+        if (h.inst >= (int)S.mesh.instances) {
+          const float4 cn4 = __ldg(&S.sf.cn[h.prim]);
+          V3 n = xyz(cn4);
+          if (dot(n, -d) < 0.0f) n = -n;
+          ++queries;
+          V3 E = gather_irradiance(S.grid, h.pos, n, scanned);
+          const float4 al = __ldg(&S.sf.alb[h.prim]);
+          V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
+          float ae = __ldg(&S.sf.n[h.prim]).w * h.alpha;
+          acc = acc + scale(Lo, T * ae);
+          T *= (1.0f - ae);
+          o = h.pos + scale(d, 1e-4f);
+          continue;
+        }
+        const float4 mat = __ldg(&S.mesh.materials[__ldg(&S.mesh.material[h.inst])]);
+        if (mat.w > 0.f) {
+          V3 Le = scale(xyz(mat), mat.w);
+          Le = v3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
+          acc = acc + scale(Le, T);
+        } else {
+          V3 nrm = hit_normal(S, h);
+          ++queries;
+          V3 E = gather_irradiance(S.grid, h.pos, nrm, scanned);
+          V3 Lo = mul(scale(xyz(mat), kInvPi), E);
+          acc = acc + scale(Lo, T);
+        }
+        break;
+      }
+      if (layer == kMaxLayers) flag_error(A.st, kErrLayerCap);
+      float inv = 1.f / spp;
+      float cur[4] = {acc.x * inv, acc.y * inv, acc.z * inv, 1.0f * inv};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) fb[k] = cur[k] + fb[k];
+    }
+    const size_t o4 = 4 * (size_t)gp;
+    if (A.raw) *reinterpret_cast<float4*>(A.raw + o4) = make_float4(fb[0], fb[1], fb[2], fb[3]);
+    if (A.ldr) {
+      float ig = (A.gamma > 0.0f) ? (1.0f / A.gamma) : 1.0f;
+      float l[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float x = fb[c] * A.exposure;
+        x = fmaxf(x, 0.0f);
+        x = powf(x, ig);
+        l[c] = clampf(x, 0.0f, 1.0f);
+      }
+      *reinterpret_cast<float4*>(A.ldr + o4) = make_float4(l[0], l[1], l[2], 1.0f);
+    }
+  }
+  warp_count(&A.st->gather_segments, segs);
+  warp_count(&A.st->gather_queries, queries);
+  warp_count(&A.st->photons_scanned, scanned);
+  warp_count(&A.st->node_visits, ctr.nodes);
+  warp_count(&A.st->surfel_tests, ctr.tests);
+}
+
+void camera_gather(const FrameArgs& a, cudaStream_t s) {
+  if (a.total_pixels == 0) return;
+  k_camera_gather<<<blocks_for(a.total_pixels), kBlock, top_smem(a.scene), s>>>(a);
+}
+
+// ------------------------------------------------------------- adjoint
+enum : uint32_t { kKindNone = 0, kKindNull = 1, kKindReflect = 2, kKindTransmit = 3, kKindProjection = 4 };
+
+// launchRayGenAdjointKernel (AdjointKernels.cpp:15-84) + the per-spp
+// reset of the pending states (SyclBridge.cpp:222).
+__global__ void k_adj_raygen(AdjointArgs A) {
+  const CameraRec& C = A.cam;
+  const uint32_t npix = C.w * C.h;
+  const uint32_t p = blockIdx.x * kBlock + threadIdx.x;
+  if (p == 0) A.st->active[0] = npix;
+  if (p >= npix) return;
+  const uint64_t base = A.rng_mode == 1 ? (uint64_t)A.seeds[A.st->seed_cursor] : (uint64_t)A.fixed_seed;
+  Rng r(per_item_seed(base, p));
+  float jx = r.next_float() - 0.5f, jy = r.next_float() - 0.5f;
+  V3 o, d;
+  primary_ray(C, (float)(p % C.w), (float)(p / C.w), jx, jy, o, d);
+  const float4 g = *reinterpret_cast<const float4*>(A.dldi + 4 * ((size_t)C.pixel_offset + p));
+  A.qb.q[0][p] = make_ray(o, d, v3(g.x, g.y, g.z), p, 0u, p);
+  A.pend.a[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+  A.pend.b[p] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kKindNone));
+  A.pend.c[p] = make_uint4(kInvalid, kInvalid, 0u, 0u);
+}
+
+// launchAdjointIntersectKernel (AdjointKernels.cpp:87-386).
+__global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index) {
+  extern __shared__ BvhNode s_top[];
+  const uint32_t n_in = A.st->active[parity];
+  if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
+  stage_top_nodes(A.scene, s_top);
+  const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
+  bool alive = false, has_ev = false;
+  TraceCounters ctr{0, 0};
+  if (slot < n_in) {
+    const SceneView& S = A.scene;
+    const uint64_t base = A.rng_mode == 1 ? (uint64_t)A.seeds[A.st->seed_cursor] : (uint64_t)A.fixed_seed;
+    Rng r(per_item_seed(base, slot));
+    const RayRec ry = A.qb.q[parity][slot];
+    const V3 o = xyz(ry.o), d = xyz(ry.d), thr = xyz(ry.t);
+    const uint32_t path = __float_as_uint(ry.o.w), bounce = __float_as_uint(ry.d.w) + 1u;
+    const uint32_t pixel = __float_as_uint(ry.t.w);
+    Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
+    if (h.inst >= 0) {
+      const bool is_mesh = h.inst < (int)S.mesh.instances;
+      V3 nrm = hit_normal(S, h);
+      V3 on, dir;
+      float pdf = 0.f;
+      if (is_mesh) {
+        sample_cosine(r, nrm, dir, pdf);
+        on = nrm;
+      } else {
+        float sc = dot(nrm, -d);
+        on = scale(nrm, (float)(sc >= 0.0f ? 1 : -1));
+        sample_uniform_hemi(r, on, dir, pdf);
+      }
+      // complete the pending interaction with this hit as its endpoint
+      const float4 pa = A.pend.a[path], pb = A.pend.b[path];
+      const uint4 pc = A.pend.c[path];
+      const uint32_t pkind = __float_as_uint(pb.w);
+      EventRec ev;
+      if ((pkind == kKindReflect && !is_mesh) || pkind == kKindNull) {
+        const bool refl = pkind == kKindReflect;
+        V3 pthr = scale(xyz(pb), refl ? A.q_reflect : A.q_null);
+        float endcos = fmaxf(0.0f, dot(dir, on));
+        uint32_t mat = kInvalid;
+        if (refl) mat = __ldg(&S.mesh.material[pc.y]);
+        else if (is_mesh) mat = __ldg(&S.mesh.material[h.inst]);
+        ev.a = f4(h.pos, refl ? h.alpha : pa.w);
+        ev.b = f4(on, refl ? pdf : endcos);
+        ev.c = f4(pthr, 0.f);
+        ev.d = make_uint4(pkind, refl ? h.prim : pc.x, mat, pc.z);
+        has_ev = true;
+        A.pend.b[path] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kKindNone));
+        A.pend.a[path] = make_float4(0.f, 0.f, 0.f, 0.f);
+        A.pend.c[path] = make_uint4(kInvalid, pc.y, 0u, 0u);
+      }
+      V3 no, nd, nt;
+      if (is_mesh) {
+        const float4 mat = __ldg(&S.mesh.materials[__ldg(&S.mesh.material[h.inst])]);
+        no = h.pos + scale(nrm, 1e-6f);
+        nd = dir;
+        nt = mul(thr, xyz(mat));
+        alive = russian_roulette(r, bounce, nt, A.rr_start);
+        if (alive) {
+          V3 pt = mul(thr, xyz(mat));
+          A.pend.a[path] = f4(h.pos, 0.0f);
+          A.pend.b[path] = f4(pt, __uint_as_float(kKindReflect));
+          A.pend.c[path] = make_uint4(kInvalid, (uint32_t)h.inst, pixel, 0u);
+        }
+      } else {
+        const float opacity = __ldg(&S.sf.n[h.prim]).w;
+        float u = r.next_float();
+        if (u < A.q_null) {
+          float att = 1.0f - h.alpha * opacity;
+          float w = att / A.q_null;
+          no = h.pos + scale(d, 1e-5f);
+          nd = d;
+          nt = scale(thr, w);
+          alive = russian_roulette(r, bounce, nt, A.rr_start);
+          if (alive) {
+            A.pend.a[path] = f4(h.pos, h.alpha);
+            A.pend.b[path] = f4(divs(thr, A.q_null), __uint_as_float(kKindNull));
+            A.pend.c[path] = make_uint4(h.prim, kInvalid, pixel, 0u);
+          }
+        } else if (u < A.q_null + A.q_reflect) {
+          const float4 al = __ldg(&S.sf.alb[h.prim]);
+          V3 fs = scale(scale(xyz(al), al.w), kInvPi);
+          float ct = fmaxf(0.0f, dot(dir, on));
+          float alpha = h.alpha * opacity;
+          V3 m = divs(scale(scale(fs, ct), alpha / A.q_reflect), pdf);
+          no = h.pos + scale(on, 1e-5f);
+          nd = dir;
+          nt = mul(thr, m);
+          alive = russian_roulette(r, bounce, nt, A.rr_start);
+          if (alive && bounce_index == 0) {
+            ev.a = f4(h.pos, h.alpha);
+            ev.b = f4(on, 0.f);
+            ev.c = f4(divs(thr, A.q_reflect), 0.f);
+            ev.d = make_uint4(kKindProjection, h.prim, kInvalid, pixel);
+            has_ev = true;
+          }
+        } else if (u < A.q_null + A.q_reflect + A.q_transmit) {
+          float alpha = h.alpha * opacity;
+          float w = (alpha * 0.0f) / A.q_transmit;   // alpha_t = 0
+          V3 t2 = scale(thr, w);
+          V3 on2 = on;
+          float pdf2;
+          sample_uniform_hemi(r, on2, nd, pdf2);
+          const float4 al = __ldg(&S.sf.alb[h.prim]);
+          no = h.pos + scale(-on2, 1e-5f);
+          nt = mul(t2, xyz(al));
+          alive = russian_roulette(r, bounce, nt, A.rr_start);
+        }
+      }
+      if (alive) A.qb.stage[slot] = make_ray(no, nd, nt, path, bounce, pixel);
+      if (has_ev) A.ev.stage[slot] = ev;
+    }
+    A.qb.flags[slot] = (alive ? 1 : 0) | (has_ev ? 2 : 0);
+  }
+  warp_count(&A.st->adjoint_segments, slot < n_in ? 1u : 0u);
+  warp_count(&A.st->node_visits, ctr.nodes);
+  warp_count(&A.st->surfel_tests, ctr.tests);
+  uint32_t ca = __syncthreads_count(alive), ce = __syncthreads_count(has_ev);
+  if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, ce);
+}
+
+// launchAdjointTransportKernel (AdjointKernels.cpp:389-509).  Lanes of a
+// warp that update the same surfel add their terms with shuffles first and
+// issue one atomicAdd per surfel.
+__global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
+  const uint32_t count = A.st->event_count;
+  const uint32_t e = blockIdx.x * kBlock + threadIdx.x;
+  if ((uint64_t)blockIdx.x * kBlock >= count) return;
+  const SceneView& S = A.scene;
+  float g = 0.f;
+  uint32_t target = kInvalid;
+  uint32_t pixel = 0;
+  uint32_t queries = 0, scanned = 0;
+  if (e < count) {
+    const EventRec ev = A.ev.list[e];
+    const uint32_t kind = ev.d.x;
+    pixel = ev.d.w;
+    const V3 pos = xyz(ev.a), nrm = xyz(ev.b), thr = xyz(ev.c);
+    if (kind == kKindProjection) {
+      target = ev.d.y;
+      const float4 al = __ldg(&S.sf.alb[target]);
+      ++queries;
+      V3 E = gather_irradiance(S.grid, pos, nrm, scanned);
+      V3 fr = scale(scale(xyz(al), al.w), kInvPi);
+      V3 Lo = mul(fr, E);
+      g = vsum(mul(scale(thr, ev.a.w), Lo)) * A.inv_spp;
+    } else if (kind == kKindNull) {
+      target = ev.d.y;
+      // a surfel endpoint has no material (the reference reads
+      // materials[0xFFFFFFFF], AdjointKernels.cpp:446-447): no contribution
+      if (ev.d.z != kInvalid) {
+        const float4 mat = __ldg(&S.mesh.materials[ev.d.z]);
+        ++queries;
+        V3 Lr = scale(mul(gather_irradiance(S.grid, pos, nrm, scanned), xyz(mat)), kInvPi);
+        V3 Le = v3(0.f, 0.f, 0.f);
+        if (mat.w > 0.f) {
+          float area = A.light0_valid ? A.light0_area : 0.f;
+          Le = scale(scale(xyz(mat), mat.w / (kPi * area)), ev.b.w);
+        }
+        V3 Lo = Le + Lr;
+        g = vsum(mul(scale(thr, -ev.a.w), Lo)) * A.inv_spp;
+      }
+    } else if (kind == kKindReflect) {
+      target = ev.d.y;
+      const float4 mat = __ldg(&S.mesh.materials[ev.d.z]);
+      ++queries;
+      V3 Lo = scale(mul(gather_irradiance(S.grid, pos, nrm, scanned), xyz(mat)), kInvPi);
+      V3 p = divs(thr, ev.b.w);
+      g = vsum(scale(mul(p, Lo), ev.a.w)) * A.inv_spp;
+    }
+    if (target >= S.sf.count && target != kInvalid) {
+      flag_error(A.st, kErrBounds);
+      target = kInvalid;
+    }
+  }
+  const unsigned full = __activemask();
+  const int lane = threadIdx.x & 31;
+  unsigned peers = __match_any_sync(full, target);
+  float sum = 0.f;
+  for (int k = 0; k < 32; ++k) {
+    float v = __shfl_sync(full, g, k);
+    if ((peers >> k) & 1u) sum += v;
+  }
+  if (target != kInvalid && lane == __ffs(peers) - 1) atomicAdd(&A.grad_opacity[target], sum);
+  if (A.debug_opacity && target != kInvalid && e < count) {
+    float* px = A.debug_opacity + 4 * ((size_t)A.cam.pixel_offset + pixel);
+    atomicAdd(px + 0, g);
+    atomicAdd(px + 1, g);
+    atomicAdd(px + 2, g);
+    px[3] = 1.0f;
+  }
+  warp_count(&A.st->gradient_events, e < count ? 1u : 0u);
+  warp_count(&A.st->gather_queries, queries);
+  warp_count(&A.st->photons_scanned, scanned);
+}
+
+void adjoint_raygen(const AdjointArgs& a, cudaStream_t s) {
+  const uint32_t npix = a.cam.w * a.cam.h;
+  k_adj_raygen<<<blocks_for(npix), kBlock, 0, s>>>(a);
+  k_advance<<<1, 32, 0, s>>>(a.st, 1u);
+}
+
+void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, cudaStream_t s) {
+  const uint32_t nb = blocks_for(a.qb.capacity);
+  const uint32_t parity = bounce & 1u;
+  k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce);
+  k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0);
+  k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev);
+  k_transport<<<nb, kBlock, 0, s>>>(a);
+}
+
+// ------------------------------------------------------ component queries
+__global__ void __launch_bounds__(kBlock) k_trace_rays(SceneView S, RunState* st, uint32_t n,
+                                                       const float* __restrict__ o, const float* __restrict__ d,
+                                                       int32_t* inst, int32_t* prim, float* t, float* alpha,
+                                                       float* pos) {
+  extern __shared__ BvhNode s_top[];
+  stage_top_nodes(S, s_top);
+  uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  TraceCounters ctr{0, 0};
+  Hit h = intersect_scene(S, s_top, v3(o[3 * i], o[3 * i + 1], o[3 * i + 2]), v3(d[3 * i], d[3 * i + 1], d[3 * i + 2]),
+                          ctr, st);
+  inst[i] = h.inst;
+  prim[i] = h.inst >= 0 ? (int32_t)h.prim : -1;
+  t[i] = h.inst >= 0 ? h.t : 3.402823466e+38f;
+  alpha[i] = h.inst >= 0 ? h.alpha : 0.f;
+  if (pos) {
+    pos[3 * i] = h.pos.x;
+    pos[3 * i + 1] = h.pos.y;
+    pos[3 * i + 2] = h.pos.z;
+  }
+}
+
+void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d, int32_t* inst,
+                int32_t* prim, float* t, float* alpha, float* pos, cudaStream_t s) {
+  if (n == 0) return;
+  k_trace_rays<<<blocks_for(n), kBlock, top_smem(sv), s>>>(sv, st, n, o, d, inst, prim, t, alpha, pos);
+}
+
+__global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict__ p, const float* __restrict__ nrm,
+                                float* E) {
+  uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  uint32_t sc = 0;
+  V3 e = gather_irradiance(S.grid, v3(p[3 * i], p[3 * i + 1], p[3 * i + 2]),
+                           v3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]), sc);
+  E[3 * i] = e.x;
+  E[3 * i + 1] = e.y;
+  E[3 * i + 2] = e.z;
+}
+
+void gather_points(const SceneView& sv, uint32_t n, const float* p, const float* nrm, float* E, cudaStream_t s) {
+  if (n == 0) return;
+  k_gather_points<<<blocks_for(n), kBlock, 0, s>>>(sv, n, p, nrm, E);
+}
+
+__global__ void k_load_photons(uint32_t n, const float* __restrict__ pos, const float* __restrict__ pw,
+                               const float* __restrict__ dir, PhotonStore ps) {
+  uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  ps.a[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], pw[3 * i]);
+  ps.b[i] = make_float4(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2], pw[3 * i + 1]);
+  ps.c[i] = pw[3 * i + 2];
+}
+
+void load_photon_arrays(uint32_t n, const float* pos, const float* pw, const float* dir, const PhotonStore& ps,
+                        cudaStream_t s) {
+  if (n == 0) return;
+  k_load_photons<<<blocks_for(n), kBlock, 0, s>>>(n, pos, pw, dir, ps);
+}
+
+}  // namespace pale

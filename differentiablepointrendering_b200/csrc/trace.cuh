@@ -1,0 +1,423 @@
+// trace.cuh -- closest-hit scene queries, sampling and photon lookups.
+//
+// intersect_scene() returns the closest hit over the mesh instances and the
+// surfel cloud, the FirstHit mode of intersectScene
+// (Pale/Renderer/Kernels/IntersectionKernels.h:954-1097).  The surfel part
+// walks the LBVH with a short stack of (node, entry distance) pairs; the
+// first `top_nodes` nodes are read from a shared-memory copy staged by the
+// calling kernel.
+#pragma once
+
+#include "common.cuh"
+
+namespace pale {
+
+struct Hit {
+  int inst;        // -1 miss; mesh instance index; == mesh.instances for a surfel
+  uint32_t prim;   // triangle id or surfel index (BVH order)
+  float t;         // world-space distance along the ray
+  float alpha;     // alpha_geom of a surfel hit (0 for meshes)
+  V3 pos;          // world hit position
+};
+
+struct TraceCounters {
+  uint32_t nodes;
+  uint32_t tests;
+};
+
+// safeInvDir (KernelHelpers.h:140-148).
+__device__ __forceinline__ V3 safe_inv(V3 d) {
+  return v3(fabsf(d.x) < 1e-6f ? 1e30f : 1.f / d.x, fabsf(d.y) < 1e-6f ? 1e30f : 1.f / d.y,
+            fabsf(d.z) < 1e-6f ? 1e30f : 1.f / d.z);
+}
+
+// slabIntersectAABB (KernelHelpers.h:150-214): returns the entry distance
+// or +inf on a miss.
+__device__ __forceinline__ float slab_entry(V3 o, V3 inv, float lx, float ly, float lz, float hx, float hy,
+                                            float hz, float limit) {
+  float t0x = (lx - o.x) * inv.x, t1x = (hx - o.x) * inv.x;
+  float t0y = (ly - o.y) * inv.y, t1y = (hy - o.y) * inv.y;
+  float t0z = (lz - o.z) * inv.z, t1z = (hz - o.z) * inv.z;
+  float tmin = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
+  float tmax = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+  if (tmin > tmax || tmax < 0.0f || tmin > limit) return __int_as_float(0x7f800000);
+  return tmin;
+}
+
+// intersectTriangle (KernelHelpers.h:248-277).
+__device__ __forceinline__ bool tri_hit(V3 o, V3 d, V3 v0, V3 v1, V3 v2, float tmin, float& t_out) {
+  V3 e1 = v1 - v0, e2 = v2 - v0;
+  V3 h = cross(d, e2);
+  float a = dot(e1, h);
+  if (fabsf(a) < 1.0e-4f) return false;
+  float f = 1.0f / a;
+  V3 s = o - v0;
+  float u = f * dot(s, h);
+  if (u < 0.0f || u > 1.0f) return false;
+  V3 q = cross(s, e1);
+  float v = f * dot(d, q);
+  if (v < 0.0f || u + v > 1.0f) return false;
+  float t = f * dot(e2, q);
+  if (t <= tmin) return false;
+  t_out = t;
+  return true;
+}
+
+// intersectSurfel + opacityBeta (KernelHelpers.h:506-669) on the
+// precomputed surfel arrays.
+__device__ __forceinline__ bool surfel_hit(const SurfelView& sf, uint32_t i, V3 o, V3 d, float tmin, float tmax,
+                                           float& t_out, V3& x_out, float& a_out) {
+  const float4 n4 = __ldg(&sf.n[i]);
+  const float4 pe = __ldg(&sf.pe[i]);
+  V3 n = xyz(n4);
+  float nd = dot(n, d);
+  if (fabsf(nd) < 1e-6f) return false;
+  V3 p = xyz(pe);
+  float th = dot(n, p - o) / nd;
+  if (th <= tmin || th >= tmax) return false;
+  const float4 u4 = __ldg(&sf.u[i]);
+  const float4 v4 = __ldg(&sf.v[i]);
+  V3 x = o + scale(d, th);
+  V3 r = x - p;
+  float u = dot(xyz(u4), r) / u4.w;
+  float v = dot(xyz(v4), r) / v4.w;
+  float r2 = u * u + v * v;
+  if (r2 >= 1.0f) return false;
+  a_out = powf(1.0f - r2, pe.w);
+  t_out = th;
+  x_out = x;
+  return true;
+}
+
+__device__ __forceinline__ void load_node(const SceneView& S, const BvhNode* __restrict__ smem_top, uint32_t idx,
+                                          float4& a, float4& b, float4& c, uint4& w) {
+  if (idx < S.top_nodes) {
+    const BvhNode& nd = smem_top[idx];
+    a = nd.a; b = nd.b; c = nd.c; w = nd.d;
+  } else {
+    const BvhNode* nd = S.nodes + idx;
+    a = __ldg(&nd->a); b = __ldg(&nd->b); c = __ldg(&nd->c); w = __ldg(&nd->d);
+  }
+}
+
+// Closest surfel with t in (1e-5, limit) along (o, d) (the surfel cloud's
+// transform is the identity, so this is intersectBLASPointCloudFirstHit,
+// IntersectionKernels.h:585-675).  Returns false on a miss.
+__device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
+                                               float limit, uint32_t& prim, float& t, V3& x, float& alpha,
+                                               TraceCounters& ctr, RunState* st) {
+  if (S.node_count == 0) return false;
+  const V3 inv = safe_inv(d);
+  float best = limit;
+  bool hit = false;
+  uint32_t stack_node[kStackDepth];
+  float stack_t[kStackDepth];
+  int sp = 0;
+  uint32_t node = 0;
+  while (true) {
+    float4 a, b, c;
+    uint4 w;
+    if (node >= S.node_count) {
+      flag_error(st, kErrBounds);
+      break;
+    }
+    load_node(S, smem_top, node, a, b, c, w);
+    ctr.nodes++;
+    float e0 = w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
+    float e1 = w.y == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, b.z, b.w, c.x, c.y, c.z, c.w, best);
+    bool h0 = e0 <= best, h1 = e1 <= best;
+    // leaves: test their surfels now, nearer leaf first
+    uint32_t lw[2] = {w.x, w.y};
+    bool lh[2] = {h0 && (w.x & kLeafFlag) != 0, h1 && (w.y & kLeafFlag) != 0};
+    int first = (e1 < e0) ? 1 : 0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      int cidx = k == 0 ? first : 1 - first;
+      if (!lh[cidx]) continue;
+      uint32_t word = lw[cidx];
+      uint32_t f0 = word & 0x0FFFFFFFu, cnt = ((word >> 28) & 7u) + 1u;
+      if (f0 + cnt > S.sf.count) {
+        flag_error(st, kErrBounds);
+        continue;
+      }
+      for (uint32_t j = 0; j < cnt; ++j) {
+        float th, aa;
+        V3 xx;
+        ctr.tests++;
+        if (surfel_hit(S.sf, f0 + j, o, d, 1e-5f, best, th, xx, aa)) {
+          best = th;
+          hit = true;
+          prim = f0 + j;
+          x = xx;
+          alpha = aa;
+        }
+      }
+    }
+    h0 = h0 && !(w.x & kLeafFlag) && e0 <= best;
+    h1 = h1 && !(w.y & kLeafFlag) && e1 <= best;
+    if (h0 && h1) {
+      uint32_t nearN = e0 <= e1 ? w.x : w.y, farN = e0 <= e1 ? w.y : w.x;
+      float farT = e0 <= e1 ? e1 : e0;
+      if (sp < kStackDepth) {
+        stack_node[sp] = farN;
+        stack_t[sp] = farT;
+        ++sp;
+      } else {
+        flag_error(st, kErrStackOverflow);
+      }
+      node = nearN;
+      continue;
+    }
+    if (h0) { node = w.x; continue; }
+    if (h1) { node = w.y; continue; }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (stack_t[sp] <= best) {
+        node = stack_node[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  if (hit) t = best;
+  return hit;
+}
+
+// intersectScene, FirstHit mode: mesh instances in object space
+// (intersectBLASMesh, IntersectionKernels.h:37-105) and the surfel cloud;
+// the closest world-space distance wins (:1060-1081).
+__device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
+                                               TraceCounters& ctr, RunState* st) {
+  Hit h;
+  h.inst = -1;
+  h.prim = 0;
+  h.t = 3.402823466e+38f;
+  h.alpha = 0.f;
+  h.pos = v3(0.f, 0.f, 0.f);
+  float best = __int_as_float(0x7f800000);
+  const V3 invw = safe_inv(d);
+  const MeshView& M = S.mesh;
+  for (uint32_t i = 0; i < M.instances; ++i) {
+    const float4 lo = __ldg(&M.box[2 * i]), hi = __ldg(&M.box[2 * i + 1]);
+    if (!(slab_entry(o, invw, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, best) <= best)) continue;
+    const float* W2O = M.w2o + 16 * i;
+    float w2o[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) w2o[k] = __ldg(&W2O[k]);
+    V3 oo = xform_point(w2o, o);
+    V3 dd = xform_dir(w2o, d);
+    uint2 rg = __ldg(&M.tri_range[i]);
+    float bt = __int_as_float(0x7f800000);
+    bool any = false;
+    uint32_t bprim = 0;
+    for (uint32_t k = 0; k < rg.y; ++k) {
+      const float4* tv = M.tri + 3 * (rg.x + k);
+      float t;
+      if (tri_hit(oo, dd, xyz(__ldg(&tv[0])), xyz(__ldg(&tv[1])), xyz(__ldg(&tv[2])), 1e-4f, t) && t < bt &&
+          t > 0.0f) {
+        bt = t;
+        any = true;
+        bprim = rg.x + k;
+      }
+    }
+    if (!any) continue;
+    float o2w[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) o2w[k] = __ldg(&M.o2w[16 * i + k]);
+    V3 hw = xform_point(o2w, oo + scale(dd, bt));
+    float tw = dot(hw - o, d);
+    if (tw > 0.0f && tw < best) {
+      best = tw;
+      h.inst = (int)i;
+      h.t = tw;
+      h.pos = hw;
+      h.prim = bprim;
+      h.alpha = 0.0f;
+    }
+  }
+  if (S.has_pc &&
+      slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best) <= best) {
+    V3 dd = normalize(d);
+    // prune with the mesh hit plus a relative margin: a surfel beyond the
+    // margin cannot have a smaller world distance than the mesh hit
+    float limit = best < 3.0e38f ? best * 1.00001f + 1e-6f : __int_as_float(0x7f800000);
+    uint32_t prim;
+    float t, a;
+    V3 x;
+    if (surfel_closest(S, smem_top, o, dd, limit, prim, t, x, a, ctr, st)) {
+      float tw = dot(x - o, d);
+      if (tw > 0.0f && tw < best) {
+        best = tw;
+        h.inst = (int)M.instances;
+        h.t = tw;
+        h.pos = x;
+        h.prim = prim;
+        h.alpha = a;
+      }
+    }
+  }
+  return h;
+}
+
+// buildIntersectionNormal (KernelHelpers.h:480-503).
+__device__ __forceinline__ V3 hit_normal(const SceneView& S, const Hit& h) {
+  if (h.inst < (int)S.mesh.instances) {
+    float o2w[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) o2w[k] = __ldg(&S.mesh.o2w[16 * h.inst + k]);
+    const float4* tv = S.mesh.tri + 3 * h.prim;
+    V3 p0 = xform_point(o2w, xyz(__ldg(&tv[0])));
+    V3 p1 = xform_point(o2w, xyz(__ldg(&tv[1])));
+    V3 p2 = xform_point(o2w, xyz(__ldg(&tv[2])));
+    return normalize(cross(p1 - p0, p2 - p0));
+  }
+  return xyz(__ldg(&S.sf.cn[h.prim]));
+}
+
+// ------------------------------------------------------------- sampling
+// sampleCosineHemisphere, rng-first overload (KernelHelpers.h:317-337).
+__device__ __forceinline__ void sample_cosine(Rng& r, V3 n, V3& out, float& pdf) {
+  float u1 = r.next_float(), u2 = r.next_float();
+  float z = sqrtf(1.f - u1);
+  float rr = sqrtf(1 - (z * z));
+  float phi = 2.f * kPi * u2;
+  float x = rr * cosf(phi), y = rr * sinf(phi);
+  V3 up = fabsf(n.z) < .999f ? v3(0, 0, 1) : v3(1, 0, 0);
+  V3 tang = normalize(cross(up, n));
+  V3 bit = cross(n, tang);
+  out = normalize(scale(tang, x) + scale(bit, y) + scale(n, z));
+  pdf = fmaxf(0.f, dot(out, n)) / kPi;
+}
+
+// sampleUniformHemisphereAroundNormal with the Frisvad basis
+// (KernelHelpers.h:541-611).
+__device__ __forceinline__ void sample_uniform_hemi(Rng& r, V3 normal, V3& out, float& pdf) {
+  V3 n = normalize(normal);
+  float u1 = r.next_float(), u2 = r.next_float();
+  float z = u1;
+  float phi = 2.0f * kPi * u2;
+  float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+  float x = rr * cosf(phi), y = rr * sinf(phi);
+  float sign = copysignf(1.0f, n.z);
+  float a = -1.0f / (sign + n.z);
+  float b = n.x * n.y * a;
+  V3 T = v3(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
+  V3 B = v3(b, sign + n.y * n.y * a, -n.y);
+  out = normalize(scale(T, x) + scale(B, y) + scale(n, z));
+  pdf = 1.0f / (2.0f * kPi);
+}
+
+// applyRussianRoulette (KernelHelpers.h:1612-1657).
+__device__ __forceinline__ bool russian_roulette(Rng& r, uint32_t bounce, V3& thr, uint32_t start) {
+  if (bounce < start) return true;
+  if (!isfinite(thr.x) || !isfinite(thr.y) || !isfinite(thr.z)) return false;
+  float lum = 0.2126f * thr.x + 0.7152f * thr.y + 0.0722f * thr.z;
+  float p = clampf(lum, 0.0f, 0.99f);
+  if (r.next_float() > p) return false;
+  float c = 1.0f / p;
+  c = fminf(c, 10.0f);
+  thr = scale(thr, c);
+  return true;
+}
+
+// sampleMeshAreaLight (KernelHelpers.h:340-449).
+__device__ __forceinline__ bool sample_light(const SceneView& S, Rng& r, V3& pos, V3& nrm, V3& dir, V3& power) {
+  const LightView& L = S.lights;
+  if (L.count == 0) return false;
+  float ul = r.next_float();
+  uint32_t li = (uint32_t)(ul * (float)L.count);
+  if (li > L.count - 1u) li = L.count - 1u;
+  uint4 rec = __ldg(&L.rec[li]);
+  float area = __ldg(&L.area[li]);
+  if (rec.z == 0u || area <= 0.0f) return false;
+  float ut = r.next_float();
+  uint32_t lo = 0, hi = rec.z - 1u;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1u;
+    if (ut <= __ldg(&L.cdf[rec.y + mid])) hi = mid;
+    else lo = mid + 1u;
+  }
+  uint32_t tri = __ldg(&L.tri[rec.y + lo]);
+  const float4* tv = S.mesh.tri + 3 * tri;
+  V3 p0 = xyz(__ldg(&tv[0])), p1 = xyz(__ldg(&tv[1])), p2 = xyz(__ldg(&tv[2]));
+  float u1 = r.next_float(), u2 = r.next_float();
+  float su1 = sqrtf(u1);
+  float b0 = 1.0f - su1, b1 = su1 * (1.0f - u2), b2 = su1 * u2;
+  V3 xo = scale(p0, b0) + scale(p1, b1) + scale(p2, b2);
+  float o2w[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) o2w[k] = __ldg(&S.mesh.o2w[16 * rec.x + k]);
+  V3 w0 = xform_point(o2w, p0), w1 = xform_point(o2w, p1), w2 = xform_point(o2w, p2);
+  V3 e0 = w1 - w0, e1 = w2 - w0;
+  V3 nw = v3(e0.y * e1.z - e0.z * e1.y, e0.z * e1.x - e0.x * e1.z, e0.x * e1.y - e0.y * e1.x);
+  float nl = sqrtf(dot(nw, nw));
+  if (nl <= 0.0f) return false;
+  nw = divs(nw, nl);
+  float pdf;
+  sample_cosine(r, nw, dir, pdf);
+  pos = xform_point(o2w, xo);
+  nrm = nw;
+  float4 col = __ldg(&L.col[li]);
+  power = scale(xyz(col), col.w);
+  return true;
+}
+
+// --------------------------------------------------------------- photons
+// worldToCellClamped / linearCellIndex (KernelHelpers.h:900-987).
+__device__ __forceinline__ void world_to_cell(const GridView& G, V3 p, int c[3]) {
+  V3 l = p - G.origin;
+  float f[3] = {l.x / G.cell.x, l.y / G.cell.y, l.z / G.cell.z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int v = (int)floorf(f[a]);
+    v = v < 0 ? 0 : v;
+    v = v > G.res[a] - 1 ? G.res[a] - 1 : v;
+    c[a] = v;
+  }
+}
+
+// gatherDiffuseIrradianceAtPoint (KernelHelpers.h:990-1037).  Photons are
+// stored sorted by cell with ascending deposit index inside a cell, and the
+// cells of one grid row (fixed y, z) are contiguous, so each row is a single
+// contiguous photon range; the summation order equals the reference's
+// cell-by-cell loop.
+__device__ __forceinline__ V3 gather_irradiance(const GridView& G, V3 x, V3 n, uint32_t& scanned) {
+  const float r = G.radius, r2 = r * r;
+  const float invArea = 1.0f / (kPi * r2);
+  int c0[3], c1[3];
+  world_to_cell(G, x - v3(r, r, r), c0);
+  world_to_cell(G, x + v3(r, r, r), c1);
+  float ex = 0.f, ey = 0.f, ez = 0.f;
+  uint32_t sc = 0;
+  for (int cz = c0[2]; cz <= c1[2]; ++cz) {
+    for (int cy = c0[1]; cy <= c1[1]; ++cy) {
+      uint32_t row = (uint32_t)((cz * G.res[1] + cy) * G.res[0]);
+      uint32_t j0 = __ldg(&G.cell_off[row + c0[0]]);
+      uint32_t j1 = __ldg(&G.cell_off[row + c1[0] + 1]);
+      sc += j1 - j0;
+      for (uint32_t j = j0; j < j1; ++j) {
+        float4 pa = __ldg(&G.pa[j]);
+        float dx = pa.x - x.x, dy = pa.y - x.y, dz = pa.z - x.z;
+        float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 > r2) continue;
+        float4 pb = __ldg(&G.pb[j]);
+        float cosine = n.x * (-pb.x) + n.y * (-pb.y) + n.z * (-pb.z);
+        if (cosine < 0.0f) continue;
+        float pcb = __ldg(&G.pc[j]);
+        ex = ex + pa.w * invArea;
+        ey = ey + pb.w * invArea;
+        ez = ez + pcb * invArea;
+      }
+    }
+  }
+  scanned += sc;
+  uint32_t T = *G.attempts;
+  uint32_t D = (uint64_t)T < G.capacity ? T : (uint32_t)G.capacity;
+  if (D == 0u) return v3(0.f, 0.f, 0.f);
+  float s = (float)T / (float)D;
+  return v3(ex * s, ey * s, ez * s);
+}
+
+}  // namespace pale

@@ -1,0 +1,386 @@
+"""``pale.Renderer`` on the B200 renderer.
+
+This module mirrors the pybind11 surface of Pale (Pale/pale_bindings.cpp:
+1613-1650) -- method names, argument names and defaults, dict keys, array
+shapes and error types -- so Pale's optimisation loop (python/training.py,
+python/render_hooks.py) and its finite-difference scripts run unchanged with
+``import differentiablepointrendering_b200.pale as pale``.
+
+Every call goes through the C-ABI of ``libpale_b200.so``; there is no CPU
+path.  Arrays returned are fresh host copies; parameters and gradients are
+in BVH order, as in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+from .scene import (POINT_FIELDS, SceneArrays, as_points, load_mitsuba_scene, load_surfel_ply,
+                    resolve_point_cloud)
+
+
+def _check(lib, h, rc: int, what: str):
+    if rc != 0:
+        msg = lib.pale_last_error(h)
+        msg = msg.decode(errors="replace") if msg else ""
+        raise RuntimeError(f"{what} failed ({rc}): {msg}")
+
+
+class Renderer:
+    """Adjoint photon-mapping renderer for beta surfels on one B200.
+
+    Renderer(assetRootDir, sceneXml="cbox_custom.xml",
+             pointCloudFile="initial.ply", settings={})
+    """
+
+    def __init__(self, assetRootDir: str, sceneXml: str = "cbox_custom.xml",
+                 pointCloudFile: str = "initial.ply", settings: Optional[dict] = None,
+                 *, scene: Optional[SceneArrays] = None):
+        self._lib = N.load_library()
+        self._h = C.c_void_p()
+        if scene is None:
+            root = os.path.abspath(assetRootDir)
+            pts = load_surfel_ply(resolve_point_cloud(root, pointCloudFile))
+            scene = load_mitsuba_scene(root, sceneXml, pts)
+        self._scene = scene
+        self._settings = N.settings_from_dict(settings)
+        self._asset = {k: v.copy() for k, v in as_points(scene.points).items()}
+        desc = N.SceneDescHolder(scene)
+        rc = self._lib.pale_create(C.byref(desc.struct), C.byref(self._settings), C.byref(self._h))
+        if rc != 0:
+            msg = self._lib.pale_last_error(None)
+            raise RuntimeError(f"pale_create failed ({rc}): {msg.decode(errors='replace') if msg else ''}")
+        self._names = list(scene.camera_names)
+        self._sizes = [(int(w), int(h)) for w, h in scene.camera_size]
+        self._adjoint = [bool(a) for a in scene.camera_adjoint]
+
+    @classmethod
+    def from_scene(cls, scene: SceneArrays, settings: Optional[dict] = None) -> "Renderer":
+        """Renderer over in-memory scene arrays (no files)."""
+        return cls("", settings=settings, scene=scene)
+
+    # ------------------------------------------------------------ basics
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.pale_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_camera_names(self) -> List[str]:
+        return list(self._names)
+
+    @property
+    def num_points(self) -> int:
+        n = C.c_uint32()
+        _check(self._lib, self._h, self._lib.pale_point_count(self._h, C.byref(n)), "pale_point_count")
+        return int(n.value)
+
+    @property
+    def settings(self) -> N.PaleSettings:
+        return self._settings
+
+    # ----------------------------------------------------------- forward
+    def render_forward(self, camera_name: str = "") -> Dict[str, np.ndarray]:
+        """{cam: LDR (H,W,4), cam+'_raw': HDR (H,W,4)} float32
+        (render_forward, pale_bindings.cpp:180-277)."""
+        idx = [i for i, n in enumerate(self._names) if (not camera_name or n == camera_name)]
+        pix = sum(self._sizes[i][0] * self._sizes[i][1] for i in idx)
+        ldr = np.empty(max(1, pix) * 4, np.float32)
+        raw = np.empty(max(1, pix) * 4, np.float32)
+        cams = N.cams_array(idx)
+        rc = self._lib.pale_render_forward(self._h, len(idx), cams.ctypes.data_as(N.u32p),
+                                           ldr.ctypes.data_as(N.f32p), raw.ctypes.data_as(N.f32p))
+        _check(self._lib, self._h, rc, "render_forward")
+        out, off = {}, 0
+        for i in idx:
+            w, h = self._sizes[i]
+            n = w * h * 4
+            out[self._names[i]] = ldr[off:off + n].reshape(h, w, 4).copy()
+            out[self._names[i] + "_raw"] = raw[off:off + n].reshape(h, w, 4).copy()
+            off += n
+        return out
+
+    # ---------------------------------------------------------- backward
+    def render_backward(self, targetRgb32f: Dict[str, np.ndarray]) -> Tuple[dict, dict]:
+        """Adjoint pass with dL/dI images {cam: (H,W,3) float32}; returns
+        (gradients, {"adjoint_source": {...}[, "debug": {...}]})
+        (render_backward, pale_bindings.cpp:279-731)."""
+        idx, imgs = [], []
+        for i, name in enumerate(self._names):
+            if not self._adjoint[i] or name not in targetRgb32f:
+                continue
+            arr = np.asarray(targetRgb32f[name])
+            if arr.ndim != 3 or arr.shape[2] != 3:
+                raise RuntimeError(f"render_backward: target image for camera '{name}' must be HxWx3 float32")
+            if arr.dtype.itemsize != 4:
+                raise RuntimeError(f"render_backward: target image for camera '{name}' must have dtype float32")
+            h, w = arr.shape[0], arr.shape[1]
+            sw, sh = self._sizes[i]
+            if w != sw or h != sh:
+                raise RuntimeError(f"render_backward: resolution mismatch for camera '{name}': target image is "
+                                   f"{w}x{h}, but sensor is {sw}x{sh}")
+            rgb = np.ascontiguousarray(arr).view(np.float32).reshape(h, w, 3)
+            rgba = np.ones((h, w, 4), np.float32)
+            rgba[..., :3] = rgb
+            idx.append(i)
+            imgs.append(rgba)
+        n = self.num_points
+        grads = N.PointsHolder(n=n)
+        pix = sum(im.size for im in imgs)
+        dldi = np.concatenate([im.reshape(-1) for im in imgs]) if imgs else np.zeros(4, np.float32)
+        dbg = np.zeros(max(4, pix), np.float32) if self._settings.debug_images else None
+        cams = N.cams_array(idx)
+        rc = self._lib.pale_render_backward(self._h, len(idx), cams.ctypes.data_as(N.u32p),
+                                            dldi.ctypes.data_as(N.f32p), C.byref(grads.struct),
+                                            dbg.ctypes.data_as(N.f32p) if dbg is not None else None)
+        _check(self._lib, self._h, rc, "render_backward")
+        g = {k: grads.arrays[k].copy() for k in POINT_FIELDS}
+        images = {"adjoint_source": {self._names[i]: im for i, im in zip(idx, imgs)}}
+        if self._settings.debug_images:
+            dbg_out, off = {}, 0
+            for i, im in zip(idx, imgs):
+                k = im.size
+                zero = np.zeros_like(im)
+                op = dbg[off:off + k].reshape(im.shape).copy()
+                dbg_out[self._names[i]] = {"position_x": zero, "position_y": zero.copy(),
+                                           "position_z": zero.copy(), "rotation": zero.copy(),
+                                           "scale": zero.copy(), "albedo": zero.copy(), "opacity": op,
+                                           "beta": zero.copy()}
+                off += k
+            images["debug"] = dbg_out
+        return g, images
+
+    # -------------------------------------------------------- parameters
+    def get_point_parameters(self) -> Dict[str, np.ndarray]:
+        """Surfel parameters in BVH order (pale_bindings.cpp:733-850)."""
+        out = N.PointsHolder(n=self.num_points)
+        _check(self._lib, self._h, self._lib.pale_get_points(self._h, C.byref(out.struct)), "get_point_parameters")
+        return {k: out.arrays[k].copy() for k in POINT_FIELDS}
+
+    def get_point_order(self) -> np.ndarray:
+        """order[bvh_index] = asset index of the last BVH build."""
+        o = np.zeros(max(1, self.num_points), np.uint32)
+        _check(self._lib, self._h, self._lib.pale_get_order(self._h, o.ctypes.data_as(N.u32p)), "get_order")
+        return o[: self.num_points].copy()
+
+    def apply_point_optimization(self, parameters: Dict[str, np.ndarray]):
+        """Writes BVH-ordered parameters without a BVH rebuild and mirrors
+        them into the asset (pale_bindings.cpp:853-1056)."""
+        if "position" not in parameters:
+            return
+        pos = np.asarray(parameters["position"])
+        if pos.ndim != 2 or pos.shape[1] != 3:
+            raise RuntimeError("Expected 'position' to have shape (N,3)")
+        n_in, n = pos.shape[0], self.num_points
+        if n_in == 0:
+            return
+        if n_in != n:
+            raise RuntimeError("apply_point_optimization expects consistent point count; "
+                               "use densification API for adding/removing points.")
+        cur = self.get_point_parameters()
+        for key, width in (("position", 3), ("tangent_u", 3), ("tangent_v", 3), ("scale", 2), ("albedo", 3),
+                           ("opacity", 1), ("beta", 1)):
+            if key not in parameters:
+                raise RuntimeError("New points dictionary does not contain key: " + key)
+            a = np.asarray(parameters[key])
+            shape_ok = (a.ndim == 2 and a.shape == (n, width)) if width > 1 else (a.ndim == 1 and a.shape[0] == n)
+            if not shape_ok:
+                raise RuntimeError(f"Expected '{key}' to have shape (N,{width})" if width > 1
+                                   else f"Expected '{key}' to have shape (N,)")
+            if a.dtype.itemsize != 4:
+                raise RuntimeError(f"Expected '{key}' to be float32")
+            cur[key] = np.ascontiguousarray(a).view(np.float32).reshape(cur[key].shape).copy()
+        hold = N.PointsHolder(cur)
+        _check(self._lib, self._h, self._lib.pale_apply_points(self._h, C.byref(hold.struct)),
+               "apply_point_optimization")
+        for key in ("position", "tangent_u", "tangent_v", "scale", "albedo", "opacity", "beta"):
+            self._asset[key] = cur[key].copy()
+
+    def rebuild_bvh(self):
+        """Rebuilds the surfel LBVH from the asset (pale_bindings.cpp:1058-1079)."""
+        hold = N.PointsHolder(self._asset)
+        _check(self._lib, self._h, self._lib.pale_rebuild(self._h, C.byref(hold.struct)), "rebuild_bvh")
+
+    def remove_points(self, parameters: Dict[str, np.ndarray]):
+        """Removes asset points by index, then rebuilds (:1081-1189)."""
+        if "indices" not in parameters:
+            raise RuntimeError("remove_points: expected key 'indices' (1D int32 / int64 array)")
+        ind = np.asarray(parameters["indices"])
+        if ind.ndim != 1:
+            raise RuntimeError("remove_points: 'indices' must be a 1D array")
+        if ind.shape[0] == 0:
+            return
+        if ind.dtype not in (np.int32, np.int64, np.uint32, np.uint64):
+            raise RuntimeError("remove_points: 'indices' must have dtype int32 or int64")
+        n = self._asset["position"].shape[0]
+        if n == 0:
+            return
+        keep = np.ones(n, bool)
+        for v in ind.tolist():
+            if v < 0:
+                raise IndexError("remove_points: negative index is not allowed")
+            if v >= n:
+                raise IndexError("remove_points: index out of range")
+            keep[v] = False
+        self._asset = {k: v[keep].copy() for k, v in self._asset.items()}
+        self.rebuild_bvh()
+
+    def add_points(self, parameters: Dict[str, dict]):
+        """Appends points given as {"new": {...7 keys}}, then rebuilds
+        (add_new_points, :1191-1395)."""
+        if "new" not in parameters:
+            return
+        new = parameters["new"]
+        for key in ("position", "tangent_u", "tangent_v", "scale", "albedo", "opacity", "beta"):
+            if key not in new:
+                raise RuntimeError(f"add_new_points: missing key 'new.{key}'")
+        pos = np.asarray(new["position"])
+        if pos.ndim != 2 or pos.shape[1] != 3:
+            raise RuntimeError("add_new_points: 'new.position' must have shape (N,3)")
+        if pos.dtype.itemsize != 4:
+            raise RuntimeError("add_new_points: 'new.position' must be float32")
+        m = pos.shape[0]
+        if m == 0:
+            return
+        for key, width in (("tangent_u", 3), ("tangent_v", 3), ("scale", 2), ("albedo", 3)):
+            a = np.asarray(new[key])
+            if a.ndim != 2 or a.shape != (m, width):
+                raise RuntimeError(f"add_new_points: 'new.{key}' must have shape (N,{width})")
+            if a.dtype.itemsize != 4:
+                raise RuntimeError(f"add_new_points: 'new.{key}' must be float32")
+        for key in ("opacity", "beta"):
+            a = np.asarray(new[key])
+            if a.ndim != 1 or a.shape[0] != m:
+                raise RuntimeError("add_new_points: 'new.opacity' must have shape (N,)")
+            if a.dtype.itemsize != 4:
+                raise RuntimeError("add_new_points: 'new.opacity' must be float32")
+        add = as_points({k: np.ascontiguousarray(np.asarray(new[k])).view(np.float32) for k in
+                         ("position", "tangent_u", "tangent_v", "scale", "albedo", "opacity", "beta")})
+        add["shape"] = np.zeros(m, np.float32)
+        self._asset = {k: np.concatenate([self._asset[k], add[k]]) for k in POINT_FIELDS}
+        self.rebuild_bvh()
+
+    def set_point_opacity(self, opacity: float, index: int):
+        n = self._asset["opacity"].shape[0]
+        if index < 0 or index >= n:
+            raise RuntimeError("set_gaussian_opacity: index out of range")
+        self._asset["opacity"][index] = np.float32(opacity)
+        self.rebuild_bvh()
+
+    def set_point_beta(self, beta: float, index: int):
+        n = self._asset["opacity"].shape[0]
+        if index < 0 or index >= n:
+            raise RuntimeError("set_point_beta: index out of range")
+        self._asset["beta"][index] = np.float32(beta)
+        self.rebuild_bvh()
+
+    def set_point_properties(self, translation3, rotation_quat4, scale3, albedo3, opacity: float, beta: float,
+                             index: int = -1):
+        """Perturbs asset points (pale_bindings.cpp:1485-1600).  With
+        index < 0 the reference's loop advances by two, so every second
+        point is perturbed; that behaviour is kept."""
+        if len(translation3) != 3 or len(rotation_quat4) != 4 or len(scale3) != 3:
+            raise RuntimeError("Expected translation(3), rotation_quat(4), scale(3)")
+        t = np.asarray(translation3, np.float32)
+        col = np.asarray(albedo3, np.float32)
+        qx, qy, qz, qw = (np.float32(v) for v in rotation_quat4)
+        sc = np.asarray(scale3[:2], np.float32)
+        A = self._asset
+        n = A["position"].shape[0]
+
+        def rot(v):
+            qv = np.array([qx, qy, qz], np.float32)
+            uv = np.cross(qv, v).astype(np.float32)
+            uuv = np.cross(qv, uv).astype(np.float32)
+            return (v + ((uv * qw) + uuv) * np.float32(2)).astype(np.float32)
+
+        if index < 0:
+            for i in range(0, n, 2):
+                A["position"][i] += t
+                A["tangent_u"][i] = rot(A["tangent_u"][i])
+                A["tangent_v"][i] = rot(A["tangent_v"][i])
+                A["albedo"][i] += col
+                A["opacity"][i] += np.float32(opacity)
+                A["beta"][i] += np.float32(beta)
+                A["scale"][i] *= sc
+        else:
+            if index > n - 1:
+                raise RuntimeError("add_new_points: index out of range")
+            A["position"][index] += t
+            A["tangent_u"][index] = rot(A["tangent_u"][index])
+            A["tangent_v"][index] = rot(A["tangent_v"][index])
+            A["albedo"][index] = col
+            A["opacity"][index] = np.float32(opacity)
+            A["beta"][index] = np.float32(beta)
+            A["scale"][index] = sc
+        self.rebuild_bvh()
+
+    # ------------------------------------------------------- diagnostics
+    def stats(self) -> Dict[str, float]:
+        st = N.PaleStats()
+        _check(self._lib, self._h, self._lib.pale_get_stats(self._h, C.byref(st)), "get_stats")
+        return st.as_dict()
+
+    def trace_rays(self, origins: np.ndarray, directions: np.ndarray):
+        """Closest hits: (instance, primitive, t, alpha_geom, position)."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        inst, prim = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        t, a, p = np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros((n, 3), np.float32)
+        rc = self._lib.pale_trace_rays(self._h, n, o.ctypes.data_as(N.f32p), d.ctypes.data_as(N.f32p),
+                                       inst.ctypes.data_as(N.i32p), prim.ctypes.data_as(N.i32p),
+                                       t.ctypes.data_as(N.f32p), a.ctypes.data_as(N.f32p), p.ctypes.data_as(N.f32p))
+        _check(self._lib, self._h, rc, "trace_rays")
+        return inst, prim, t, a, p
+
+    def gather_irradiance(self, points: np.ndarray, normals: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        nm = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        E = np.zeros_like(x)
+        rc = self._lib.pale_gather_irradiance(self._h, x.shape[0], x.ctypes.data_as(N.f32p),
+                                              nm.ctypes.data_as(N.f32p), E.ctypes.data_as(N.f32p))
+        _check(self._lib, self._h, rc, "gather_irradiance")
+        return E
+
+    def load_photons(self, position, power, direction):
+        p = np.ascontiguousarray(position, np.float32).reshape(-1, 3)
+        w = np.ascontiguousarray(power, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(direction, np.float32).reshape(-1, 3)
+        rc = self._lib.pale_load_photons(self._h, p.shape[0], p.ctypes.data_as(N.f32p), w.ctypes.data_as(N.f32p),
+                                         d.ctypes.data_as(N.f32p))
+        _check(self._lib, self._h, rc, "load_photons")
+
+    def get_photons(self):
+        cnt = C.c_uint32()
+        _check(self._lib, self._h, self._lib.pale_get_photons(self._h, C.byref(cnt), None, None, None, None,
+                                                              None, None), "get_photons")
+        n = int(cnt.value)
+        pos, pw, dr = (np.zeros((max(1, n), 3), np.float32) for _ in range(3))
+        cid, srt = np.zeros(max(1, n), np.uint32), np.zeros(max(1, n), np.uint32)
+        gi = np.zeros(7, np.float32)
+        rc = self._lib.pale_get_photons(self._h, C.byref(cnt), pos.ctypes.data_as(N.f32p), pw.ctypes.data_as(N.f32p),
+                                        dr.ctypes.data_as(N.f32p), cid.ctypes.data_as(N.u32p),
+                                        srt.ctypes.data_as(N.u32p), gi.ctypes.data_as(N.f32p))
+        _check(self._lib, self._h, rc, "get_photons")
+        return dict(position=pos[:n], power=pw[:n], direction=dr[:n], cell_id=cid[:n], sorted=srt[:n], grid=gi)
+
+    def get_bvh(self):
+        n = self.num_points
+        cnt = C.c_uint32()
+        _check(self._lib, self._h, self._lib.pale_get_bvh(self._h, None, C.byref(cnt), None, 0), "get_bvh")
+        codes = np.zeros(max(1, n), np.uint32)
+        nodes = np.zeros((max(1, cnt.value), 16), np.float32)
+        rc = self._lib.pale_get_bvh(self._h, codes.ctypes.data_as(N.u32p), C.byref(cnt),
+                                    nodes.ctypes.data_as(N.f32p), cnt.value)
+        _check(self._lib, self._h, rc, "get_bvh")
+        return codes[:n], nodes[: cnt.value]

@@ -1,0 +1,243 @@
+/*
+ * pale_b200.h -- C-ABI of the B200-native adjoint renderer for beta surfels.
+ *
+ * This is the drop-in boundary for Pale's `pale.Renderer` pybind11 module
+ * (Pale/pale_bindings.cpp:1613-1650).  Every entry point takes plain pointers
+ * and sizes; no C++ or torch types cross it and no exception escapes it.
+ *
+ * Return codes: 0 = ok, >0 = recoverable (capacity exceeded, iteration cap
+ * hit inside a kernel), <0 = fatal (bad argument, CUDA error).  After a
+ * non-zero return, pale_last_error() describes the failure.
+ *
+ * Orders of surfels: the "asset order" is the order the caller supplies
+ * points in (PLY file order); the "BVH order" is the leaf order of the
+ * device LBVH.  As in the reference (SceneBuild.cpp:710-731,
+ * pale_bindings.cpp:734-757) every per-point array that comes back
+ * (parameters, gradients) is in BVH order; pale_get_order() gives the map
+ * order[bvh_index] = asset_index.
+ */
+#ifndef PALE_B200_H
+#define PALE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PALE_OK 0
+#define PALE_ERR_CAPACITY 1      /* a queue or photon store overflowed       */
+#define PALE_ERR_DEVICE_FLAG 2   /* a kernel bounds check or loop cap fired  */
+#define PALE_ERR_ARGUMENT (-1)
+#define PALE_ERR_CUDA (-2)
+#define PALE_ERR_STATE (-3)
+
+#define PALE_RNG_REFERENCE 0     /* reproduce the reference's seeding        */
+#define PALE_RNG_DECORRELATED 1  /* fresh seed per gather pass / adjoint spp */
+
+typedef struct pale_handle pale_handle;
+
+/* Renderer settings.  Field <- settings-dict key of the reference
+ * (pale_bindings.cpp:123-139; PathTracerSettings, GPUDataStructures.h:407-422).
+ * Fill with pale_default_settings() first. */
+typedef struct pale_settings {
+    uint32_t photons_per_launch;   /* "photons"          (default 1e6)       */
+    uint32_t max_bounces;          /* "bounces"          (6)                 */
+    uint32_t forward_passes;       /* "forward_passes"   (6)                 */
+    uint32_t gather_passes;        /* "gather_passes"    (6)                 */
+    uint32_t adjoint_bounces;      /* "adjoint_bounces"  (6)                 */
+    uint32_t adjoint_passes;       /* "adjoint_passes"   (6)                 */
+    uint64_t seed;                 /* "seed"             (42)                */
+    uint32_t random_number;        /* Random::number     (42) -- adjoint base */
+    uint32_t rr_start;             /* russianRouletteStart (6)               */
+    float q_null;                  /* AdjointSampleSettings (0.5/0.5/0)      */
+    float q_reflect;
+    float q_transmit;
+    float gather_radius;           /* PathTracer.cpp:187 hard-codes 0.01     */
+    uint32_t leaf_size;            /* BuildOptions leaf size (4)             */
+    uint32_t rng_mode;             /* PALE_RNG_*                             */
+    uint32_t debug_images;         /* "debug_images"                         */
+    float exposure;                /* SensorGPU::exposureCorrection (1.0)    */
+    float gamma;                   /* SensorGPU::gammaCorrection   (2.2)     */
+} pale_settings;
+
+/* Per-point parameter block (structure of arrays, float32).
+ * position/tangent_u/tangent_v/albedo: count*3, scale: count*2,
+ * opacity/beta/shape: count.  For outputs, every pointer may be NULL to
+ * skip that field. */
+typedef struct pale_points {
+    uint32_t count;
+    float *position;
+    float *tangent_u;
+    float *tangent_v;
+    float *scale;
+    float *albedo;
+    float *opacity;
+    float *beta;
+    float *shape;
+} pale_points;
+
+/* Scene description: triangle meshes, instances, materials, cameras and the
+ * surfel cloud in asset order.  All matrices are 4x4 row-major float32 with
+ * y = M x.  Mirrors the host data SceneBuild::build collects
+ * (SceneBuild.cpp:72-392). */
+typedef struct pale_scene_desc {
+    uint32_t num_vertices;
+    const float *vertices;          /* num_vertices*3, object space          */
+    uint32_t num_triangles;
+    const uint32_t *triangles;      /* num_triangles*3 vertex indices        */
+    uint32_t num_meshes;
+    const uint32_t *mesh_ranges;    /* num_meshes*2: first triangle, count   */
+    uint32_t num_materials;
+    const float *materials;         /* num_materials*4: base colour rgb, power */
+    uint32_t num_instances;         /* mesh instances (the surfel cloud is one
+                                       implicit extra instance after them)   */
+    const uint32_t *instance_mesh;
+    const uint32_t *instance_material;
+    const float *instance_object_to_world;  /* num_instances*16             */
+    const float *instance_world_to_object;  /* num_instances*16             */
+    uint32_t num_cameras;
+    const float *camera_inv_view;   /* num_cameras*16, camera -> world       */
+    const float *camera_forward;    /* num_cameras*3                         */
+    const float *camera_fovy_deg;   /* num_cameras                           */
+    const uint32_t *camera_size;    /* num_cameras*2: width, height          */
+    const char *camera_names;       /* num_cameras*16, NUL padded            */
+    pale_points points;             /* asset-order surfels                   */
+} pale_scene_desc;
+
+/* Device-side counters of the last render call (for throughput metrics). */
+typedef struct pale_stats {
+    uint64_t photon_segments;       /* photon rays submitted to traversal    */
+    uint64_t gather_segments;       /* camera-gather layer traversals        */
+    uint64_t adjoint_segments;      /* adjoint rays submitted to traversal   */
+    uint64_t photons_stored;        /* photons deposited in the map          */
+    uint64_t gradient_events;       /* completed adjoint gradient events     */
+    uint64_t gather_queries;        /* photon-map irradiance lookups         */
+    uint64_t node_visits;           /* BVH nodes visited (instrumented only) */
+    uint64_t surfel_tests;          /* ray/surfel tests (instrumented only)  */
+    uint64_t photons_scanned;       /* photons scanned by lookups (instr.)   */
+    float forward_ms;               /* device time of the last forward pass  */
+    float backward_ms;              /* device time of the last adjoint pass  */
+    float photon_ms;                /* photon trace + grid build part        */
+    float gather_ms;                /* camera gather part                    */
+} pale_stats;
+
+/* Fills *s with the reference's PathTracerSettings defaults. */
+void pale_default_settings(pale_settings *s);
+
+/* Library version string. */
+const char *pale_version(void);
+
+/* Error text of the last failing call on this handle; with handle == NULL
+ * the last failure of pale_create on this thread. */
+const char *pale_last_error(const pale_handle *h);
+
+/* Creates a renderer on the current CUDA device: uploads meshes and cameras,
+ * builds the surfel LBVH on the device, sizes the ray queues and configures
+ * the photon grid from the scene bounds.  Replaces the constructor
+ * PythonRenderer::PythonRenderer (pale_bindings.cpp:61-170) together with
+ * PathTracer::setScene (PathTracer.cpp:22-53). */
+int pale_create(const pale_scene_desc *desc, const pale_settings *settings,
+                pale_handle **out);
+
+/* Frees every device buffer of the handle.  (pale_bindings.cpp:172-177) */
+int pale_destroy(pale_handle *h);
+
+/* Number of surfels and cameras. */
+int pale_point_count(const pale_handle *h, uint32_t *count);
+int pale_camera_count(const pale_handle *h, uint32_t *count);
+/* Camera name (16 bytes incl. NUL) and size.  (getCameraNames,
+ * pale_bindings.cpp:1397-1403) */
+int pale_camera_info(const pale_handle *h, uint32_t index, char name[16],
+                     uint32_t *width, uint32_t *height);
+
+/* Forward photon-mapped render of the selected cameras
+ * (render_forward, pale_bindings.cpp:180-277; submitPhotonMappingKernel,
+ * SyclBridge.cpp:82-166).  ldr_out / raw_out receive, per selected camera in
+ * order, H*W*4 floats (row 0 = top).  Either may be NULL.  Host pointers. */
+int pale_render_forward(pale_handle *h, uint32_t num_selected,
+                        const uint32_t *camera_indices, float *ldr_out,
+                        float *raw_out);
+
+/* Same render, but the LDR/RAW images are written to DEVICE pointers
+ * (no host copies).  `stream` is a cudaStream_t or NULL. */
+int pale_render_forward_device(pale_handle *h, uint32_t num_selected,
+                               const uint32_t *camera_indices, float *d_ldr,
+                               float *d_raw, void *stream);
+
+/* Adjoint pass (render_backward, pale_bindings.cpp:279-731;
+ * submitAdjointKernel, SyclBridge.cpp:169-294).  dldi holds, per selected
+ * camera in order, H*W*4 floats of dL/dI (alpha ignored).  Gradients are
+ * written in BVH order into *grads (fields may be NULL).  debug_opacity,
+ * when not NULL, receives per camera H*W*4 floats of the opacity-gradient
+ * debug image (DebugImages::framebufferOpacity).  Host pointers. */
+int pale_render_backward(pale_handle *h, uint32_t num_selected,
+                         const uint32_t *camera_indices, const float *dldi,
+                         pale_points *grads, float *debug_opacity);
+
+/* Same adjoint pass with DEVICE pointers for dL/dI and the gradient fields. */
+int pale_render_backward_device(pale_handle *h, uint32_t num_selected,
+                                const uint32_t *camera_indices,
+                                const float *d_dldi, pale_points *d_grads,
+                                void *stream);
+
+/* Current per-point parameters in BVH order (get_point_parameters,
+ * pale_bindings.cpp:733-850). */
+int pale_get_points(pale_handle *h, pale_points *out);
+
+/* order[bvh_index] = asset_index of the last build. */
+int pale_get_order(pale_handle *h, uint32_t *order);
+
+/* Overwrites the BVH-ordered surfel parameters WITHOUT rebuilding the BVH
+ * (apply_point_optimization, pale_bindings.cpp:853-1056: the BVH nodes stay
+ * as they were).  params->count must equal the current count. */
+int pale_apply_points(pale_handle *h, const pale_points *params);
+
+/* Rebuilds the LBVH from an asset-order point set of any size (rebuild_bvh,
+ * pale_bindings.cpp:1058-1079; also behind add_points / remove_points /
+ * set_point_* which edit the asset and rebuild). */
+int pale_rebuild(pale_handle *h, const pale_points *asset_points);
+
+/* Closest-hit queries against the scene (intersectScene in FirstHit mode,
+ * IntersectionKernels.h:954-1097).  Host arrays of n rays; outputs:
+ * instance (-1 = miss), primitive (surfel in BVH order or triangle id),
+ * world t, alpha_geom, hit position (n*3). */
+int pale_trace_rays(pale_handle *h, uint32_t n, const float *origins,
+                    const float *directions, int32_t *instance,
+                    int32_t *primitive, float *t, float *alpha_geom,
+                    float *hit_position);
+
+/* Irradiance lookups in the current photon map
+ * (gatherDiffuseIrradianceAtPoint, KernelHelpers.h:990-1037). */
+int pale_gather_irradiance(pale_handle *h, uint32_t n, const float *points,
+                           const float *normals, float *irradiance);
+
+/* Replaces the photon map by caller photons (n records: position 3,
+ * power 3, incoming direction 3) and rebuilds the grid.  Used to check the
+ * grid build and lookups on identical inputs. */
+int pale_load_photons(pale_handle *h, uint32_t n, const float *position,
+                      const float *power, const float *direction);
+
+/* Copies the photon map out: count, and (each may be NULL) the photons in
+ * deposit order, the per-photon cell ids in deposit order, and the sorted
+ * order (sorted[i] = deposit index) plus the grid geometry
+ * (origin xyz, cell size, resolution xyz as floats). */
+int pale_get_photons(pale_handle *h, uint32_t *count, float *position,
+                     float *power, float *direction, uint32_t *cell_id,
+                     uint32_t *sorted, float *grid_info);
+
+/* Exports the LBVH: Morton codes and sorted order of the last build
+ * (codes[i] / order[i] for sorted position i), the node count, and the
+ * traversal nodes (each 16 words: child0 box lo/hi, child1 box lo/hi,
+ * child words).  Any pointer may be NULL. */
+int pale_get_bvh(pale_handle *h, uint32_t *codes, uint32_t *node_count,
+                 float *nodes, uint32_t max_nodes);
+
+/* Counters of the last render. */
+int pale_get_stats(pale_handle *h, pale_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PALE_B200_H */
