@@ -245,15 +245,31 @@ void build_surfels(pale_handle* h, const pale_points* asset) {
   A.lc = h->lc.p; A.rc = h->rc.p; A.rfirst = h->rfirst.p; A.rlast = h->rlast.p; A.parent = h->parent.p;
   A.leaf_parent = h->leaf_parent.p; A.visits = h->visits.p; A.box = h->box.p;
   A.nodes = h->nodes.p;
+  A.err = &h->run.p->error;
+  CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   lbvh_build(A, s);
   CK(cudaGetLastError());
   float b[12];
+  uint32_t err = 0;
   CK(cudaMemcpyAsync(b, h->bounds.p, sizeof(b), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&err, &h->run.p->error, 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  if (err) throw std::runtime_error("LBVH build failed a consistency check (device error flags " +
+                                    std::to_string(err) + ")");
   for (int k = 0; k < 3; ++k) {
     h->pc_lo[k] = b[6 + k];
     h->pc_hi[k] = b[9 + k];
   }
+}
+
+// Photon store (deposit order) and the sorted copy of the grid.
+void alloc_photon_store(pale_handle* h, uint64_t cap) {
+  h->photon_cap = cap;
+  const size_t pc = (size_t)cap;
+  h->ph_a.alloc(pc); h->ph_b.alloc(pc); h->ph_c.alloc(pc);
+  h->g_pa.alloc(pc); h->g_pb.alloc(pc); h->g_pc.alloc(pc);
+  h->g_cell_id.alloc(pc); h->g_sorted.alloc(pc); h->g_keys.alloc(2 * pc); h->g_vals_tmp.alloc(pc);
+  h->g_sort_temp.alloc(radix_temp_words((uint32_t)pc));
 }
 
 // Host restatement of toWorldPoint with the device's operation order.
@@ -261,6 +277,8 @@ V3 host_xform_point(const float* M, V3 p) { return xform_point(M, p); }
 
 void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   cudaStream_t s = h->stream;
+  h->run.alloc(1);
+  CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   // ---- meshes: per instance transforms, world boxes, triangles
   h->n_inst = d->num_instances;
   h->n_tris = d->num_triangles;
@@ -438,12 +456,7 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   const pale_settings& st = h->st;
   uint64_t req = (uint64_t)st.photons_per_launch * st.forward_passes * st.max_bounces;
   uint64_t mx = (10ull << 30) / 64ull;
-  h->photon_cap = std::max<uint64_t>(1, std::min(req, mx));
-  const size_t pc = (size_t)h->photon_cap;
-  h->ph_a.alloc(pc); h->ph_b.alloc(pc); h->ph_c.alloc(pc);
-  h->g_pa.alloc(pc); h->g_pb.alloc(pc); h->g_pc.alloc(pc);
-  h->g_cell_id.alloc(pc); h->g_sorted.alloc(pc); h->g_keys.alloc(2 * pc); h->g_vals_tmp.alloc(pc);
-  h->g_sort_temp.alloc(radix_temp_words((uint32_t)pc));
+  alloc_photon_store(h, std::max<uint64_t>(1, std::min(req, mx)));
   h->g_cell_count.alloc((size_t)h->cells + 1);
   h->g_cell_off.alloc((size_t)h->cells + 1);
   h->g_scan_temp.alloc(scan_temp_words(h->cells + 1));
@@ -461,7 +474,6 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
   h->pend_a.alloc(qc); h->pend_b.alloc(qc); h->pend_c.alloc(qc);
   h->ev_stage.alloc(qc); h->ev_list.alloc(qc);
-  h->run.alloc(1);
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   CK(cudaStreamSynchronize(s));
 }
@@ -961,8 +973,12 @@ int pale_load_photons(pale_handle* h, uint32_t n, const float* pos, const float*
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
     if (n && (!pos || !pw || !dir)) throw ArgError("pale_load_photons: null array");
-    if (n > h->photon_cap) throw ArgError("more photons than the photon store holds");
     cudaStream_t s = h->stream;
+    if (n > (1u << 30)) throw ArgError("at most 2^30 photons can be loaded");
+    if (n > h->photon_cap) {
+      CK(cudaStreamSynchronize(s));
+      alloc_photon_store(h, n);
+    }
     DBuf<float> dP, dW, dD;
     dP.alloc(3ull * n); dW.alloc(3ull * n); dD.alloc(3ull * n);
     if (n) {

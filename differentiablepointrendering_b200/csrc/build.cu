@@ -62,23 +62,26 @@ __global__ void k_scan_reduce(const uint32_t* __restrict__ in, uint32_t n, uint3
 }
 
 // Single block: exclusive scan of up to 1024*32 partial sums.
-__global__ void k_scan_partials(uint32_t* __restrict__ partial, uint32_t nb, uint32_t* __restrict__ total_out) {
+__global__ void __launch_bounds__(1024) k_scan_partials(uint32_t* __restrict__ partial, uint32_t nb,
+                                                        uint32_t* __restrict__ total_out) {
   __shared__ uint32_t s_warp[32];
   const int items = 32;
-  uint32_t v[items];
   uint32_t sum = 0;
   const uint32_t base = threadIdx.x * items;
   for (int k = 0; k < items; ++k) {
     uint32_t i = base + k;
-    v[k] = i < nb ? partial[i] : 0u;
-    sum += v[k];
+    sum += i < nb ? partial[i] : 0u;
   }
   uint32_t total;
   uint32_t run = block_exclusive_sum(sum, s_warp, total);
+  // each thread rewrites only its own consecutive range
   for (int k = 0; k < items; ++k) {
     uint32_t i = base + k;
-    if (i < nb) partial[i] = run;
-    run += v[k];
+    if (i < nb) {
+      uint32_t v = partial[i];
+      partial[i] = run;
+      run += v;
+    }
   }
   if (threadIdx.x == 0 && total_out) *total_out = total;
 }
@@ -329,27 +332,37 @@ __device__ __forceinline__ int delta_key(const uint32_t* __restrict__ codes, uin
 // < 0 leaf -(k+1).
 __global__ void k_karras(const uint32_t* __restrict__ codes, uint32_t n, int32_t* __restrict__ lc,
                          int32_t* __restrict__ rc, uint32_t* __restrict__ rfirst, uint32_t* __restrict__ rlast,
-                         uint32_t* __restrict__ parent, uint32_t* __restrict__ leaf_parent) {
+                         uint32_t* __restrict__ parent, uint32_t* __restrict__ leaf_parent, uint32_t* err) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (int64_t)n - 1) return;
   int d = (delta_key(codes, n, i, i + 1) - delta_key(codes, n, i, i - 1)) >= 0 ? 1 : -1;
   int dmin = delta_key(codes, n, i, i - d);
   int64_t lmax = 2;
-  while (delta_key(codes, n, i, i + lmax * d) > dmin) lmax *= 2;
+  for (int it = 0; it < 40 && delta_key(codes, n, i, i + lmax * d) > dmin; ++it) lmax *= 2;
   int64_t l = 0;
   for (int64_t t = lmax / 2; t >= 1; t /= 2)
     if (delta_key(codes, n, i, i + (l + t) * d) > dmin) l += t;
+  // sorted, distinct keys give l >= 1; anything else is a sort failure
+  if (l < 1 || i + l * d < 0 || i + l * d >= (int64_t)n) {
+    atomicOr(err, kErrBounds);
+    l = 1;
+    d = (i + 1 < (int64_t)n) ? 1 : -1;
+  }
   int64_t j = i + l * d;
   int dnode = delta_key(codes, n, i, j);
   int64_t s = 0, div = 2, t = (l + div - 1) / div;
-  while (true) {
+  for (int it = 0; it < 64; ++it) {
     if (delta_key(codes, n, i, i + (s + t) * d) > dnode) s += t;
-    if (t == 1) break;
+    if (t <= 1) break;
     div *= 2;
     t = (l + div - 1) / div;
   }
   int64_t gamma = i + s * d + (d < 0 ? d : 0);
   int64_t mn = i < j ? i : j, mx = i < j ? j : i;
+  if (gamma < mn || gamma >= mx) {
+    atomicOr(err, kErrBounds);
+    gamma = mn;
+  }
   int32_t L = (mn == gamma) ? -(int32_t)(gamma + 1) : (int32_t)gamma;
   int32_t R = (mx == gamma + 1) ? -(int32_t)(gamma + 2) : (int32_t)(gamma + 1);
   lc[i] = L;
@@ -573,7 +586,7 @@ void lbvh_build(const LbvhArgs& A, cudaStream_t s) {
     k_small_root<<<1, 32, 0, s>>>(A.order, n, A.lo, A.hi, A.nodes);
   } else {
     k_karras<<<blocks_for(n - 1), kBlock, 0, s>>>(A.codes, n, A.lc, A.rc, A.rfirst, A.rlast, A.parent,
-                                                  A.leaf_parent);
+                                                  A.leaf_parent, A.err);
     cudaMemsetAsync(A.visits, 0, (size_t)(n - 1) * 4, s);
     k_refit<<<blocks_for(n), kBlock, 0, s>>>(A.order, n, A.lo, A.hi, A.lc, A.rc, A.parent, A.leaf_parent, A.visits,
                                              A.box);

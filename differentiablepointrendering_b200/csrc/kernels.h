@@ -39,6 +39,7 @@ struct LbvhArgs {
   uint32_t *rfirst, *rlast, *parent, *leaf_parent, *visits;
   float* box;
   BvhNode* nodes;
+  uint32_t* err;            // device error word
 };
 
 size_t scan_temp_words(uint32_t n);

@@ -37,7 +37,7 @@ __device__ __forceinline__ RayRec make_ray(V3 o, V3 d, V3 thr, uint32_t path, ui
 // ---------------------------------------------------------- compaction
 // One block: exclusive scan of the per-tile (alive, deposit/event) counts
 // of `n_in` slots; updates queue length, deposit/event bases and seeds.
-__global__ void k_queue_scan(RunState* st, const uint2* __restrict__ counts, uint2* __restrict__ offsets,
+__global__ void __launch_bounds__(1024) k_queue_scan(RunState* st, const uint2* __restrict__ counts, uint2* __restrict__ offsets,
                              uint32_t parity, int emission, uint32_t emission_n, int events, uint64_t photon_cap) {
   __shared__ uint32_t s_wx[32], s_wy[32];
   __shared__ uint32_t s_carry[2];

@@ -114,10 +114,12 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode
   float stack_t[kStackDepth];
   int sp = 0;
   uint32_t node = 0;
-  while (true) {
+  // an acyclic tree visits each node at most once
+  const uint32_t visit_cap = 2u * S.node_count + 64u;
+  for (uint32_t visit = 0;; ++visit) {
     float4 a, b, c;
     uint4 w;
-    if (node >= S.node_count) {
+    if (node >= S.node_count || visit > visit_cap) {
       flag_error(st, kErrBounds);
       break;
     }
@@ -396,6 +398,9 @@ __device__ __forceinline__ V3 gather_irradiance(const GridView& G, V3 x, V3 n, u
       uint32_t row = (uint32_t)((cz * G.res[1] + cy) * G.res[0]);
       uint32_t j0 = __ldg(&G.cell_off[row + c0[0]]);
       uint32_t j1 = __ldg(&G.cell_off[row + c1[0] + 1]);
+      const uint32_t total = __ldg(&G.cell_off[G.cells]);
+      j1 = j1 < total ? j1 : total;
+      j0 = j0 < j1 ? j0 : j1;
       sc += j1 - j0;
       for (uint32_t j = j0; j < j1; ++j) {
         float4 pa = __ldg(&G.pa[j]);
