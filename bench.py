@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Forward + adjoint throughput of the beta-surfel renderer on one node.
+
+Workload "box200k" (default): the synthetic box scene with 200k surfels,
+8 cameras on a ring of radius 1.5 at 512x512, 16 gather passes and 16
+adjoint passes per pixel, depth 6 (photon and adjoint bounces), 1M photons,
+gather radius 0.01.  One step = photon pass + photon grid + camera gather of
+all views, dL/dI of the L2 image loss against a target render (positions
+jittered N(0, 0.005), albedo N(0, 0.05)), adjoint pass of all views with
+gradient accumulation, and (N > 1) a sum all-reduce of the gradients.
+
+Metric: Mrays/s = ray segments submitted to scene traversal (photon bounces
++ camera-gather layers + adjoint bounces) per second of the step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # the 200k-surfel, 8-view workload (throughput headline)
+    "box200k": dict(n=200000, cams=8, res=512, photons=1000000, bounces=6, forward_passes=1, spp=16,
+                    adjoint_bounces=6, adjoint_spp=16, radius=0.01),
+    # the 10k-surfel, single-view workload
+    "box10k": dict(n=10000, cams=1, res=256, photons=100000, bounces=4, forward_passes=1, spp=4,
+                   adjoint_bounces=4, adjoint_spp=4, radius=0.02),
+}
+
+METRIC = "fwd+adjoint Mrays/s"
+
+
+def settings_for(w: dict) -> dict:
+    return {"photons": w["photons"], "bounces": w["bounces"], "forward_passes": w["forward_passes"],
+            "gather_passes": w["spp"], "adjoint_bounces": w["adjoint_bounces"], "adjoint_passes": w["adjoint_spp"],
+            "gather_radius": w["radius"], "seed": 42, "rng_mode": "decorrelated"}
+
+
+def sample_settings(w: dict) -> dict:
+    """Bounded CPU sample of a workload: same scene, photon count / 4,
+    one camera at half resolution, one gather and one adjoint pass."""
+    s = settings_for(w)
+    s.update(photons=max(1000, w["photons"] // 4), gather_passes=1, adjoint_passes=1)
+    return s
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- helpers
+def algorithmic_bytes_gather(st: dict) -> float:
+    """Algorithmic bytes of one camera-gather launch: per ray segment 64 B of
+    ray state + 16 B hit record, 32 B per BVH node visited, 52 B per
+    surfel test; per photon scanned 36 B and per photon-map query 8 B per
+    grid row range read (two offsets)."""
+    return (80.0 * st["gather_segments"] + 32.0 * st["gather_node_visits"] + 52.0 * st["gather_surfel_tests"]
+            + 36.0 * st["gather_photons_scanned"] + 8.0 * 25.0 * st["gather_queries_fwd"])
+
+
+def read_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def read_traffic(kernel: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(p)).get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_sample_run(w: dict, steps: int = 1):
+    """The CPU oracle (the reference's algorithm restated in C, all host
+    threads) on a bounded sample of the workload; returns (Mrays/s, secs,
+    description)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import OracleRenderer
+    from differentiablepointrendering_b200.scene import make_box_scene, jitter_target, make_surfels
+    import numpy as np
+
+    res = max(32, w["res"] // 2)
+    pts = make_surfels(w["n"], 1234)
+    scene = make_box_scene(w["n"], cameras=1, resolution=res, points=pts)
+    st = sample_settings(w)
+    o = OracleRenderer(scene, st)
+    tgt = np.zeros((res, res, 3), np.float32)
+    total_rays, total_t = 0, 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        img = o.render_forward()
+        s1 = o.stats()
+        raw = img["camera0"][..., :3]
+        o.render_backward({"camera0": ((raw - tgt) / raw.size).astype(np.float32)})
+        s2 = o.stats()
+        total_t += time.perf_counter() - t0
+        total_rays += s1["photon_segments"] + s1["gather_segments"] + s2["adjoint_segments"]
+    o.close()
+    desc = (f"CPU oracle, same {w['n']}-surfel scene, 1 camera at {res}x{res}, {st['photons']} photons, "
+            f"1 gather + 1 adjoint pass, depth {w['bounces']}/{w['adjoint_bounces']}")
+    return total_rays / total_t / 1e6, total_t, desc
+
+
+# -------------------------------------------------------------- reference
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    cores = os.cpu_count()
+    value, secs, desc = cpu_sample_run(w, steps=max(1, args.steps))
+    line = {"metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, **w},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference needs AdaptiveCpp SYCL, absent here; its algorithm runs as the C oracle port"}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- ours
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from differentiablepointrendering_b200.build import build_library
+    from differentiablepointrendering_b200.device import DeviceFrame, l2_grad_
+    from differentiablepointrendering_b200.pale import Renderer
+    from differentiablepointrendering_b200.scene import jitter_target, make_box_scene, make_surfels
+
+    build_library()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device(f"cuda:{local_rank}")
+    w = WORKLOADS[args.workload]
+    st = settings_for(w)
+    pts = make_surfels(w["n"], 1234)
+    offset = rank / max(1, world)          # rank r renders views rotated by r/N of the spacing
+    scene = make_box_scene(w["n"], cameras=w["cams"], resolution=w["res"], points=pts, ring_offset=offset)
+    tscene = scene.with_points(jitter_target(pts, 5678))
+
+    # target images (renders of the jittered cloud), resident on the device
+    tr = Renderer.from_scene(tscene, st)
+    tf = DeviceFrame(tr, device=dev)
+    tf.forward()
+    target = tf.ldr[:, :3].clone()
+    torch.cuda.synchronize()
+    del tf
+    tr.close()
+
+    r = Renderer.from_scene(scene, st)
+    frame = DeviceFrame(r, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        frame.forward()
+        l2_grad_(frame.dldi, frame.ldr, target)
+        frame.backward()
+        if world > 1:
+            for g in frame.grads.values():
+                dist.all_reduce(g)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # work per step (fixed seeds: every step traces the same rays)
+    frame.forward()
+    sf = frame.stats()
+    l2_grad_(frame.dldi, frame.ldr, target)
+    frame.backward()
+    sb = frame.stats()
+    rays = sf["photon_segments"] + sf["gather_segments"] + sb["adjoint_segments"]
+    launches = int(sf["kernel_launches"] + sb["kernel_launches"])
+    gather_ms = sf["gather_ms"]
+    gstats = dict(sf)
+    gstats["gather_queries_fwd"] = sf["gather_queries"]
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        step()
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    total_rays = torch.tensor([float(rays)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(total_rays)
+    ms_per_step = ms / args.steps
+    value = float(total_rays.item()) / (ms_per_step / 1e3) / 1e6
+
+    # ---- end to end through the public API with host buffers
+    cams = r.get_camera_names()
+    tgt_np = {}
+    for i, name in enumerate(cams):
+        ww, hh = frame.sizes[i]
+        off = sum(a * b for a, b in frame.sizes[:i])
+        tgt_np[name] = target[off:off + ww * hh].view(hh, ww, 3).cpu().numpy()
+    e2e_steps = max(1, min(args.steps, 3))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        imgs = r.render_forward()
+        dl = {n: ((imgs[n][..., :3] - tgt_np[n]) / tgt_np[n].size).astype(np.float32) for n in cams}
+        grads, _ = r.render_backward(dl)
+        if world > 1:
+            for k2, v in grads.items():
+                gt = torch.from_numpy(v).to(dev)
+                dist.all_reduce(gt)
+                grads[k2] = gt.cpu().numpy()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    et = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = float(total_rays.item()) * e2e_steps / float(et.item()) / 1e6
+    pix = frame.pixels
+    h2d = pix * 16
+    d2h = 2 * pix * 16 + r.num_points * 17 * 4
+
+    if rank != 0:
+        r.close()
+        return
+    peaks = read_peaks()
+    hbm = peaks["hbm_gbs"] if peaks else 6650.0
+    ab = algorithmic_bytes_gather(gstats)
+    achieved = ab / (gather_ms / 1e3) / 1e9
+    traffic = read_traffic("k_camera_gather")
+    cpu_val, cpu_secs, cpu_desc = cpu_sample_run(w, steps=1) if not args.skip_cpu else (None, 0, "skipped")
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, **w, "iters_per_s": round(1e3 / ms_per_step, 4),
+                   "rays_per_step_per_gpu": int(rays), "l2": "256 MB buffer zeroed between timed steps",
+                   "parallelism": f"views sharded over {world} GPU(s), gradients all-reduced"},
+        "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+        "gpu_launches": launches * args.steps,
+        "roofline": {"kernel": "k_camera_gather", "bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                     "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
+                     "algorithmic_bytes_per_launch": int(ab), "launch_ms": round(gather_ms, 3)},
+        "cpu_baseline": {"value": round(cpu_val, 4) if cpu_val else None, "unit": "Mrays/s",
+                         "cores": os.cpu_count(), "kind": "port", "sample": cpu_desc},
+        "clocks": clk,
+        "breakdown_ms": {"photon": round(sf["photon_ms"], 3), "gather": round(sf["gather_ms"], 3),
+                         "adjoint": round(sb["backward_ms"], 3)},
+    }
+    print(json.dumps(line), flush=True)
+    r.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--workload", default="box200k", choices=sorted(WORKLOADS))
+    ap.add_argument("--skip-cpu", dest="skip_cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

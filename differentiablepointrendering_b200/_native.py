@@ -50,7 +50,8 @@ class PaleSceneDesc(C.Structure):
 class PaleStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in (
         "photon_segments", "gather_segments", "adjoint_segments", "photons_stored", "gradient_events",
-        "gather_queries", "node_visits", "surfel_tests", "photons_scanned")] + \
+        "gather_queries", "node_visits", "surfel_tests", "photons_scanned", "gather_node_visits",
+        "gather_surfel_tests", "gather_photons_scanned", "kernel_launches")] + \
         [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms")]
 
     def as_dict(self) -> Dict[str, float]:

@@ -19,6 +19,12 @@
 
 using namespace pale;
 
+namespace pale {
+static thread_local uint64_t g_launches = 0;
+void note_launch() { ++g_launches; }
+uint64_t launches_issued() { return g_launches; }
+}  // namespace pale
+
 namespace {
 
 thread_local std::string g_create_error;
@@ -133,13 +139,17 @@ struct pale_handle {
   DBuf<float> img_raw, img_ldr, dldi, dbg;
   PointsBufs grads;
   pale_stats stats{};
+  uint64_t launches_last = 0;  // kernels launched by the last render call
+  int stats_pending = 0;   // a render ran without reading its run state yet
+  int timed = 0;           // 1 forward events, 2 adjoint events pending
+  cudaStream_t own_stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 
   ~pale_handle() {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (ev2) cudaEventDestroy(ev2);
-    if (stream) cudaStreamDestroy(stream);
+    if (own_stream) cudaStreamDestroy(own_stream);
   }
 
   SceneView view() const {
@@ -504,10 +514,27 @@ int guarded(pale_handle* h, F&& f) {
   }
 }
 
+// Reads the run state of the last render (synchronising its stream) into
+// h->stats, with the device times of the recorded events; throws when a
+// kernel raised an error flag.
 void copy_stats(pale_handle* h) {
+  h->stats_pending = 0;
   RunState rs;
   CK(cudaMemcpyAsync(&rs, h->run.p, sizeof(rs), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  if (h->timed == 1) {
+    float a = 0.f, b = 0.f;
+    CK(cudaEventElapsedTime(&a, h->ev0, h->ev1));
+    CK(cudaEventElapsedTime(&b, h->ev1, h->ev2));
+    h->stats.photon_ms = a;
+    h->stats.gather_ms = b;
+    h->stats.forward_ms = a + b;
+  } else if (h->timed == 2) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->stats.backward_ms = ms;
+  }
+  h->timed = 0;
   h->stats.photon_segments = rs.photon_segments;
   h->stats.gather_segments = rs.gather_segments;
   h->stats.adjoint_segments = rs.adjoint_segments;
@@ -517,12 +544,28 @@ void copy_stats(pale_handle* h) {
   h->stats.node_visits = rs.node_visits;
   h->stats.surfel_tests = rs.surfel_tests;
   h->stats.photons_scanned = rs.photons_scanned;
+  h->stats.gather_node_visits = rs.gather_node_visits;
+  h->stats.gather_surfel_tests = rs.gather_surfel_tests;
+  h->stats.gather_photons_scanned = rs.gather_photons_scanned;
+  h->stats.kernel_launches = h->launches_last;
   if (rs.error) {
     char buf[128];
     std::snprintf(buf, sizeof(buf), "device error flags 0x%x (1 stack, 2 layer cap, 4 photon capacity, 8 bounds, 16 queue)",
                   rs.error);
     throw std::runtime_error(buf);
   }
+}
+
+// Makes `s` the stream of the following work, ordered after everything
+// already queued on the previous stream of this handle.
+void use_stream(pale_handle* h, cudaStream_t s) {
+  if (s == h->stream) return;
+  cudaEvent_t e;
+  CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CK(cudaEventRecord(e, h->stream));
+  CK(cudaStreamWaitEvent(s, e, 0));
+  CK(cudaEventDestroy(e));
+  h->stream = s;
 }
 
 void validate_cams(pale_handle* h, uint32_t nsel, const uint32_t* idx) {
@@ -532,8 +575,9 @@ void validate_cams(pale_handle* h, uint32_t nsel, const uint32_t* idx) {
 }
 
 // Forward render into the handle's packed device images.
-uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr) {
+uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr, bool sync) {
   cudaStream_t s = h->stream;
+  const uint64_t launches0 = launches_issued();
   const pale_settings& st = h->st;
   validate_cams(h, nsel, idx);
   std::vector<CameraRec> sel(nsel);
@@ -602,13 +646,10 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   camera_gather(F, s);
   CK(cudaEventRecord(h->ev2, s));
   CK(cudaGetLastError());
-  copy_stats(h);
-  float a = 0.f, b = 0.f;
-  CK(cudaEventElapsedTime(&a, h->ev0, h->ev1));
-  CK(cudaEventElapsedTime(&b, h->ev1, h->ev2));
-  h->stats.photon_ms = a;
-  h->stats.gather_ms = b;
-  h->stats.forward_ms = a + b;
+  h->launches_last = launches_issued() - launches0;
+  h->timed = 1;
+  h->stats_pending = 1;
+  if (sync) copy_stats(h);
   return total;
 }
 
@@ -626,8 +667,9 @@ void zero_grads(pale_handle* h, cudaStream_t s) {
 }
 
 // Adjoint pass reading packed dL/dI at d_dldi (device).
-void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi, float* d_dbg) {
+void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi, float* d_dbg, bool sync) {
   cudaStream_t s = h->stream;
+  const uint64_t launches0 = launches_issued();
   const pale_settings& st = h->st;
   validate_cams(h, nsel, idx);
   std::vector<uint32_t> seeds =
@@ -670,10 +712,10 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   }
   CK(cudaEventRecord(h->ev1, s));
   CK(cudaGetLastError());
-  copy_stats(h);
-  float ms = 0.f;
-  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-  h->stats.backward_ms = ms;
+  h->launches_last = launches_issued() - launches0;
+  h->timed = 2;
+  h->stats_pending = 1;
+  if (sync) copy_stats(h);
 }
 
 void download_points(pale_handle* h, const PointsBufs& src, pale_points* out) {
@@ -734,7 +776,8 @@ int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale
     if (!(h->st.gather_radius > 0.f)) throw ArgError("gather radius must be > 0");
     check_points(&desc->points, "pale_create");
     if (desc->points.count >= (1u << 28)) throw ArgError("at most 2^28 surfels are supported");
-    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
     CK(cudaEventCreate(&h->ev2));
@@ -785,9 +828,10 @@ int pale_render_forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, floa
     validate_cams(h, nsel, idx);
     size_t pix = 0;
     for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    use_stream(h, h->own_stream);
     h->img_raw.ensure(4 * std::max<size_t>(1, pix));
     h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
-    forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p);
+    forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, true);
     if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
     if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -802,15 +846,9 @@ int pale_render_forward_device(pale_handle* h, uint32_t nsel, const uint32_t* id
     validate_cams(h, nsel, idx);
     size_t pix = 0;
     for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
-    if (stream) {
-      cudaEvent_t e;
-      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      CK(cudaEventRecord(e, (cudaStream_t)stream));
-      CK(cudaStreamWaitEvent(h->stream, e, 0));
-      CK(cudaEventDestroy(e));
-    }
+    use_stream(h, stream ? (cudaStream_t)stream : h->own_stream);
     h->img_raw.ensure(4 * std::max<size_t>(1, pix));
-    forward(h, nsel, idx, d_raw ? d_raw : h->img_raw.p, d_ldr);
+    forward(h, nsel, idx, d_raw ? d_raw : h->img_raw.p, d_ldr, false);
     return PALE_OK;
   });
 }
@@ -823,6 +861,7 @@ int pale_render_backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, con
     if (!dldi && nsel) throw ArgError("dL/dI is null");
     size_t pix = 0;
     for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    use_stream(h, h->own_stream);
     h->dldi.ensure(4 * std::max<size_t>(1, pix));
     if (pix) CK(cudaMemcpyAsync(h->dldi.p, dldi, 16 * pix, cudaMemcpyHostToDevice, h->stream));
     float* dbg = nullptr;
@@ -831,7 +870,7 @@ int pale_render_backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, con
       CK(cudaMemsetAsync(h->dbg.p, 0, 16 * pix, h->stream));
       dbg = h->dbg.p;
     }
-    backward(h, nsel, idx, h->dldi.p, dbg);
+    backward(h, nsel, idx, h->dldi.p, dbg, true);
     if (grads) download_points(h, h->grads, grads);
     if (debug_opacity) {
       if (dbg) CK(cudaMemcpyAsync(debug_opacity, dbg, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
@@ -847,14 +886,8 @@ int pale_render_backward_device(pale_handle* h, uint32_t nsel, const uint32_t* i
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
     validate_cams(h, nsel, idx);
-    if (stream) {
-      cudaEvent_t e;
-      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      CK(cudaEventRecord(e, (cudaStream_t)stream));
-      CK(cudaStreamWaitEvent(h->stream, e, 0));
-      CK(cudaEventDestroy(e));
-    }
-    backward(h, nsel, idx, d_dldi, nullptr);
+    use_stream(h, stream ? (cudaStream_t)stream : h->own_stream);
+    backward(h, nsel, idx, d_dldi, nullptr, false);
     if (d_grads) {
       const size_t n = h->np;
       cudaStream_t s = h->stream;
@@ -869,7 +902,6 @@ int pale_render_backward_device(pale_handle* h, uint32_t nsel, const uint32_t* i
       cp(d_grads->opacity, h->grads.op.p, 4 * n);
       cp(d_grads->beta, h->grads.beta.p, 4 * n);
       cp(d_grads->shape, h->grads.shape.p, 4 * n);
-      CK(cudaStreamSynchronize(s));
     }
     return PALE_OK;
   });
@@ -878,6 +910,7 @@ int pale_render_backward_device(pale_handle* h, uint32_t nsel, const uint32_t* i
 int pale_get_points(pale_handle* h, pale_points* out) {
   if (!h || !out) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
+    use_stream(h, h->own_stream);
     download_points(h, h->params, out);
     return PALE_OK;
   });
@@ -886,6 +919,7 @@ int pale_get_points(pale_handle* h, pale_points* out) {
 int pale_get_order(pale_handle* h, uint32_t* order) {
   if (!h || !order) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
+    use_stream(h, h->own_stream);
     if (h->np) CK(cudaMemcpyAsync(order, h->order.p, 4ull * h->np, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return PALE_OK;
@@ -897,6 +931,7 @@ int pale_apply_points(pale_handle* h, const pale_points* p) {
   return guarded(h, [&]() {
     check_points(p, "pale_apply_points");
     if (p->count != h->np) throw ArgError("apply_point_optimization expects consistent point count");
+    use_stream(h, h->own_stream);
     cudaStream_t s = h->stream;
     const size_t n = h->np;
     if (!n) return PALE_OK;
@@ -920,6 +955,7 @@ int pale_rebuild(pale_handle* h, const pale_points* asset) {
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
     check_points(asset, "pale_rebuild");
+    use_stream(h, h->own_stream);
     if (asset->count >= (1u << 28)) throw ArgError("at most 2^28 surfels are supported");
     build_surfels(h, asset);
     return PALE_OK;
@@ -932,6 +968,7 @@ int pale_trace_rays(pale_handle* h, uint32_t n, const float* o, const float* d, 
   return guarded(h, [&]() {
     if (n && (!o || !d || !inst || !prim || !t || !alpha)) throw ArgError("pale_trace_rays: null array");
     if (!n) return PALE_OK;
+    use_stream(h, h->own_stream);
     cudaStream_t s = h->stream;
     DBuf<float> dO, dD, dT, dA, dP;
     DBuf<int32_t> dI, dR;
@@ -946,7 +983,9 @@ int pale_trace_rays(pale_handle* h, uint32_t n, const float* o, const float* d, 
     CK(cudaMemcpyAsync(t, dT.p, 4ull * n, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(alpha, dA.p, 4ull * n, cudaMemcpyDeviceToHost, s));
     if (pos) CK(cudaMemcpyAsync(pos, dP.p, 12ull * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    h->timed = 0;
+    h->launches_last = 1;
+    copy_stats(h);
     return PALE_OK;
   });
 }
@@ -956,6 +995,7 @@ int pale_gather_irradiance(pale_handle* h, uint32_t n, const float* pts, const f
   return guarded(h, [&]() {
     if (n && (!pts || !nrm || !E)) throw ArgError("pale_gather_irradiance: null array");
     if (!n) return PALE_OK;
+    use_stream(h, h->own_stream);
     cudaStream_t s = h->stream;
     DBuf<float> dP, dN, dE;
     dP.alloc(3ull * n); dN.alloc(3ull * n); dE.alloc(3ull * n);
@@ -973,6 +1013,7 @@ int pale_load_photons(pale_handle* h, uint32_t n, const float* pos, const float*
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
     if (n && (!pos || !pw || !dir)) throw ArgError("pale_load_photons: null array");
+    use_stream(h, h->own_stream);
     cudaStream_t s = h->stream;
     if (n > (1u << 30)) throw ArgError("at most 2^30 photons can be loaded");
     if (n > h->photon_cap) {
@@ -1006,6 +1047,7 @@ int pale_get_photons(pale_handle* h, uint32_t* count, float* position, float* po
                      uint32_t* cell_id, uint32_t* sorted, float* grid_info) {
   if (!h || !count) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
+    use_stream(h, h->own_stream);
     cudaStream_t s = h->stream;
     uint32_t n = 0;
     CK(cudaMemcpyAsync(&n, h->g_stored.p, 4, cudaMemcpyDeviceToHost, s));
@@ -1039,6 +1081,7 @@ int pale_get_photons(pale_handle* h, uint32_t* count, float* position, float* po
 int pale_get_bvh(pale_handle* h, uint32_t* codes, uint32_t* node_count, float* nodes, uint32_t max_nodes) {
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
+    use_stream(h, h->own_stream);
     cudaStream_t s = h->stream;
     if (node_count) *node_count = h->np ? h->node_count : 0;
     if (codes && h->np) CK(cudaMemcpyAsync(codes, h->codes.p, 4ull * h->np, cudaMemcpyDeviceToHost, s));
@@ -1053,8 +1096,11 @@ int pale_get_bvh(pale_handle* h, uint32_t* codes, uint32_t* node_count, float* n
 
 int pale_get_stats(pale_handle* h, pale_stats* out) {
   if (!h || !out) return PALE_ERR_ARGUMENT;
-  *out = h->stats;
-  return PALE_OK;
+  return guarded(h, [&]() {
+    if (h->stats_pending) copy_stats(h);
+    *out = h->stats;
+    return PALE_OK;
+  });
 }
 
 }  // extern "C"

@@ -107,9 +107,9 @@ void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tem
                     cudaStream_t s) {
   if (n == 0) return;
   uint32_t nb = (n + kScanTile - 1) / kScanTile;
-  k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, temp);
-  k_scan_partials<<<1, 1024, 0, s>>>(temp, nb, total);
-  k_scan_apply<<<nb, kScanThreads, 0, s>>>(in, n, temp, out);
+  k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, temp); note_launch();
+  k_scan_partials<<<1, 1024, 0, s>>>(temp, nb, total); note_launch();
+  k_scan_apply<<<nb, kScanThreads, 0, s>>>(in, n, temp, out); note_launch();
 }
 
 // ------------------------------------------------------------ radix sort
@@ -195,9 +195,9 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32
   uint32_t *ka = keys, *va = vals, *kb = keys_tmp, *vb = vals_tmp;
   for (int p = 0; p < passes; ++p) {
     uint32_t shift = 8u * p;
-    k_radix_hist<<<tiles, kSortThreads, 0, s>>>(ka, d_n, shift, tiles, hist);
+    k_radix_hist<<<tiles, kSortThreads, 0, s>>>(ka, d_n, shift, tiles, hist); note_launch();
     exclusive_scan(hist, offs, (uint32_t)h, stemp, nullptr, s);
-    k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(ka, va, d_n, shift, tiles, offs, kb, vb);
+    k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(ka, va, d_n, shift, tiles, offs, kb, vb); note_launch();
     uint32_t* t = ka; ka = kb; kb = t;
     t = va; va = vb; vb = t;
   }
@@ -576,32 +576,32 @@ static inline uint32_t blocks_for(uint64_t n, int b = kBlock) { return (uint32_t
 void lbvh_build(const LbvhArgs& A, cudaStream_t s) {
   const uint32_t n = A.n;
   if (n == 0) return;
-  k_collect<<<blocks_for(n), kBlock, 0, s>>>(A.asset, n, A.collected, A.lo, A.hi);
+  k_collect<<<blocks_for(n), kBlock, 0, s>>>(A.asset, n, A.collected, A.lo, A.hi); note_launch();
   uint32_t nb = blocks_for(n) < 148u * 4u ? blocks_for(n) : 148u * 4u;
-  k_bounds_partial<<<nb, kBlock, 0, s>>>(A.collected.position, A.lo, A.hi, n, A.bounds_part);
-  k_bounds_final<<<1, 32, 0, s>>>(A.bounds_part, nb, A.bounds);
-  k_morton<<<blocks_for(n), kBlock, 0, s>>>(A.collected.position, n, A.bounds, A.codes, A.order);
+  k_bounds_partial<<<nb, kBlock, 0, s>>>(A.collected.position, A.lo, A.hi, n, A.bounds_part); note_launch();
+  k_bounds_final<<<1, 32, 0, s>>>(A.bounds_part, nb, A.bounds); note_launch();
+  k_morton<<<blocks_for(n), kBlock, 0, s>>>(A.collected.position, n, A.bounds, A.codes, A.order); note_launch();
   radix_sort_pairs(A.codes, A.order, A.codes_tmp, A.order_tmp, A.d_n, n, 30, A.sort_temp, s);
   if (n <= A.leaf_size) {
-    k_small_root<<<1, 32, 0, s>>>(A.order, n, A.lo, A.hi, A.nodes);
+    k_small_root<<<1, 32, 0, s>>>(A.order, n, A.lo, A.hi, A.nodes); note_launch();
   } else {
     k_karras<<<blocks_for(n - 1), kBlock, 0, s>>>(A.codes, n, A.lc, A.rc, A.rfirst, A.rlast, A.parent,
-                                                  A.leaf_parent, A.err);
+                                                  A.leaf_parent, A.err); note_launch();
     cudaMemsetAsync(A.visits, 0, (size_t)(n - 1) * 4, s);
     k_refit<<<blocks_for(n), kBlock, 0, s>>>(A.order, n, A.lo, A.hi, A.lc, A.rc, A.parent, A.leaf_parent, A.visits,
-                                             A.box);
+                                             A.box); note_launch();
     k_emit_nodes<<<blocks_for(n - 1), kBlock, 0, s>>>(A.order, n, A.lo, A.hi, A.lc, A.rc, A.rfirst, A.rlast, A.box,
-                                                      A.leaf_size, A.top, A.nodes);
+                                                      A.leaf_size, A.top, A.nodes); note_launch();
     if (A.top > 0)
-      k_top_nodes<<<1, kBlock, A.top * sizeof(uint32_t), s>>>(A.rfirst, A.rlast, n, A.leaf_size, A.top, A.nodes);
+      k_top_nodes<<<1, kBlock, A.top * sizeof(uint32_t), s>>>(A.rfirst, A.rlast, n, A.leaf_size, A.top, A.nodes); note_launch();
   }
-  k_permute<<<blocks_for(n), kBlock, 0, s>>>(A.collected, A.order, n, A.params);
+  k_permute<<<blocks_for(n), kBlock, 0, s>>>(A.collected, A.order, n, A.params); note_launch();
   derive_surfels(A.params, n, A.derived, s);
 }
 
 void derive_surfels(const PointsDev& p, uint32_t n, const SurfelArrays& d, cudaStream_t s) {
   if (n == 0) return;
-  k_derive<<<blocks_for(n), kBlock, 0, s>>>(p, n, d.pe, d.n, d.u, d.v, d.cn, d.alb);
+  k_derive<<<blocks_for(n), kBlock, 0, s>>>(p, n, d.pe, d.n, d.u, d.v, d.cn, d.alb); note_launch();
 }
 
 }  // namespace pale

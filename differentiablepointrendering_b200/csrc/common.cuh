@@ -211,6 +211,9 @@ struct RunState {
   unsigned long long node_visits;
   unsigned long long surfel_tests;
   unsigned long long photons_scanned;
+  unsigned long long gather_node_visits;   // camera-gather kernel only
+  unsigned long long gather_surfel_tests;
+  unsigned long long gather_photons_scanned;
 };
 
 // Per-camera constants of makePrimaryRayFromPixelJitteredFov

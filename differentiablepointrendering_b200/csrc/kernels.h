@@ -168,3 +168,9 @@ void load_photon_arrays(uint32_t n, const float* pos, const float* pw, const flo
                         cudaStream_t s);
 
 }  // namespace pale
+
+namespace pale {
+// Counts kernel launches issued by this thread (reported in pale_stats).
+void note_launch();
+uint64_t launches_issued();
+}  // namespace pale

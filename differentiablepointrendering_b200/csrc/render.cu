@@ -250,17 +250,17 @@ static size_t top_smem(const SceneView& s) { return (size_t)s.top_nodes * sizeof
 void photon_emit(const PhotonArgs& a, cudaStream_t s) {
   const uint32_t nb = blocks_for(a.photons_per_launch);
   if (nb == 0) return;
-  k_photon_emit<<<nb, kBlock, 0, s>>>(a);
+  k_photon_emit<<<nb, kBlock, 0, s>>>(a); note_launch();
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, 0, 1, a.photons_per_launch, 0,
-                                  a.ps.capacity);
-  k_queue_scatter<0><<<nb, kBlock, 0, s>>>(a.st, a.qb, 0, 1, a.photons_per_launch, a.ps, EventBufs{});
+                                  a.ps.capacity); note_launch();
+  k_queue_scatter<0><<<nb, kBlock, 0, s>>>(a.st, a.qb, 0, 1, a.photons_per_launch, a.ps, EventBufs{}); note_launch();
 }
 
 void photon_bounce(const PhotonArgs& a, uint32_t parity, cudaStream_t s) {
   const uint32_t nb = blocks_for(a.qb.capacity);
-  k_photon_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity);
-  k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 0, a.ps.capacity);
-  k_queue_scatter<0><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, a.ps, EventBufs{});
+  k_photon_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity); note_launch();
+  k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 0, a.ps.capacity); note_launch();
+  k_queue_scatter<0><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, a.ps, EventBufs{}); note_launch();
 }
 
 // ------------------------------------------------------------ photon grid
@@ -303,15 +303,15 @@ __global__ void k_gather_sorted(const uint32_t* __restrict__ sorted, const uint3
 void grid_build(const SceneView& sv, RunState* st, const PhotonStore& ps, const GridBufs& g, uint32_t cells,
                 int key_bits, cudaStream_t s) {
   const uint32_t cap = (uint32_t)ps.capacity;
-  k_stored<<<1, 32, 0, s>>>(st, ps.capacity, g.d_stored, g.d_attempts);
+  k_stored<<<1, 32, 0, s>>>(st, ps.capacity, g.d_stored, g.d_attempts); note_launch();
   cudaMemsetAsync(g.cell_count, 0, ((size_t)cells + 1) * 4, s);
   uint32_t* sort_keys = g.keys_tmp;            // first half: keys, second: ping-pong
   uint32_t* sort_keys_tmp = g.keys_tmp + cap;
   k_cell_ids<<<blocks_for(cap), kBlock, 0, s>>>(sv.grid, ps.a, g.d_stored, g.cell_id, sort_keys, g.sorted,
-                                                g.cell_count);
+                                                g.cell_count); note_launch();
   exclusive_scan(g.cell_count, g.cell_off, cells + 1, g.scan_temp, nullptr, s);
   radix_sort_pairs(sort_keys, g.sorted, sort_keys_tmp, g.vals_tmp, g.d_stored, cap, key_bits, g.sort_temp, s);
-  k_gather_sorted<<<blocks_for(cap), kBlock, 0, s>>>(g.sorted, g.d_stored, ps.a, ps.b, ps.c, g.pa, g.pb, g.pc);
+  k_gather_sorted<<<blocks_for(cap), kBlock, 0, s>>>(g.sorted, g.d_stored, ps.a, ps.b, ps.c, g.pa, g.pb, g.pc); note_launch();
 }
 
 // ---------------------------------------------------------- primary rays
@@ -419,11 +419,14 @@ __global__ void __launch_bounds__(kBlock) k_camera_gather(FrameArgs A) {
   warp_count(&A.st->photons_scanned, scanned);
   warp_count(&A.st->node_visits, ctr.nodes);
   warp_count(&A.st->surfel_tests, ctr.tests);
+  warp_count(&A.st->gather_photons_scanned, scanned);
+  warp_count(&A.st->gather_node_visits, ctr.nodes);
+  warp_count(&A.st->gather_surfel_tests, ctr.tests);
 }
 
 void camera_gather(const FrameArgs& a, cudaStream_t s) {
   if (a.total_pixels == 0) return;
-  k_camera_gather<<<blocks_for(a.total_pixels), kBlock, top_smem(a.scene), s>>>(a);
+  k_camera_gather<<<blocks_for(a.total_pixels), kBlock, top_smem(a.scene), s>>>(a); note_launch();
 }
 
 // ------------------------------------------------------------- adjoint
@@ -648,17 +651,17 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
 
 void adjoint_raygen(const AdjointArgs& a, cudaStream_t s) {
   const uint32_t npix = a.cam.w * a.cam.h;
-  k_adj_raygen<<<blocks_for(npix), kBlock, 0, s>>>(a);
-  k_advance<<<1, 32, 0, s>>>(a.st, 1u);
+  k_adj_raygen<<<blocks_for(npix), kBlock, 0, s>>>(a); note_launch();
+  k_advance<<<1, 32, 0, s>>>(a.st, 1u); note_launch();
 }
 
 void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, cudaStream_t s) {
   const uint32_t nb = blocks_for(a.qb.capacity);
   const uint32_t parity = bounce & 1u;
-  k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce);
-  k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0);
-  k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev);
-  k_transport<<<nb, kBlock, 0, s>>>(a);
+  k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce); note_launch();
+  k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
+  k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev); note_launch();
+  k_transport<<<nb, kBlock, 0, s>>>(a); note_launch();
 }
 
 // ------------------------------------------------------ component queries
@@ -682,12 +685,14 @@ __global__ void __launch_bounds__(kBlock) k_trace_rays(SceneView S, RunState* st
     pos[3 * i + 1] = h.pos.y;
     pos[3 * i + 2] = h.pos.z;
   }
+  atomicAdd(&st->node_visits, (unsigned long long)ctr.nodes);
+  atomicAdd(&st->surfel_tests, (unsigned long long)ctr.tests);
 }
 
 void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d, int32_t* inst,
                 int32_t* prim, float* t, float* alpha, float* pos, cudaStream_t s) {
   if (n == 0) return;
-  k_trace_rays<<<blocks_for(n), kBlock, top_smem(sv), s>>>(sv, st, n, o, d, inst, prim, t, alpha, pos);
+  k_trace_rays<<<blocks_for(n), kBlock, top_smem(sv), s>>>(sv, st, n, o, d, inst, prim, t, alpha, pos); note_launch();
 }
 
 __global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict__ p, const float* __restrict__ nrm,
@@ -704,7 +709,7 @@ __global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict
 
 void gather_points(const SceneView& sv, uint32_t n, const float* p, const float* nrm, float* E, cudaStream_t s) {
   if (n == 0) return;
-  k_gather_points<<<blocks_for(n), kBlock, 0, s>>>(sv, n, p, nrm, E);
+  k_gather_points<<<blocks_for(n), kBlock, 0, s>>>(sv, n, p, nrm, E); note_launch();
 }
 
 __global__ void k_load_photons(uint32_t n, const float* __restrict__ pos, const float* __restrict__ pw,
@@ -719,7 +724,7 @@ __global__ void k_load_photons(uint32_t n, const float* __restrict__ pos, const 
 void load_photon_arrays(uint32_t n, const float* pos, const float* pw, const float* dir, const PhotonStore& ps,
                         cudaStream_t s) {
   if (n == 0) return;
-  k_load_photons<<<blocks_for(n), kBlock, 0, s>>>(n, pos, pw, dir, ps);
+  k_load_photons<<<blocks_for(n), kBlock, 0, s>>>(n, pos, pw, dir, ps); note_launch();
 }
 
 }  // namespace pale

@@ -44,6 +44,11 @@ __device__ __forceinline__ float slab_entry(V3 o, V3 inv, float lx, float ly, fl
   return tmin;
 }
 
+// A box is entered when the slab test hit it (finite entry) no farther
+// than the current closest hit.  The finiteness check matters while `best`
+// is still +inf: a miss (+inf) must not compare as "<= best".
+__device__ __forceinline__ bool entered(float e, float best) { return e < 3.402823466e+38f && e <= best; }
+
 // intersectTriangle (KernelHelpers.h:248-277).
 __device__ __forceinline__ bool tri_hit(V3 o, V3 d, V3 v0, V3 v1, V3 v2, float tmin, float& t_out) {
   V3 e1 = v1 - v0, e2 = v2 - v0;
@@ -127,7 +132,7 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode
     ctr.nodes++;
     float e0 = w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
     float e1 = w.y == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, b.z, b.w, c.x, c.y, c.z, c.w, best);
-    bool h0 = e0 <= best, h1 = e1 <= best;
+    bool h0 = entered(e0, best), h1 = entered(e1, best);
     // leaves: test their surfels now, nearer leaf first
     uint32_t lw[2] = {w.x, w.y};
     bool lh[2] = {h0 && (w.x & kLeafFlag) != 0, h1 && (w.y & kLeafFlag) != 0};
@@ -203,7 +208,7 @@ __device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode
   const MeshView& M = S.mesh;
   for (uint32_t i = 0; i < M.instances; ++i) {
     const float4 lo = __ldg(&M.box[2 * i]), hi = __ldg(&M.box[2 * i + 1]);
-    if (!(slab_entry(o, invw, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, best) <= best)) continue;
+    if (!entered(slab_entry(o, invw, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, best), best)) continue;
     const float* W2O = M.w2o + 16 * i;
     float w2o[16];
 #pragma unroll
@@ -240,7 +245,7 @@ __device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode
     }
   }
   if (S.has_pc &&
-      slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best) <= best) {
+      entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best), best)) {
     V3 dd = normalize(d);
     // prune with the mesh hit plus a relative margin: a surfel beyond the
     // margin cannot have a smaller world distance than the mesh hit

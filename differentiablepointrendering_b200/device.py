@@ -1,0 +1,82 @@
+"""Device-resident rendering on CUDA tensors.
+
+``DeviceFrame`` drives a :class:`~differentiablepointrendering_b200.pale.Renderer`
+through the C-ABI's device entry points: images, dL/dI and gradients stay in
+HBM as torch tensors and every kernel runs on the caller's CUDA stream, with
+no host synchronisation.  Counters of a call are fetched on demand with
+:meth:`stats`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Optional, Sequence
+
+import torch
+
+from . import _native as N
+from .pale import Renderer, _check
+from .scene import POINT_FIELDS, POINT_WIDTH
+
+
+class DeviceFrame:
+    """Forward / adjoint passes of selected cameras into device tensors."""
+
+    def __init__(self, renderer: Renderer, cameras: Optional[Sequence[int]] = None, device=None):
+        self.r = renderer
+        self.device = torch.device(device or f"cuda:{torch.cuda.current_device()}")
+        self.cams = list(range(len(renderer.get_camera_names()))) if cameras is None else list(cameras)
+        self._cams = N.cams_array(self.cams)
+        self.sizes = [renderer._sizes[i] for i in self.cams]
+        self.pixels = sum(w * h for w, h in self.sizes)
+        f = dict(dtype=torch.float32, device=self.device)
+        self.ldr = torch.zeros(self.pixels, 4, **f)
+        self.raw = torch.zeros(self.pixels, 4, **f)
+        self.dldi = torch.zeros(self.pixels, 4, **f)
+        n = renderer.num_points
+        self.grads = {k: torch.zeros((n, POINT_WIDTH[k]) if POINT_WIDTH[k] > 1 else (n,), **f) for k in POINT_FIELDS}
+        self._gstruct = N.PalePoints()
+        self._gstruct.count = n
+        for k in POINT_FIELDS:
+            setattr(self._gstruct, k, C.cast(C.c_void_p(self.grads[k].data_ptr()), N.f32p))
+
+    def _stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def forward(self):
+        """Renders LDR and RAW images (packed (P, 4), camera after camera)."""
+        L = self.r._lib
+        rc = L.pale_render_forward_device(self.r._h, len(self.cams), self._cams.ctypes.data_as(N.u32p),
+                                          C.c_void_p(self.ldr.data_ptr()), C.c_void_p(self.raw.data_ptr()),
+                                          self._stream())
+        _check(L, self.r._h, rc, "render_forward_device")
+        return self.ldr, self.raw
+
+    def backward(self, dldi: Optional[torch.Tensor] = None):
+        """Adjoint pass with packed dL/dI (P, 4) (alpha ignored); gradients
+        land in self.grads (BVH order)."""
+        d = self.dldi if dldi is None else dldi.contiguous()
+        L = self.r._lib
+        rc = L.pale_render_backward_device(self.r._h, len(self.cams), self._cams.ctypes.data_as(N.u32p),
+                                           C.c_void_p(d.data_ptr()), C.byref(self._gstruct), self._stream())
+        _check(L, self.r._h, rc, "render_backward_device")
+        return self.grads
+
+    def split(self, packed: torch.Tensor) -> List[torch.Tensor]:
+        """Packed (P, 4) -> list of (H, W, 4) views, one per camera."""
+        out, off = [], 0
+        for w, h in self.sizes:
+            out.append(packed[off:off + w * h].view(h, w, 4))
+            off += w * h
+        return out
+
+    def stats(self) -> Dict[str, float]:
+        return self.r.stats()
+
+
+def l2_grad_(dldi: torch.Tensor, ldr: torch.Tensor, target_rgb: torch.Tensor) -> torch.Tensor:
+    """dL/dI of L = 1/2 mean((I - T)^2) over the RGB channels
+    (compute_l2_grad, python/losses.py:28-45), written into dldi (P, 4)."""
+    n = target_rgb.numel()
+    torch.sub(ldr[:, :3], target_rgb, out=dldi[:, :3])
+    dldi[:, :3].div_(n)
+    return dldi

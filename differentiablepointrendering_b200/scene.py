@@ -253,19 +253,20 @@ def jitter_target(points: Dict[str, np.ndarray], seed: int = 5678, pos_sigma=0.0
     return out
 
 
-def ring_cameras(count: int, radius: float = 1.5, height: float = 0.0):
-    """Eye positions on a horizontal circle; camera 0 looks through the open
-    -y side of the box."""
+def ring_cameras(count: int, radius: float = 1.5, height: float = 0.0, offset: float = 0.0):
+    """Eye positions on a horizontal circle; camera 0 (offset 0) looks
+    through the open -y side of the box.  `offset` rotates the ring by a
+    fraction of the camera spacing."""
     eyes = []
     for k in range(count):
-        th = 2.0 * math.pi * k / count
+        th = 2.0 * math.pi * (k + offset) / count
         eyes.append((radius * math.sin(th), -radius * math.cos(th), height))
     return eyes
 
 
 def make_box_scene(n_surfels: int, cameras: int = 1, resolution: int = 256, fovy: float = 40.0,
                    seed: int = 1234, radiance: float = 15.0,
-                   points: Optional[Dict[str, np.ndarray]] = None) -> SceneArrays:
+                   points: Optional[Dict[str, np.ndarray]] = None, ring_offset: float = 0.0) -> SceneArrays:
     """The synthetic box of the throughput workloads.
 
     Walls are instances of the rectangle quad (front faces inward), albedo
@@ -287,7 +288,7 @@ def make_box_scene(n_surfels: int, cameras: int = 1, resolution: int = 256, fovy
     B.add_instance(quad, red, trs((-0.5, 0, 0), (0, 1, 0), 90.0, h), "left")
     B.add_instance(quad, green, trs((0.5, 0, 0), (0, 1, 0), -90.0, h), "right")
     B.add_instance(quad, light, trs((0, 0, 0.499), (1, 0, 0), 180.0, (0.125, 0.125, 1.0)), "light")
-    for k, eye in enumerate(ring_cameras(cameras)):
+    for k, eye in enumerate(ring_cameras(cameras, offset=ring_offset)):
         B.add_camera(f"camera{k}", eye, (0, 0, 0), (0, 0, 1), fovy, resolution, resolution)
     if points is None:
         points = make_surfels(n_surfels, seed)

@@ -117,6 +117,10 @@ typedef struct pale_stats {
     uint64_t node_visits;           /* BVH nodes visited (instrumented only) */
     uint64_t surfel_tests;          /* ray/surfel tests (instrumented only)  */
     uint64_t photons_scanned;       /* photons scanned by lookups (instr.)   */
+    uint64_t gather_node_visits;    /* ... of the camera-gather kernel alone */
+    uint64_t gather_surfel_tests;
+    uint64_t gather_photons_scanned;
+    uint64_t kernel_launches;       /* kernels launched by the last call     */
     float forward_ms;               /* device time of the last forward pass  */
     float backward_ms;              /* device time of the last adjoint pass  */
     float photon_ms;                /* photon trace + grid build part        */

@@ -1440,6 +1440,9 @@ int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float 
         s->stats.photons_scanned += scanned;
         s->stats.node_visits += nodes;
         s->stats.surfel_tests += tests;
+        s->stats.gather_photons_scanned += scanned;
+        s->stats.gather_node_visits += nodes;
+        s->stats.gather_surfel_tests += tests;
         if (raw) memcpy(raw + off, fb, (size_t)npix * 4 * sizeof(float));
         if (ldr) postprocess(s, fb, ldr + off, npix);
         off += (size_t)npix * 4;
@@ -1770,15 +1773,22 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
 int orc_trace_rays(orc_scene *s, uint32_t n, const float *o, const float *d, int32_t *inst,
                    int32_t *prim, float *t, float *alpha, float *hitpos) {
     apply_threads();
-#pragma omp parallel for schedule(dynamic, 256)
+    uint64_t nodes = 0, tests = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : nodes, tests)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
-        hit_t h = intersect_scene(s, vload(o + 3 * i), vload(d + 3 * i), NULL);
+        trav_ctr c = {0, 0};
+        hit_t h = intersect_scene(s, vload(o + 3 * i), vload(d + 3 * i), &c);
+        nodes += c.nodes;
+        tests += c.tests;
         inst[i] = h.hit ? h.inst : -1;
         prim[i] = h.hit ? (int32_t)h.prim : -1;
         t[i] = h.hit ? h.t : FLT_MAX;
         alpha[i] = h.hit ? h.alpha : 0.f;
         if (hitpos) vstore(hitpos + 3 * i, h.hit ? h.pos : V3(0, 0, 0));
     }
+    memset(&s->stats, 0, sizeof(s->stats));
+    s->stats.node_visits = nodes;
+    s->stats.surfel_tests = tests;
     return 0;
 }
 int orc_gather_irradiance(orc_scene *s, uint32_t n, const float *pts, const float *nrm, float *E) {

@@ -152,3 +152,20 @@ def test_opacity_gradients_match_oracle(pair, box):
     assert cos >= 0.99 and rel <= 1e-2, (cos, rel)
     for k in ("position", "tangent_u", "tangent_v", "scale", "albedo", "beta", "shape"):
         assert gg[k].shape[0] == g.num_points
+
+
+def test_traversal_cost_close_to_oracle(pair, box):
+    """Node visits per ray on the GPU stay within 2x of the oracle's on the
+    same rays (catches culling regressions that keep results correct)."""
+    g, o = pair
+    rng = np.random.default_rng(11)
+    n = 4000
+    orig = rng.uniform(-0.39, 0.39, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    g.trace_rays(orig, d)
+    o.trace_rays(orig, d)
+    ng, no = g.stats()["node_visits"] / n, o.stats()["node_visits"] / n
+    tg, to = g.stats()["surfel_tests"] / n, o.stats()["surfel_tests"] / n
+    assert ng <= 2.0 * no + 8, (ng, no)
+    assert tg <= 2.0 * to + 8, (tg, to)
