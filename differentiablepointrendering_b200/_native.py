@@ -196,6 +196,9 @@ def load_library() -> C.CDLL:
         "pale_get_photons": (C.c_int, [H, u32p, f32p, f32p, f32p, u32p, u32p, f32p]),
         "pale_get_bvh": (C.c_int, [H, u32p, u32p, f32p, C.c_uint32]),
         "pale_get_stats": (C.c_int, [H, C.POINTER(PaleStats)]),
+        "pale_build_lbvh_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                              C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -210,7 +213,8 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_render_forward_device", "pale_render_backward", "pale_render_backward_device",
             "pale_get_points", "pale_get_order", "pale_apply_points", "pale_rebuild", "pale_trace_rays",
             "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
-            "pale_get_stats")
+            "pale_get_stats", "pale_build_lbvh_noalloc")
+NOALLOC_MAX_SURFELS = 16384
 
 
 def cams_array(idx: Sequence[int]) -> np.ndarray:

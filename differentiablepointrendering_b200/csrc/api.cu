@@ -29,6 +29,12 @@ namespace {
 
 thread_local std::string g_create_error;
 
+}  // namespace
+
+void pale::set_thread_error(const std::string& msg) { g_create_error = msg; }
+
+namespace {
+
 struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };

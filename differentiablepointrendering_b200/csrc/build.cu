@@ -11,6 +11,10 @@
 //   of the node array so the traversal can stage them in shared memory.
 // Surfels are then permuted into leaf order, the order in which parameters
 // and gradients are exchanged (SceneBuild.cpp:723-731).
+#include <mutex>
+#include <string>
+
+#include "../../include/pale_b200.h"
 #include "kernels.h"
 
 namespace pale {
@@ -604,4 +608,139 @@ void derive_surfels(const PointsDev& p, uint32_t n, const SurfelArrays& d, cudaS
   k_derive<<<blocks_for(n), kBlock, 0, s>>>(p, n, d.pe, d.n, d.u, d.v, d.cn, d.alb); note_launch();
 }
 
+// ------------------------------------------- LBVH build without allocation
+// Some callers cannot allocate device memory around a call: code that runs
+// while a CUDA graph is being captured (cudaMalloc is not capturable), host
+// applications that own all device memory through their own allocator and
+// forbid the runtime allocator, and latency-critical loops that cannot
+// afford cudaMalloc's implicit device synchronisation.  For them the LBVH
+// build is also offered with all of its temporaries in this file-scope
+// device array.  Every GPU that loads the library holds the array until the
+// process exits; every call shares it, so calls that overlap on the GPU race.
+constexpr uint32_t kNoAllocMax = PALE_NOALLOC_MAX_SURFELS;
+constexpr uint32_t kNoAllocTiles = (kNoAllocMax + kSortTile - 1) / kSortTile;
+constexpr size_t kNoAllocSortWords = 2 * ((size_t)kNoAllocTiles * 256 + 1) +
+                                     ((size_t)kNoAllocTiles * 256 + 1 + kScanTile - 1) / kScanTile + 1 + 8;
+constexpr size_t kNoAllocWords = 17 * (size_t)kNoAllocMax   // collected parameters
+                                 + 3 * (size_t)kNoAllocMax  // dummy albedo / opacity / beta inputs
+                                 + 6 * (size_t)kNoAllocMax  // boxes lo, hi
+                                 + 2 * (size_t)kNoAllocMax  // sort ping-pong
+                                 + 7 * (size_t)kNoAllocMax  // topology
+                                 + 6 * (size_t)kNoAllocMax  // node boxes
+                                 + kNoAllocSortWords + 12 * 592 + 12 + 8;
+static __device__ __align__(256) uint32_t g_lbvh_scratch[kNoAllocWords];
+
+__global__ void k_set_words(uint32_t* p, uint32_t n, uint32_t a, uint32_t b) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    p[0] = n;
+    p[1] = a;
+    (void)b;
+  }
+}
+
+namespace {
+std::mutex g_scratch_mu;
+void* g_scratch_addr[128] = {};
+
+// Device address of g_lbvh_scratch on the current device, looked up once
+// per device (the host-side symbol is not a device address).
+cudaError_t scratch_address(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_lbvh_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
 }  // namespace pale
+
+extern "C" int pale_build_lbvh_noalloc(const float* d_position, const float* d_tangent_u, const float* d_tangent_v,
+                                       const float* d_scale, uint32_t n, uint32_t leaf_size, uint32_t* d_codes,
+                                       uint32_t* d_order, float* d_nodes, uint32_t* d_status, void* stream) {
+  using namespace pale;
+  if (n > kNoAllocMax) {
+    set_thread_error("pale_build_lbvh_noalloc: " + std::to_string(n) + " surfels exceed the fixed maximum of " +
+                     std::to_string(kNoAllocMax));
+    return PALE_ERR_ARGUMENT;
+  }
+  if (n == 0) return PALE_OK;
+  if (!d_position || !d_tangent_u || !d_tangent_v || !d_scale || !d_codes || !d_order || !d_nodes) {
+    set_thread_error("pale_build_lbvh_noalloc: null device pointer");
+    return PALE_ERR_ARGUMENT;
+  }
+  void* base = nullptr;
+  cudaError_t e = scratch_address(&base);
+  if (e != cudaSuccess) {
+    set_thread_error(std::string("pale_build_lbvh_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+    return PALE_ERR_CUDA;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const uint32_t N = kNoAllocMax;
+  uint32_t* w = static_cast<uint32_t*>(base);
+  auto take = [&](size_t words) {
+    uint32_t* p = w;
+    w += words;
+    return p;
+  };
+  float* f_col = reinterpret_cast<float*>(take(17ull * N));
+  float* f_dummy = reinterpret_cast<float*>(take(3ull * N));
+  float* lo = reinterpret_cast<float*>(take(3ull * N));
+  float* hi = reinterpret_cast<float*>(take(3ull * N));
+  uint32_t* codes_tmp = take(N);
+  uint32_t* order_tmp = take(N);
+  int32_t* lc = reinterpret_cast<int32_t*>(take(N));
+  int32_t* rc = reinterpret_cast<int32_t*>(take(N));
+  uint32_t* rfirst = take(N);
+  uint32_t* rlast = take(N);
+  uint32_t* parent = take(N);
+  uint32_t* leaf_parent = take(N);
+  uint32_t* visits = take(N);
+  float* box = reinterpret_cast<float*>(take(6ull * N));
+  uint32_t* sort_temp = take(kNoAllocSortWords);
+  float* bounds_part = reinterpret_cast<float*>(take(12 * 592));
+  float* bounds = reinterpret_cast<float*>(take(12));
+  uint32_t* words = take(8);   // [0] n for the radix sort, [1] error flags
+  uint32_t* err = d_status ? d_status : words + 1;
+
+  PointsDev asset{const_cast<float*>(d_position), const_cast<float*>(d_tangent_u), const_cast<float*>(d_tangent_v),
+                  const_cast<float*>(d_scale), f_dummy, f_dummy + N, f_dummy + 2 * N, nullptr};
+  PointsDev col{f_col, f_col + 3 * N, f_col + 6 * N, f_col + 9 * N, f_col + 11 * N, f_col + 14 * N, f_col + 15 * N,
+                f_col + 16 * N};
+  const uint32_t leaf = leaf_size < 1 ? 1u : (leaf_size > 8 ? 8u : leaf_size);
+  const uint32_t top = 256;
+  // zero what must start at zero: the error word and the refit counters
+  cudaMemsetAsync(err, 0, 4, s);
+  cudaMemsetAsync(f_dummy, 0, 12ull * N, s);
+  k_set_words<<<1, 32, 0, s>>>(words, n, 0u, 0u);
+  k_collect<<<blocks_for(n), kBlock, 0, s>>>(asset, n, col, lo, hi);
+  uint32_t nb = blocks_for(n) < 148u * 4u ? blocks_for(n) : 148u * 4u;
+  k_bounds_partial<<<nb, kBlock, 0, s>>>(col.position, lo, hi, n, bounds_part);
+  k_bounds_final<<<1, 32, 0, s>>>(bounds_part, nb, bounds);
+  k_morton<<<blocks_for(n), kBlock, 0, s>>>(col.position, n, bounds, d_codes, d_order);
+  radix_sort_pairs(d_codes, d_order, codes_tmp, order_tmp, words, n, 30, sort_temp, s);
+  if (n <= leaf) {
+    k_small_root<<<1, 32, 0, s>>>(d_order, n, lo, hi, reinterpret_cast<BvhNode*>(d_nodes));
+  } else {
+    BvhNode* nodes = reinterpret_cast<BvhNode*>(d_nodes);
+    k_karras<<<blocks_for(n - 1), kBlock, 0, s>>>(d_codes, n, lc, rc, rfirst, rlast, parent, leaf_parent, err);
+    cudaMemsetAsync(visits, 0, (size_t)(n - 1) * 4, s);
+    k_refit<<<blocks_for(n), kBlock, 0, s>>>(d_order, n, lo, hi, lc, rc, parent, leaf_parent, visits, box);
+    k_emit_nodes<<<blocks_for(n - 1), kBlock, 0, s>>>(d_order, n, lo, hi, lc, rc, rfirst, rlast, box, leaf, top, nodes);
+    k_top_nodes<<<1, kBlock, top * sizeof(uint32_t), s>>>(rfirst, rlast, n, leaf, top, nodes);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_thread_error(std::string("pale_build_lbvh_noalloc: launch failed: ") + cudaGetErrorString(e));
+    return PALE_ERR_CUDA;
+  }
+  return PALE_OK;
+}

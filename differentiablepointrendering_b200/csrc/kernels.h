@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "common.cuh"
 
 namespace pale {
@@ -173,4 +175,6 @@ namespace pale {
 // Counts kernel launches issued by this thread (reported in pale_stats).
 void note_launch();
 uint64_t launches_issued();
+// Error text returned by pale_last_error(NULL) on this thread.
+void set_thread_error(const std::string& msg);
 }  // namespace pale

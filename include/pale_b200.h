@@ -241,6 +241,37 @@ int pale_get_bvh(pale_handle *h, uint32_t *codes, uint32_t *node_count,
 /* Counters of the last render. */
 int pale_get_stats(pale_handle *h, pale_stats *stats);
 
+/* Largest surfel count pale_build_lbvh_noalloc accepts. */
+#define PALE_NOALLOC_MAX_SURFELS 16384u
+
+/* LBVH build that allocates nothing.  No counterpart in the reference (its
+ * BVH is built on the CPU); it serves callers that cannot allocate device
+ * memory around the call: code running while a CUDA graph is captured
+ * (cudaMalloc cannot be captured), host applications whose own allocator
+ * owns all device memory, and loops that cannot afford cudaMalloc's
+ * implicit device synchronisation.
+ *
+ * Inputs (device, asset order, n <= PALE_NOALLOC_MAX_SURFELS): position n*3,
+ * tangent_u n*3, tangent_v n*3, scale n*2.  Outputs (device, caller owned):
+ * codes[n] and order[n] by sorted position, nodes as 16 floats per node
+ * (1 node when n <= leaf_size, else 256 + n - 1), and optionally the
+ * error flags in *d_status (0 = ok).  The result equals the LBVH that
+ * pale_create / pale_rebuild build (see pale_get_bvh, pale_get_order).
+ *
+ * Temporaries live in one fixed device array of about 2.6 MB that every
+ * GPU loading the library holds until exit.  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress), so make the
+ * first call on each device outside any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race.  Work is enqueued on
+ * `stream` (a cudaStream_t, NULL = default stream) without synchronising.
+ * Returns PALE_ERR_ARGUMENT (with pale_last_error(NULL) text) when n is
+ * above the maximum. */
+int pale_build_lbvh_noalloc(const float *d_position, const float *d_tangent_u,
+                            const float *d_tangent_v, const float *d_scale,
+                            uint32_t n, uint32_t leaf_size, uint32_t *d_codes,
+                            uint32_t *d_order, float *d_nodes,
+                            uint32_t *d_status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
