@@ -139,6 +139,11 @@ struct pale_handle {
   DBuf<float4> pend_a, pend_b;
   DBuf<uint4> pend_c;
   DBuf<EventRec> ev_stage, ev_list;
+  // camera-gather wavefront
+  uint32_t path_cap = 0;
+  DBuf<RayRec> cg_q0, cg_q1;
+  DBuf<uint32_t> cg_counts;
+  DBuf<float4> cg_res, cg_fb;
   // run state, seeds, images, gradients
   DBuf<RunState> run;
   DBuf<uint32_t> seeds_fwd, seeds_adj;
@@ -414,6 +419,7 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->cams.resize(d->num_cameras);
   h->cam_names.resize(d->num_cameras);
   uint32_t max_pix = 0;
+  uint64_t all_pix = 0;
   for (uint32_t c = 0; c < d->num_cameras; ++c) {
     CameraRec& C = h->cams[c];
     std::memset(&C, 0, sizeof(C));
@@ -428,6 +434,7 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
     C.fy = 0.5f * C.height / std::tan(0.5f * (d->camera_fovy_deg[c] * 0.01745329251994329576923690768489f));
     C.fx = C.fy * (C.width / C.height);
     max_pix = std::max(max_pix, C.w * C.h);
+    all_pix += (uint64_t)C.w * C.h;
     char nm[17];
     std::memset(nm, 0, sizeof(nm));
     if (d->camera_names) std::memcpy(nm, d->camera_names + 16 * c, 16);
@@ -490,6 +497,14 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
   h->pend_a.alloc(qc); h->pend_b.alloc(qc); h->pend_c.alloc(qc);
   h->ev_stage.alloc(qc); h->ev_list.alloc(qc);
+  // camera paths in flight: every pass of every pixel when that fits in
+  // 2^25 paths (3.5 GB of queues), else chunks of whole passes
+  if (all_pix >= (1ull << 31)) throw ArgError("too many camera pixels");
+  const uint64_t want = all_pix * std::max<uint32_t>(1u, st.gather_passes);
+  h->path_cap = (uint32_t)std::max<uint64_t>(std::max<uint64_t>(all_pix, 1), std::min<uint64_t>(want, 1ull << 25));
+  h->cg_q0.alloc(h->path_cap); h->cg_q1.alloc(h->path_cap); h->cg_res.alloc(h->path_cap);
+  h->cg_fb.alloc(std::max<uint64_t>(all_pix, 1));
+  h->cg_counts.alloc(kMaxLayers + 2);
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   CK(cudaStreamSynchronize(s));
 }
@@ -649,6 +664,12 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.rng_mode = st.rng_mode;
   F.exposure = st.exposure;
   F.gamma = st.gamma;
+  F.cq[0] = h->cg_q0.p;
+  F.cq[1] = h->cg_q1.p;
+  F.counts = h->cg_counts.p;
+  F.res = h->cg_res.p;
+  F.fb = h->cg_fb.p;
+  F.path_capacity = h->path_cap;
   camera_gather(F, s);
   CK(cudaEventRecord(h->ev2, s));
   CK(cudaGetLastError());

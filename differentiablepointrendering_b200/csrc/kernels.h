@@ -120,6 +120,13 @@ struct FrameArgs {
   uint32_t gather_passes;
   uint32_t rng_mode;
   float exposure, gamma;
+  // wavefront buffers: live-path queues, live count per layer
+  // (kMaxLayers + 2 words), per-path radiance, running framebuffer
+  RayRec* cq[2];
+  uint32_t* counts;
+  float4* res;
+  float4* fb;
+  uint32_t path_capacity;  // >= total_pixels
 };
 
 struct PhotonArgs {

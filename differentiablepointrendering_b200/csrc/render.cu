@@ -332,86 +332,115 @@ __device__ __forceinline__ void primary_ray(const CameraRec& C, float px, float 
 }
 
 // -------------------------------------------------------- camera gather
-// launchCameraGatherKernel (PrimalKernels.cpp:500-653) fused with
-// launchPostProcessKernel (PostprocessKernel.cpp:11-106).  One thread per
-// pixel of all cameras; the gather passes run in order inside the thread so
-// the framebuffer sum has the reference's order.
-__global__ void __launch_bounds__(kBlock) k_camera_gather(FrameArgs A) {
+// launchCameraGatherKernel (PrimalKernels.cpp:500-653) as a wavefront.  A
+// camera path is one (pixel, gather pass); it walks the surfel layers of its
+// ray front to back, compositing L += T*alpha*Lo, T *= 1 - alpha, until a
+// mesh (emitter or diffuse lookup) or a miss ends it.  Each layer is one
+// launch over the compacted queue of live paths, so the lanes of a warp all
+// trace and shade one layer instead of walking different numbers of layers.
+// The layer loop draws no random numbers, so queue order does not matter.
+// Each finished path writes its radiance to res[path]; k_cg_finalize then
+// adds the passes of a pixel in pass order, cur + fb, as the reference's
+// sequence of launches does, and applies launchPostProcessKernel
+// (PostprocessKernel.cpp:11-106).
+
+__device__ __forceinline__ uint32_t find_camera(const FrameArgs& A, uint32_t gp) {
+  uint32_t ci = 0;
+  while (ci + 1 < A.ncams && A.cams[ci + 1].pixel_offset <= gp) ++ci;
+  return ci;
+}
+
+// Primary rays of passes [p0, p1): path = (pass - p0) * total_pixels + gp.
+__global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1) {
+  const uint32_t n = (p1 - p0) * A.total_pixels;
+  const uint32_t path = blockIdx.x * kBlock + threadIdx.x;
+  if (path == 0) A.counts[0] = n;
+  if (path >= n) return;
+  const uint32_t pass = p0 + path / A.total_pixels, gp = path % A.total_pixels;
+  const CameraRec& C = A.cams[find_camera(A, gp)];
+  const uint32_t pix = gp - C.pixel_offset;
+  const uint64_t cseed = A.seeds[A.st->seed_cursor + C.seed_slot];
+  const uint64_t base = A.rng_mode == 1 ? per_item_seed(cseed, pass) : cseed;
+  Rng r(per_item_seed(base, pix));
+  float jx = r.next_float() - 0.5f, jy = r.next_float() - 0.5f;
+  V3 o, d;
+  primary_ray(C, (float)(pix % C.w), (float)(pix / C.w), jx, jy, o, d);
+  RayRec rec;
+  rec.o = make_float4(o.x, o.y, o.z, __uint_as_float(path));
+  rec.d = make_float4(d.x, d.y, d.z, 1.0f);
+  rec.t = make_float4(0.f, 0.f, 0.f, 0.f);
+  A.cq[0][path] = rec;
+}
+
+// One surfel layer of every live path (persistent, grid-stride).
+__global__ void __launch_bounds__(kBlock) k_cg_layer(FrameArgs A, uint32_t layer) {
   extern __shared__ BvhNode s_top[];
   stage_top_nodes(A.scene, s_top);
-  const uint32_t gp = blockIdx.x * kBlock + threadIdx.x;
+  const SceneView& S = A.scene;
+  const uint32_t n = A.counts[layer];
+  const RayRec* __restrict__ qin = A.cq[layer & 1u];
+  RayRec* __restrict__ qout = A.cq[(layer & 1u) ^ 1u];
+  const int lane = threadIdx.x & 31;
   TraceCounters ctr{0, 0};
   uint32_t segs = 0, queries = 0, scanned = 0;
-  if (gp < A.total_pixels) {
-    uint32_t ci = 0;
-    while (ci + 1 < A.ncams && A.cams[ci + 1].pixel_offset <= gp) ++ci;
-    const CameraRec& C = A.cams[ci];
-    const uint32_t pix = gp - C.pixel_offset;
-    const uint32_t px = pix % C.w, py = pix / C.w;
-    const SceneView& S = A.scene;
-    const uint64_t cseed = A.seeds[A.st->seed_cursor + C.seed_slot];
-    const float spp = (float)A.gather_passes;
-    float fb[4] = {0.f, 0.f, 0.f, 0.f};
-    for (uint32_t pass = 0; pass < A.gather_passes; ++pass) {
-      const uint64_t base = A.rng_mode == 1 ? per_item_seed(cseed, pass) : cseed;
-      Rng r(per_item_seed(base, pix));
-      float jx = r.next_float() - 0.5f, jy = r.next_float() - 0.5f;
-      V3 o, d;
-      primary_ray(C, (float)px, (float)py, jx, jy, o, d);
-      V3 acc = v3(0.f, 0.f, 0.f);
-      float T = 1.0f;
-      int layer = 0;
-      for (; layer < kMaxLayers; ++layer) {
-        ++segs;
-        Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
-        if (h.inst < 0) break;
-        if (h.inst >= (int)S.mesh.instances) {
-          const float4 cn4 = __ldg(&S.sf.cn[h.prim]);
-          V3 n = xyz(cn4);
-          if (dot(n, -d) < 0.0f) n = -n;
-          ++queries;
-          V3 E = gather_irradiance(S.grid, h.pos, n, scanned);
-          const float4 al = __ldg(&S.sf.alb[h.prim]);
-          V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
-          float ae = __ldg(&S.sf.n[h.prim]).w * h.alpha;
-          acc = acc + scale(Lo, T * ae);
-          T *= (1.0f - ae);
-          o = h.pos + scale(d, 1e-4f);
-          continue;
+  for (uint32_t b = blockIdx.x * kBlock; b < n; b += gridDim.x * kBlock) {
+    const uint32_t slot = b + threadIdx.x;
+    bool alive = false;
+    RayRec rec;
+    if (slot < n) {
+      rec = qin[slot];
+      const V3 o = xyz(rec.o), d = xyz(rec.d);
+      const uint32_t path = __float_as_uint(rec.o.w);
+      float T = rec.d.w;
+      V3 acc = xyz(rec.t);
+      ++segs;
+      Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
+      if (h.inst >= (int)S.mesh.instances) {
+        const float4 cn4 = __ldg(&S.sf.cn[h.prim]);
+        V3 nrm = xyz(cn4);
+        if (dot(nrm, -d) < 0.0f) nrm = -nrm;
+        ++queries;
+        V3 E = gather_irradiance(S.grid, h.pos, nrm, scanned);
+        const float4 al = __ldg(&S.sf.alb[h.prim]);
+        V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
+        float ae = __ldg(&S.sf.n[h.prim]).w * h.alpha;
+        acc = acc + scale(Lo, T * ae);
+        T *= (1.0f - ae);
+        V3 no = h.pos + scale(d, 1e-4f);
+        rec.o = make_float4(no.x, no.y, no.z, rec.o.w);
+        rec.d.w = T;
+        rec.t = make_float4(acc.x, acc.y, acc.z, 0.f);
+        alive = layer + 1 < (uint32_t)kMaxLayers;
+        if (!alive) {
+          flag_error(A.st, kErrLayerCap);
+          A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
         }
-        const float4 mat = __ldg(&S.mesh.materials[__ldg(&S.mesh.material[h.inst])]);
-        if (mat.w > 0.f) {
-          V3 Le = scale(xyz(mat), mat.w);
-          Le = v3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
-          acc = acc + scale(Le, T);
-        } else {
-          V3 nrm = hit_normal(S, h);
-          ++queries;
-          V3 E = gather_irradiance(S.grid, h.pos, nrm, scanned);
-          V3 Lo = mul(scale(xyz(mat), kInvPi), E);
-          acc = acc + scale(Lo, T);
+      } else {
+        if (h.inst >= 0) {
+          const float4 mat = __ldg(&S.mesh.materials[__ldg(&S.mesh.material[h.inst])]);
+          if (mat.w > 0.f) {
+            V3 Le = scale(xyz(mat), mat.w);
+            Le = v3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
+            acc = acc + scale(Le, T);
+          } else {
+            V3 nrm = hit_normal(S, h);
+            ++queries;
+            V3 E = gather_irradiance(S.grid, h.pos, nrm, scanned);
+            V3 Lo = mul(scale(xyz(mat), kInvPi), E);
+            acc = acc + scale(Lo, T);
+          }
         }
-        break;
+        A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
       }
-      if (layer == kMaxLayers) flag_error(A.st, kErrLayerCap);
-      float inv = 1.f / spp;
-      float cur[4] = {acc.x * inv, acc.y * inv, acc.z * inv, 1.0f * inv};
-#pragma unroll
-      for (int k = 0; k < 4; ++k) fb[k] = cur[k] + fb[k];
     }
-    const size_t o4 = 4 * (size_t)gp;
-    if (A.raw) *reinterpret_cast<float4*>(A.raw + o4) = make_float4(fb[0], fb[1], fb[2], fb[3]);
-    if (A.ldr) {
-      float ig = (A.gamma > 0.0f) ? (1.0f / A.gamma) : 1.0f;
-      float l[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float x = fb[c] * A.exposure;
-        x = fmaxf(x, 0.0f);
-        x = powf(x, ig);
-        l[c] = clampf(x, 0.0f, 1.0f);
-      }
-      *reinterpret_cast<float4*>(A.ldr + o4) = make_float4(l[0], l[1], l[2], 1.0f);
+    // warp-aggregated append of the surviving paths
+    const unsigned ballot = __ballot_sync(0xffffffffu, alive);
+    if (ballot) {
+      const int leader = __ffs(ballot) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(&A.counts[layer + 1], (uint32_t)__popc(ballot));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (alive) qout[base + __popc(ballot & ((1u << lane) - 1u))] = rec;
     }
   }
   warp_count(&A.st->gather_segments, segs);
@@ -424,9 +453,70 @@ __global__ void __launch_bounds__(kBlock) k_camera_gather(FrameArgs A) {
   warp_count(&A.st->gather_surfel_tests, ctr.tests);
 }
 
+// fb += res/spp over passes [p0, p1) in pass order; the last chunk writes the
+// RAW image and the post-processed LDR image.
+__global__ void k_cg_finalize(FrameArgs A, uint32_t p0, uint32_t p1, int first, int last) {
+  const uint32_t gp = blockIdx.x * kBlock + threadIdx.x;
+  if (gp >= A.total_pixels) return;
+  float4 f = first ? make_float4(0.f, 0.f, 0.f, 0.f) : A.fb[gp];
+  float fb[4] = {f.x, f.y, f.z, f.w};
+  const float inv = 1.f / (float)A.gather_passes;
+  for (uint32_t p = p0; p < p1; ++p) {
+    const float4 a = A.res[(size_t)(p - p0) * A.total_pixels + gp];
+    float cur[4] = {a.x * inv, a.y * inv, a.z * inv, 1.0f * inv};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) fb[k] = cur[k] + fb[k];
+  }
+  if (!last) {
+    A.fb[gp] = make_float4(fb[0], fb[1], fb[2], fb[3]);
+    return;
+  }
+  const size_t o4 = 4 * (size_t)gp;
+  if (A.raw) *reinterpret_cast<float4*>(A.raw + o4) = make_float4(fb[0], fb[1], fb[2], fb[3]);
+  if (A.ldr) {
+    float ig = (A.gamma > 0.0f) ? (1.0f / A.gamma) : 1.0f;
+    float l[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float x = fb[c] * A.exposure;
+      x = fmaxf(x, 0.0f);
+      x = powf(x, ig);
+      l[c] = clampf(x, 0.0f, 1.0f);
+    }
+    *reinterpret_cast<float4*>(A.ldr + o4) = make_float4(l[0], l[1], l[2], 1.0f);
+  }
+}
+
 void camera_gather(const FrameArgs& a, cudaStream_t s) {
   if (a.total_pixels == 0) return;
-  k_camera_gather<<<blocks_for(a.total_pixels), kBlock, top_smem(a.scene), s>>>(a); note_launch();
+  if (a.gather_passes == 0) {
+    k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, 0, 0, 1, 1); note_launch();
+    return;
+  }
+  const uint32_t ppc = std::max<uint32_t>(1u, std::min(a.gather_passes, a.path_capacity / a.total_pixels));
+  // persistent layer grid: every SM filled once
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_layer, kBlock, top_smem(a.scene));
+  const uint32_t grid = (uint32_t)std::max(1, sms * std::max(1, per_sm));
+  for (uint32_t p0 = 0; p0 < a.gather_passes; p0 += ppc) {
+    const uint32_t p1 = std::min(a.gather_passes, p0 + ppc);
+    const uint32_t n = (p1 - p0) * a.total_pixels;
+    cudaMemsetAsync(a.counts, 0, (kMaxLayers + 2) * sizeof(uint32_t), s);
+    k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1); note_launch();
+    uint32_t layer = 0;
+    while (layer < (uint32_t)kMaxLayers) {
+      for (int k = 0; k < 16 && layer < (uint32_t)kMaxLayers; ++k, ++layer) {
+        k_cg_layer<<<grid, kBlock, top_smem(a.scene), s>>>(a, layer); note_launch();
+      }
+      uint32_t left = 0;
+      cudaMemcpyAsync(&left, a.counts + layer, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+      cudaStreamSynchronize(s);
+      if (left == 0) break;
+    }
+    k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1, p0 == 0, p1 == a.gather_passes); note_launch();
+  }
 }
 
 // ------------------------------------------------------------- adjoint
