@@ -139,6 +139,11 @@ struct pale_handle {
   DBuf<float4> pend_a, pend_b;
   DBuf<uint4> pend_c;
   DBuf<EventRec> ev_stage, ev_list;
+  // adjoint batches
+  uint32_t adj_cap = 0;
+  DBuf<AdjJob> d_jobs;
+  DBuf<CameraRec> d_adj_cams;
+  DBuf<uint32_t> job_count, job_start;
   // camera-gather wavefront
   uint32_t path_cap = 0;
   DBuf<RayRec> cg_q0, cg_q1;
@@ -492,11 +497,18 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   // ---- queues: next power of two >= max(photons per launch, pixels)
   h->qcap = next_pow2(std::max(std::max(st.photons_per_launch, max_pix), 256u));
   const size_t qc = h->qcap;
-  h->q0.alloc(qc); h->q1.alloc(qc); h->qstage.alloc(qc); h->qflags.alloc(qc);
-  h->tile_counts.alloc(qc / kBlock + 1); h->tile_offsets.alloc(qc / kBlock + 1);
+  // adjoint batches: the (camera, pass) jobs of a backward call trace
+  // together, up to 2^24 paths (about 5.4 GB of queues and events)
+  const uint64_t adj_want = all_pix * std::max<uint32_t>(1u, st.adjoint_passes);
+  h->adj_cap = (uint32_t)std::max<uint64_t>(max_pix, std::min<uint64_t>(adj_want, 1ull << 24));
+  const size_t qa = std::max<size_t>(qc, h->adj_cap);
+  h->q0.alloc(qa); h->q1.alloc(qa); h->qstage.alloc(qa); h->qflags.alloc(qa);
+  h->tile_counts.alloc(qa / kBlock + 1); h->tile_offsets.alloc(qa / kBlock + 1);
   h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
-  h->pend_a.alloc(qc); h->pend_b.alloc(qc); h->pend_c.alloc(qc);
-  h->ev_stage.alloc(qc); h->ev_list.alloc(qc);
+  h->pend_a.alloc(qa); h->pend_b.alloc(qa); h->pend_c.alloc(qa);
+  h->ev_stage.alloc(qa); h->ev_list.alloc(qa);
+  h->job_count.alloc(2 * kMaxJobsPerBatch);
+  h->job_start.alloc(2 * kMaxJobsPerBatch);
   // camera paths in flight: every pass of every pixel when that fits in
   // 2^25 paths (3.5 GB of queues), else chunks of whole passes
   if (all_pix >= (1ull << 31)) throw ArgError("too many camera pixels");
@@ -711,7 +723,8 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.scene = h->view();
   A.st = h->run.p;
   A.seeds = h->seeds_adj.p;
-  A.qb = QueueBufs{{h->q0.p, h->q1.p}, h->qstage.p, h->qflags.p, h->tile_counts.p, h->tile_offsets.p, h->qcap};
+  A.qb = QueueBufs{{h->q0.p, h->q1.p}, h->qstage.p, h->qflags.p, h->tile_counts.p, h->tile_offsets.p,
+                   std::max(h->qcap, h->adj_cap)};
   A.pend = PendingBufs{h->pend_a.p, h->pend_b.p, h->pend_c.p};
   A.ev = EventBufs{h->ev_stage.p, h->ev_list.p};
   A.dldi = d_dldi;
@@ -726,16 +739,49 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.rng_mode = st.rng_mode;
   A.light0_valid = h->n_lights > 0;
   A.light0_area = h->light0_area;
+  // jobs in the reference's order (camera-major, then pass), packed into
+  // batches of at most adj_cap paths and kMaxJobsPerBatch jobs
+  std::vector<CameraRec> sel(nsel);
   uint32_t offset = 0;
   for (uint32_t i = 0; i < nsel; ++i) {
-    A.cam = h->cams[idx[i]];
-    A.cam.pixel_offset = offset;
-    if (A.cam.w * A.cam.h > h->qcap) throw ArgError("camera larger than the queue capacity");
+    sel[i] = h->cams[idx[i]];
+    sel[i].pixel_offset = offset;
+    if (sel[i].w * sel[i].h > h->adj_cap) throw ArgError("camera larger than the queue capacity");
+    offset += sel[i].w * sel[i].h;
+  }
+  std::vector<AdjJob> jobs;
+  std::vector<std::pair<uint32_t, uint32_t>> batches;  // (first job, paths)
+  uint32_t in_batch = 0, first = 0;
+  for (uint32_t i = 0; i < nsel; ++i) {
+    const uint32_t npix = sel[i].w * sel[i].h;
     for (uint32_t spp = 0; spp < st.adjoint_passes; ++spp) {
-      adjoint_raygen(A, s);
-      for (uint32_t b = 0; b < st.adjoint_bounces; ++b) adjoint_bounce(A, b, s);
+      const uint32_t j = (uint32_t)jobs.size();
+      if (in_batch + npix > h->adj_cap || j - first == kMaxJobsPerBatch) {
+        batches.emplace_back(first, in_batch);
+        first = j;
+        in_batch = 0;
+      }
+      jobs.push_back(AdjJob{i, in_batch, npix, (i * st.adjoint_passes + spp) * (1u + st.adjoint_bounces)});
+      in_batch += npix;
     }
-    offset += A.cam.w * A.cam.h;
+  }
+  if (!jobs.empty()) batches.emplace_back(first, in_batch);
+  h->d_adj_cams.ensure(std::max<size_t>(1, nsel));
+  h->d_jobs.ensure(std::max<size_t>(1, jobs.size()));
+  if (nsel) CK(cudaMemcpyAsync(h->d_adj_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
+  if (!jobs.empty())
+    CK(cudaMemcpyAsync(h->d_jobs.p, jobs.data(), jobs.size() * sizeof(AdjJob), cudaMemcpyHostToDevice, s));
+  A.cams = h->d_adj_cams.p;
+  A.job_count = h->job_count.p;
+  A.job_start = h->job_start.p;
+  for (size_t bi = 0; bi < batches.size(); ++bi) {
+    const uint32_t j0 = batches[bi].first;
+    const uint32_t j1 = bi + 1 < batches.size() ? batches[bi + 1].first : (uint32_t)jobs.size();
+    A.jobs = h->d_jobs.p + j0;
+    A.njobs = j1 - j0;
+    const uint32_t npaths = batches[bi].second;
+    adjoint_raygen(A, npaths, s);
+    for (uint32_t b = 0; b < st.adjoint_bounces; ++b) adjoint_bounce(A, b, npaths, s);
   }
   CK(cudaEventRecord(h->ev1, s));
   CK(cudaGetLastError());
@@ -801,6 +847,7 @@ int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale
     if (h->st.forward_passes == 0 || h->st.photons_per_launch == 0) throw ArgError("photons and forward passes must be > 0");
     if (h->st.gather_passes == 0 || h->st.adjoint_passes == 0) throw ArgError("gather and adjoint passes must be > 0");
     if (!(h->st.gather_radius > 0.f)) throw ArgError("gather radius must be > 0");
+    if (h->st.adjoint_bounces > 255) throw ArgError("at most 255 adjoint bounces are supported");
     check_points(&desc->points, "pale_create");
     if (desc->points.count >= (1u << 28)) throw ArgError("at most 2^28 surfels are supported");
     CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));

@@ -141,6 +141,19 @@ struct PhotonArgs {
   float q_null, q_reflect, q_transmit;
 };
 
+// One adjoint job: every pixel of one selected camera for one pass.  The
+// jobs of a batch trace as one wavefront; their rays stay grouped by job in
+// the queues (stable compaction), and a ray's random stream is keyed by its
+// rank inside its own job, as when each job runs alone.
+struct AdjJob {
+  uint32_t cam;           // index into the selected cameras
+  uint32_t path_start;    // first path of the job in the batch
+  uint32_t npix;
+  uint32_t seed_index;    // first of the job's 1 + bounces seed-table words
+};
+
+constexpr uint32_t kMaxJobsPerBatch = 1024;
+
 struct AdjointArgs {
   SceneView scene;
   RunState* st;
@@ -151,7 +164,11 @@ struct AdjointArgs {
   const float* dldi;       // packed H*W*4 per camera
   float* grad_opacity;
   float* debug_opacity;    // packed H*W*4 per camera or null
-  CameraRec cam;
+  const CameraRec* cams;   // selected cameras, packed pixel offsets
+  const AdjJob* jobs;      // jobs of this batch
+  uint32_t njobs;
+  uint32_t* job_count;     // [2][kMaxJobsPerBatch] survivors per job
+  uint32_t* job_start;     // [2][kMaxJobsPerBatch] queue start per job
   uint32_t rr_start;
   float q_null, q_reflect, q_transmit;
   float inv_spp;
@@ -166,8 +183,8 @@ void photon_bounce(const PhotonArgs& a, uint32_t parity, cudaStream_t s);
 void grid_build(const SceneView& sv, RunState* st, const PhotonStore& ps, const GridBufs& g, uint32_t cells,
                 int key_bits, cudaStream_t s);
 void camera_gather(const FrameArgs& a, cudaStream_t s);
-void adjoint_raygen(const AdjointArgs& a, cudaStream_t s);
-void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, cudaStream_t s);
+void adjoint_raygen(const AdjointArgs& a, uint32_t npaths, cudaStream_t s);
+void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cudaStream_t s);
 
 // Component queries.
 void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d, int32_t* inst,

@@ -523,23 +523,75 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
 enum : uint32_t { kKindNone = 0, kKindNull = 1, kKindReflect = 2, kKindTransmit = 3, kKindProjection = 4 };
 
 // launchRayGenAdjointKernel (AdjointKernels.cpp:15-84) + the per-spp
-// reset of the pending states (SyclBridge.cpp:222).
-__global__ void k_adj_raygen(AdjointArgs A) {
-  const CameraRec& C = A.cam;
-  const uint32_t npix = C.w * C.h;
-  const uint32_t p = blockIdx.x * kBlock + threadIdx.x;
-  if (p == 0) A.st->active[0] = npix;
-  if (p >= npix) return;
-  const uint64_t base = A.rng_mode == 1 ? (uint64_t)A.seeds[A.st->seed_cursor] : (uint64_t)A.fixed_seed;
-  Rng r(per_item_seed(base, p));
+// reset of the pending states (SyclBridge.cpp:222), for every job of a batch.
+__device__ __forceinline__ uint32_t find_job(const AdjointArgs& A, uint32_t path) {
+  uint32_t lo = 0, hi = A.njobs - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (A.jobs[mid].path_start <= path) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint64_t adjoint_base(const AdjointArgs& A, uint32_t job, uint32_t word) {
+  return A.rng_mode == 1 ? (uint64_t)A.seeds[A.jobs[job].seed_index + word] : (uint64_t)A.fixed_seed;
+}
+
+__global__ void k_adj_raygen(AdjointArgs A, uint32_t npaths) {
+  const uint32_t path = blockIdx.x * kBlock + threadIdx.x;
+  if (path == 0) A.st->active[0] = npaths;
+  if (path < kMaxJobsPerBatch) {
+    A.job_count[path] = 0u;
+    A.job_count[kMaxJobsPerBatch + path] = 0u;
+    A.job_start[path] = path < A.njobs ? A.jobs[path].path_start : 0u;
+  }
+  if (path >= npaths) return;
+  const uint32_t job = find_job(A, path);
+  const AdjJob J = A.jobs[job];
+  const CameraRec& C = A.cams[J.cam];
+  const uint32_t p = path - J.path_start;
+  Rng r(per_item_seed(adjoint_base(A, job, 0), p));
   float jx = r.next_float() - 0.5f, jy = r.next_float() - 0.5f;
   V3 o, d;
   primary_ray(C, (float)(p % C.w), (float)(p / C.w), jx, jy, o, d);
-  const float4 g = *reinterpret_cast<const float4*>(A.dldi + 4 * ((size_t)C.pixel_offset + p));
-  A.qb.q[0][p] = make_ray(o, d, v3(g.x, g.y, g.z), p, 0u, p);
-  A.pend.a[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-  A.pend.b[p] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kKindNone));
-  A.pend.c[p] = make_uint4(kInvalid, kInvalid, 0u, 0u);
+  const uint32_t pixel = C.pixel_offset + p;
+  const float4 g = *reinterpret_cast<const float4*>(A.dldi + 4 * (size_t)pixel);
+  A.qb.q[0][path] = make_ray(o, d, v3(g.x, g.y, g.z), path, job << 8, pixel);
+  A.pend.a[path] = make_float4(0.f, 0.f, 0.f, 0.f);
+  A.pend.b[path] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kKindNone));
+  A.pend.c[path] = make_uint4(kInvalid, kInvalid, 0u, 0u);
+}
+
+// Queue start of every job after a compaction: exclusive scan of the
+// survivor counts, which are cleared for the bounce after next.
+__global__ void __launch_bounds__(kMaxJobsPerBatch) k_job_scan(AdjointArgs A, uint32_t parity) {
+  __shared__ uint32_t s_w[32];
+  uint32_t* cnt = A.job_count + (size_t)(parity ^ 1u) * kMaxJobsPerBatch;
+  uint32_t* start = A.job_start + (size_t)(parity ^ 1u) * kMaxJobsPerBatch;
+  const uint32_t j = threadIdx.x;
+  const int lane = j & 31, wid = j >> 5;
+  const uint32_t c = j < A.njobs ? cnt[j] : 0u;
+  uint32_t x = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_w[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = s_w[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_w[lane] = w;
+  }
+  __syncthreads();
+  start[j] = (wid > 0 ? s_w[wid - 1] : 0u) + x - c;
+  cnt[j] = 0u;
 }
 
 // launchAdjointIntersectKernel (AdjointKernels.cpp:87-386).
@@ -550,14 +602,18 @@ __global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t p
   stage_top_nodes(A.scene, s_top);
   const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
   bool alive = false, has_ev = false;
+  uint32_t job = kInvalid;
   TraceCounters ctr{0, 0};
   if (slot < n_in) {
     const SceneView& S = A.scene;
-    const uint64_t base = A.rng_mode == 1 ? (uint64_t)A.seeds[A.st->seed_cursor] : (uint64_t)A.fixed_seed;
-    Rng r(per_item_seed(base, slot));
     const RayRec ry = A.qb.q[parity][slot];
+    const uint32_t jb = __float_as_uint(ry.d.w);
+    job = jb >> 8;
+    // the RNG key is the slot the ray holds in its own job's queue
+    const uint32_t jslot = slot - A.job_start[(size_t)parity * kMaxJobsPerBatch + job];
+    Rng r(per_item_seed(adjoint_base(A, job, 1u + bounce_index), jslot));
     const V3 o = xyz(ry.o), d = xyz(ry.d), thr = xyz(ry.t);
-    const uint32_t path = __float_as_uint(ry.o.w), bounce = __float_as_uint(ry.d.w) + 1u;
+    const uint32_t path = __float_as_uint(ry.o.w), bounce = (jb & 0xFFu) + 1u;
     const uint32_t pixel = __float_as_uint(ry.t.w);
     Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
     if (h.inst >= 0) {
@@ -652,10 +708,17 @@ __global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t p
           alive = russian_roulette(r, bounce, nt, A.rr_start);
         }
       }
-      if (alive) A.qb.stage[slot] = make_ray(no, nd, nt, path, bounce, pixel);
+      if (alive) A.qb.stage[slot] = make_ray(no, nd, nt, path, bounce | (job << 8), pixel);
       if (has_ev) A.ev.stage[slot] = ev;
     }
     A.qb.flags[slot] = (alive ? 1 : 0) | (has_ev ? 2 : 0);
+  }
+  {
+    // survivors per job, one atomic per job present in the warp
+    const uint32_t key = alive ? job : kInvalid;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (alive && (threadIdx.x & 31) == __ffs(peers) - 1)
+      atomicAdd(&A.job_count[(size_t)(parity ^ 1u) * kMaxJobsPerBatch + job], (uint32_t)__popc(peers));
   }
   warp_count(&A.st->adjoint_segments, slot < n_in ? 1u : 0u);
   warp_count(&A.st->node_visits, ctr.nodes);
@@ -728,7 +791,7 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
   }
   if (target != kInvalid && lane == __ffs(peers) - 1) atomicAdd(&A.grad_opacity[target], sum);
   if (A.debug_opacity && target != kInvalid && e < count) {
-    float* px = A.debug_opacity + 4 * ((size_t)A.cam.pixel_offset + pixel);
+    float* px = A.debug_opacity + 4 * (size_t)pixel;
     atomicAdd(px + 0, g);
     atomicAdd(px + 1, g);
     atomicAdd(px + 2, g);
@@ -739,17 +802,18 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
   warp_count(&A.st->photons_scanned, scanned);
 }
 
-void adjoint_raygen(const AdjointArgs& a, cudaStream_t s) {
-  const uint32_t npix = a.cam.w * a.cam.h;
-  k_adj_raygen<<<blocks_for(npix), kBlock, 0, s>>>(a); note_launch();
-  k_advance<<<1, 32, 0, s>>>(a.st, 1u); note_launch();
+void adjoint_raygen(const AdjointArgs& a, uint32_t npaths, cudaStream_t s) {
+  k_adj_raygen<<<blocks_for(std::max<uint32_t>(npaths, kMaxJobsPerBatch)), kBlock, 0, s>>>(a, npaths); note_launch();
 }
 
-void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, cudaStream_t s) {
-  const uint32_t nb = blocks_for(a.qb.capacity);
+// One bounce of every job of the batch; npaths bounds the live queue.
+void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cudaStream_t s) {
+  const uint32_t nb = blocks_for(npaths);
+  if (nb == 0) return;
   const uint32_t parity = bounce & 1u;
   k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce); note_launch();
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
+  k_job_scan<<<1, kMaxJobsPerBatch, 0, s>>>(a, parity); note_launch();
   k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev); note_launch();
   k_transport<<<nb, kBlock, 0, s>>>(a); note_launch();
 }

@@ -1668,8 +1668,12 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
         float *dbg = debug_opacity ? debug_opacity + off : NULL;
         if (dbg) memset(dbg, 0, (size_t)npix * 4 * sizeof(float));
         for (uint32_t spp = 0; spp < st->adjoint_passes; ++spp) {
+            /* decorrelated mode: one seed for the ray generation and one per
+               bounce of every pass, drawn whether or not the bounce has work */
             uint32_t sspp = (uint32_t)mt_next(&mt);
             uint64_t rbase = st->rng_mode == 1 ? sspp : st->random_number;
+            uint32_t *sbounce = (uint32_t *)malloc((st->adjoint_bounces + 1) * sizeof(uint32_t));
+            for (uint32_t b = 0; b < st->adjoint_bounces; ++b) sbounce[b] = (uint32_t)mt_next(&mt);
             /* launchRayGenAdjointKernel (AdjointKernels.cpp:15-84) */
             for (uint32_t p = 0; p < npix; ++p) {
                 rng_t r = rng_make(orc_per_item_seed(rbase, p));
@@ -1687,8 +1691,7 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
             }
             uint32_t active = npix;
             for (uint32_t b = 0; b < st->adjoint_bounces && active > 0; ++b) {
-                uint32_t sb = (uint32_t)mt_next(&mt);
-                uint64_t bbase = st->rng_mode == 1 ? sb : st->random_number;
+                uint64_t bbase = st->rng_mode == 1 ? sbounce[b] : st->random_number;
                 s->stats.adjoint_segments += active;
                 uint64_t nodes = 0, tests = 0;
 #pragma omp parallel for schedule(dynamic, 256) reduction(+ : nodes, tests)
@@ -1749,6 +1752,7 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
                 ray_t *t = q; q = q2; q2 = t;
                 active = m;
             }
+            free(sbounce);
         }
         free(q); free(q2); free(stg); free(pend);
         off += (size_t)npix * 4;
