@@ -52,7 +52,8 @@ class PaleStats(C.Structure):
         "photon_segments", "gather_segments", "adjoint_segments", "photons_stored", "gradient_events",
         "gather_queries", "node_visits", "surfel_tests", "photons_scanned", "gather_node_visits",
         "gather_surfel_tests", "gather_photons_scanned", "kernel_launches")] + \
-        [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms")]
+        [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms", "gather_layer_ms")] + \
+        [("gather_layer_launches", C.c_uint32)]
 
     def as_dict(self) -> Dict[str, float]:
         return {k: getattr(self, k) for k, _ in self._fields_}

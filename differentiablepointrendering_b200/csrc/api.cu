@@ -146,6 +146,8 @@ struct pale_handle {
   DBuf<uint32_t> job_count, job_start;
   // camera-gather wavefront
   uint32_t path_cap = 0;
+  float layer_ms = 0.f;
+  uint32_t layer_launches = 0;
   DBuf<RayRec> cg_q0, cg_q1;
   DBuf<uint32_t> cg_counts;
   DBuf<float4> cg_res, cg_fb;
@@ -562,6 +564,8 @@ void copy_stats(pale_handle* h) {
     h->stats.photon_ms = a;
     h->stats.gather_ms = b;
     h->stats.forward_ms = a + b;
+    h->stats.gather_layer_ms = h->layer_ms;
+    h->stats.gather_layer_launches = h->layer_launches;
   } else if (h->timed == 2) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
@@ -682,6 +686,10 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.res = h->cg_res.p;
   F.fb = h->cg_fb.p;
   F.path_capacity = h->path_cap;
+  h->layer_ms = 0.f;
+  h->layer_launches = 0;
+  F.layer_ms = &h->layer_ms;
+  F.layer_launches = &h->layer_launches;
   camera_gather(F, s);
   CK(cudaEventRecord(h->ev2, s));
   CK(cudaGetLastError());

@@ -127,6 +127,9 @@ struct FrameArgs {
   float4* res;
   float4* fb;
   uint32_t path_capacity;  // >= total_pixels
+  // host side: device time and number of the per-layer launches
+  float* layer_ms;
+  uint32_t* layer_launches;
 };
 
 struct PhotonArgs {

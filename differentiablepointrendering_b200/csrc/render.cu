@@ -500,6 +500,10 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_layer, kBlock, top_smem(a.scene));
   const uint32_t grid = (uint32_t)std::max(1, sms * std::max(1, per_sm));
+  // events around each group of back-to-back layer launches time the layer
+  // kernel alone (the host reads the live count between groups)
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const bool timed = a.layer_ms && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
   for (uint32_t p0 = 0; p0 < a.gather_passes; p0 += ppc) {
     const uint32_t p1 = std::min(a.gather_passes, p0 + ppc);
     const uint32_t n = (p1 - p0) * a.total_pixels;
@@ -507,16 +511,24 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
     k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1); note_launch();
     uint32_t layer = 0;
     while (layer < (uint32_t)kMaxLayers) {
-      for (int k = 0; k < 16 && layer < (uint32_t)kMaxLayers; ++k, ++layer) {
+      if (timed) cudaEventRecord(e0, s);
+      uint32_t group = 0;
+      for (; group < 16 && layer < (uint32_t)kMaxLayers; ++group, ++layer) {
         k_cg_layer<<<grid, kBlock, top_smem(a.scene), s>>>(a, layer); note_launch();
       }
+      if (timed) cudaEventRecord(e1, s);
       uint32_t left = 0;
       cudaMemcpyAsync(&left, a.counts + layer, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
       cudaStreamSynchronize(s);
+      float ms = 0.f;
+      if (timed && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) *a.layer_ms += ms;
+      if (a.layer_launches) *a.layer_launches += group;
       if (left == 0) break;
     }
     k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1, p0 == 0, p1 == a.gather_passes); note_launch();
   }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
 }
 
 // ------------------------------------------------------------- adjoint

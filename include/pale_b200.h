@@ -125,6 +125,9 @@ typedef struct pale_stats {
     float backward_ms;              /* device time of the last adjoint pass  */
     float photon_ms;                /* photon trace + grid build part        */
     float gather_ms;                /* camera gather part                    */
+    float gather_layer_ms;          /* device time of the gather's per-layer
+                                       kernel launches (back-to-back groups) */
+    uint32_t gather_layer_launches; /* ... and their number                  */
 } pale_stats;
 
 /* Fills *s with the reference's PathTracerSettings defaults. */
