@@ -148,7 +148,8 @@ struct pale_handle {
   uint32_t path_cap = 0;
   float layer_ms = 0.f;
   uint32_t layer_launches = 0;
-  DBuf<RayRec> cg_q0, cg_q1;
+  DBuf<RayRec> cg_paths;
+  DBuf<float4> cg_qrec;
   DBuf<uint32_t> cg_counts;
   DBuf<float4> cg_res, cg_fb;
   // run state, seeds, images, gradients
@@ -512,11 +513,12 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->job_count.alloc(2 * kMaxJobsPerBatch);
   h->job_start.alloc(2 * kMaxJobsPerBatch);
   // camera paths in flight: every pass of every pixel when that fits in
-  // 2^25 paths (3.5 GB of queues), else chunks of whole passes
+  // 2^25 paths (4.3 GB of paths, lookup records and results), else chunks of whole
+  // passes
   if (all_pix >= (1ull << 31)) throw ArgError("too many camera pixels");
   const uint64_t want = all_pix * std::max<uint32_t>(1u, st.gather_passes);
   h->path_cap = (uint32_t)std::max<uint64_t>(std::max<uint64_t>(all_pix, 1), std::min<uint64_t>(want, 1ull << 25));
-  h->cg_q0.alloc(h->path_cap); h->cg_q1.alloc(h->path_cap); h->cg_res.alloc(h->path_cap);
+  h->cg_paths.alloc(h->path_cap); h->cg_qrec.alloc(4 * (size_t)h->path_cap); h->cg_res.alloc(h->path_cap);
   h->cg_fb.alloc(std::max<uint64_t>(all_pix, 1));
   h->cg_counts.alloc(kMaxLayers + 2);
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
@@ -680,8 +682,8 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.rng_mode = st.rng_mode;
   F.exposure = st.exposure;
   F.gamma = st.gamma;
-  F.cq[0] = h->cg_q0.p;
-  F.cq[1] = h->cg_q1.p;
+  F.paths = h->cg_paths.p;
+  F.qrec = h->cg_qrec.p;
   F.counts = h->cg_counts.p;
   F.res = h->cg_res.p;
   F.fb = h->cg_fb.p;

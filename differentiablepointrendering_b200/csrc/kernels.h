@@ -120,9 +120,11 @@ struct FrameArgs {
   uint32_t gather_passes;
   uint32_t rng_mode;
   float exposure, gamma;
-  // wavefront buffers: live-path queues, live count per layer
-  // (kMaxLayers + 2 words), per-path radiance, running framebuffer
-  RayRec* cq[2];
+  // wavefront buffers: path queue, lookup records (4 float4 each), queue
+  // length per layer (kMaxLayers + 2 words), per-path radiance, running
+  // framebuffer
+  RayRec* paths;
+  float4* qrec;
   uint32_t* counts;
   float4* res;
   float4* fb;

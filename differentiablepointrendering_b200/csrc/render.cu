@@ -369,88 +369,154 @@ __global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1) {
   rec.o = make_float4(o.x, o.y, o.z, __uint_as_float(path));
   rec.d = make_float4(d.x, d.y, d.z, 1.0f);
   rec.t = make_float4(0.f, 0.f, 0.f, 0.f);
-  A.cq[0][path] = rec;
+  A.paths[path] = rec;
 }
 
-// One surfel layer of every live path (persistent, grid-stride).
-__global__ void __launch_bounds__(kBlock) k_cg_layer(FrameArgs A, uint32_t layer) {
+// Layer step 1: trace.  One lane per queue entry; entries whose path ended
+// in the previous layer's lookup carry path id kInvalid and are skipped.
+// Misses and emitter hits finish their path here; surfel hits and diffuse
+// mesh hits append a lookup record (warp-aggregated atomic on
+// counts[layer + 1]), whose index becomes the path's queue entry for the
+// next layer.
+// Lookup record (4 x float4): (hit position, path) (ray direction or mesh
+// normal, T) (radiance so far, alpha_geom) (surfel or material index, kind).
+enum : uint32_t { kQuerySurfel = 0, kQueryMesh = 1 };
+
+__global__ void __launch_bounds__(kBlock) k_cg_trace(FrameArgs A, uint32_t layer) {
   extern __shared__ BvhNode s_top[];
   stage_top_nodes(A.scene, s_top);
   const SceneView& S = A.scene;
   const uint32_t n = A.counts[layer];
-  const RayRec* __restrict__ qin = A.cq[layer & 1u];
-  RayRec* __restrict__ qout = A.cq[(layer & 1u) ^ 1u];
   const int lane = threadIdx.x & 31;
   TraceCounters ctr{0, 0};
-  uint32_t segs = 0, queries = 0, scanned = 0;
+  uint32_t segs = 0;
   for (uint32_t b = blockIdx.x * kBlock; b < n; b += gridDim.x * kBlock) {
     const uint32_t slot = b + threadIdx.x;
-    bool alive = false;
-    RayRec rec;
+    bool q = false;
+    float4 qa, qb, qc;
+    uint4 qd;
     if (slot < n) {
-      rec = qin[slot];
-      const V3 o = xyz(rec.o), d = xyz(rec.d);
+      const RayRec rec = A.paths[slot];
       const uint32_t path = __float_as_uint(rec.o.w);
-      float T = rec.d.w;
-      V3 acc = xyz(rec.t);
-      ++segs;
-      Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
-      if (h.inst >= (int)S.mesh.instances) {
-        const float4 cn4 = __ldg(&S.sf.cn[h.prim]);
-        V3 nrm = xyz(cn4);
-        if (dot(nrm, -d) < 0.0f) nrm = -nrm;
-        ++queries;
-        V3 E = gather_irradiance(S.grid, h.pos, nrm, scanned);
-        const float4 al = __ldg(&S.sf.alb[h.prim]);
-        V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
-        float ae = __ldg(&S.sf.n[h.prim]).w * h.alpha;
-        acc = acc + scale(Lo, T * ae);
-        T *= (1.0f - ae);
-        V3 no = h.pos + scale(d, 1e-4f);
-        rec.o = make_float4(no.x, no.y, no.z, rec.o.w);
-        rec.d.w = T;
-        rec.t = make_float4(acc.x, acc.y, acc.z, 0.f);
-        alive = layer + 1 < (uint32_t)kMaxLayers;
-        if (!alive) {
-          flag_error(A.st, kErrLayerCap);
-          A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
-        }
-      } else {
-        if (h.inst >= 0) {
-          const float4 mat = __ldg(&S.mesh.materials[__ldg(&S.mesh.material[h.inst])]);
+      if (path != kInvalid) {
+        ++segs;
+        const V3 d = xyz(rec.d);
+        const float T = rec.d.w;
+        V3 acc = xyz(rec.t);
+        const Hit h = intersect_scene(S, s_top, xyz(rec.o), d, ctr, A.st);
+        if (h.inst >= (int)S.mesh.instances) {
+          q = true;
+          qa = make_float4(h.pos.x, h.pos.y, h.pos.z, rec.o.w);
+          qb = make_float4(d.x, d.y, d.z, T);
+          qc = make_float4(acc.x, acc.y, acc.z, h.alpha);
+          qd = make_uint4(h.prim, kQuerySurfel, 0u, 0u);
+        } else if (h.inst >= 0) {
+          const uint32_t mi = __ldg(&S.mesh.material[h.inst]);
+          const float4 mat = __ldg(&S.mesh.materials[mi]);
           if (mat.w > 0.f) {
             V3 Le = scale(xyz(mat), mat.w);
             Le = v3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
             acc = acc + scale(Le, T);
+            A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
           } else {
-            V3 nrm = hit_normal(S, h);
-            ++queries;
-            V3 E = gather_irradiance(S.grid, h.pos, nrm, scanned);
-            V3 Lo = mul(scale(xyz(mat), kInvPi), E);
-            acc = acc + scale(Lo, T);
+            const V3 nrm = hit_normal(S, h);
+            q = true;
+            qa = make_float4(h.pos.x, h.pos.y, h.pos.z, rec.o.w);
+            qb = make_float4(nrm.x, nrm.y, nrm.z, T);
+            qc = make_float4(acc.x, acc.y, acc.z, 0.f);
+            qd = make_uint4(mi, kQueryMesh, 0u, 0u);
           }
+        } else {
+          A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
         }
-        A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
       }
     }
-    // warp-aggregated append of the surviving paths
-    const unsigned ballot = __ballot_sync(0xffffffffu, alive);
+    const unsigned ballot = __ballot_sync(0xffffffffu, q);
     if (ballot) {
       const int leader = __ffs(ballot) - 1;
       uint32_t base = 0;
       if (lane == leader) base = atomicAdd(&A.counts[layer + 1], (uint32_t)__popc(ballot));
       base = __shfl_sync(0xffffffffu, base, leader);
-      if (alive) qout[base + __popc(ballot & ((1u << lane) - 1u))] = rec;
+      if (q) {
+        float4* r = A.qrec + 4 * (size_t)(base + __popc(ballot & ((1u << lane) - 1u)));
+        r[0] = qa;
+        r[1] = qb;
+        r[2] = qc;
+        r[3] = make_float4(__uint_as_float(qd.x), __uint_as_float(qd.y), 0.f, 0.f);
+      }
     }
   }
   warp_count(&A.st->gather_segments, segs);
-  warp_count(&A.st->gather_queries, queries);
-  warp_count(&A.st->photons_scanned, scanned);
   warp_count(&A.st->node_visits, ctr.nodes);
   warp_count(&A.st->surfel_tests, ctr.tests);
-  warp_count(&A.st->gather_photons_scanned, scanned);
   warp_count(&A.st->gather_node_visits, ctr.nodes);
   warp_count(&A.st->gather_surfel_tests, ctr.tests);
+}
+
+// Layer step 2: one warp per lookup record (warps stride over the records,
+// so in deep layers, where few paths are left, every lookup has a warp of
+// its own).  Lane 0 then composites the hit: a surfel adds T*alpha*Lo and
+// passes the path on (record index = queue entry for the next layer); a
+// diffuse mesh hit adds T*Lo and ends the path.
+__global__ void __launch_bounds__(kBlock) k_cg_lookup(FrameArgs A, uint32_t layer) {
+  __shared__ float4 s_terms[kBlock];
+  const SceneView& S = A.scene;
+  const uint32_t n = A.counts[layer + 1];
+  const int lane = threadIdx.x & 31;
+  float4* terms = s_terms + (threadIdx.x & ~31u);
+  const uint32_t warps = gridDim.x * (kBlock / 32);
+  uint32_t queries = 0, scanned = 0;
+  for (uint32_t i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); i < n; i += warps) {
+    const float4* r = A.qrec + 4 * (size_t)i;
+    const float4 qa = r[0], qb = r[1], qc = r[2], qd = r[3];
+    const uint32_t idx = __float_as_uint(qd.x), kind = __float_as_uint(qd.y);
+    const V3 pos = xyz(qa);
+    V3 nrm = xyz(qb);
+    if (kind == kQuerySurfel) {
+      const V3 d = xyz(qb);
+      nrm = xyz(__ldg(&S.sf.cn[idx]));
+      if (dot(nrm, -d) < 0.0f) nrm = -nrm;
+    }
+    uint32_t cnt = 0;
+    const V3 E = gather_irradiance_warp(S.grid, pos, nrm, terms, cnt);
+    if (lane == 0) {
+      ++queries;
+      scanned += cnt;
+      const uint32_t path = __float_as_uint(qa.w);
+      float T = qb.w;
+      V3 acc = xyz(qc);
+      RayRec next;
+      next.o = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
+      next.d = make_float4(0.f, 0.f, 0.f, 0.f);
+      next.t = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (kind == kQuerySurfel) {
+        const V3 d = xyz(qb);
+        const float4 al = __ldg(&S.sf.alb[idx]);
+        V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
+        float ae = __ldg(&S.sf.n[idx]).w * qc.w;
+        acc = acc + scale(Lo, T * ae);
+        T *= (1.0f - ae);
+        if (layer + 1 < (uint32_t)kMaxLayers) {
+          V3 no = pos + scale(d, 1e-4f);
+          next.o = make_float4(no.x, no.y, no.z, qa.w);
+          next.d = make_float4(d.x, d.y, d.z, T);
+          next.t = make_float4(acc.x, acc.y, acc.z, 0.f);
+        } else {
+          flag_error(A.st, kErrLayerCap);
+          A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
+        }
+      } else {
+        const float4 mat = __ldg(&S.mesh.materials[idx]);
+        V3 Lo = mul(scale(xyz(mat), kInvPi), E);
+        acc = acc + scale(Lo, T);
+        A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
+      }
+      A.paths[i] = next;
+    }
+  }
+  warp_count(&A.st->gather_queries, queries);
+  warp_count(&A.st->photons_scanned, scanned);
+  warp_count(&A.st->gather_photons_scanned, scanned);
 }
 
 // fb += res/spp over passes [p0, p1) in pass order; the last chunk writes the
@@ -494,14 +560,17 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
     return;
   }
   const uint32_t ppc = std::max<uint32_t>(1u, std::min(a.gather_passes, a.path_capacity / a.total_pixels));
-  // persistent layer grid: every SM filled once
-  int dev = 0, sms = 148, per_sm = 1;
+  // persistent grids: every SM filled once
+  int dev = 0, sms = 148, per_sm_t = 1, per_sm_l = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_layer, kBlock, top_smem(a.scene));
-  const uint32_t grid = (uint32_t)std::max(1, sms * std::max(1, per_sm));
+  const size_t smem = top_smem(a.scene);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_cg_trace, kBlock, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup, kBlock, 0);
+  const uint32_t grid_t = (uint32_t)std::max(1, sms * std::max(1, per_sm_t));
+  const uint32_t grid_l = (uint32_t)std::max(1, sms * std::max(1, per_sm_l));
   // events around each group of back-to-back layer launches time the layer
-  // kernel alone (the host reads the live count between groups)
+  // kernels alone (the host reads the queue length between groups)
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   const bool timed = a.layer_ms && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
   for (uint32_t p0 = 0; p0 < a.gather_passes; p0 += ppc) {
@@ -514,7 +583,8 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
       if (timed) cudaEventRecord(e0, s);
       uint32_t group = 0;
       for (; group < 16 && layer < (uint32_t)kMaxLayers; ++group, ++layer) {
-        k_cg_layer<<<grid, kBlock, top_smem(a.scene), s>>>(a, layer); note_launch();
+        k_cg_trace<<<grid_t, kBlock, smem, s>>>(a, layer); note_launch();
+        k_cg_lookup<<<grid_l, kBlock, 0, s>>>(a, layer); note_launch();
       }
       if (timed) cudaEventRecord(e1, s);
       uint32_t left = 0;
@@ -522,7 +592,7 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
       cudaStreamSynchronize(s);
       float ms = 0.f;
       if (timed && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) *a.layer_ms += ms;
-      if (a.layer_launches) *a.layer_launches += group;
+      if (a.layer_launches) *a.layer_launches += 2 * group;
       if (left == 0) break;
     }
     k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1, p0 == 0, p1 == a.gather_passes); note_launch();
@@ -739,77 +809,78 @@ __global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t p
   if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, ce);
 }
 
-// launchAdjointTransportKernel (AdjointKernels.cpp:389-509).  Lanes of a
-// warp that update the same surfel add their terms with shuffles first and
-// issue one atomicAdd per surfel.
+// launchAdjointTransportKernel (AdjointKernels.cpp:389-509).  One warp per
+// gradient event (warps stride over the event list): the warp does the
+// photon lookup of the event's end point together (gather_irradiance_warp)
+// and lane 0 adds the event's opacity-gradient term with one atomicAdd.
 __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
+  __shared__ float4 s_terms[kBlock];
   const uint32_t count = A.st->event_count;
-  const uint32_t e = blockIdx.x * kBlock + threadIdx.x;
-  if ((uint64_t)blockIdx.x * kBlock >= count) return;
   const SceneView& S = A.scene;
-  float g = 0.f;
-  uint32_t target = kInvalid;
-  uint32_t pixel = 0;
-  uint32_t queries = 0, scanned = 0;
-  if (e < count) {
+  const int lane = threadIdx.x & 31;
+  float4* terms = s_terms + (threadIdx.x & ~31u);
+  const uint32_t warps = gridDim.x * (kBlock / 32);
+  uint32_t events = 0, queries = 0, scanned = 0;
+  for (uint32_t e = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); e < count; e += warps) {
     const EventRec ev = A.ev.list[e];
     const uint32_t kind = ev.d.x;
-    pixel = ev.d.w;
-    const V3 pos = xyz(ev.a), nrm = xyz(ev.b), thr = xyz(ev.c);
-    if (kind == kKindProjection) {
-      target = ev.d.y;
-      const float4 al = __ldg(&S.sf.alb[target]);
-      ++queries;
-      V3 E = gather_irradiance(S.grid, pos, nrm, scanned);
-      V3 fr = scale(scale(xyz(al), al.w), kInvPi);
-      V3 Lo = mul(fr, E);
-      g = vsum(mul(scale(thr, ev.a.w), Lo)) * A.inv_spp;
-    } else if (kind == kKindNull) {
-      target = ev.d.y;
-      // a surfel endpoint has no material (the reference reads
-      // materials[0xFFFFFFFF], AdjointKernels.cpp:446-447): no contribution
-      if (ev.d.z != kInvalid) {
-        const float4 mat = __ldg(&S.mesh.materials[ev.d.z]);
+    // a null event ending on a surfel has no material (the reference reads
+    // materials[0xFFFFFFFF], AdjointKernels.cpp:446-447): no contribution
+    const bool need = kind == kKindProjection || kind == kKindReflect || (kind == kKindNull && ev.d.z != kInvalid);
+    V3 E = v3(0.f, 0.f, 0.f);
+    uint32_t cnt = 0;
+    if (need) E = gather_irradiance_warp(S.grid, xyz(ev.a), xyz(ev.b), terms, cnt);
+    if (lane == 0) {
+      ++events;
+      if (need) {
         ++queries;
-        V3 Lr = scale(mul(gather_irradiance(S.grid, pos, nrm, scanned), xyz(mat)), kInvPi);
-        V3 Le = v3(0.f, 0.f, 0.f);
-        if (mat.w > 0.f) {
-          float area = A.light0_valid ? A.light0_area : 0.f;
-          Le = scale(scale(xyz(mat), mat.w / (kPi * area)), ev.b.w);
-        }
-        V3 Lo = Le + Lr;
-        g = vsum(mul(scale(thr, -ev.a.w), Lo)) * A.inv_spp;
+        scanned += cnt;
       }
-    } else if (kind == kKindReflect) {
-      target = ev.d.y;
-      const float4 mat = __ldg(&S.mesh.materials[ev.d.z]);
-      ++queries;
-      V3 Lo = scale(mul(gather_irradiance(S.grid, pos, nrm, scanned), xyz(mat)), kInvPi);
-      V3 p = divs(thr, ev.b.w);
-      g = vsum(scale(mul(p, Lo), ev.a.w)) * A.inv_spp;
+      const V3 thr = xyz(ev.c);
+      float g = 0.f;
+      uint32_t target = kInvalid;
+      if (kind == kKindProjection) {
+        target = ev.d.y;
+        const float4 al = __ldg(&S.sf.alb[target < S.sf.count ? target : 0u]);
+        V3 fr = scale(scale(xyz(al), al.w), kInvPi);
+        V3 Lo = mul(fr, E);
+        g = vsum(mul(scale(thr, ev.a.w), Lo)) * A.inv_spp;
+      } else if (kind == kKindNull) {
+        target = ev.d.y;
+        if (ev.d.z != kInvalid) {
+          const float4 mat = __ldg(&S.mesh.materials[ev.d.z]);
+          V3 Lr = scale(mul(E, xyz(mat)), kInvPi);
+          V3 Le = v3(0.f, 0.f, 0.f);
+          if (mat.w > 0.f) {
+            float area = A.light0_valid ? A.light0_area : 0.f;
+            Le = scale(scale(xyz(mat), mat.w / (kPi * area)), ev.b.w);
+          }
+          V3 Lo = Le + Lr;
+          g = vsum(mul(scale(thr, -ev.a.w), Lo)) * A.inv_spp;
+        }
+      } else if (kind == kKindReflect) {
+        target = ev.d.y;
+        const float4 mat = __ldg(&S.mesh.materials[ev.d.z]);
+        V3 Lo = scale(mul(E, xyz(mat)), kInvPi);
+        V3 p = divs(thr, ev.b.w);
+        g = vsum(scale(mul(p, Lo), ev.a.w)) * A.inv_spp;
+      }
+      if (target != kInvalid && target >= S.sf.count) {
+        flag_error(A.st, kErrBounds);
+      } else if (target != kInvalid) {
+        atomicAdd(&A.grad_opacity[target], g);
+        if (A.debug_opacity) {
+          float* px = A.debug_opacity + 4 * (size_t)ev.d.w;
+          atomicAdd(px + 0, g);
+          atomicAdd(px + 1, g);
+          atomicAdd(px + 2, g);
+          px[3] = 1.0f;
+        }
+      }
     }
-    if (target >= S.sf.count && target != kInvalid) {
-      flag_error(A.st, kErrBounds);
-      target = kInvalid;
-    }
+    __syncwarp();
   }
-  const unsigned full = __activemask();
-  const int lane = threadIdx.x & 31;
-  unsigned peers = __match_any_sync(full, target);
-  float sum = 0.f;
-  for (int k = 0; k < 32; ++k) {
-    float v = __shfl_sync(full, g, k);
-    if ((peers >> k) & 1u) sum += v;
-  }
-  if (target != kInvalid && lane == __ffs(peers) - 1) atomicAdd(&A.grad_opacity[target], sum);
-  if (A.debug_opacity && target != kInvalid && e < count) {
-    float* px = A.debug_opacity + 4 * (size_t)pixel;
-    atomicAdd(px + 0, g);
-    atomicAdd(px + 1, g);
-    atomicAdd(px + 2, g);
-    px[3] = 1.0f;
-  }
-  warp_count(&A.st->gradient_events, e < count ? 1u : 0u);
+  warp_count(&A.st->gradient_events, events);
   warp_count(&A.st->gather_queries, queries);
   warp_count(&A.st->photons_scanned, scanned);
 }
@@ -827,7 +898,12 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
   k_job_scan<<<1, kMaxJobsPerBatch, 0, s>>>(a, parity); note_launch();
   k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev); note_launch();
-  k_transport<<<nb, kBlock, 0, s>>>(a); note_launch();
+  // one warp per event: a grid that fills every SM once
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport, kBlock, 0);
+  k_transport<<<(uint32_t)std::max(1, sms * std::max(1, per_sm)), kBlock, 0, s>>>(a); note_launch();
 }
 
 // ------------------------------------------------------ component queries
@@ -863,11 +939,28 @@ void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, c
 
 __global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict__ p, const float* __restrict__ nrm,
                                 float* E) {
-  uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n) return;
-  uint32_t sc = 0;
-  V3 e = gather_irradiance(S.grid, v3(p[3 * i], p[3 * i + 1], p[3 * i + 2]),
-                           v3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]), sc);
+  __shared__ float4 s_terms[kBlock];
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool in = i < n;
+  V3 x = v3(0.f, 0.f, 0.f), nv = v3(0.f, 0.f, 0.f), e = v3(0.f, 0.f, 0.f);
+  if (in) {
+    x = v3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+    nv = v3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
+  }
+  unsigned qm = __ballot_sync(0xffffffffu, in);
+  while (qm) {
+    const int src = __ffs(qm) - 1;
+    qm &= qm - 1u;
+    const V3 qx = v3(__shfl_sync(0xffffffffu, x.x, src), __shfl_sync(0xffffffffu, x.y, src),
+                     __shfl_sync(0xffffffffu, x.z, src));
+    const V3 qv = v3(__shfl_sync(0xffffffffu, nv.x, src), __shfl_sync(0xffffffffu, nv.y, src),
+                     __shfl_sync(0xffffffffu, nv.z, src));
+    uint32_t cnt = 0;
+    const V3 r = gather_irradiance_warp(S.grid, qx, qv, s_terms + (threadIdx.x & ~31u), cnt);
+    if (lane == src) e = r;
+  }
+  if (!in) return;
   E[3 * i] = e.x;
   E[3 * i + 1] = e.y;
   E[3 * i + 2] = e.z;

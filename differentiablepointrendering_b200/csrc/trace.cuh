@@ -385,44 +385,101 @@ __device__ __forceinline__ void world_to_cell(const GridView& G, V3 p, int c[3])
   }
 }
 
-// gatherDiffuseIrradianceAtPoint (KernelHelpers.h:990-1037).  Photons are
+// gatherDiffuseIrradianceAtPoint (KernelHelpers.h:990-1037), done by a
+// whole warp for one query (x, n), which every lane passes.  Photons are
 // stored sorted by cell with ascending deposit index inside a cell, and the
-// cells of one grid row (fixed y, z) are contiguous, so each row is a single
-// contiguous photon range; the summation order equals the reference's
-// cell-by-cell loop.
-__device__ __forceinline__ V3 gather_irradiance(const GridView& G, V3 x, V3 n, uint32_t& scanned) {
+// cells of one grid row (fixed y, z) are contiguous, so each row of the
+// query window is one contiguous photon range and walking the rows in
+// (z, y) order visits the photons in the reference's cell-by-cell order.
+// The rows of the window are concatenated (a warp scan of their lengths),
+// and each round the 32 lanes test 32 consecutive photons of that sequence
+// with coalesced loads.  The sums keep the reference's order: the lanes
+// whose photon passes the radius and cosine tests write their three terms
+// to `terms`, packed in photon order (ballot ranks), and lanes 0, 1 and 2
+// add the x, y and z terms in sequence, so the result equals the
+// reference's one-photon-at-a-time loop bit for bit.  `terms` is this
+// warp's 32 float4 of shared memory.
+// Returns the irradiance in every lane and the photons scanned in `count`.
+__device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3 n, float4* terms, uint32_t& count) {
+  const int lane = threadIdx.x & 31;
   const float r = G.radius, r2 = r * r;
   const float invArea = 1.0f / (kPi * r2);
   int c0[3], c1[3];
   world_to_cell(G, x - v3(r, r, r), c0);
   world_to_cell(G, x + v3(r, r, r), c1);
-  float ex = 0.f, ey = 0.f, ez = 0.f;
-  uint32_t sc = 0;
-  for (int cz = c0[2]; cz <= c1[2]; ++cz) {
-    for (int cy = c0[1]; cy <= c1[1]; ++cy) {
-      uint32_t row = (uint32_t)((cz * G.res[1] + cy) * G.res[0]);
-      uint32_t j0 = __ldg(&G.cell_off[row + c0[0]]);
-      uint32_t j1 = __ldg(&G.cell_off[row + c1[0] + 1]);
-      const uint32_t total = __ldg(&G.cell_off[G.cells]);
-      j1 = j1 < total ? j1 : total;
-      j0 = j0 < j1 ? j0 : j1;
-      sc += j1 - j0;
-      for (uint32_t j = j0; j < j1; ++j) {
-        float4 pa = __ldg(&G.pa[j]);
-        float dx = pa.x - x.x, dy = pa.y - x.y, dz = pa.z - x.z;
-        float d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 > r2) continue;
-        float4 pb = __ldg(&G.pb[j]);
-        float cosine = n.x * (-pb.x) + n.y * (-pb.y) + n.z * (-pb.z);
-        if (cosine < 0.0f) continue;
-        float pcb = __ldg(&G.pc[j]);
-        ex = ex + pa.w * invArea;
-        ey = ey + pb.w * invArea;
-        ez = ez + pcb * invArea;
+  const int ny = c1[1] - c0[1] + 1;
+  const int rows = (c1[2] - c0[2] + 1) * ny;
+  const uint32_t total_ph = __ldg(&G.cell_off[G.cells]);
+  float acc = 0.f;   // lane c < 3: running sum of component c
+  uint32_t scanned = 0;
+  for (int rb = 0; rb < rows; rb += 32) {
+    // this lane's row: offsets and length
+    const int k = rb + lane;
+    uint32_t j0 = 0, len = 0;
+    if (k < rows) {
+      const int cz = c0[2] + k / ny, cy = c0[1] + k % ny;
+      const uint32_t row = (uint32_t)((cz * G.res[1] + cy) * G.res[0]);
+      uint32_t a = __ldg(&G.cell_off[row + c0[0]]);
+      uint32_t b = __ldg(&G.cell_off[row + c1[0] + 1]);
+      b = b < total_ph ? b : total_ph;
+      a = a < b ? a : b;
+      j0 = a;
+      len = b - a;
+    }
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t excl = incl - len;
+    const uint32_t seq = __shfl_sync(0xffffffffu, incl, 31);
+    scanned += seq;
+    for (uint32_t base = 0; base < seq; base += 32) {
+      const uint32_t v = base + lane;
+      // row holding sequence index v: the last lane whose exclusive start <= v
+      int lo = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t s = __shfl_sync(0xffffffffu, excl, lo + step);
+        if (lo + step < 32 && s <= v && (rb + lo + step) < rows) lo += step;
       }
+      const uint32_t rj0 = __shfl_sync(0xffffffffu, j0, lo);
+      const uint32_t rex = __shfl_sync(0xffffffffu, excl, lo);
+      float tx = 0.f, ty = 0.f, tz = 0.f;
+      bool in = false;
+      if (v < seq) {
+        const uint32_t j = rj0 + (v - rex);
+        const float4 pa = __ldg(&G.pa[j]);
+        const float dx = pa.x - x.x, dy = pa.y - x.y, dz = pa.z - x.z;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 <= r2) {
+          const float4 pb = __ldg(&G.pb[j]);
+          const float cosine = n.x * (-pb.x) + n.y * (-pb.y) + n.z * (-pb.z);
+          if (!(cosine < 0.0f)) {
+            in = true;
+            tx = pa.w * invArea;
+            ty = pb.w * invArea;
+            tz = __ldg(&G.pc[j]) * invArea;
+          }
+        }
+      }
+      // accepted terms packed in photon order
+      const unsigned m = __ballot_sync(0xffffffffu, in);
+      if (in) terms[__popc(m & ((1u << lane) - 1u))] = make_float4(tx, ty, tz, 0.f);
+      __syncwarp();
+      if (lane < 3) {
+        const float* t = reinterpret_cast<const float*>(terms) + lane;
+        const int c = __popc(m);
+        for (int q = 0; q < c; ++q) acc = acc + t[4 * q];
+      }
+      __syncwarp();
     }
   }
-  scanned += sc;
+  count += scanned;
+  const float ex = __shfl_sync(0xffffffffu, acc, 0);
+  const float ey = __shfl_sync(0xffffffffu, acc, 1);
+  const float ez = __shfl_sync(0xffffffffu, acc, 2);
   uint32_t T = *G.attempts;
   uint32_t D = (uint64_t)T < G.capacity ? T : (uint32_t)G.capacity;
   if (D == 0u) return v3(0.f, 0.f, 0.f);

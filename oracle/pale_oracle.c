@@ -1797,9 +1797,16 @@ int orc_trace_rays(orc_scene *s, uint32_t n, const float *o, const float *d, int
 }
 int orc_gather_irradiance(orc_scene *s, uint32_t n, const float *pts, const float *nrm, float *E) {
     apply_threads();
-#pragma omp parallel for schedule(dynamic, 64)
-    for (int64_t i = 0; i < (int64_t)n; ++i)
-        vstore(E + 3 * i, gather(s, vload(pts + 3 * i), vload(nrm + 3 * i), NULL));
+    uint64_t scanned = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : scanned)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        uint64_t sc = 0;
+        vstore(E + 3 * i, gather(s, vload(pts + 3 * i), vload(nrm + 3 * i), &sc));
+        scanned += sc;
+    }
+    memset(&s->stats, 0, sizeof(s->stats));
+    s->stats.gather_queries = n;
+    s->stats.photons_scanned = scanned;
     return 0;
 }
 int orc_load_photons(orc_scene *s, uint32_t n, const float *pos, const float *pw, const float *dir) {

@@ -112,6 +112,26 @@ def test_photon_grid_and_lookup_exact(pair):
     np.testing.assert_array_equal(Eg, Eo)
 
 
+def test_dense_lookup_exact(pair):
+    """Thousands of photons per query (a dense cluster, as inside a surfel
+    cloud): many 32-photon rounds per lookup, still bit-exact."""
+    g, o = pair
+    rng = np.random.default_rng(4)
+    n = 100000
+    pos = (rng.normal(size=(n, 3)) * 0.03).astype(np.float32)
+    pw = rng.uniform(0, 1e-4, (n, 3)).astype(np.float32)
+    dr = rng.normal(size=(n, 3))
+    dr = (dr / np.linalg.norm(dr, axis=1, keepdims=True)).astype(np.float32)
+    g.load_photons(pos, pw, dr)
+    o.load_photons(pos, pw, dr)
+    q = (rng.normal(size=(1000, 3)) * 0.03).astype(np.float32)
+    nq = rng.normal(size=(1000, 3))
+    nq = (nq / np.linalg.norm(nq, axis=1, keepdims=True)).astype(np.float32)
+    Eg, Eo = g.gather_irradiance(q, nq), o.gather_irradiance(q, nq)
+    assert o.stats()["photons_scanned"] > 1000 * 1000
+    np.testing.assert_array_equal(Eg, Eo)
+
+
 def test_forward_images_match_oracle(pair, box):
     g, o = pair
     ig, io = g.render_forward(), o.render_forward()
