@@ -28,7 +28,8 @@ class PaleSettings(C.Structure):
                 ("seed", C.c_uint64), ("random_number", C.c_uint32), ("rr_start", C.c_uint32),
                 ("q_null", C.c_float), ("q_reflect", C.c_float), ("q_transmit", C.c_float),
                 ("gather_radius", C.c_float), ("leaf_size", C.c_uint32), ("rng_mode", C.c_uint32),
-                ("debug_images", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float)]
+                ("debug_images", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float),
+                ("null_weight", C.c_uint32)]
 
 
 class PalePoints(C.Structure):
@@ -88,6 +89,9 @@ def settings_from_dict(d: Optional[dict]) -> PaleSettings:
             continue
         if k == "rng_mode":
             s.rng_mode = {"reference": 0, "decorrelated": 1}.get(v, v) if isinstance(v, str) else int(v)
+            continue
+        if k == "null_weight":
+            s.null_weight = {"reference": 0, "unbiased": 1}.get(v, v) if isinstance(v, str) else int(v)
             continue
         if k not in SETTINGS_KEYS:
             raise KeyError(f"unknown renderer setting '{k}'")
@@ -183,6 +187,7 @@ def load_library() -> C.CDLL:
         "pale_camera_count": (C.c_int, [H, u32p]),
         "pale_camera_info": (C.c_int, [H, C.c_uint32, C.c_char_p, u32p, u32p]),
         "pale_render_forward": (C.c_int, [H, C.c_uint32, u32p, f32p, f32p]),
+        "pale_render_gather": (C.c_int, [H, C.c_uint32, u32p, f32p, f32p]),
         "pale_render_forward_device": (C.c_int, [H, C.c_uint32, u32p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "pale_render_backward": (C.c_int, [H, C.c_uint32, u32p, f32p, C.POINTER(PalePoints), f32p]),
         "pale_render_backward_device": (C.c_int, [H, C.c_uint32, u32p, C.c_void_p, C.POINTER(PalePoints),
@@ -192,6 +197,7 @@ def load_library() -> C.CDLL:
         "pale_apply_points": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_rebuild": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_trace_rays": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, i32p, f32p, f32p, f32p]),
+        "pale_trace_transmittance": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, f32p, f32p]),
         "pale_gather_irradiance": (C.c_int, [H, C.c_uint32, f32p, f32p, f32p]),
         "pale_load_photons": (C.c_int, [H, C.c_uint32, f32p, f32p, f32p]),
         "pale_get_photons": (C.c_int, [H, u32p, f32p, f32p, f32p, u32p, u32p, f32p]),
@@ -210,10 +216,10 @@ def load_library() -> C.CDLL:
 
 
 EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_create", "pale_destroy",
-            "pale_point_count", "pale_camera_count", "pale_camera_info", "pale_render_forward",
+            "pale_point_count", "pale_camera_count", "pale_camera_info", "pale_render_forward", "pale_render_gather",
             "pale_render_forward_device", "pale_render_backward", "pale_render_backward_device",
             "pale_get_points", "pale_get_order", "pale_apply_points", "pale_rebuild", "pale_trace_rays",
-            "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
+            "pale_trace_transmittance", "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
             "pale_get_stats", "pale_build_lbvh_noalloc")
 NOALLOC_MAX_SURFELS = 16384
 

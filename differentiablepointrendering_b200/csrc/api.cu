@@ -155,6 +155,7 @@ struct pale_handle {
   // run state, seeds, images, gradients
   DBuf<RunState> run;
   DBuf<uint32_t> seeds_fwd, seeds_adj;
+  DBuf<uint32_t> cam_cursor;   // seed cursor after the last photon pass
   DBuf<float> img_raw, img_ldr, dldi, dbg;
   PointsBufs grads;
   pale_stats stats{};
@@ -493,6 +494,8 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->g_scan_temp.alloc(scan_temp_words(h->cells + 1));
   h->g_stored.alloc(1);
   h->g_attempts.alloc(1);
+  h->cam_cursor.alloc(1);
+  CK(cudaMemsetAsync(h->cam_cursor.p, 0, 4, s));
   CK(cudaMemsetAsync(h->g_stored.p, 0, 4, s));
   CK(cudaMemsetAsync(h->g_attempts.p, 0, 4, s));
   CK(cudaMemsetAsync(h->g_cell_off.p, 0, ((size_t)h->cells + 1) * 4, s));
@@ -614,7 +617,11 @@ void validate_cams(pale_handle* h, uint32_t nsel, const uint32_t* idx) {
 }
 
 // Forward render into the handle's packed device images.
-uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr, bool sync) {
+// trace_photons false: the camera gather alone, from the current photon
+// map (the last forward's or loaded photons), with the camera seeds the
+// last forward used.
+uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr, bool sync,
+                 bool trace_photons = true) {
   cudaStream_t s = h->stream;
   const uint64_t launches0 = launches_issued();
   const pale_settings& st = h->st;
@@ -649,25 +656,31 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   P.q_reflect = st.q_reflect;
   P.q_transmit = st.q_transmit;
   if (st.photons_per_launch > h->qcap) throw ArgError("photons per launch exceed the queue capacity");
-  for (uint32_t pass = 0; pass < st.forward_passes; ++pass) {
-    photon_emit(P, s);
-    for (uint32_t b = 0; b < st.max_bounces; ++b) photon_bounce(P, b & 1u, s);
+  uint32_t* cursor = &h->run.p->seed_cursor;
+  if (!trace_photons) {
+    CK(cudaMemcpyAsync(cursor, h->cam_cursor.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  } else {
+    for (uint32_t pass = 0; pass < st.forward_passes; ++pass) {
+      photon_emit(P, s);
+      for (uint32_t b = 0; b < st.max_bounces; ++b) photon_bounce(P, b & 1u, s);
+    }
+    GridBufs G{};
+    G.cell_id = h->g_cell_id.p;
+    G.sorted = h->g_sorted.p;
+    G.keys_tmp = h->g_keys.p;
+    G.vals_tmp = h->g_vals_tmp.p;
+    G.sort_temp = h->g_sort_temp.p;
+    G.cell_count = h->g_cell_count.p;
+    G.cell_off = h->g_cell_off.p;
+    G.scan_temp = h->g_scan_temp.p;
+    G.pa = h->g_pa.p;
+    G.pb = h->g_pb.p;
+    G.pc = h->g_pc.p;
+    G.d_stored = h->g_stored.p;
+    G.d_attempts = h->g_attempts.p;
+    grid_build(sv, h->run.p, P.ps, G, h->cells, h->key_bits, s);
+    CK(cudaMemcpyAsync(h->cam_cursor.p, cursor, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
   }
-  GridBufs G{};
-  G.cell_id = h->g_cell_id.p;
-  G.sorted = h->g_sorted.p;
-  G.keys_tmp = h->g_keys.p;
-  G.vals_tmp = h->g_vals_tmp.p;
-  G.sort_temp = h->g_sort_temp.p;
-  G.cell_count = h->g_cell_count.p;
-  G.cell_off = h->g_cell_off.p;
-  G.scan_temp = h->g_scan_temp.p;
-  G.pa = h->g_pa.p;
-  G.pb = h->g_pb.p;
-  G.pc = h->g_pc.p;
-  G.d_stored = h->g_stored.p;
-  G.d_attempts = h->g_attempts.p;
-  grid_build(sv, h->run.p, P.ps, G, h->cells, h->key_bits, s);
   CK(cudaEventRecord(h->ev1, s));
   FrameArgs F{};
   F.scene = sv;
@@ -747,6 +760,7 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.inv_spp = 1.0f / (float)st.adjoint_passes;
   A.fixed_seed = st.random_number;
   A.rng_mode = st.rng_mode;
+  A.null_scale = st.null_weight == PALE_NULL_WEIGHT_UNBIASED ? 1.0f / st.q_null : 1.0f;
   A.light0_valid = h->n_lights > 0;
   A.light0_area = h->light0_area;
   // jobs in the reference's order (camera-major, then pass), packed into
@@ -839,6 +853,7 @@ void pale_default_settings(pale_settings* s) {
   s->gather_radius = 0.01f;
   s->leaf_size = 4;
   s->rng_mode = PALE_RNG_REFERENCE;
+  s->null_weight = PALE_NULL_WEIGHT_REFERENCE;
   s->debug_images = 0;
   s->exposure = 1.0f;
   s->gamma = 2.2f;
@@ -858,6 +873,9 @@ int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale
     if (h->st.gather_passes == 0 || h->st.adjoint_passes == 0) throw ArgError("gather and adjoint passes must be > 0");
     if (!(h->st.gather_radius > 0.f)) throw ArgError("gather radius must be > 0");
     if (h->st.adjoint_bounces > 255) throw ArgError("at most 255 adjoint bounces are supported");
+    if (h->st.null_weight > PALE_NULL_WEIGHT_UNBIASED) throw ArgError("null_weight must be reference or unbiased");
+    if (h->st.null_weight == PALE_NULL_WEIGHT_UNBIASED && !(h->st.q_null > 0.f))
+      throw ArgError("unbiased null weighting needs q_null > 0");
     check_points(&desc->points, "pale_create");
     if (desc->points.count >= (1u << 28)) throw ArgError("at most 2^28 surfels are supported");
     CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
@@ -916,6 +934,23 @@ int pale_render_forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, floa
     h->img_raw.ensure(4 * std::max<size_t>(1, pix));
     h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
     forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, true);
+    if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+    if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PALE_OK;
+  });
+}
+
+int pale_render_gather(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* ldr, float* raw) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    validate_cams(h, nsel, idx);
+    size_t pix = 0;
+    for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    use_stream(h, h->own_stream);
+    h->img_raw.ensure(4 * std::max<size_t>(1, pix));
+    h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
+    forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, true, false);
     if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
     if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -1067,6 +1102,32 @@ int pale_trace_rays(pale_handle* h, uint32_t n, const float* o, const float* d, 
     CK(cudaMemcpyAsync(t, dT.p, 4ull * n, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(alpha, dA.p, 4ull * n, cudaMemcpyDeviceToHost, s));
     if (pos) CK(cudaMemcpyAsync(pos, dP.p, 12ull * n, cudaMemcpyDeviceToHost, s));
+    h->timed = 0;
+    h->launches_last = 1;
+    copy_stats(h);
+    return PALE_OK;
+  });
+}
+
+int pale_trace_transmittance(pale_handle* h, uint32_t n, const float* o, const float* d, int32_t* inst, float* t,
+                             float* transmit) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    if (n && (!o || !d || !inst || !t || !transmit)) throw ArgError("pale_trace_transmittance: null array");
+    if (!n) return PALE_OK;
+    use_stream(h, h->own_stream);
+    cudaStream_t s = h->stream;
+    DBuf<float> dO, dD, dT, dX;
+    DBuf<int32_t> dI;
+    dO.alloc(3ull * n); dD.alloc(3ull * n); dT.alloc(n); dX.alloc(n); dI.alloc(n);
+    CK(cudaMemcpyAsync(dO.p, o, 12ull * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dD.p, d, 12ull * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+    trace_transmittance(h->view(), h->run.p, n, dO.p, dD.p, dI.p, dT.p, dX.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(inst, dI.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(t, dT.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(transmit, dX.p, 4ull * n, cudaMemcpyDeviceToHost, s));
     h->timed = 0;
     h->launches_last = 1;
     copy_stats(h);

@@ -179,6 +179,7 @@ struct AdjointArgs {
   float inv_spp;
   uint32_t fixed_seed;     // reference mode: settings.random.number
   uint32_t rng_mode;
+  float null_scale;        // NullTransmittance weight: 1 or 1 / q_null
   uint32_t light0_valid;
   float light0_area;
 };
@@ -194,6 +195,8 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
 // Component queries.
 void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d, int32_t* inst,
                 int32_t* prim, float* t, float* alpha, float* pos, cudaStream_t s);
+void trace_transmittance(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d,
+                         int32_t* inst, float* t, float* transmit, cudaStream_t s);
 void gather_points(const SceneView& sv, uint32_t n, const float* p, const float* nrm, float* E, cudaStream_t s);
 void load_photon_arrays(uint32_t n, const float* pos, const float* pw, const float* dir, const PhotonStore& ps,
                         cudaStream_t s);

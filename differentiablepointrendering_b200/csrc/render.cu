@@ -856,7 +856,7 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
             Le = scale(scale(xyz(mat), mat.w / (kPi * area)), ev.b.w);
           }
           V3 Lo = Le + Lr;
-          g = vsum(mul(scale(thr, -ev.a.w), Lo)) * A.inv_spp;
+          g = vsum(mul(scale(thr, -ev.a.w * A.null_scale), Lo)) * A.inv_spp;
         }
       } else if (kind == kKindReflect) {
         target = ev.d.y;
@@ -935,6 +935,35 @@ void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, c
                 int32_t* prim, float* t, float* alpha, float* pos, cudaStream_t s) {
   if (n == 0) return;
   k_trace_rays<<<blocks_for(n), kBlock, top_smem(sv), s>>>(sv, st, n, o, d, inst, prim, t, alpha, pos); note_launch();
+}
+
+// Transmit-mode scene query, one ray per thread: the closest mesh hit and
+// the surfel cloud's transmissivity (intersect_scene_transmit).  The walk
+// is bounded at 2^16 surfel hits per ray.
+__global__ void __launch_bounds__(kBlock) k_trace_transmittance(SceneView S, RunState* st, uint32_t n,
+                                                                const float* __restrict__ o,
+                                                                const float* __restrict__ d, int32_t* inst,
+                                                                float* t, float* transmit) {
+  extern __shared__ BvhNode s_top[];
+  stage_top_nodes(S, s_top);
+  uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  TraceCounters ctr{0, 0};
+  float T = 1.0f;
+  Hit h = intersect_scene_transmit(S, s_top, v3(o[3 * i], o[3 * i + 1], o[3 * i + 2]),
+                                   v3(d[3 * i], d[3 * i + 1], d[3 * i + 2]), T, 1u << 16, ctr, st);
+  inst[i] = h.inst;
+  t[i] = h.inst >= 0 ? h.t : 3.402823466e+38f;
+  transmit[i] = T;
+  atomicAdd(&st->node_visits, (unsigned long long)ctr.nodes);
+  atomicAdd(&st->surfel_tests, (unsigned long long)ctr.tests);
+}
+
+void trace_transmittance(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d,
+                         int32_t* inst, float* t, float* transmit, cudaStream_t s) {
+  if (n == 0) return;
+  k_trace_transmittance<<<blocks_for(n), kBlock, top_smem(sv), s>>>(sv, st, n, o, d, inst, t, transmit);
+  note_launch();
 }
 
 __global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict__ p, const float* __restrict__ nrm,

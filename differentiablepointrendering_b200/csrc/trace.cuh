@@ -105,12 +105,13 @@ __device__ __forceinline__ void load_node(const SceneView& S, const BvhNode* __r
   }
 }
 
-// Closest surfel with t in (1e-5, limit) along (o, d) (the surfel cloud's
+// Closest surfel with t in (tmin, limit) along (o, d) (the surfel cloud's
 // transform is the identity, so this is intersectBLASPointCloudFirstHit,
-// IntersectionKernels.h:585-675).  Returns false on a miss.
+// IntersectionKernels.h:585-675, where tmin is rayEpsilon = 1e-5).  Returns
+// false on a miss.
 __device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
-                                               float limit, uint32_t& prim, float& t, V3& x, float& alpha,
-                                               TraceCounters& ctr, RunState* st) {
+                                               float tmin, float limit, uint32_t& prim, float& t, V3& x,
+                                               float& alpha, TraceCounters& ctr, RunState* st) {
   if (S.node_count == 0) return false;
   const V3 inv = safe_inv(d);
   float best = limit;
@@ -151,7 +152,7 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode
         float th, aa;
         V3 xx;
         ctr.tests++;
-        if (surfel_hit(S.sf, f0 + j, o, d, 1e-5f, best, th, xx, aa)) {
+        if (surfel_hit(S.sf, f0 + j, o, d, tmin, best, th, xx, aa)) {
           best = th;
           hit = true;
           prim = f0 + j;
@@ -192,19 +193,17 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode
   return hit;
 }
 
-// intersectScene, FirstHit mode: mesh instances in object space
-// (intersectBLASMesh, IntersectionKernels.h:37-105) and the surfel cloud;
-// the closest world-space distance wins (:1060-1081).
-__device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
-                                               TraceCounters& ctr, RunState* st) {
+// The closest mesh hit, in object space per instance (intersectBLASMesh,
+// IntersectionKernels.h:37-105); `best` is the world distance of the hit
+// (+inf on a miss).
+__device__ __forceinline__ Hit intersect_meshes(const SceneView& S, V3 o, V3 d, V3 invw, float& best) {
   Hit h;
   h.inst = -1;
   h.prim = 0;
   h.t = 3.402823466e+38f;
   h.alpha = 0.f;
   h.pos = v3(0.f, 0.f, 0.f);
-  float best = __int_as_float(0x7f800000);
-  const V3 invw = safe_inv(d);
+  best = __int_as_float(0x7f800000);
   const MeshView& M = S.mesh;
   for (uint32_t i = 0; i < M.instances; ++i) {
     const float4 lo = __ldg(&M.box[2 * i]), hi = __ldg(&M.box[2 * i + 1]);
@@ -244,6 +243,16 @@ __device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode
       h.alpha = 0.0f;
     }
   }
+  return h;
+}
+
+// intersectScene, FirstHit mode: mesh instances, then the surfel cloud;
+// the closest world-space distance wins (:1060-1081).
+__device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
+                                               TraceCounters& ctr, RunState* st) {
+  float best;
+  const V3 invw = safe_inv(d);
+  Hit h = intersect_meshes(S, o, d, invw, best);
   if (S.has_pc &&
       entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best), best)) {
     V3 dd = normalize(d);
@@ -253,17 +262,53 @@ __device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode
     uint32_t prim;
     float t, a;
     V3 x;
-    if (surfel_closest(S, smem_top, o, dd, limit, prim, t, x, a, ctr, st)) {
+    if (surfel_closest(S, smem_top, o, dd, 1e-5f, limit, prim, t, x, a, ctr, st)) {
       float tw = dot(x - o, d);
       if (tw > 0.0f && tw < best) {
         best = tw;
-        h.inst = (int)M.instances;
+        h.inst = (int)S.mesh.instances;
         h.t = tw;
         h.pos = x;
         h.prim = prim;
         h.alpha = a;
       }
     }
+  }
+  return h;
+}
+
+// intersectScene, Transmit mode (:1066-1090): the closest mesh hit, and the
+// surfel cloud's transmissivity T over the whole ray
+// (intersectBLASPointCloudTransmit, :837-948): the successive closest
+// surfels from the same origin, t in (tMin, inf) with tMin = t_hit + 1e-4
+// after each hit (the reference rejects t <= tMin after intersectSurfel's
+// t > 1e-5, and tMin >= 1e-5), T *= 1 - opacity * alpha_geom, stopping once
+// T <= 0.001.  The cloud is skipped (T = 1) when its box starts beyond the
+// mesh hit, as the instance loop culls it.  `max_hits` bounds the walk (the
+// kernel flags kErrLayerCap when it is reached).
+__device__ __forceinline__ Hit intersect_scene_transmit(const SceneView& S, const BvhNode* __restrict__ smem_top,
+                                                        V3 o, V3 d, float& T, uint32_t max_hits,
+                                                        TraceCounters& ctr, RunState* st) {
+  float best;
+  const V3 invw = safe_inv(d);
+  Hit h = intersect_meshes(S, o, d, invw, best);
+  T = 1.0f;
+  if (S.has_pc &&
+      entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best), best)) {
+    const V3 dd = normalize(d);
+    float tmin = 1e-5f;
+    uint32_t k = 0;
+    for (; k < max_hits; ++k) {
+      uint32_t prim;
+      float t, a;
+      V3 x;
+      if (!surfel_closest(S, smem_top, o, dd, tmin, __int_as_float(0x7f800000), prim, t, x, a, ctr, st)) break;
+      const float alpha_eff = __ldg(&S.sf.n[prim]).w * a;
+      T *= 1.0f - alpha_eff;
+      tmin = t + 1e-4f;
+      if (T <= 0.001f) break;
+    }
+    if (k == max_hits) flag_error(st, kErrLayerCap);
   }
   return h;
 }

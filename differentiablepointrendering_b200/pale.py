@@ -92,14 +92,22 @@ class Renderer:
     def render_forward(self, camera_name: str = "") -> Dict[str, np.ndarray]:
         """{cam: LDR (H,W,4), cam+'_raw': HDR (H,W,4)} float32
         (render_forward, pale_bindings.cpp:180-277)."""
+        return self._render(camera_name, self._lib.pale_render_forward, "render_forward")
+
+    def render_gather(self, camera_name: str = "") -> Dict[str, np.ndarray]:
+        """render_forward without retracing the photons: the camera gather
+        from the current photon map (the last forward's or loaded photons),
+        with the last forward's camera seeds."""
+        return self._render(camera_name, self._lib.pale_render_gather, "render_gather")
+
+    def _render(self, camera_name, fn, what) -> Dict[str, np.ndarray]:
         idx = [i for i, n in enumerate(self._names) if (not camera_name or n == camera_name)]
         pix = sum(self._sizes[i][0] * self._sizes[i][1] for i in idx)
         ldr = np.empty(max(1, pix) * 4, np.float32)
         raw = np.empty(max(1, pix) * 4, np.float32)
         cams = N.cams_array(idx)
-        rc = self._lib.pale_render_forward(self._h, len(idx), cams.ctypes.data_as(N.u32p),
-                                           ldr.ctypes.data_as(N.f32p), raw.ctypes.data_as(N.f32p))
-        _check(self._lib, self._h, rc, "render_forward")
+        rc = fn(self._h, len(idx), cams.ctypes.data_as(N.u32p), ldr.ctypes.data_as(N.f32p), raw.ctypes.data_as(N.f32p))
+        _check(self._lib, self._h, rc, what)
         out, off = {}, 0
         for i in idx:
             w, h = self._sizes[i]
@@ -342,6 +350,19 @@ class Renderer:
                                        t.ctypes.data_as(N.f32p), a.ctypes.data_as(N.f32p), p.ctypes.data_as(N.f32p))
         _check(self._lib, self._h, rc, "trace_rays")
         return inst, prim, t, a, p
+
+    def trace_transmittance(self, origins: np.ndarray, directions: np.ndarray):
+        """Transmit-mode queries: (mesh instance, world t, transmissivity of
+        the surfel cloud along the ray)."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        inst, t, T = np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+        rc = self._lib.pale_trace_transmittance(self._h, n, o.ctypes.data_as(N.f32p), d.ctypes.data_as(N.f32p),
+                                                inst.ctypes.data_as(N.i32p), t.ctypes.data_as(N.f32p),
+                                                T.ctypes.data_as(N.f32p))
+        _check(self._lib, self._h, rc, "trace_transmittance")
+        return inst, t, T
 
     def gather_irradiance(self, points: np.ndarray, normals: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(points, np.float32).reshape(-1, 3)

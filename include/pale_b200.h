@@ -41,6 +41,16 @@ typedef struct pale_handle pale_handle;
 /* Renderer settings.  Field <- settings-dict key of the reference
  * (pale_bindings.cpp:123-139; PathTracerSettings, GPUDataStructures.h:407-422).
  * Fill with pale_default_settings() first. */
+/* Weight of the adjoint's NullTransmittance gradient events.  The
+ * reference completes a pending null event with throughput
+ * (p / qNull) * qNull = p (AdjointKernels.cpp:171-204, 314-323), but a path
+ * only takes the null branch with probability qNull, so the events' expected
+ * sum is qNull times the occlusion term of d(image)/d(opacity).  REFERENCE
+ * keeps that weighting (gradients identical to the reference's); UNBIASED
+ * divides the term by qNull. */
+#define PALE_NULL_WEIGHT_REFERENCE 0u
+#define PALE_NULL_WEIGHT_UNBIASED 1u
+
 typedef struct pale_settings {
     uint32_t photons_per_launch;   /* "photons"          (default 1e6)       */
     uint32_t max_bounces;          /* "bounces"          (6)                 */
@@ -60,6 +70,7 @@ typedef struct pale_settings {
     uint32_t debug_images;         /* "debug_images"                         */
     float exposure;                /* SensorGPU::exposureCorrection (1.0)    */
     float gamma;                   /* SensorGPU::gammaCorrection   (2.2)     */
+    uint32_t null_weight;          /* PALE_NULL_WEIGHT_*                     */
 } pale_settings;
 
 /* Per-point parameter block (structure of arrays, float32).
@@ -167,6 +178,18 @@ int pale_render_forward(pale_handle *h, uint32_t num_selected,
                         const uint32_t *camera_indices, float *ldr_out,
                         float *raw_out);
 
+/* The camera gather alone (launchCameraGatherKernel + post-process) from
+ * the current photon map: the last forward's, or photons given to
+ * pale_load_photons.  The camera seeds are those the last forward used, so
+ * right after pale_render_forward it returns the same images.  With the
+ * photon map held fixed, finite differences of these images are what the
+ * adjoint pass differentiates (it does not follow the photon map).  Host
+ * pointers, layout as pale_render_forward.  No counterpart in the reference,
+ * which always retraces the photons. */
+int pale_render_gather(pale_handle *h, uint32_t num_selected,
+                       const uint32_t *camera_indices, float *ldr_out,
+                       float *raw_out);
+
 /* Same render, but the LDR/RAW images are written to DEVICE pointers
  * (no host copies).  `stream` is a cudaStream_t or NULL. */
 int pale_render_forward_device(pale_handle *h, uint32_t num_selected,
@@ -214,6 +237,16 @@ int pale_trace_rays(pale_handle *h, uint32_t n, const float *origins,
                     const float *directions, int32_t *instance,
                     int32_t *primitive, float *t, float *alpha_geom,
                     float *hit_position);
+
+/* Transmittance queries (intersectScene in Transmit mode,
+ * IntersectionKernels.h:1066-1090, with intersectBLASPointCloudTransmit,
+ * :837-948): for n host rays, the closest mesh hit (instance, -1 = miss;
+ * world t, FLT_MAX on a miss) and the surfel cloud's transmissivity
+ * T = prod(1 - opacity * alpha_geom) over the successive surfel hits along
+ * the ray (stopping once T <= 0.001). */
+int pale_trace_transmittance(pale_handle *h, uint32_t n, const float *origins,
+                             const float *directions, int32_t *instance,
+                             float *t, float *transmissivity);
 
 /* Irradiance lookups in the current photon map
  * (gatherDiffuseIrradianceAtPoint, KernelHelpers.h:990-1037). */

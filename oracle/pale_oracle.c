@@ -203,6 +203,10 @@ typedef struct {
 struct orc_scene {
     orc_settings st;
     int bvh_kind;
+    /* seed stream position after the last photon pass: where the camera
+     * seeds of a gather-only render start */
+    mt64_t cam_mt;
+    int cam_mt_valid;
     /* meshes */
     uint32_t nv, nt, nm, nmat, ninst, ncam;
     float *verts; uint32_t *tris; uint32_t *mranges; float *mats;
@@ -715,9 +719,11 @@ static inline int surfel_hit(v3 o, v3 d, const point_t *sf, float tmin, float tm
 
 typedef struct { uint64_t nodes, tests; } trav_ctr;
 
-/* intersectBLASPointCloudFirstHit (IntersectionKernels.h:585-675). */
-static int blas_firsthit(const orc_scene *s, v3 o, v3 d, uint32_t *prim, float *t, v3 *x,
-                         float *alpha, trav_ctr *ctr) {
+/* intersectBLASPointCloudFirstHit (IntersectionKernels.h:585-675): the
+ * closest surfel with t in (tmin, inf); tmin is 1e-5 (rayEpsilon) except
+ * in the transmittance walk below. */
+static int blas_firsthit_from(const orc_scene *s, v3 o, v3 d, float tmin, uint32_t *prim, float *t, v3 *x,
+                              float *alpha, trav_ctr *ctr) {
     if (!s->nnodes) return 0;
     v3 inv = safe_inv(d);
     float best = INFINITY;
@@ -748,7 +754,7 @@ static int blas_firsthit(const orc_scene *s, v3 o, v3 d, uint32_t *prim, float *
             float th, a;
             v3 xx;
             if (ctr) ctr->tests++;
-            if (!surfel_hit(o, d, &s->pts[idx], 1e-5f, best, &th, &xx, &a)) continue;
+            if (!surfel_hit(o, d, &s->pts[idx], tmin, best, &th, &xx, &a)) continue;
             hit = 1;
             best = th;
             *prim = idx;
@@ -760,10 +766,35 @@ static int blas_firsthit(const orc_scene *s, v3 o, v3 d, uint32_t *prim, float *
     return hit;
 }
 
+static int blas_firsthit(const orc_scene *s, v3 o, v3 d, uint32_t *prim, float *t, v3 *x,
+                         float *alpha, trav_ctr *ctr) {
+    return blas_firsthit_from(s, o, d, 1e-5f, prim, t, x, alpha, ctr);
+}
+
+/* intersectBLASPointCloudTransmit (IntersectionKernels.h:837-948): walks the
+ * successive closest surfels along the whole ray from the same origin
+ * (t in (tMin, inf), tMin = t_hit + 1e-4 after each hit; the reference
+ * rejects t <= tMin after intersectSurfel's t > 1e-5, and tMin >= 1e-5) and
+ * returns T = prod(1 - opacity * alpha_geom), stopping once T <= 0.001. */
+static float blas_transmit(const orc_scene *s, v3 o, v3 d, trav_ctr *ctr) {
+    float T = 1.0f, tmin = 1e-5f;
+    for (uint32_t guard = 0; guard < (1u << 22); ++guard) {
+        uint32_t prim;
+        float t, a;
+        v3 x;
+        if (!blas_firsthit_from(s, o, d, tmin, &prim, &t, &x, &a, ctr)) break;
+        float alpha_eff = s->pts[prim].opacity * a;
+        T *= 1.0f - alpha_eff;
+        tmin = t + 1e-4f;
+        if (T <= 0.001f) break;
+    }
+    return T;
+}
+
 /* intersectScene in FirstHit mode (IntersectionKernels.h:954-1097):
  * closest world-space hit over the mesh instances (object-space
  * Moller-Trumbore, intersectBLASMesh :37-105) and the surfel cloud. */
-static hit_t intersect_scene(const orc_scene *s, v3 o, v3 d, trav_ctr *ctr) {
+static hit_t intersect_scene_mode(const orc_scene *s, v3 o, v3 d, trav_ctr *ctr, float *transmit) {
     hit_t h;
     memset(&h, 0, sizeof(h));
     h.inst = -1;
@@ -813,7 +844,10 @@ static hit_t intersect_scene(const orc_scene *s, v3 o, v3 d, trav_ctr *ctr) {
             uint32_t prim;
             float t, a;
             v3 x;
-            if (blas_firsthit(s, o, dd, &prim, &t, &x, &a, ctr)) {
+            /* Transmit mode (:1066-1090): the cloud adds no surface hit, only
+             * its transmissivity over the whole ray */
+            if (transmit) *transmit = blas_transmit(s, o, dd, ctr);
+            else if (blas_firsthit(s, o, dd, &prim, &t, &x, &a, ctr)) {
                 float tw = vdot(vsub(x, o), d);
                 if (tw > 0.0f && tw < best) {
                     best = tw;
@@ -842,6 +876,10 @@ static hit_t intersect_scene(const orc_scene *s, v3 o, v3 d, trav_ctr *ctr) {
         }
     }
     return h;
+}
+
+static hit_t intersect_scene(const orc_scene *s, v3 o, v3 d, trav_ctr *ctr) {
+    return intersect_scene_mode(s, o, d, ctr, NULL);
 }
 
 /* ---------------------------------------------------------------- sampling */
@@ -1405,6 +1443,8 @@ static void postprocess(const orc_scene *s, const float *raw, float *ldr, uint32
     }
 }
 
+static void gather_cameras(orc_scene *s, mt64_t mt, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw);
+
 int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw) {
     apply_threads();
     memset(&s->stats, 0, sizeof(s->stats));
@@ -1413,7 +1453,33 @@ int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float 
     mt_seed(&mt, s->st.seed);
     photon_pass(s, &mt);
     build_grid(s);
+    s->cam_mt = mt;
+    s->cam_mt_valid = 1;
     double t1 = now_ms();
+    gather_cameras(s, mt, nsel, cams, ldr, raw);
+    double t2 = now_ms();
+    s->stats.photon_ms = (float)(t1 - t0);
+    s->stats.gather_ms = (float)(t2 - t1);
+    s->stats.forward_ms = (float)(t2 - t0);
+    return 0;
+}
+
+/* The camera gather alone, from the current photon map (the last forward's
+ * or loaded ones), with the camera seeds a forward render uses. */
+int orc_render_gather(orc_scene *s, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw) {
+    apply_threads();
+    memset(&s->stats, 0, sizeof(s->stats));
+    mt64_t mt;
+    if (s->cam_mt_valid) mt = s->cam_mt;
+    else mt_seed(&mt, s->st.seed);
+    double t1 = now_ms();
+    gather_cameras(s, mt, nsel, cams, ldr, raw);
+    s->stats.gather_ms = (float)(now_ms() - t1);
+    s->stats.forward_ms = s->stats.gather_ms;
+    return 0;
+}
+
+static void gather_cameras(orc_scene *s, mt64_t mt, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw) {
     size_t off = 0;
     for (uint32_t ci = 0; ci < nsel; ++ci) {
         uint32_t cam = cams[ci];
@@ -1448,11 +1514,6 @@ int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float 
         off += (size_t)npix * 4;
         free(fb);
     }
-    double t2 = now_ms();
-    s->stats.photon_ms = (float)(t1 - t0);
-    s->stats.gather_ms = (float)(t2 - t1);
-    s->stats.forward_ms = (float)(t2 - t0);
-    return 0;
 }
 
 /* --------------------------------------------------------- adjoint pass */
@@ -1630,7 +1691,10 @@ static float transport_event(const orc_scene *s, const event_t *e, float invSpp,
             Le = vscale(vscale(bc, mat[3] / (M_PIf_ * area)), e->end_cos);
         }
         v3 Lo = vadd(Le, Lr);
-        v3 g = vmul(vscale(e->thr, -e->alpha), Lo);
+        /* the reference's weighting: thr, on a branch taken with
+         * probability q_null; null_weight 1 divides by q_null */
+        float w = s->st.null_weight == 1 ? -e->alpha / s->st.q_null : -e->alpha;
+        v3 g = vmul(vscale(e->thr, w), Lo);
         return vsum(g) * invSpp;
     }
     if (e->kind == PK_REFLECT) {
@@ -1789,6 +1853,28 @@ int orc_trace_rays(orc_scene *s, uint32_t n, const float *o, const float *d, int
         t[i] = h.hit ? h.t : FLT_MAX;
         alpha[i] = h.hit ? h.alpha : 0.f;
         if (hitpos) vstore(hitpos + 3 * i, h.hit ? h.pos : V3(0, 0, 0));
+    }
+    memset(&s->stats, 0, sizeof(s->stats));
+    s->stats.node_visits = nodes;
+    s->stats.surfel_tests = tests;
+    return 0;
+}
+/* intersectScene in Transmit mode: closest mesh hit (instance, world t;
+ * -1 and FLT_MAX on a miss) and the surfel cloud's transmissivity. */
+int orc_trace_transmittance(orc_scene *s, uint32_t n, const float *o, const float *d, int32_t *inst, float *t,
+                            float *transmit) {
+    apply_threads();
+    uint64_t nodes = 0, tests = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : nodes, tests)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        trav_ctr c = {0, 0};
+        float T = 1.0f;
+        hit_t h = intersect_scene_mode(s, vload(o + 3 * i), vload(d + 3 * i), &c, &T);
+        nodes += c.nodes;
+        tests += c.tests;
+        inst[i] = h.hit ? h.inst : -1;
+        t[i] = h.hit ? h.t : FLT_MAX;
+        transmit[i] = T;
     }
     memset(&s->stats, 0, sizeof(s->stats));
     s->stats.node_visits = nodes;

@@ -38,6 +38,7 @@ typedef struct orc_settings {
     float q_null, q_reflect, q_transmit, gather_radius;
     uint32_t leaf_size, rng_mode, debug_images;
     float exposure, gamma;
+    uint32_t null_weight;   /* 0 reference, 1 unbiased (divide by q_null) */
 } orc_settings;
 
 typedef struct orc_points {
@@ -61,7 +62,8 @@ typedef struct orc_stats {
     uint64_t photon_segments, gather_segments, adjoint_segments, photons_stored;
     uint64_t gradient_events, gather_queries, node_visits, surfel_tests, photons_scanned;
     uint64_t gather_node_visits, gather_surfel_tests, gather_photons_scanned, kernel_launches;
-    float forward_ms, backward_ms, photon_ms, gather_ms;
+    float forward_ms, backward_ms, photon_ms, gather_ms, gather_layer_ms;
+    uint32_t gather_layer_launches;
 } orc_stats;
 
 typedef struct orc_scene orc_scene;
@@ -77,10 +79,13 @@ int orc_get_points(const orc_scene *s, orc_points *out);
 int orc_apply_points(orc_scene *s, const orc_points *p);
 int orc_rebuild(orc_scene *s, const orc_points *asset);
 int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw);
+int orc_render_gather(orc_scene *s, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw);
 int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const float *dldi,
                         orc_points *grads, float *debug_opacity);
 int orc_trace_rays(orc_scene *s, uint32_t n, const float *o, const float *d, int32_t *inst,
                    int32_t *prim, float *t, float *alpha, float *hitpos);
+int orc_trace_transmittance(orc_scene *s, uint32_t n, const float *o, const float *d, int32_t *inst, float *t,
+                            float *transmit);
 int orc_gather_irradiance(orc_scene *s, uint32_t n, const float *pts, const float *nrm, float *E);
 int orc_load_photons(orc_scene *s, uint32_t n, const float *pos, const float *pw, const float *dir);
 int orc_get_photons(orc_scene *s, uint32_t *count, float *pos, float *pw, float *dir,

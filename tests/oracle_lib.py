@@ -38,8 +38,10 @@ def lib() -> C.CDLL:
             "orc_apply_points": (C.c_int, [P, C.POINTER(N.PalePoints)]),
             "orc_rebuild": (C.c_int, [P, C.POINTER(N.PalePoints)]),
             "orc_render_forward": (C.c_int, [P, C.c_uint32, N.u32p, N.f32p, N.f32p]),
+            "orc_render_gather": (C.c_int, [P, C.c_uint32, N.u32p, N.f32p, N.f32p]),
             "orc_render_backward": (C.c_int, [P, C.c_uint32, N.u32p, N.f32p, C.POINTER(N.PalePoints), N.f32p]),
             "orc_trace_rays": (C.c_int, [P, C.c_uint32, N.f32p, N.f32p, N.i32p, N.i32p, N.f32p, N.f32p, N.f32p]),
+            "orc_trace_transmittance": (C.c_int, [P, C.c_uint32, N.f32p, N.f32p, N.i32p, N.f32p, N.f32p]),
             "orc_gather_irradiance": (C.c_int, [P, C.c_uint32, N.f32p, N.f32p, N.f32p]),
             "orc_load_photons": (C.c_int, [P, C.c_uint32, N.f32p, N.f32p, N.f32p]),
             "orc_get_photons": (C.c_int, [P, N.u32p, N.f32p, N.f32p, N.f32p, N.u32p, N.u32p, N.f32p]),
@@ -98,12 +100,18 @@ class OracleRenderer:
         return int(self.L.orc_point_count(self.h))
 
     def render_forward(self, camera_name: str = "") -> Dict[str, np.ndarray]:
+        return self._render(camera_name, self.L.orc_render_forward)
+
+    def render_gather(self, camera_name: str = "") -> Dict[str, np.ndarray]:
+        return self._render(camera_name, self.L.orc_render_gather)
+
+    def _render(self, camera_name, fn) -> Dict[str, np.ndarray]:
         idx = [i for i, n in enumerate(self.names) if (not camera_name or n == camera_name)]
         pix = sum(self.sizes[i][0] * self.sizes[i][1] for i in idx)
         ldr = np.empty(max(1, pix) * 4, np.float32)
         raw = np.empty(max(1, pix) * 4, np.float32)
         cams = np.asarray(idx, np.uint32)
-        assert self.L.orc_render_forward(self.h, len(idx), uptr(cams), fptr(ldr), fptr(raw)) == 0
+        assert fn(self.h, len(idx), uptr(cams), fptr(ldr), fptr(raw)) == 0
         out, off = {}, 0
         for i in idx:
             w, h = self.sizes[i]
@@ -159,6 +167,14 @@ class OracleRenderer:
         self.L.orc_trace_rays(self.h, n, fptr(o), fptr(d), inst.ctypes.data_as(N.i32p), prim.ctypes.data_as(N.i32p),
                               fptr(t), fptr(a), fptr(p))
         return inst, prim, t, a, p
+
+    def trace_transmittance(self, o, d):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        inst, t, T = np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self.L.orc_trace_transmittance(self.h, n, fptr(o), fptr(d), inst.ctypes.data_as(N.i32p), fptr(t), fptr(T))
+        return inst, t, T
 
     def gather_irradiance(self, pts, nrm):
         x = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
