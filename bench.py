@@ -110,14 +110,35 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- helpers
-def algorithmic_bytes_gather(st: dict) -> float:
-    """Algorithmic bytes of the camera gather's layer launches: per ray
-    segment 96 B (48 B path record read, 48 B survivor or result written),
-    32 B per BVH node visited, 52 B per surfel test; per photon scanned 36 B
-    and per photon-map query 8 B per grid row range read (two offsets, 25
-    rows)."""
-    return (96.0 * st["gather_segments"] + 32.0 * st["gather_node_visits"] + 52.0 * st["gather_surfel_tests"]
-            + 36.0 * st["gather_photons_scanned"] + 8.0 * 25.0 * st["gather_queries_fwd"])
+# Algorithmic bytes per kernel of one step, from the device counters:
+# a ray segment reads/writes 32 + 32 B of ray state and a 16 B hit record,
+# 32 B per BVH node visited and 52 B per surfel test; a photon lookup reads
+# 36 B per photon scanned and 8 B (two cell offsets) per grid row of its
+# window (25 rows); the adjoint bounce also reads and writes its 48 B
+# pending state; a gradient event is a 64 B record, its lookup and an 8 B
+# atomic read-modify-write.
+ROWS_PER_QUERY = 25
+
+
+def kernel_bytes(sf: dict, sb: dict) -> dict:
+    seg = lambda segs, nodes, tests: 80.0 * segs + 32.0 * nodes + 52.0 * tests
+    look = lambda q, scanned: 36.0 * scanned + 8.0 * ROWS_PER_QUERY * q
+    fwd_q = sf["gather_queries"]
+    adj_q = sb["gather_queries"]
+    return {
+        "k_cg_trace": seg(sf["gather_segments"], sf["gather_node_visits"], sf["gather_surfel_tests"]),
+        "k_cg_lookup": look(fwd_q, sf["gather_photons_scanned"]),
+        "k_adj_bounce": seg(sb["adjoint_segments"], sb["node_visits"], sb["surfel_tests"])
+        + 96.0 * sb["adjoint_segments"],
+        "k_transport": 72.0 * sb["gradient_events"] + look(adj_q, sb["photons_scanned"]),
+    }
+
+
+def kernel_times(sf: dict, sb: dict) -> dict:
+    return {"k_cg_trace": (sf["trace_ms"], sf["trace_launches"]),
+            "k_cg_lookup": (sf["lookup_ms"], sf["lookup_launches"]),
+            "k_adj_bounce": (sb["adjoint_bounce_ms"], sb["adjoint_bounce_launches"]),
+            "k_transport": (sb["transport_ms"], sb["transport_launches"])}
 
 
 def read_peaks():
@@ -237,9 +258,6 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     sb = frame.stats()
     rays = sf["photon_segments"] + sf["gather_segments"] + sb["adjoint_segments"]
     launches = int(sf["kernel_launches"] + sb["kernel_launches"])
-    gather_ms = sf["gather_ms"]
-    gstats = dict(sf)
-    gstats["gather_queries_fwd"] = sf["gather_queries"]
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -305,12 +323,20 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         return
     peaks = read_peaks()
     hbm = peaks["hbm_gbs"] if peaks else 6650.0
-    # dominant kernel: the camera gather's per-layer launch (k_cg_layer)
-    ab = algorithmic_bytes_gather(gstats)
-    layer_ms = sf["gather_layer_ms"] or gather_ms
-    layer_launches = max(1, int(sf["gather_layer_launches"]))
-    achieved = ab / (layer_ms / 1e3) / 1e9
-    traffic = read_traffic("k_cg_layer")
+    # per-kernel device time (events around every launch, stats step) and
+    # algorithmic bytes; the roofline entry is the kernel with the most time
+    kb, kt = kernel_bytes(sf, sb), kernel_times(sf, sb)
+    kernels = {}
+    for k in kb:
+        ms, n = kt[k]
+        n = max(1, int(n))
+        ach = kb[k] / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        kernels[k] = {"ms_per_step": round(ms, 3), "launches": n, "launch_ms": round(ms / n, 4),
+                      "algorithmic_bytes_per_launch": int(kb[k] / n), "achieved_gbs": round(ach, 1),
+                      "frac": round(ach / hbm, 4)}
+    top = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    achieved = kernels[top]["achieved_gbs"]
+    traffic = read_traffic(top)
     cpu_val, cpu_secs, cpu_desc = cpu_sample_run(w, steps=1) if not args.skip_cpu else (None, 0, "skipped")
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
@@ -322,11 +348,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "gpu_launches": launches * args.steps,
-        "roofline": {"kernel": "k_cg_layer", "bound": "hbm", "achieved": round(achieved, 1),
+        "roofline": {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
-                     "algorithmic_bytes_per_launch": int(ab / layer_launches),
-                     "launch_ms": round(layer_ms / layer_launches, 4), "launches_per_step": layer_launches},
+                     "algorithmic_bytes_per_launch": kernels[top]["algorithmic_bytes_per_launch"],
+                     "launch_ms": kernels[top]["launch_ms"], "launches_per_step": kernels[top]["launches"]},
+        "kernels": kernels,
         "cpu_baseline": {"value": round(cpu_val, 4) if cpu_val else None, "unit": "Mrays/s",
                          "cores": os.cpu_count(), "kind": "port", "sample": cpu_desc},
         "clocks": clk,

@@ -53,11 +53,17 @@ class PaleStats(C.Structure):
         "photon_segments", "gather_segments", "adjoint_segments", "photons_stored", "gradient_events",
         "gather_queries", "node_visits", "surfel_tests", "photons_scanned", "gather_node_visits",
         "gather_surfel_tests", "gather_photons_scanned", "kernel_launches")] + \
-        [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms", "gather_layer_ms")] + \
-        [("gather_layer_launches", C.c_uint32)]
+        [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms")] + \
+        [("timed_ms", C.c_float * 4), ("timed_launches", C.c_uint32 * 4)]
+
+    TIMED = ("trace", "lookup", "adjoint_bounce", "transport")
 
     def as_dict(self) -> Dict[str, float]:
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        out = {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("timed")}
+        for i, name in enumerate(self.TIMED):
+            out[f"{name}_ms"] = float(self.timed_ms[i])
+            out[f"{name}_launches"] = int(self.timed_launches[i])
+        return out
 
 
 # Settings-dict keys of the reference (pale_bindings.cpp:123-139) plus the

@@ -146,8 +146,7 @@ struct pale_handle {
   DBuf<uint32_t> job_count, job_start;
   // camera-gather wavefront
   uint32_t path_cap = 0;
-  float layer_ms = 0.f;
-  uint32_t layer_launches = 0;
+  KernelTimer timer;          // device time of the hot kernels of the last call
   DBuf<RayRec> cg_paths;
   DBuf<float4> cg_qrec;
   DBuf<uint32_t> cg_counts;
@@ -569,14 +568,17 @@ void copy_stats(pale_handle* h) {
     h->stats.photon_ms = a;
     h->stats.gather_ms = b;
     h->stats.forward_ms = a + b;
-    h->stats.gather_layer_ms = h->layer_ms;
-    h->stats.gather_layer_launches = h->layer_launches;
   } else if (h->timed == 2) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->stats.backward_ms = ms;
   }
   h->timed = 0;
+  for (int k = 0; k < kTimedKernels; ++k) {
+    h->stats.timed_ms[k] = 0.f;
+    h->stats.timed_launches[k] = 0;
+  }
+  h->timer.collect(h->stats.timed_ms, h->stats.timed_launches);
   h->stats.photon_segments = rs.photon_segments;
   h->stats.gather_segments = rs.gather_segments;
   h->stats.adjoint_segments = rs.adjoint_segments;
@@ -623,6 +625,7 @@ void validate_cams(pale_handle* h, uint32_t nsel, const uint32_t* idx) {
 uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr, bool sync,
                  bool trace_photons = true) {
   cudaStream_t s = h->stream;
+  h->timer.used = 0;
   const uint64_t launches0 = launches_issued();
   const pale_settings& st = h->st;
   validate_cams(h, nsel, idx);
@@ -701,10 +704,7 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.res = h->cg_res.p;
   F.fb = h->cg_fb.p;
   F.path_capacity = h->path_cap;
-  h->layer_ms = 0.f;
-  h->layer_launches = 0;
-  F.layer_ms = &h->layer_ms;
-  F.layer_launches = &h->layer_launches;
+  F.timer = &h->timer;
   camera_gather(F, s);
   CK(cudaEventRecord(h->ev2, s));
   CK(cudaGetLastError());
@@ -731,6 +731,7 @@ void zero_grads(pale_handle* h, cudaStream_t s) {
 // Adjoint pass reading packed dL/dI at d_dldi (device).
 void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi, float* d_dbg, bool sync) {
   cudaStream_t s = h->stream;
+  h->timer.used = 0;
   const uint64_t launches0 = launches_issued();
   const pale_settings& st = h->st;
   validate_cams(h, nsel, idx);
@@ -763,6 +764,7 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.null_scale = st.null_weight == PALE_NULL_WEIGHT_UNBIASED ? 1.0f / st.q_null : 1.0f;
   A.light0_valid = h->n_lights > 0;
   A.light0_area = h->light0_area;
+  A.timer = &h->timer;
   // jobs in the reference's order (camera-major, then pass), packed into
   // batches of at most adj_cap paths and kMaxJobsPerBatch jobs
   std::vector<CameraRec> sel(nsel);

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -52,6 +53,24 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32
                       uint32_t n_max, int bits, uint32_t* temp, cudaStream_t s);
 void lbvh_build(const LbvhArgs& a, cudaStream_t s);
 void derive_surfels(const PointsDev& p, uint32_t n, const SurfelArrays& d, cudaStream_t s);
+
+// Device time of the hot kernels: a pair of CUDA events around every launch
+// of a timed kernel, summed per kernel after the stream is synchronised.
+// Host-side only (kernels receive the pointer inside their argument
+// structs but never touch it).
+enum TimedKernel : int { kTimeTrace = 0, kTimeLookup = 1, kTimeAdjBounce = 2, kTimeTransport = 3, kTimedKernels = 4 };
+
+struct KernelTimer {
+  std::vector<cudaEvent_t> pool;   // start, end, start, end, ...
+  std::vector<int> kind;
+  size_t used = 0;
+  bool open = false;
+  void begin(int k, cudaStream_t s);
+  void end(cudaStream_t s);
+  // Adds the elapsed times of the recorded pairs to ms[] / n[] and starts over.
+  void collect(float* ms, uint32_t* n);
+  ~KernelTimer();
+};
 
 // ------------------------------------------------------------ rendering
 struct QueueBufs {
@@ -129,9 +148,7 @@ struct FrameArgs {
   float4* res;
   float4* fb;
   uint32_t path_capacity;  // >= total_pixels
-  // host side: device time and number of the per-layer launches
-  float* layer_ms;
-  uint32_t* layer_launches;
+  KernelTimer* timer;      // host side, may be null
 };
 
 struct PhotonArgs {
@@ -182,6 +199,7 @@ struct AdjointArgs {
   float null_scale;        // NullTransmittance weight: 1 or 1 / q_null
   uint32_t light0_valid;
   float light0_area;
+  KernelTimer* timer;      // host side, may be null
 };
 
 void photon_emit(const PhotonArgs& a, cudaStream_t s);

@@ -569,10 +569,6 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup, kBlock, 0);
   const uint32_t grid_t = (uint32_t)std::max(1, sms * std::max(1, per_sm_t));
   const uint32_t grid_l = (uint32_t)std::max(1, sms * std::max(1, per_sm_l));
-  // events around each group of back-to-back layer launches time the layer
-  // kernels alone (the host reads the queue length between groups)
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  const bool timed = a.layer_ms && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
   for (uint32_t p0 = 0; p0 < a.gather_passes; p0 += ppc) {
     const uint32_t p1 = std::min(a.gather_passes, p0 + ppc);
     const uint32_t n = (p1 - p0) * a.total_pixels;
@@ -580,25 +576,22 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
     k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1); note_launch();
     uint32_t layer = 0;
     while (layer < (uint32_t)kMaxLayers) {
-      if (timed) cudaEventRecord(e0, s);
-      uint32_t group = 0;
-      for (; group < 16 && layer < (uint32_t)kMaxLayers; ++group, ++layer) {
+      for (uint32_t group = 0; group < 16 && layer < (uint32_t)kMaxLayers; ++group, ++layer) {
+        if (a.timer) a.timer->begin(kTimeTrace, s);
         k_cg_trace<<<grid_t, kBlock, smem, s>>>(a, layer); note_launch();
+        if (a.timer) a.timer->end(s);
+        if (a.timer) a.timer->begin(kTimeLookup, s);
         k_cg_lookup<<<grid_l, kBlock, 0, s>>>(a, layer); note_launch();
+        if (a.timer) a.timer->end(s);
       }
-      if (timed) cudaEventRecord(e1, s);
+      // the host reads the queue length after each group of 16 layers
       uint32_t left = 0;
       cudaMemcpyAsync(&left, a.counts + layer, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
       cudaStreamSynchronize(s);
-      float ms = 0.f;
-      if (timed && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) *a.layer_ms += ms;
-      if (a.layer_launches) *a.layer_launches += 2 * group;
       if (left == 0) break;
     }
     k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1, p0 == 0, p1 == a.gather_passes); note_launch();
   }
-  if (e0) cudaEventDestroy(e0);
-  if (e1) cudaEventDestroy(e1);
 }
 
 // ------------------------------------------------------------- adjoint
@@ -894,7 +887,9 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
   const uint32_t nb = blocks_for(npaths);
   if (nb == 0) return;
   const uint32_t parity = bounce & 1u;
+  if (a.timer) a.timer->begin(kTimeAdjBounce, s);
   k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce); note_launch();
+  if (a.timer) a.timer->end(s);
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
   k_job_scan<<<1, kMaxJobsPerBatch, 0, s>>>(a, parity); note_launch();
   k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev); note_launch();
@@ -903,7 +898,9 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport, kBlock, 0);
+  if (a.timer) a.timer->begin(kTimeTransport, s);
   k_transport<<<(uint32_t)std::max(1, sms * std::max(1, per_sm)), kBlock, 0, s>>>(a); note_launch();
+  if (a.timer) a.timer->end(s);
 }
 
 // ------------------------------------------------------ component queries
@@ -1013,6 +1010,46 @@ void load_photon_arrays(uint32_t n, const float* pos, const float* pw, const flo
                         cudaStream_t s) {
   if (n == 0) return;
   k_load_photons<<<blocks_for(n), kBlock, 0, s>>>(n, pos, pw, dir, ps); note_launch();
+}
+
+// ----------------------------------------------------------- KernelTimer
+void KernelTimer::begin(int k, cudaStream_t s) {
+  if (2 * used + 2 > pool.size()) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+      if (a) cudaEventDestroy(a);
+      open = false;
+      return;
+    }
+    pool.push_back(a);
+    pool.push_back(b);
+  }
+  if (kind.size() <= used) kind.resize(used + 1);
+  kind[used] = k;
+  cudaEventRecord(pool[2 * used], s);
+  open = true;
+}
+
+void KernelTimer::end(cudaStream_t s) {
+  if (!open) return;
+  cudaEventRecord(pool[2 * used + 1], s);
+  ++used;
+  open = false;
+}
+
+void KernelTimer::collect(float* ms, uint32_t* n) {
+  for (size_t i = 0; i < used; ++i) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, pool[2 * i], pool[2 * i + 1]) == cudaSuccess) {
+      ms[kind[i]] += t;
+      n[kind[i]] += 1;
+    }
+  }
+  used = 0;
+}
+
+KernelTimer::~KernelTimer() {
+  for (cudaEvent_t e : pool) cudaEventDestroy(e);
 }
 
 }  // namespace pale

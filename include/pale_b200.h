@@ -136,9 +136,11 @@ typedef struct pale_stats {
     float backward_ms;              /* device time of the last adjoint pass  */
     float photon_ms;                /* photon trace + grid build part        */
     float gather_ms;                /* camera gather part                    */
-    float gather_layer_ms;          /* device time of the gather's per-layer
-                                       kernel launches (back-to-back groups) */
-    uint32_t gather_layer_launches; /* ... and their number                  */
+    float timed_ms[4];              /* device time of the hot kernels: camera
+                                       trace, photon lookup, adjoint bounce,
+                                       adjoint transport (CUDA events around
+                                       each launch)                          */
+    uint32_t timed_launches[4];     /* ... and their launch counts           */
 } pale_stats;
 
 /* Fills *s with the reference's PathTracerSettings defaults. */

@@ -62,8 +62,9 @@ typedef struct orc_stats {
     uint64_t photon_segments, gather_segments, adjoint_segments, photons_stored;
     uint64_t gradient_events, gather_queries, node_visits, surfel_tests, photons_scanned;
     uint64_t gather_node_visits, gather_surfel_tests, gather_photons_scanned, kernel_launches;
-    float forward_ms, backward_ms, photon_ms, gather_ms, gather_layer_ms;
-    uint32_t gather_layer_launches;
+    float forward_ms, backward_ms, photon_ms, gather_ms;
+    float timed_ms[4];
+    uint32_t timed_launches[4];
 } orc_stats;
 
 typedef struct orc_scene orc_scene;
