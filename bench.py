@@ -105,7 +105,15 @@ class ClockSampler:
                     reasons.add(name)
         os.unlink(self.path)
         sm.sort()
+        # other processes computing on this GPU would slow every kernel down
+        try:
+            apps = subprocess.run(["nvidia-smi", f"--id={self.idx}", "--query-compute-apps=pid",
+                                   "--format=csv,noheader"], capture_output=True, text=True, timeout=20).stdout
+            procs = len([x for x in apps.split() if x.strip()])
+        except Exception:
+            procs = None
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "compute_processes": procs,
                 "samples": len(sm)}
 
 

@@ -602,6 +602,11 @@ void copy_stats(pale_handle* h) {
 
 // Makes `s` the stream of the following work, ordered after everything
 // already queued on the previous stream of this handle.
+// The stream a device entry point runs on: the caller's, where NULL is the
+// default stream (the legacy stream), so that the work is ordered with the
+// caller's default-stream work.
+cudaStream_t caller_stream(void* stream) { return stream ? (cudaStream_t)stream : cudaStreamLegacy; }
+
 void use_stream(pale_handle* h, cudaStream_t s) {
   if (s == h->stream) return;
   cudaEvent_t e;
@@ -967,7 +972,7 @@ int pale_render_forward_device(pale_handle* h, uint32_t nsel, const uint32_t* id
     validate_cams(h, nsel, idx);
     size_t pix = 0;
     for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
-    use_stream(h, stream ? (cudaStream_t)stream : h->own_stream);
+    use_stream(h, caller_stream(stream));
     h->img_raw.ensure(4 * std::max<size_t>(1, pix));
     forward(h, nsel, idx, d_raw ? d_raw : h->img_raw.p, d_ldr, false);
     return PALE_OK;
@@ -1007,7 +1012,7 @@ int pale_render_backward_device(pale_handle* h, uint32_t nsel, const uint32_t* i
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
     validate_cams(h, nsel, idx);
-    use_stream(h, stream ? (cudaStream_t)stream : h->own_stream);
+    use_stream(h, caller_stream(stream));
     backward(h, nsel, idx, d_dldi, nullptr, false);
     if (d_grads) {
       const size_t n = h->np;

@@ -193,7 +193,9 @@ int pale_render_gather(pale_handle *h, uint32_t num_selected,
                        float *raw_out);
 
 /* Same render, but the LDR/RAW images are written to DEVICE pointers
- * (no host copies).  `stream` is a cudaStream_t or NULL. */
+ * (no host copies).  `stream` is a cudaStream_t; NULL is the default
+ * (legacy) stream.  The call returns without waiting for the work, except
+ * that the camera gather reads one queue length per 16 surfel layers. */
 int pale_render_forward_device(pale_handle *h, uint32_t num_selected,
                                const uint32_t *camera_indices, float *d_ldr,
                                float *d_raw, void *stream);
@@ -208,7 +210,8 @@ int pale_render_backward(pale_handle *h, uint32_t num_selected,
                          const uint32_t *camera_indices, const float *dldi,
                          pale_points *grads, float *debug_opacity);
 
-/* Same adjoint pass with DEVICE pointers for dL/dI and the gradient fields. */
+/* Same adjoint pass with DEVICE pointers for dL/dI and the gradient fields,
+ * enqueued on `stream` (NULL = the default stream) without waiting. */
 int pale_render_backward_device(pale_handle *h, uint32_t num_selected,
                                 const uint32_t *camera_indices,
                                 const float *d_dldi, pale_points *d_grads,
