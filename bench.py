@@ -221,6 +221,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     from differentiablepointrendering_b200.build import build_library
     from differentiablepointrendering_b200.device import DeviceFrame, l2_grad_
+    from differentiablepointrendering_b200.multigpu import reduce_gradients, view_offset
     from differentiablepointrendering_b200.pale import Renderer
     from differentiablepointrendering_b200.scene import jitter_target, make_box_scene, make_surfels
 
@@ -230,7 +231,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     w = WORKLOADS[args.workload]
     st = settings_for(w)
     pts = make_surfels(w["n"], 1234)
-    offset = rank / max(1, world)          # rank r renders views rotated by r/N of the spacing
+    offset = view_offset(rank, world)      # rank r renders views rotated by r/N of the spacing
     scene = make_box_scene(w["n"], cameras=w["cams"], resolution=w["res"], points=pts, ring_offset=offset)
     tscene = scene.with_points(jitter_target(pts, 5678))
 
@@ -252,8 +253,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         l2_grad_(frame.dldi, frame.ldr, target)
         frame.backward()
         if world > 1:
-            for g in frame.grads.values():
-                dist.all_reduce(g)
+            reduce_gradients(frame.grads)
 
     for _ in range(args.warmup):
         step()
