@@ -466,9 +466,17 @@ __global__ void __launch_bounds__(kBlock) k_cg_lookup(FrameArgs A, uint32_t laye
   float4* terms = s_terms + (threadIdx.x & ~31u);
   const uint32_t warps = gridDim.x * (kBlock / 32);
   uint32_t queries = 0, scanned = 0;
-  for (uint32_t i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); i < n; i += warps) {
-    const float4* r = A.qrec + 4 * (size_t)i;
-    const float4 qa = r[0], qb = r[1], qc = r[2], qd = r[3];
+  // lanes 0-15 hold the 16 floats of the next record, loaded one query ahead
+  uint32_t i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+  float pre = (i < n && lane < 16) ? reinterpret_cast<const float*>(A.qrec + 4 * (size_t)i)[lane] : 0.f;
+  for (; i < n; i += warps) {
+    const float cur = pre;
+    if (i + warps < n && lane < 16) pre = reinterpret_cast<const float*>(A.qrec + 4 * (size_t)(i + warps))[lane];
+    auto field = [&](int f) { return __shfl_sync(0xffffffffu, cur, f); };
+    const float4 qa = make_float4(field(0), field(1), field(2), field(3));
+    const float4 qb = make_float4(field(4), field(5), field(6), field(7));
+    const float4 qc = make_float4(field(8), field(9), field(10), field(11));
+    const float4 qd = make_float4(field(12), field(13), field(14), field(15));
     const uint32_t idx = __float_as_uint(qd.x), kind = __float_as_uint(qd.y);
     const V3 pos = xyz(qa);
     V3 nrm = xyz(qb);
@@ -814,8 +822,19 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
   float4* terms = s_terms + (threadIdx.x & ~31u);
   const uint32_t warps = gridDim.x * (kBlock / 32);
   uint32_t events = 0, queries = 0, scanned = 0;
-  for (uint32_t e = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); e < count; e += warps) {
-    const EventRec ev = A.ev.list[e];
+  // lanes 0-15 hold the 16 words of the next event, loaded one event ahead
+  uint32_t e = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+  float pre = (e < count && lane < 16) ? reinterpret_cast<const float*>(A.ev.list + e)[lane] : 0.f;
+  for (; e < count; e += warps) {
+    const float cur = pre;
+    if (e + warps < count && lane < 16) pre = reinterpret_cast<const float*>(A.ev.list + e + warps)[lane];
+    auto field = [&](int f) { return __shfl_sync(0xffffffffu, cur, f); };
+    EventRec ev;
+    ev.a = make_float4(field(0), field(1), field(2), field(3));
+    ev.b = make_float4(field(4), field(5), field(6), field(7));
+    ev.c = make_float4(field(8), field(9), field(10), field(11));
+    ev.d = make_uint4(__float_as_uint(field(12)), __float_as_uint(field(13)), __float_as_uint(field(14)),
+                      __float_as_uint(field(15)));
     const uint32_t kind = ev.d.x;
     // a null event ending on a surfel has no material (the reference reads
     // materials[0xFFFFFFFF], AdjointKernels.cpp:446-447): no contribution

@@ -464,12 +464,34 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
     if (k < rows) {
       const int cz = c0[2] + k / ny, cy = c0[1] + k % ny;
       const uint32_t row = (uint32_t)((cz * G.res[1] + cy) * G.res[0]);
-      uint32_t a = __ldg(&G.cell_off[row + c0[0]]);
-      uint32_t b = __ldg(&G.cell_off[row + c1[0] + 1]);
-      b = b < total_ph ? b : total_ph;
-      a = a < b ? a : b;
-      j0 = a;
-      len = b - a;
+      // Clip the row to the sphere of radius r around x.  A photon binned
+      // to cell c lies in [c, c + 1] cells from the origin up to rounding
+      // (1% of a cell covers it), except in the edge cells, which also hold
+      // the clamped photons from beyond the grid.  Every photon left out
+      // lies farther than r * 1.001 from x, so the reference's loop rejects
+      // it; the photons kept are summed in the same order.
+      const float reach2 = r2 * 1.002f;
+      float dy = 0.f, dz = 0.f;
+      if (cy > 0) dy = fmaxf(dy, (G.origin.y + (float)cy * G.cell.y - 0.01f * G.cell.y) - x.y);
+      if (cy < G.res[1] - 1) dy = fmaxf(dy, x.y - (G.origin.y + (float)(cy + 1) * G.cell.y + 0.01f * G.cell.y));
+      if (cz > 0) dz = fmaxf(dz, (G.origin.z + (float)cz * G.cell.z - 0.01f * G.cell.z) - x.z);
+      if (cz < G.res[2] - 1) dz = fmaxf(dz, x.z - (G.origin.z + (float)(cz + 1) * G.cell.z + 0.01f * G.cell.z));
+      const float rho2 = dy * dy + dz * dz;
+      if (rho2 <= reach2) {
+        const float w = sqrtf(reach2 - rho2) * 1.001f + 0.01f * G.cell.x;
+        int lo = (int)floorf(((x.x - w) - G.origin.x) / G.cell.x);
+        int hi = (int)floorf(((x.x + w) - G.origin.x) / G.cell.x);
+        lo = lo > c0[0] ? lo : c0[0];
+        hi = hi < c1[0] ? hi : c1[0];
+        if (lo <= hi) {
+          uint32_t a = __ldg(&G.cell_off[row + lo]);
+          uint32_t b = __ldg(&G.cell_off[row + hi + 1]);
+          b = b < total_ph ? b : total_ph;
+          a = a < b ? a : b;
+          j0 = a;
+          len = b - a;
+        }
+      }
     }
     uint32_t incl = len;
 #pragma unroll
@@ -494,18 +516,20 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
       float tx = 0.f, ty = 0.f, tz = 0.f;
       bool in = false;
       if (v < seq) {
+        // all three records at once: one memory round trip per round
         const uint32_t j = rj0 + (v - rex);
         const float4 pa = __ldg(&G.pa[j]);
+        const float4 pb = __ldg(&G.pb[j]);
+        const float pc = __ldg(&G.pc[j]);
         const float dx = pa.x - x.x, dy = pa.y - x.y, dz = pa.z - x.z;
         const float d2 = dx * dx + dy * dy + dz * dz;
         if (d2 <= r2) {
-          const float4 pb = __ldg(&G.pb[j]);
           const float cosine = n.x * (-pb.x) + n.y * (-pb.y) + n.z * (-pb.z);
           if (!(cosine < 0.0f)) {
             in = true;
             tx = pa.w * invArea;
             ty = pb.w * invArea;
-            tz = __ldg(&G.pc[j]) * invArea;
+            tz = pc * invArea;
           }
         }
       }
