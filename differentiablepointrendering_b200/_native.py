@@ -84,7 +84,7 @@ def default_settings(lib=None) -> PaleSettings:
     s.photons_per_launch, s.max_bounces, s.forward_passes, s.gather_passes = 1000000, 6, 6, 6
     s.adjoint_bounces, s.adjoint_passes, s.seed, s.random_number, s.rr_start = 6, 6, 42, 42, 6
     s.q_null, s.q_reflect, s.q_transmit, s.gather_radius = 0.5, 0.5, 0.0, 0.01
-    s.leaf_size, s.rng_mode, s.debug_images, s.exposure, s.gamma = 4, 0, 0, 1.0, 2.2
+    s.leaf_size, s.rng_mode, s.debug_images, s.exposure, s.gamma = 1, 0, 0, 1.0, 2.2
     return s
 
 

@@ -252,7 +252,7 @@ void build_surfels(pale_handle* h, const pale_points* asset) {
   h->lc.ensure(n); h->rc.ensure(n); h->rfirst.ensure(n); h->rlast.ensure(n); h->parent.ensure(n);
   h->leaf_parent.ensure(n); h->visits.ensure(n); h->box.ensure(6 * (size_t)n);
   h->d_n.ensure(1);
-  const uint32_t leaf = std::max(1u, std::min(8u, h->st.leaf_size ? h->st.leaf_size : 4u));
+  const uint32_t leaf = std::max(1u, std::min(8u, h->st.leaf_size ? h->st.leaf_size : 1u));
   h->top = 256;
   h->node_count = (n <= leaf) ? 1 : h->top + (n - 1);
   if (n <= leaf) h->top = 0;
@@ -858,7 +858,7 @@ void pale_default_settings(pale_settings* s) {
   s->q_reflect = 0.5f;
   s->q_transmit = 0.0f;
   s->gather_radius = 0.01f;
-  s->leaf_size = 4;
+  s->leaf_size = 1;
   s->rng_mode = PALE_RNG_REFERENCE;
   s->null_weight = PALE_NULL_WEIGHT_REFERENCE;
   s->debug_images = 0;

@@ -65,7 +65,9 @@ typedef struct pale_settings {
     float q_reflect;
     float q_transmit;
     float gather_radius;           /* PathTracer.cpp:187 hard-codes 0.01     */
-    uint32_t leaf_size;            /* BuildOptions leaf size (4)             */
+    uint32_t leaf_size;            /* surfels per LBVH leaf (1); the hits do
+                                      not depend on it (the reference's
+                                      BuildOptions use 4, SceneBuild.ixx:72) */
     uint32_t rng_mode;             /* PALE_RNG_*                             */
     uint32_t debug_images;         /* "debug_images"                         */
     float exposure;                /* SensorGPU::exposureCorrection (1.0)    */

@@ -628,7 +628,10 @@ static void build_points(orc_scene *s, const orc_points *a) {
         vstore(cent + 3 * i, col[i].p);
     }
     s->order = (uint32_t *)malloc(s->np * sizeof(uint32_t));
-    uint32_t leaf = s->st.leaf_size ? s->st.leaf_size : 4;
+    /* the reference's median split always uses BuildOptions' leaf size 4
+     * (SceneBuild.ixx:72-75); the LBVH restatement uses the settings' leaf
+     * size, as the CUDA build does */
+    uint32_t leaf = s->bvh_kind == 0 ? 4u : (s->st.leaf_size ? s->st.leaf_size : 1u);
     if (s->bvh_kind == 0) {
         nodevec nv = {0};
         for (uint32_t i = 0; i < s->np; ++i) s->order[i] = i;

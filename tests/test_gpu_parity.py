@@ -42,15 +42,18 @@ def to_asset(values, order):
     return out
 
 
-def test_lbvh_bit_exact(pair, box):
-    g, _ = pair
+@pytest.mark.parametrize("leaf", [1, 4])
+def test_lbvh_bit_exact(gpu, box, leaf):
+    g = Renderer.from_scene(box, dict(SETTINGS, leaf_size=leaf))
     col = collected_asset_points(box)
     lo, hi = surfel_aabbs(col["position"], col["tangent_u"], col["tangent_v"], col["scale"])
-    codes_ref, order_ref, nodes_ref = lbvh_reference(col["position"], lo, hi, leaf_size=4, top=256)
+    codes_ref, order_ref, nodes_ref = lbvh_reference(col["position"], lo, hi, leaf_size=leaf, top=256)
     codes, nodes = g.get_bvh()
+    order = g.get_point_order()
+    g.close()
     assert np.array_equal(codes, codes_ref)
     assert np.all(np.diff(codes.astype(np.int64)) >= 0)
-    assert np.array_equal(g.get_point_order(), order_ref)
+    assert np.array_equal(order, order_ref)
     assert nodes.shape == nodes_ref.shape
     assert np.array_equal(nodes.view(np.uint32), nodes_ref.view(np.uint32))
 

@@ -31,7 +31,7 @@ def test_noalloc_lbvh_equals_allocating_build_on_two_calls(gpu):
     import torch
 
     scene = make_box_scene(3000, cameras=1, resolution=32)
-    r = Renderer.from_scene(scene, {"photons": 1000, "forward_passes": 1, "gather_radius": 0.02})
+    r = Renderer.from_scene(scene, {"photons": 1000, "forward_passes": 1, "gather_radius": 0.02, "leaf_size": 4})
     codes_ref, nodes_ref = r.get_bvh()
     order_ref = r.get_point_order()
     r.close()
