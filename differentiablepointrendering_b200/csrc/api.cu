@@ -758,6 +758,8 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.ev = EventBufs{h->ev_stage.p, h->ev_list.p};
   A.dldi = d_dldi;
   A.grad_opacity = h->grads.op.p;
+  A.grads = h->grads.view();
+  A.all_grads = st.gradients == PALE_GRADIENTS_ALL;
   A.debug_opacity = d_dbg;
   A.rr_start = st.rr_start;
   A.q_null = st.q_null;
@@ -861,6 +863,7 @@ void pale_default_settings(pale_settings* s) {
   s->leaf_size = 1;
   s->rng_mode = PALE_RNG_REFERENCE;
   s->null_weight = PALE_NULL_WEIGHT_REFERENCE;
+  s->gradients = PALE_GRADIENTS_OPACITY;
   s->debug_images = 0;
   s->exposure = 1.0f;
   s->gamma = 2.2f;
@@ -881,6 +884,7 @@ int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale
     if (!(h->st.gather_radius > 0.f)) throw ArgError("gather radius must be > 0");
     if (h->st.adjoint_bounces > 255) throw ArgError("at most 255 adjoint bounces are supported");
     if (h->st.null_weight > PALE_NULL_WEIGHT_UNBIASED) throw ArgError("null_weight must be reference or unbiased");
+    if (h->st.gradients > PALE_GRADIENTS_ALL) throw ArgError("gradients must be opacity or all");
     if (h->st.null_weight == PALE_NULL_WEIGHT_UNBIASED && !(h->st.q_null > 0.f))
       throw ArgError("unbiased null weighting needs q_null > 0");
     check_points(&desc->points, "pale_create");

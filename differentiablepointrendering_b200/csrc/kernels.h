@@ -120,6 +120,8 @@ struct EventRec {
   float4 b;   // gather normal, endpoint pdf or endpoint cosine
   float4 c;   // path throughput, -
   uint4 d;    // kind, target surfel, material, pixel
+  float4 e;   // hit position on the target surfel (its alpha term's point), -
+  float4 f;   // unit ray direction at that hit, -
 };
 
 struct EventBufs {
@@ -185,6 +187,8 @@ struct AdjointArgs {
   EventBufs ev;
   const float* dldi;       // packed H*W*4 per camera
   float* grad_opacity;
+  PointsDev grads;         // all seven groups (BVH order), written when all_grads
+  uint32_t all_grads;
   float* debug_opacity;    // packed H*W*4 per camera or null
   const CameraRec* cams;   // selected cameras, packed pixel offsets
   const AdjJob* jobs;      // jobs of this batch

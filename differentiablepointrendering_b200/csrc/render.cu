@@ -728,6 +728,10 @@ __global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t p
         ev.b = f4(on, refl ? pdf : endcos);
         ev.c = f4(pthr, 0.f);
         ev.d = make_uint4(pkind, refl ? h.prim : pc.x, mat, pc.z);
+        // the target surfel's hit: the endpoint (reflect) or the pending
+        // null surfel, on the same line (a null continuation keeps d)
+        ev.e = f4(refl ? h.pos : xyz(pa), 0.f);
+        ev.f = f4(normalize(d), 0.f);
         has_ev = true;
         A.pend.b[path] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kKindNone));
         A.pend.a[path] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -776,6 +780,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t p
             ev.b = f4(on, 0.f);
             ev.c = f4(divs(thr, A.q_reflect), 0.f);
             ev.d = make_uint4(kKindProjection, h.prim, kInvalid, pixel);
+            ev.e = f4(h.pos, 0.f);
+            ev.f = f4(normalize(d), 0.f);
             has_ev = true;
           }
         } else if (u < A.q_null + A.q_reflect + A.q_transmit) {
@@ -810,6 +816,59 @@ __global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t p
   if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, ce);
 }
 
+// Derivatives of eta * alpha_geom for the hit at x on surfel k along the
+// unit direction d, with alpha_geom = (1 - r^2)^B, B = 4 e^beta,
+// r^2 = u^2 + v^2, u = U.(x - p) / s_u, v = V.(x - p) / s_v, and x on the
+// plane through p with normal n = U x V / |U x V| (x = o + t d,
+// t = n.(p - o) / (n.d)).  These are the reference's helpers
+// computeDuvDPositionFull, computeFullDuDvWrtTangents, computeDuvDScale and
+// computeDAlphaDb (AdjointGradientKernels.h:212-272, 321-368, 440-451)
+// chained through d alpha_geom / d r^2 = -B alpha_geom / (1 - r^2):
+//   du/dp = ((U.d) / (n.d) n - U) / s_u,
+//   du/dU = (r + (U.d) dt/dU) / s_u,  dv/dU = (V.d) dt/dU / s_v,
+//   dt/dU = (r x V) / ((U x V).d),    dt/dV = (U x r) / ((U x V).d),
+//   du/ds_u = -u / s_u,  d alpha_geom / d beta = alpha_geom B ln(1 - r^2).
+// U and V are the tangents as given (the intersection does not normalize
+// them); zero at the rim (r^2 >= 1) and for rays in the surfel's plane.
+struct AlphaGrad {
+  float beta;
+  V3 pos, tu, tv;
+  float su, sv;
+};
+
+__device__ __forceinline__ AlphaGrad alpha_grad(const SurfelView& S, uint32_t k, V3 x, V3 d) {
+  AlphaGrad g;
+  g.beta = 0.f;
+  g.pos = g.tu = g.tv = v3(0.f, 0.f, 0.f);
+  g.su = g.sv = 0.f;
+  const float4 pe = __ldg(&S.pe[k]), n4 = __ldg(&S.n[k]), u4 = __ldg(&S.u[k]), v4 = __ldg(&S.v[k]);
+  const V3 p = xyz(pe), U = xyz(u4), V = xyz(v4);
+  const float B = pe.w, eta = n4.w, su = u4.w, sv = v4.w;
+  const V3 r = x - p;
+  const float u = dot(U, r) / su, v = dot(V, r) / sv;
+  const float one = 1.0f - (u * u + v * v);
+  if (!(one > 0.0f)) return g;
+  const float alpha = powf(one, B);
+  g.beta = eta * alpha * B * logf(one);
+  const V3 m = cross(U, V);
+  const V3 n = normalize(m);
+  const float nd = dot(n, d), md = dot(m, d);
+  if (fabsf(nd) < 1e-6f) return g;
+  const float k2 = -2.0f * eta * B * alpha / one;   // d(eta alpha) / d(u) = k2 * u, d/dv = k2 * v
+  const float ud = dot(U, d), vd = dot(V, d);
+  const V3 dudp = scale(scale(n, ud / nd) - U, 1.0f / su);
+  const V3 dvdp = scale(scale(n, vd / nd) - V, 1.0f / sv);
+  g.pos = scale(scale(dudp, u) + scale(dvdp, v), k2);
+  const V3 gU = scale(cross(r, V), 1.0f / md), gV = scale(cross(U, r), 1.0f / md);
+  const V3 dudU = scale(r + scale(gU, ud), 1.0f / su), dvdU = scale(gU, vd / sv);
+  const V3 dudV = scale(gV, ud / su), dvdV = scale(r + scale(gV, vd), 1.0f / sv);
+  g.tu = scale(scale(dudU, u) + scale(dvdU, v), k2);
+  g.tv = scale(scale(dudV, u) + scale(dvdV, v), k2);
+  g.su = k2 * u * (-u / su);
+  g.sv = k2 * v * (-v / sv);
+  return g;
+}
+
 // launchAdjointTransportKernel (AdjointKernels.cpp:389-509).  One warp per
 // gradient event (warps stride over the event list): the warp does the
 // photon lookup of the event's end point together (gather_irradiance_warp)
@@ -822,12 +881,13 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
   float4* terms = s_terms + (threadIdx.x & ~31u);
   const uint32_t warps = gridDim.x * (kBlock / 32);
   uint32_t events = 0, queries = 0, scanned = 0;
-  // lanes 0-15 hold the 16 words of the next event, loaded one event ahead
+  // lanes 0-23 hold the 24 words of the next event, loaded one event ahead
+  constexpr int kWords = sizeof(EventRec) / 4;
   uint32_t e = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-  float pre = (e < count && lane < 16) ? reinterpret_cast<const float*>(A.ev.list + e)[lane] : 0.f;
+  float pre = (e < count && lane < kWords) ? reinterpret_cast<const float*>(A.ev.list + e)[lane] : 0.f;
   for (; e < count; e += warps) {
     const float cur = pre;
-    if (e + warps < count && lane < 16) pre = reinterpret_cast<const float*>(A.ev.list + e + warps)[lane];
+    if (e + warps < count && lane < kWords) pre = reinterpret_cast<const float*>(A.ev.list + e + warps)[lane];
     auto field = [&](int f) { return __shfl_sync(0xffffffffu, cur, f); };
     EventRec ev;
     ev.a = make_float4(field(0), field(1), field(2), field(3));
@@ -835,6 +895,8 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
     ev.c = make_float4(field(8), field(9), field(10), field(11));
     ev.d = make_uint4(__float_as_uint(field(12)), __float_as_uint(field(13)), __float_as_uint(field(14)),
                       __float_as_uint(field(15)));
+    ev.e = make_float4(field(16), field(17), field(18), field(19));
+    ev.f = make_float4(field(20), field(21), field(22), field(23));
     const uint32_t kind = ev.d.x;
     // a null event ending on a surfel has no material (the reference reads
     // materials[0xFFFFFFFF], AdjointKernels.cpp:446-447): no contribution
@@ -849,7 +911,9 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
         scanned += cnt;
       }
       const V3 thr = xyz(ev.c);
-      float g = 0.f;
+      float g = 0.f;       // opacity term, as the reference computes it
+      float W = 0.f;       // the event's weight: g = W * alpha_geom
+      V3 dalb = v3(0.f, 0.f, 0.f);
       uint32_t target = kInvalid;
       if (kind == kKindProjection) {
         target = ev.d.y;
@@ -857,6 +921,12 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
         V3 fr = scale(scale(xyz(al), al.w), kInvPi);
         V3 Lo = mul(fr, E);
         g = vsum(mul(scale(thr, ev.a.w), Lo)) * A.inv_spp;
+        if (A.all_grads && target < S.sf.count) {
+          W = vsum(mul(thr, Lo)) * A.inv_spp;
+          // d/d albedo of eta alpha_geom (alpha_r albedo / pi) E, per channel
+          const float eta = __ldg(&S.sf.n[target]).w;
+          dalb = scale(mul(thr, E), eta * ev.a.w * al.w * kInvPi * A.inv_spp);
+        }
       } else if (kind == kKindNull) {
         target = ev.d.y;
         if (ev.d.z != kInvalid) {
@@ -869,6 +939,7 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
           }
           V3 Lo = Le + Lr;
           g = vsum(mul(scale(thr, -ev.a.w * A.null_scale), Lo)) * A.inv_spp;
+          if (A.all_grads) W = -vsum(mul(thr, Lo)) * A.null_scale * A.inv_spp;
         }
       } else if (kind == kKindReflect) {
         target = ev.d.y;
@@ -876,11 +947,33 @@ __global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
         V3 Lo = scale(mul(E, xyz(mat)), kInvPi);
         V3 p = divs(thr, ev.b.w);
         g = vsum(scale(mul(p, Lo), ev.a.w)) * A.inv_spp;
+        if (A.all_grads) W = vsum(mul(p, Lo)) * A.inv_spp;
       }
       if (target != kInvalid && target >= S.sf.count) {
         flag_error(A.st, kErrBounds);
       } else if (target != kInvalid) {
         atomicAdd(&A.grad_opacity[target], g);
+        if (A.all_grads && W != 0.f) {
+          const AlphaGrad ag = alpha_grad(S.sf, target, xyz(ev.e), xyz(ev.f));
+          const PointsDev& G = A.grads;
+          atomicAdd(&G.beta[target], W * ag.beta);
+          atomicAdd(&G.position[3 * target + 0], W * ag.pos.x);
+          atomicAdd(&G.position[3 * target + 1], W * ag.pos.y);
+          atomicAdd(&G.position[3 * target + 2], W * ag.pos.z);
+          atomicAdd(&G.tangent_u[3 * target + 0], W * ag.tu.x);
+          atomicAdd(&G.tangent_u[3 * target + 1], W * ag.tu.y);
+          atomicAdd(&G.tangent_u[3 * target + 2], W * ag.tu.z);
+          atomicAdd(&G.tangent_v[3 * target + 0], W * ag.tv.x);
+          atomicAdd(&G.tangent_v[3 * target + 1], W * ag.tv.y);
+          atomicAdd(&G.tangent_v[3 * target + 2], W * ag.tv.z);
+          atomicAdd(&G.scale[2 * target + 0], W * ag.su);
+          atomicAdd(&G.scale[2 * target + 1], W * ag.sv);
+        }
+        if (A.all_grads && kind == kKindProjection) {
+          atomicAdd(&A.grads.albedo[3 * target + 0], dalb.x);
+          atomicAdd(&A.grads.albedo[3 * target + 1], dalb.y);
+          atomicAdd(&A.grads.albedo[3 * target + 2], dalb.z);
+        }
         if (A.debug_opacity) {
           float* px = A.debug_opacity + 4 * (size_t)ev.d.w;
           atomicAdd(px + 0, g);

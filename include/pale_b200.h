@@ -51,6 +51,15 @@ typedef struct pale_handle pale_handle;
 #define PALE_NULL_WEIGHT_REFERENCE 0u
 #define PALE_NULL_WEIGHT_UNBIASED 1u
 
+/* Gradient groups the adjoint pass writes.  OPACITY is the reference's
+ * live adjoint (AdjointKernels.cpp:389-509; the other six groups are zero,
+ * SyclBridge.cpp:172-179).  ALL also writes beta, position, tangents and
+ * scale through each event surfel's alpha_geom = (1 - r^2)^(4 e^beta),
+ * r^2 = u^2 + v^2 at the ray-plane hit, and albedo through ProjectionScatter
+ * events (the derivatives of AdjointGradientKernels.h:212-451, 757-808). */
+#define PALE_GRADIENTS_OPACITY 0u
+#define PALE_GRADIENTS_ALL 1u
+
 typedef struct pale_settings {
     uint32_t photons_per_launch;   /* "photons"          (default 1e6)       */
     uint32_t max_bounces;          /* "bounces"          (6)                 */
@@ -73,6 +82,7 @@ typedef struct pale_settings {
     float exposure;                /* SensorGPU::exposureCorrection (1.0)    */
     float gamma;                   /* SensorGPU::gammaCorrection   (2.2)     */
     uint32_t null_weight;          /* PALE_NULL_WEIGHT_*                     */
+    uint32_t gradients;            /* PALE_GRADIENTS_*                       */
 } pale_settings;
 
 /* Per-point parameter block (structure of arrays, float32).

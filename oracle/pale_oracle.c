@@ -198,6 +198,7 @@ typedef struct {
     uint32_t end_inst, end_prim;
     float end_alpha, end_pdf, end_cos;
     v3 end_pos, end_normal;
+    v3 tpos, tdir;              /* hit on the target surfel, unit direction */
 } event_t;                      /* CompletedGradientEvent (:338-369) */
 
 struct orc_scene {
@@ -1570,6 +1571,10 @@ static void adjoint_bounce(const orc_scene *s, uint64_t base, uint32_t slot, uin
         e->end_pdf = pdf;
         e->end_type = is_mesh ? 0 : 1;
         e->end_cos = fmaxf(0.0f, vdot(dir, on));
+        /* the target surfel's hit: the endpoint (reflect) or the pending null
+         * surfel, on the same line (a null continuation keeps d) */
+        e->tpos = pend->kind == PK_REFLECT ? h.pos : pend->pos;
+        e->tdir = vnorm(ray->d);
         out->has_event = 1;
         out->clear_pending = 1;
     }
@@ -1640,6 +1645,8 @@ static void adjoint_bounce(const orc_scene *s, uint64_t base, uint32_t slot, uin
             e->normal = on;
             e->thr = vdivs(ray->thr, st->q_reflect);
             e->pixel = ray->pixel;
+            e->tpos = h.pos;
+            e->tdir = vnorm(ray->d);
             out->has_event = 1;
         }
         out->alive = 1;
@@ -1664,10 +1671,51 @@ static void adjoint_bounce(const orc_scene *s, uint64_t base, uint32_t slot, uin
     }
 }
 
+/* Derivatives of eta * alpha_geom for the hit at x on surfel sf along the
+ * unit direction d: alpha_geom = (1 - r^2)^B, B = 4 e^beta, r^2 = u^2 + v^2,
+ * u = tu.(x - p) / su, v = tv.(x - p) / sv, x on the plane through p with
+ * normal n = tu x tv / |tu x tv|.  The chain of AdjointGradientKernels.h
+ * (computeDuvDPositionFull :212-272, computeFullDuDvWrtTangents :321-355,
+ * computeDuvDScale :361-368, computeDAlphaDb :440-451) through
+ * d alpha_geom / d r^2 = -B alpha_geom / (1 - r^2).  out: beta, position[3],
+ * tangent_u[3], tangent_v[3], scale[2]; zero at the rim and in-plane. */
+static void alpha_grad(const point_t *sf, v3 x, v3 d, float out[12]) {
+    memset(out, 0, 12 * sizeof(float));
+    const v3 U = sf->tu, V = sf->tv, r = vsub(x, sf->p);
+    const float B = 4.0f * expf(sf->beta), eta = sf->opacity, su = sf->su, sv = sf->sv;
+    const float u = vdot(U, r) / su, v = vdot(V, r) / sv;
+    const float one = 1.0f - (u * u + v * v);
+    if (!(one > 0.0f)) return;
+    const float alpha = powf(one, B);
+    out[0] = eta * alpha * B * logf(one);
+    const v3 m = vcross(U, V), n = vnorm(m);
+    const float nd = vdot(n, d), md = vdot(m, d);
+    if (fabsf(nd) < 1e-6f) return;
+    const float k2 = -2.0f * eta * B * alpha / one;
+    const float ud = vdot(U, d), vd = vdot(V, d);
+    const v3 dudp = vscale(vsub(vscale(n, ud / nd), U), 1.0f / su);
+    const v3 dvdp = vscale(vsub(vscale(n, vd / nd), V), 1.0f / sv);
+    const v3 gp = vscale(vadd(vscale(dudp, u), vscale(dvdp, v)), k2);
+    const v3 gU = vscale(vcross(r, V), 1.0f / md), gV = vscale(vcross(U, r), 1.0f / md);
+    const v3 dudU = vscale(vadd(r, vscale(gU, ud)), 1.0f / su), dvdU = vscale(gU, vd / sv);
+    const v3 dudV = vscale(gV, ud / su), dvdV = vscale(vadd(r, vscale(gV, vd)), 1.0f / sv);
+    const v3 gtu = vscale(vadd(vscale(dudU, u), vscale(dvdU, v)), k2);
+    const v3 gtv = vscale(vadd(vscale(dudV, u), vscale(dvdV, v)), k2);
+    vstore(out + 1, gp);
+    vstore(out + 4, gtu);
+    vstore(out + 7, gtv);
+    out[10] = k2 * u * (-u / su);
+    out[11] = k2 * v * (-v / sv);
+}
+
 /* launchAdjointTransportKernel for one event (AdjointKernels.cpp:389-509).
- * Returns the opacity-gradient contribution and its surfel index. */
+ * Returns the opacity-gradient contribution and its surfel index; *W gets
+ * the event's weight (opacity term = W alpha_geom) and dalb the albedo term
+ * of a ProjectionScatter event. */
 static float transport_event(const orc_scene *s, const event_t *e, float invSpp, uint32_t *target,
-                             uint64_t *queries, uint64_t *scanned) {
+                             uint64_t *queries, uint64_t *scanned, float *W, v3 *dalb) {
+    *W = 0.0f;
+    *dalb = V3(0, 0, 0);
     if (e->kind == PK_PROJECTION) {
         const point_t *sf = &s->pts[e->prim];
         (*queries)++;
@@ -1676,6 +1724,8 @@ static float transport_event(const orc_scene *s, const event_t *e, float invSpp,
         v3 Lo = vmul(fr, E);
         v3 g = vmul(vscale(e->thr, e->alpha), Lo);
         *target = e->prim;
+        *W = vsum(vmul(e->thr, Lo)) * invSpp;
+        *dalb = vscale(vmul(e->thr, E), sf->opacity * e->alpha * sf->alpha_r * M_1_PIf_ * invSpp);
         return vsum(g) * invSpp;
     }
     if (e->kind == PK_NULL) {
@@ -1696,8 +1746,10 @@ static float transport_event(const orc_scene *s, const event_t *e, float invSpp,
         v3 Lo = vadd(Le, Lr);
         /* the reference's weighting: thr, on a branch taken with
          * probability q_null; null_weight 1 divides by q_null */
-        float w = s->st.null_weight == 1 ? -e->alpha / s->st.q_null : -e->alpha;
+        float scale = s->st.null_weight == 1 ? 1.0f / s->st.q_null : 1.0f;
+        float w = -e->alpha * scale;
         v3 g = vmul(vscale(e->thr, w), Lo);
+        *W = -vsum(vmul(e->thr, Lo)) * scale * invSpp;
         return vsum(g) * invSpp;
     }
     if (e->kind == PK_REFLECT) {
@@ -1708,6 +1760,7 @@ static float transport_event(const orc_scene *s, const event_t *e, float invSpp,
         v3 p = vdivs(e->thr, e->end_pdf);
         v3 g = vscale(vmul(p, Lo), e->end_alpha);
         *target = e->end_prim;
+        *W = vsum(vmul(p, Lo)) * invSpp;
         return vsum(g) * invSpp;
     }
     *target = INVALID_U32;
@@ -1721,6 +1774,10 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
     double t0 = now_ms();
     const orc_settings *st = &s->st;
     float *gop = (float *)calloc(s->np ? s->np : 1, sizeof(float));
+    /* gradients == 1: per surfel beta, position[3], tangent_u[3],
+     * tangent_v[3], scale[2], albedo[3] */
+    const int all = st->gradients == 1;
+    float *gall = all ? (float *)calloc((size_t)(s->np ? s->np : 1) * 15, sizeof(float)) : NULL;
     mt64_t mt;
     mt_seed(&mt, st->rng_mode == 1 ? st->seed : 42ull);
     size_t off = 0;
@@ -1789,6 +1846,7 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
                 s->stats.gradient_events += nev;
                 float *contrib = (float *)malloc((active ? active : 1) * sizeof(float));
                 uint32_t *tgt = (uint32_t *)malloc((active ? active : 1) * sizeof(uint32_t));
+                float *terms = all ? (float *)calloc((size_t)(active ? active : 1) * 15, sizeof(float)) : NULL;
                 uint64_t queries = 0, scanned = 0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : queries, scanned)
                 for (int64_t k = 0; k < (int64_t)active; ++k) {
@@ -1796,15 +1854,25 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
                     contrib[k] = 0.f;
                     if (!stg[k].has_event) continue;
                     uint64_t qu = 0, sc = 0;
-                    contrib[k] = transport_event(s, &stg[k].ev, invSpp, &tgt[k], &qu, &sc);
+                    float W;
+                    v3 dalb;
+                    contrib[k] = transport_event(s, &stg[k].ev, invSpp, &tgt[k], &qu, &sc, &W, &dalb);
                     queries += qu;
                     scanned += sc;
+                    if (all && tgt[k] != INVALID_U32 && W != 0.0f) {
+                        float ag[12];
+                        alpha_grad(&s->pts[tgt[k]], stg[k].ev.tpos, stg[k].ev.tdir, ag);
+                        for (int c = 0; c < 12; ++c) terms[15 * k + c] = W * ag[c];
+                    }
+                    if (all && tgt[k] != INVALID_U32) vstore(terms + 15 * k + 12, dalb);
                 }
                 s->stats.gather_queries += queries;
                 s->stats.photons_scanned += scanned;
                 for (uint32_t k = 0; k < active; ++k) {
                     if (!stg[k].has_event || tgt[k] == INVALID_U32) continue;
                     gop[tgt[k]] += contrib[k];
+                    if (all)
+                        for (int c = 0; c < 15; ++c) gall[15 * (size_t)tgt[k] + c] += terms[15 * k + c];
                     if (dbg && st->debug_images) {
                         uint32_t px = stg[k].ev.pixel;
                         for (int c = 0; c < 3; ++c) dbg[4 * px + c] += contrib[k];
@@ -1813,6 +1881,7 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
                 }
                 free(contrib);
                 free(tgt);
+                free(terms);
                 uint32_t m = 0;
                 for (uint32_t k = 0; k < active; ++k)
                     if (stg[k].alive) q2[m++] = stg[k].next;
@@ -1834,8 +1903,25 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
         if (grads->beta) memset(grads->beta, 0, n * sizeof(float));
         if (grads->shape) memset(grads->shape, 0, n * sizeof(float));
         if (grads->opacity) memcpy(grads->opacity, gop, n * sizeof(float));
+        if (all) {
+            for (uint32_t i = 0; i < n; ++i) {
+                const float *g = gall + 15 * (size_t)i;
+                if (grads->beta) grads->beta[i] = g[0];
+                for (int c = 0; c < 3; ++c) {
+                    if (grads->position) grads->position[3 * i + c] = g[1 + c];
+                    if (grads->tangent_u) grads->tangent_u[3 * i + c] = g[4 + c];
+                    if (grads->tangent_v) grads->tangent_v[3 * i + c] = g[7 + c];
+                    if (grads->albedo) grads->albedo[3 * i + c] = g[12 + c];
+                }
+                if (grads->scale) {
+                    grads->scale[2 * i] = g[10];
+                    grads->scale[2 * i + 1] = g[11];
+                }
+            }
+        }
     }
     free(gop);
+    free(gall);
     s->stats.backward_ms = (float)(now_ms() - t0);
     return 0;
 }

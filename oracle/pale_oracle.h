@@ -39,6 +39,7 @@ typedef struct orc_settings {
     uint32_t leaf_size, rng_mode, debug_images;
     float exposure, gamma;
     uint32_t null_weight;   /* 0 reference, 1 unbiased (divide by q_null) */
+    uint32_t gradients;     /* 0 opacity, 1 all seven groups */
 } orc_settings;
 
 typedef struct orc_points {

@@ -60,8 +60,30 @@ def test_create_rejects_null_arguments_without_touching_the_gpu():
     assert lib.pale_point_count(None, None) == -1
 
 
-def test_struct_layouts_match_header():
-    # pale_settings: 6 u32, u64 (aligned at 24), 2 u32, 4 f32, 3 u32, 2 f32
-    assert C.sizeof(N.PaleSettings) == 80
-    assert C.sizeof(N.PalePoints) == 8 + 8 * 8
-    assert N.PaleSettings.seed.offset == 24
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes structs equal the header's: a C program compiled against
+    include/pale_b200.h prints the size and every field offset."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    structs = {"pale_settings": N.PaleSettings, "pale_points": N.PalePoints, "pale_stats": N.PaleStats,
+               "pale_scene_desc": N.PaleSceneDesc}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pale_b200.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, cls in structs.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert got[(cname, f)] == getattr(cls, f).offset, (cname, f)

@@ -259,3 +259,29 @@ def test_adjoint_split_into_batches_matches_oracle(gpu):
     finally:
         g.close()
         o.close()
+
+
+def test_all_gradient_groups_match_oracle(gpu, box):
+    """gradients = "all": the six groups beyond opacity (a23 formulas) on the
+    GPU equal the oracle's on the same paths."""
+    st = dict(SETTINGS, gradients="all", rng_mode="decorrelated", null_weight="unbiased")
+    g = Renderer.from_scene(box, st)
+    o = OracleRenderer(box, st, bvh_kind=0)
+    try:
+        ig = g.render_forward()
+        o.render_forward()
+        tgt = {n: ((ig[n + "_raw"][..., :3] - 0.5 * ig[n + "_raw"][..., :3].mean()) / ig[n + "_raw"][..., :3].size)
+               .astype(np.float32) for n in box.camera_names}
+        gg, _ = g.render_backward(tgt)
+        go, _ = o.render_backward(tgt)
+        og, oo = g.get_point_order(), o.get_point_order()
+        for k in ("opacity", "beta", "albedo", "scale", "position", "tangent_u", "tangent_v"):
+            a = to_asset(gg[k], og).astype(np.float64).reshape(-1)
+            b = to_asset(go[k], oo).astype(np.float64).reshape(-1)
+            assert np.linalg.norm(b) > 0, k
+            cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+            rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+            assert cos >= 0.99 and rel <= 2e-2, (k, cos, rel)
+    finally:
+        g.close()
+        o.close()
