@@ -66,6 +66,50 @@ class PaleStats(C.Structure):
         return out
 
 
+class PaleOptimizer(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("flags", C.c_uint32), ("lr", C.c_double * 6), ("beta1", C.c_double),
+                ("beta2", C.c_double), ("eps", C.c_double), ("momentum", C.c_double),
+                ("opacity_reset", C.c_float), ("reference_dir", C.c_float * 3)]
+
+
+OPT_ADAM, OPT_SGD, OPT_MASKED_ADAM = 0, 1, 2
+OPT_SURFEL_MASK = 1
+OPTIMIZER_TYPES = {"adam": OPT_ADAM, "sgd": OPT_SGD, "masked_adam": OPT_MASKED_ADAM,
+                   "nullgrad_adam": OPT_MASKED_ADAM, "sparse_adam": OPT_MASKED_ADAM}
+# Learning-rate keys of OptimizationConfig (python/config.py:46-51) with
+# their defaults, in the group order of create_optimizer.
+LR_KEYS = (("learning_rate_position", 1.6e-4), ("learning_rate_tangent", 1.0e-3),
+           ("learning_rate_scale", 5.0e-3), ("learning_rate_albedo", 2.5e-3),
+           ("learning_rate_opacity", 5.0e-2), ("learning_rate_beta", 5.0e-2))
+
+
+def optimizer_from_config(cfg: Optional[dict] = None, opacity_reset: Optional[float] = None) -> PaleOptimizer:
+    """pale_optimizer from OptimizationConfig-style keys: optimizer_type,
+    learning_rate_*, plus betas / eps / momentum (torch defaults, SGD
+    momentum 0.8 as optimizers.py:62), surfel_mask (MaskedAdam with
+    per-surfel masks) and reference_dir (tangent-frame orientation, +Z)."""
+    cfg = dict(cfg or {})
+    o = PaleOptimizer()
+    name = str(cfg.pop("optimizer_type", "adam")).lower()
+    if name not in OPTIMIZER_TYPES:
+        raise ValueError(f"Unknown optimizer_type: {name}")
+    o.type = OPTIMIZER_TYPES[name]
+    o.flags = OPT_SURFEL_MASK if cfg.pop("surfel_mask", False) else 0
+    for g, (key, default) in enumerate(LR_KEYS):
+        o.lr[g] = float(cfg.pop(key, default))
+    b1, b2 = cfg.pop("betas", (0.9, 0.999))
+    o.beta1, o.beta2 = float(b1), float(b2)
+    o.eps = float(cfg.pop("eps", 1e-8))
+    o.momentum = float(cfg.pop("momentum", 0.8))
+    o.opacity_reset = -1.0 if opacity_reset is None else float(opacity_reset)
+    ref = cfg.pop("reference_dir", (0.0, 0.0, 1.0))
+    for c in range(3):
+        o.reference_dir[c] = float(ref[c])
+    if cfg:
+        raise ValueError(f"Unknown optimizer keys: {sorted(cfg)}")
+    return o
+
+
 # Settings-dict keys of the reference (pale_bindings.cpp:123-139) plus the
 # ones this build exposes that the reference hard-codes.
 SETTINGS_KEYS = {
@@ -205,6 +249,9 @@ def load_library() -> C.CDLL:
         "pale_get_order": (C.c_int, [H, u32p]),
         "pale_apply_points": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_rebuild": (C.c_int, [H, C.POINTER(PalePoints)]),
+        "pale_get_asset": (C.c_int, [H, C.POINTER(PalePoints)]),
+        "pale_optimizer_step": (C.c_int, [H, C.POINTER(PaleOptimizer), C.POINTER(PalePoints), C.c_void_p]),
+        "pale_optimizer_reset": (C.c_int, [H]),
         "pale_trace_rays": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, i32p, f32p, f32p, f32p]),
         "pale_trace_transmittance": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, f32p, f32p]),
         "pale_gather_irradiance": (C.c_int, [H, C.c_uint32, f32p, f32p, f32p]),
@@ -229,7 +276,8 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_render_forward_device", "pale_render_backward", "pale_render_backward_device",
             "pale_get_points", "pale_get_order", "pale_apply_points", "pale_rebuild", "pale_trace_rays",
             "pale_trace_transmittance", "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
-            "pale_get_stats", "pale_build_lbvh_noalloc")
+            "pale_get_stats", "pale_build_lbvh_noalloc", "pale_get_asset", "pale_optimizer_step",
+            "pale_optimizer_reset")
 NOALLOC_MAX_SURFELS = 16384
 
 

@@ -157,6 +157,13 @@ struct pale_handle {
   DBuf<uint32_t> cam_cursor;   // seed cursor after the last photon pass
   DBuf<float> img_raw, img_ldr, dldi, dbg;
   PointsBufs grads;
+  uint64_t bvh_gen = 0;        // BVH builds so far
+  uint64_t grads_gen = ~0ull;  // build the gradients belong to
+  // optimizer state (BVH order; starts over after every build)
+  PointsBufs opt_m, opt_v;
+  DBuf<uint32_t> opt_steps;
+  uint64_t opt_gen = ~0ull, opt_t = 0;
+  uint32_t opt_type = ~0u;
   pale_stats stats{};
   uint64_t launches_last = 0;  // kernels launched by the last render call
   int stats_pending = 0;   // a render ran without reading its run state yet
@@ -230,17 +237,26 @@ void upload_points(pale_handle* h, const pale_points* p, PointsBufs& dst, cudaSt
   (void)h;
 }
 
+void build_from_device_asset(pale_handle* h);
+
 // Builds the LBVH and surfel arrays from asset-order points.
 void build_surfels(pale_handle* h, const pale_points* asset) {
+  h->np = asset->count;
+  upload_points(h, asset, h->asset, h->stream);
+  build_from_device_asset(h);
+}
+
+// Builds the LBVH and surfel arrays from the device copy of the asset
+// (h->asset, h->np points).
+void build_from_device_asset(pale_handle* h) {
   cudaStream_t s = h->stream;
-  const uint32_t n = asset->count;
-  h->np = n;
-  upload_points(h, asset, h->asset, s);
+  const uint32_t n = h->np;
   h->collected.alloc(n);
   h->params.alloc(n);
   h->sf_pe.ensure(n); h->sf_n.ensure(n); h->sf_u.ensure(n); h->sf_v.ensure(n); h->sf_cn.ensure(n);
   h->sf_alb.ensure(n);
   h->grads.alloc(n);
+  ++h->bvh_gen;
   if (n == 0) {
     h->node_count = 0;
     return;
@@ -600,13 +616,13 @@ void copy_stats(pale_handle* h) {
   }
 }
 
-// Makes `s` the stream of the following work, ordered after everything
-// already queued on the previous stream of this handle.
 // The stream a device entry point runs on: the caller's, where NULL is the
 // default stream (the legacy stream), so that the work is ordered with the
 // caller's default-stream work.
 cudaStream_t caller_stream(void* stream) { return stream ? (cudaStream_t)stream : cudaStreamLegacy; }
 
+// Makes `s` the stream of the following work, ordered after everything
+// already queued on the previous stream of this handle.
 void use_stream(pale_handle* h, cudaStream_t s) {
   if (s == h->stream) return;
   cudaEvent_t e;
@@ -723,6 +739,7 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
 void zero_grads(pale_handle* h, cudaStream_t s) {
   const size_t n = h->np ? h->np : 1;
   PointsBufs& g = h->grads;
+  h->grads_gen = h->bvh_gen;
   CK(cudaMemsetAsync(g.pos.p, 0, 12 * n, s));
   CK(cudaMemsetAsync(g.tu.p, 0, 12 * n, s));
   CK(cudaMemsetAsync(g.tv.p, 0, 12 * n, s));
@@ -837,6 +854,47 @@ void download_points(pale_handle* h, const PointsBufs& src, pale_points* out) {
   if (out->beta) CK(cudaMemcpyAsync(out->beta, src.beta.p, 4 * n, cudaMemcpyDeviceToHost, s));
   if (out->shape) CK(cudaMemcpyAsync(out->shape, src.shape.p, 4 * n, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+}
+
+// dst := src for the current point count (device to device, enqueued).
+void copy_points(pale_handle* h, const PointsBufs& src, PointsBufs& dst, cudaStream_t s) {
+  const size_t n = h->np;
+  if (!n) return;
+  CK(cudaMemcpyAsync(dst.pos.p, src.pos.p, 12 * n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(dst.tu.p, src.tu.p, 12 * n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(dst.tv.p, src.tv.p, 12 * n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(dst.sc.p, src.sc.p, 8 * n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(dst.alb.p, src.alb.p, 12 * n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(dst.op.p, src.op.p, 4 * n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(dst.beta.p, src.beta.p, 4 * n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(dst.shape.p, src.shape.p, 4 * n, cudaMemcpyDeviceToDevice, s));
+}
+
+void zero_point_bufs(pale_handle* h, PointsBufs& b, cudaStream_t s) {
+  const size_t n = h->np;
+  if (!n) return;
+  CK(cudaMemsetAsync(b.pos.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(b.tu.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(b.tv.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(b.sc.p, 0, 8 * n, s));
+  CK(cudaMemsetAsync(b.alb.p, 0, 12 * n, s));
+  CK(cudaMemsetAsync(b.op.p, 0, 4 * n, s));
+  CK(cudaMemsetAsync(b.beta.p, 0, 4 * n, s));
+}
+
+void check_optimizer(const pale_optimizer* o) {
+  if (!o) throw ArgError("pale_optimizer_step: null optimizer description");
+  if (o->type > PALE_OPT_MASKED_ADAM) throw ArgError("Unknown optimizer type " + std::to_string(o->type));
+  if (o->flags & ~PALE_OPT_SURFEL_MASK) throw ArgError("Unknown optimizer flags");
+  for (int g = 0; g < 6; ++g)
+    if (!(o->lr[g] >= 0.0) || !std::isfinite(o->lr[g])) throw ArgError("Invalid learning rate");
+  if (o->type != PALE_OPT_SGD) {
+    if (!(o->beta1 >= 0.0 && o->beta1 < 1.0 && o->beta2 >= 0.0 && o->beta2 < 1.0))
+      throw ArgError("Invalid betas");
+    if (!(o->eps > 0.0)) throw ArgError("Invalid eps");
+  } else if (!(o->momentum >= 0.0)) {
+    throw ArgError("Invalid momentum");
+  }
 }
 
 }  // namespace
@@ -1075,6 +1133,7 @@ int pale_apply_points(pale_handle* h, const pale_points* p) {
     CK(cudaMemcpyAsync(d.beta.p, p->beta, 4 * n, cudaMemcpyHostToDevice, s));
     derive_surfels(d.view(), h->np, SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p},
                    s);
+    copy_points(h, d, h->asset, s);   // the asset mirrors the written parameters
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
     return PALE_OK;
@@ -1084,10 +1143,98 @@ int pale_apply_points(pale_handle* h, const pale_points* p) {
 int pale_rebuild(pale_handle* h, const pale_points* asset) {
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {
-    check_points(asset, "pale_rebuild");
     use_stream(h, h->own_stream);
+    if (!asset) {
+      build_from_device_asset(h);
+      return PALE_OK;
+    }
+    check_points(asset, "pale_rebuild");
     if (asset->count >= (1u << 28)) throw ArgError("at most 2^28 surfels are supported");
     build_surfels(h, asset);
+    return PALE_OK;
+  });
+}
+
+int pale_get_asset(pale_handle* h, pale_points* out) {
+  if (!h || !out) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    use_stream(h, h->own_stream);
+    out->count = h->np;
+    download_points(h, h->asset, out);
+    return PALE_OK;
+  });
+}
+
+int pale_optimizer_reset(pale_handle* h) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  h->opt_gen = ~0ull;
+  return PALE_OK;
+}
+
+int pale_optimizer_step(pale_handle* h, const pale_optimizer* o, const pale_points* d_grads, void* stream) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    check_optimizer(o);
+    PointsDev grads = h->grads.view();
+    if (d_grads) {
+      if (d_grads->count != h->np) throw ArgError("pale_optimizer_step: gradient count differs from the point count");
+      if (h->np && (!d_grads->position || !d_grads->tangent_u || !d_grads->tangent_v || !d_grads->scale ||
+                    !d_grads->albedo || !d_grads->opacity || !d_grads->beta))
+        throw ArgError("pale_optimizer_step: missing gradient field");
+      grads = PointsDev{d_grads->position, d_grads->tangent_u, d_grads->tangent_v, d_grads->scale,
+                        d_grads->albedo, d_grads->opacity, d_grads->beta, nullptr};
+    } else if (h->grads_gen != h->bvh_gen) {
+      throw ArgError("pale_optimizer_step: no adjoint pass since the last BVH build");
+    }
+    use_stream(h, caller_stream(stream));
+    cudaStream_t s = h->stream;
+    const uint32_t n = h->np;
+    if (h->opt_gen != h->bvh_gen || h->opt_type != o->type) {
+      // a fresh optimizer: zero moments and step counts
+      h->opt_m.alloc(n);
+      h->opt_v.alloc(n);
+      h->opt_steps.ensure(std::max(1u, n));
+      zero_point_bufs(h, h->opt_m, s);
+      zero_point_bufs(h, h->opt_v, s);
+      if (n) CK(cudaMemsetAsync(h->opt_steps.p, 0, 4ull * n, s));
+      h->opt_gen = h->bvh_gen;
+      h->opt_type = o->type;
+      h->opt_t = 0;
+    }
+    ++h->opt_t;
+    OptArgs A{};
+    A.n = n;
+    A.grads = grads;
+    A.params = h->params.view();
+    A.asset = h->asset.view();
+    A.m = h->opt_m.view();
+    A.v = h->opt_v.view();
+    A.steps = h->opt_steps.p;
+    A.mode = o->type;
+    A.use_mask = (o->type == PALE_OPT_MASKED_ADAM && (o->flags & PALE_OPT_SURFEL_MASK)) ? 1u : 0u;
+    A.first = h->opt_t == 1;
+    // Python-float scalars of the torch step (bias corrections in double),
+    // each rounded to float once where torch hands it to a float32 kernel.
+    const double t = (double)h->opt_t;
+    const double bc1 = 1.0 - std::pow(o->beta1, t);
+    const double bc2 = 1.0 - std::pow(o->beta2, t);
+    for (int g = 0; g < 6; ++g) {
+      A.lr[g] = (float)o->lr[g];
+      A.step_size[g] = o->type == PALE_OPT_SGD ? (float)o->lr[g] : (float)(o->lr[g] / bc1);
+    }
+    A.beta1 = (float)o->beta1;
+    A.beta2 = (float)o->beta2;
+    A.one_minus_beta1 = (float)(1.0 - o->beta1);
+    A.one_minus_beta2 = (float)(1.0 - o->beta2);
+    A.bc2_sqrt = (float)std::sqrt(bc2);
+    A.eps = (float)o->eps;
+    A.momentum = (float)o->momentum;
+    A.opacity_reset = o->opacity_reset;
+    for (int c = 0; c < 3; ++c) A.ref[c] = o->reference_dir[c];
+    optimizer_step(A, s);
+    derive_surfels(h->params.view(), n,
+                   SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p}, s);
+    CK(cudaGetLastError());
     return PALE_OK;
   });
 }

@@ -54,6 +54,27 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32
 void lbvh_build(const LbvhArgs& a, cudaStream_t s);
 void derive_surfels(const PointsDev& p, uint32_t n, const SurfelArrays& d, cudaStream_t s);
 
+// One optimizer step on the device (optim.cu), in BVH order like the
+// parameters and gradients it reads.  Moments have the parameter layout.
+enum OptMode : uint32_t { kOptAdam = 0, kOptSgd = 1, kOptMaskedAdam = 2 };
+struct OptArgs {
+  uint32_t n;
+  PointsDev grads;         // gradients of the last adjoint pass
+  PointsDev params;        // updated in place
+  PointsDev asset;         // receives a copy of the updated parameters
+  PointsDev m, v;          // first / second moments (SGD: m = momentum buffer)
+  uint32_t* steps;         // masked Adam: per-surfel step counts
+  uint32_t mode;           // OptMode
+  uint32_t use_mask;       // masked Adam: only surfels with a nonzero gradient
+  uint32_t first;          // SGD: first step (momentum buffer = gradient)
+  float lr[6];             // groups: position, tangents, scale, albedo, opacity, beta
+  float step_size[6];      // Adam: lr / (1 - beta1^t); SGD: lr
+  float beta1, beta2, one_minus_beta1, one_minus_beta2, bc2_sqrt, eps, momentum;
+  float opacity_reset;     // >= 0: every opacity set to it after the step
+  float ref[3];            // tangent frames: normal oriented towards ref
+};
+void optimizer_step(const OptArgs& a, cudaStream_t s);
+
 // Device time of the hot kernels: a pair of CUDA events around every launch
 // of a timed kernel, summed per kernel after the stream is synchronised.
 // Host-side only (kernels receive the pointer inside their argument

@@ -61,6 +61,11 @@ class DeviceFrame:
         _check(L, self.r._h, rc, "render_backward_device")
         return self.grads
 
+    def step(self, config: Optional[dict] = None, opacity_reset: Optional[float] = None):
+        """Optimizer step from the gradients of the last backward, on this
+        frame's stream (Renderer.optimizer_step)."""
+        self.r.optimizer_step(config, opacity_reset, stream=self._stream())
+
     def split(self, packed: torch.Tensor) -> List[torch.Tensor]:
         """Packed (P, 4) -> list of (H, W, 4) views, one per camera."""
         out, off = [], 0

@@ -19,7 +19,7 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _native as N
-from .scene import (POINT_FIELDS, SceneArrays, as_points, load_mitsuba_scene, load_surfel_ply,
+from .scene import (POINT_FIELDS, POINT_WIDTH, SceneArrays, as_points, load_mitsuba_scene, load_surfel_ply,
                     resolve_point_cloud)
 
 
@@ -48,7 +48,8 @@ class Renderer:
             scene = load_mitsuba_scene(root, sceneXml, pts)
         self._scene = scene
         self._settings = N.settings_from_dict(settings)
-        self._asset = {k: v.copy() for k, v in as_points(scene.points).items()}
+        self._asset_host = {k: v.copy() for k, v in as_points(scene.points).items()}
+        self._asset_stale = False   # the device asset is newer (optimizer_step)
         desc = N.SceneDescHolder(scene)
         rc = self._lib.pale_create(C.byref(desc.struct), C.byref(self._settings), C.byref(self._h))
         if rc != 0:
@@ -215,8 +216,65 @@ class Renderer:
 
     def rebuild_bvh(self):
         """Rebuilds the surfel LBVH from the asset (pale_bindings.cpp:1058-1079)."""
+        if self._asset_stale:       # the device holds the newest asset
+            _check(self._lib, self._h, self._lib.pale_rebuild(self._h, None), "rebuild_bvh")
+            return
         hold = N.PointsHolder(self._asset)
         _check(self._lib, self._h, self._lib.pale_rebuild(self._h, C.byref(hold.struct)), "rebuild_bvh")
+
+    @property
+    def _asset(self) -> Dict[str, np.ndarray]:
+        """Host copy of the asset, fetched from the device after optimizer steps."""
+        if self._asset_stale:
+            out = N.PointsHolder(n=self.num_points)
+            _check(self._lib, self._h, self._lib.pale_get_asset(self._h, C.byref(out.struct)), "get_asset")
+            self._asset_host = {k: out.arrays[k].copy() for k in POINT_FIELDS}
+            self._asset_stale = False
+        return self._asset_host
+
+    @_asset.setter
+    def _asset(self, value: Dict[str, np.ndarray]):
+        self._asset_host = value
+        self._asset_stale = False
+
+    # ------------------------------------------------------- training step
+    def optimizer_step(self, config: Optional[dict] = None, opacity_reset: Optional[float] = None, stream=None,
+                       grads: Optional[Dict[str, object]] = None):
+        """One optimizer step of the training loop on the device
+        (training.py:685-743): the gradients of the last render_backward go
+        through Adam / SGD / MaskedAdam with per-group learning rates
+        (OptimizationConfig keys, optimizers.py:11-66), opacities are set to
+        `opacity_reset` if given, the parameters are projected onto their
+        constraints (verify_parameters_inplane) and written back without a
+        BVH rebuild (apply_point_optimization).  Optimizer state stays on
+        the device and starts over after each BVH rebuild, as the reference
+        creates a new optimizer then.  Runs on `stream` (a torch.cuda.Stream
+        or a raw handle; None = the default stream) without waiting.
+        `grads` replaces the adjoint's gradients by CUDA tensors (float32,
+        contiguous, BVH order) of the seven fields."""
+        opt = N.optimizer_from_config(config, opacity_reset)
+        if stream is None or isinstance(stream, C.c_void_p):
+            s = stream
+        else:
+            s = C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+        g = None
+        if grads is not None:
+            g = N.PalePoints()
+            g.count = self.num_points
+            for k in POINT_FIELDS[:7]:
+                t = grads[k]
+                if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+                    raise ValueError(f"optimizer_step: gradient '{k}' must be a contiguous float32 CUDA tensor")
+                if t.numel() != self.num_points * POINT_WIDTH[k]:
+                    raise ValueError(f"optimizer_step: gradient '{k}' has {t.numel()} entries")
+                setattr(g, k, C.cast(C.c_void_p(t.data_ptr()), N.f32p))
+            g = C.byref(g)
+        _check(self._lib, self._h, self._lib.pale_optimizer_step(self._h, C.byref(opt), g, s), "optimizer_step")
+        self._asset_stale = True
+
+    def reset_optimizer(self):
+        """Drops the device optimizer state (zero moments at the next step)."""
+        _check(self._lib, self._h, self._lib.pale_optimizer_reset(self._h), "reset_optimizer")
 
     def remove_points(self, parameters: Dict[str, np.ndarray]):
         """Removes asset points by index, then rebuilds (:1081-1189)."""

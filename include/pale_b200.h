@@ -243,8 +243,54 @@ int pale_apply_points(pale_handle *h, const pale_points *params);
 
 /* Rebuilds the LBVH from an asset-order point set of any size (rebuild_bvh,
  * pale_bindings.cpp:1058-1079; also behind add_points / remove_points /
- * set_point_* which edit the asset and rebuild). */
+ * set_point_* which edit the asset and rebuild).  asset_points == NULL
+ * rebuilds from the renderer's own asset, which pale_apply_points and
+ * pale_optimizer_step keep equal to the last written parameters, as
+ * rebuild_bvh() does. */
 int pale_rebuild(pale_handle *h, const pale_points *asset_points);
+
+/* The renderer's asset (the point set the last BVH build started from, or
+ * the parameters written since): count and the seven fields plus shape. */
+int pale_get_asset(pale_handle *h, pale_points *out);
+
+/* One optimizer step of the training loop on the device
+ * (python/training.py:685-743): the gradients of the last adjoint pass go
+ * through the optimizer (python/optimizers.py:11-66, :301-337), opacities
+ * are reset if asked (training.py:707-711), the parameters are projected
+ * onto their constraints (verify_parameters_inplane, training.py:326-343)
+ * and written back without a BVH rebuild, as apply_point_optimization.
+ * Optimizer state (moments, step counts) lives on the device in BVH order
+ * and starts over after every BVH build, as training.py:730-749 creates a
+ * new optimizer after rebuild_bvh.  Enqueued on `stream` (NULL = the
+ * default stream) without waiting. */
+#define PALE_OPT_ADAM 0u          /* torch.optim.Adam                        */
+#define PALE_OPT_SGD 1u           /* torch.optim.SGD, momentum (0.8)        */
+#define PALE_OPT_MASKED_ADAM 2u   /* MaskedAdam (optimizers.py:70-214)     */
+#define PALE_OPT_SURFEL_MASK 1u   /* flags: MaskedAdam updates only surfels
+                                     with a nonzero gradient entry, each with
+                                     its own step count
+                                     (compute_surfel_update_mask)           */
+typedef struct pale_optimizer {
+    uint32_t type;            /* PALE_OPT_*                                 */
+    uint32_t flags;
+    double lr[6];             /* position, tangents, scale, albedo, opacity,
+                                 beta (config.py:46-51 defaults)           */
+    double beta1, beta2, eps; /* Adam (0.9, 0.999, 1e-8)                    */
+    double momentum;          /* SGD (0.8)                                  */
+    float opacity_reset;      /* >= 0: every opacity set to this value after
+                                 the update; < 0: no reset                  */
+    float reference_dir[3];   /* tangent-frame normals oriented towards this
+                                 direction (+Z)                             */
+} pale_optimizer;
+
+/* d_grads: the seven DEVICE gradient fields in BVH order (count = the
+ * point count; shape is ignored), e.g. the adjoint's gradients plus a
+ * regulariser's, or NULL for the gradients of the last adjoint pass. */
+int pale_optimizer_step(pale_handle *h, const pale_optimizer *opt,
+                        const pale_points *d_grads, void *stream);
+
+/* Drops the optimizer state: the next step starts from zero moments. */
+int pale_optimizer_reset(pale_handle *h);
 
 /* Closest-hit queries against the scene (intersectScene in FirstHit mode,
  * IntersectionKernels.h:954-1097).  Host arrays of n rays; outputs:

@@ -70,7 +70,7 @@ def test_struct_layouts_match_header(tmp_path):
         pytest.skip("no C compiler")
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     structs = {"pale_settings": N.PaleSettings, "pale_points": N.PalePoints, "pale_stats": N.PaleStats,
-               "pale_scene_desc": N.PaleSceneDesc}
+               "pale_scene_desc": N.PaleSceneDesc, "pale_optimizer": N.PaleOptimizer}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pale_b200.h"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
