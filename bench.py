@@ -220,7 +220,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     import torch.distributed as dist
 
     from differentiablepointrendering_b200.build import build_library
-    from differentiablepointrendering_b200.device import DeviceFrame, l2_grad_
+    from differentiablepointrendering_b200.device import DeviceFrame
     from differentiablepointrendering_b200.multigpu import reduce_gradients, view_offset
     from differentiablepointrendering_b200.pale import Renderer
     from differentiablepointrendering_b200.scene import jitter_target, make_box_scene, make_surfels
@@ -249,8 +249,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     stream = torch.cuda.current_stream(dev)
 
     def step():
-        frame.forward()
-        l2_grad_(frame.dldi, frame.ldr, target)
+        frame.forward_loss(target)      # post-process writes dL/dI and the loss
         frame.backward()
         if world > 1:
             reduce_gradients(frame.grads)
@@ -259,9 +258,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         step()
     torch.cuda.synchronize()
     # work per step (fixed seeds: every step traces the same rays)
-    frame.forward()
+    frame.forward_loss(target)
     sf = frame.stats()
-    l2_grad_(frame.dldi, frame.ldr, target)
     frame.backward()
     sb = frame.stats()
     rays = sf["photon_segments"] + sf["gather_segments"] + sb["adjoint_segments"]
@@ -308,8 +306,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        imgs = r.render_forward()
-        dl = {n: ((imgs[n][..., :3] - tgt_np[n]) / tgt_np[n].size).astype(np.float32) for n in cams}
+        imgs, dl, losses = r.render_forward_loss(tgt_np)
         grads, _ = r.render_backward(dl)
         if world > 1:
             for k2, v in grads.items():
@@ -323,8 +320,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e_value = float(total_rays.item()) * e2e_steps / float(et.item()) / 1e6
     pix = frame.pixels
-    h2d = pix * 16
-    d2h = 2 * pix * 16 + r.num_points * 17 * 4
+    h2d = pix * 12 + pix * 16                  # RGB target; dL/dI (float4 per pixel)
+    d2h = 3 * pix * 16 + 8 * len(cams) + r.num_points * 17 * 4   # LDR, raw, dL/dI, losses; gradients
 
     if rank != 0:
         r.close()

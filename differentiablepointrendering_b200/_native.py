@@ -250,6 +250,10 @@ def load_library() -> C.CDLL:
         "pale_apply_points": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_rebuild": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_get_asset": (C.c_int, [H, C.POINTER(PalePoints)]),
+        "pale_render_forward_loss": (C.c_int, [H, C.c_uint32, u32p, f32p, C.c_uint32, f32p, f32p, f32p,
+                                               C.POINTER(C.c_double)]),
+        "pale_render_forward_loss_device": (C.c_int, [H, C.c_uint32, u32p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "pale_optimizer_step": (C.c_int, [H, C.POINTER(PaleOptimizer), C.POINTER(PalePoints), C.c_void_p]),
         "pale_optimizer_reset": (C.c_int, [H]),
         "pale_trace_rays": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, i32p, f32p, f32p, f32p]),
@@ -277,7 +281,7 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_get_points", "pale_get_order", "pale_apply_points", "pale_rebuild", "pale_trace_rays",
             "pale_trace_transmittance", "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
             "pale_get_stats", "pale_build_lbvh_noalloc", "pale_get_asset", "pale_optimizer_step",
-            "pale_optimizer_reset")
+            "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device")
 NOALLOC_MAX_SURFELS = 16384
 
 

@@ -155,7 +155,8 @@ struct pale_handle {
   DBuf<RunState> run;
   DBuf<uint32_t> seeds_fwd, seeds_adj;
   DBuf<uint32_t> cam_cursor;   // seed cursor after the last photon pass
-  DBuf<float> img_raw, img_ldr, dldi, dbg;
+  DBuf<float> img_raw, img_ldr, dldi, dbg, target;
+  DBuf<double> loss_part, loss;
   PointsBufs grads;
   uint64_t bvh_gen = 0;        // BVH builds so far
   uint64_t grads_gen = ~0ull;  // build the gradients belong to
@@ -639,12 +640,20 @@ void validate_cams(pale_handle* h, uint32_t nsel, const uint32_t* idx) {
     if (idx[i] >= h->cams.size()) throw ArgError("camera index out of range");
 }
 
+// Optional image loss of a forward pass (device pointers).
+struct LossReq {
+  const float* target;
+  uint32_t channels;
+  float* dldi;     // may be null
+  double* loss;    // may be null
+};
+
 // Forward render into the handle's packed device images.
 // trace_photons false: the camera gather alone, from the current photon
 // map (the last forward's or loaded photons), with the camera seeds the
 // last forward used.
 uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr, bool sync,
-                 bool trace_photons = true) {
+                 bool trace_photons = true, const LossReq* lq = nullptr) {
   cudaStream_t s = h->stream;
   h->timer.used = 0;
   const uint64_t launches0 = launches_issued();
@@ -726,7 +735,16 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.fb = h->cg_fb.p;
   F.path_capacity = h->path_cap;
   F.timer = &h->timer;
+  if (lq) {
+    F.target = lq->target;
+    F.target_channels = lq->channels;
+    F.dldi = lq->dldi;
+  }
   camera_gather(F, s);
+  if (lq && lq->loss) {
+    h->loss_part.ensure((size_t)std::max(1u, nsel) * kLossChunks);
+    image_loss(F, h->loss_part.p, lq->loss, s);
+  }
   CK(cudaEventRecord(h->ev2, s));
   CK(cudaGetLastError());
   h->launches_last = launches_issued() - launches0;
@@ -1037,6 +1055,59 @@ int pale_render_forward_device(pale_handle* h, uint32_t nsel, const uint32_t* id
     use_stream(h, caller_stream(stream));
     h->img_raw.ensure(4 * std::max<size_t>(1, pix));
     forward(h, nsel, idx, d_raw ? d_raw : h->img_raw.p, d_ldr, false);
+    return PALE_OK;
+  });
+}
+
+int pale_render_forward_loss(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* target,
+                             uint32_t channels, float* ldr, float* raw, float* dldi, double* loss) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    validate_cams(h, nsel, idx);
+    if (!target && nsel) throw ArgError("target image is null");
+    if (channels != 3 && channels != 4) throw ArgError("target images need 3 or 4 channels");
+    if (nsel > 65535) throw ArgError("at most 65535 cameras per call");
+    size_t pix = 0;
+    for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    use_stream(h, h->own_stream);
+    const size_t p1 = std::max<size_t>(1, pix);
+    h->img_raw.ensure(4 * p1);
+    h->img_ldr.ensure(4 * p1);
+    h->dldi.ensure(4 * p1);
+    h->target.ensure(channels * p1);
+    h->loss.ensure(std::max(1u, nsel));
+    if (pix) CK(cudaMemcpyAsync(h->target.p, target, 4 * channels * pix, cudaMemcpyHostToDevice, h->stream));
+    LossReq lq{h->target.p, channels, h->dldi.p, h->loss.p};
+    forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, false, true, &lq);
+    if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+    if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+    if (dldi) CK(cudaMemcpyAsync(dldi, h->dldi.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
+    if (loss && nsel) CK(cudaMemcpyAsync(loss, h->loss.p, 8ull * nsel, cudaMemcpyDeviceToHost, h->stream));
+    copy_stats(h);
+    CK(cudaStreamSynchronize(h->stream));
+    return PALE_OK;
+  });
+}
+
+int pale_render_forward_loss_device(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_target,
+                                    uint32_t channels, float* d_ldr, float* d_raw, float* d_dldi, double* d_loss,
+                                    void* stream) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    validate_cams(h, nsel, idx);
+    if (!d_target && nsel) throw ArgError("target image is null");
+    if (channels != 3 && channels != 4) throw ArgError("target images need 3 or 4 channels");
+    if (nsel > 65535) throw ArgError("at most 65535 cameras per call");
+    size_t pix = 0;
+    for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
+    use_stream(h, caller_stream(stream));
+    h->img_raw.ensure(4 * std::max<size_t>(1, pix));
+    if (!d_ldr && d_loss) {
+      h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
+      d_ldr = h->img_ldr.p;
+    }
+    LossReq lq{d_target, channels, d_dldi, d_loss};
+    forward(h, nsel, idx, d_raw ? d_raw : h->img_raw.p, d_ldr, false, true, &lq);
     return PALE_OK;
   });
 }

@@ -172,7 +172,19 @@ struct FrameArgs {
   float4* fb;
   uint32_t path_capacity;  // >= total_pixels
   KernelTimer* timer;      // host side, may be null
+  // optional L2 image loss: target packed like the images with
+  // target_channels floats per pixel; dL/dI (float4 per pixel) written by
+  // the post-process
+  const float* target;
+  uint32_t target_channels;
+  float* dldi;
 };
+
+// Per-camera L2 loss 0.5 mean((ldr - target)^2) over the RGB values of
+// each camera of a finished frame (needs a.ldr and a.target), summed in
+// double in a fixed order: partials[ncams * kLossChunks], loss[ncams].
+constexpr uint32_t kLossChunks = 64;
+void image_loss(const FrameArgs& a, double* partials, double* loss, cudaStream_t s);
 
 struct PhotonArgs {
   SceneView scene;

@@ -547,7 +547,7 @@ __global__ void k_cg_finalize(FrameArgs A, uint32_t p0, uint32_t p1, int first, 
   }
   const size_t o4 = 4 * (size_t)gp;
   if (A.raw) *reinterpret_cast<float4*>(A.raw + o4) = make_float4(fb[0], fb[1], fb[2], fb[3]);
-  if (A.ldr) {
+  if (A.ldr || A.dldi) {
     float ig = (A.gamma > 0.0f) ? (1.0f / A.gamma) : 1.0f;
     float l[3];
 #pragma unroll
@@ -557,8 +557,59 @@ __global__ void k_cg_finalize(FrameArgs A, uint32_t p0, uint32_t p1, int first, 
       x = powf(x, ig);
       l[c] = clampf(x, 0.0f, 1.0f);
     }
-    *reinterpret_cast<float4*>(A.ldr + o4) = make_float4(l[0], l[1], l[2], 1.0f);
+    if (A.ldr) *reinterpret_cast<float4*>(A.ldr + o4) = make_float4(l[0], l[1], l[2], 1.0f);
+    if (A.dldi) {
+      // compute_l2_grad (python/losses.py:27-45) per camera: the residual
+      // over the camera's number of RGB values, in float32
+      const CameraRec& C = A.cams[find_camera(A, gp)];
+      const float size = (float)(3u * C.w * C.h);
+      const float* t = A.target + (size_t)A.target_channels * gp;
+      *reinterpret_cast<float4*>(A.dldi + o4) =
+          make_float4((l[0] - t[0]) / size, (l[1] - t[1]) / size, (l[2] - t[2]) / size, 0.0f);
+    }
   }
+}
+
+// compute_l2_loss (python/losses.py:10-24) per selected camera: block
+// (chunk, camera) sums its strided share of the camera's squared RGB
+// residuals in double; k_loss_final adds the chunks in order.
+__global__ void k_loss_partials(FrameArgs A, double* __restrict__ partials) {
+  __shared__ double s_part[kBlock / 32];
+  const uint32_t ci = blockIdx.y;
+  const CameraRec& C = A.cams[ci];
+  const uint32_t npix = C.w * C.h;
+  double acc = 0.0;
+  for (uint32_t p = blockIdx.x * kBlock + threadIdx.x; p < npix; p += gridDim.x * kBlock) {
+    const size_t gp = (size_t)C.pixel_offset + p;
+    const float4 l = *reinterpret_cast<const float4*>(A.ldr + 4 * gp);
+    const float* t = A.target + (size_t)A.target_channels * gp;
+    const float d0 = l.x - t[0], d1 = l.y - t[1], d2 = l.z - t[2];
+    acc += (double)(d0 * d0) + (double)(d1 * d1) + (double)(d2 * d2);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) s += s_part[w];
+    partials[(size_t)ci * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+__global__ void k_loss_final(FrameArgs A, const double* __restrict__ partials, uint32_t chunks,
+                             double* __restrict__ loss) {
+  const uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= A.ncams) return;
+  double s = 0.0;
+  for (uint32_t k = 0; k < chunks; ++k) s += partials[(size_t)ci * chunks + k];
+  const CameraRec& C = A.cams[ci];
+  loss[ci] = 0.5 * s / (3.0 * (double)C.w * (double)C.h);
+}
+
+void image_loss(const FrameArgs& a, double* partials, double* loss, cudaStream_t s) {
+  if (a.ncams == 0) return;
+  k_loss_partials<<<dim3(kLossChunks, a.ncams), kBlock, 0, s>>>(a, partials); note_launch();
+  k_loss_final<<<(a.ncams + 63) / 64, 64, 0, s>>>(a, partials, kLossChunks, loss); note_launch();
 }
 
 void camera_gather(const FrameArgs& a, cudaStream_t s) {

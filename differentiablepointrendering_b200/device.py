@@ -32,6 +32,7 @@ class DeviceFrame:
         self.ldr = torch.zeros(self.pixels, 4, **f)
         self.raw = torch.zeros(self.pixels, 4, **f)
         self.dldi = torch.zeros(self.pixels, 4, **f)
+        self.loss = torch.zeros(len(self.cams), dtype=torch.float64, device=self.device)
         n = renderer.num_points
         self.grads = {k: torch.zeros((n, POINT_WIDTH[k]) if POINT_WIDTH[k] > 1 else (n,), **f) for k in POINT_FIELDS}
         self._gstruct = N.PalePoints()
@@ -50,6 +51,24 @@ class DeviceFrame:
                                           self._stream())
         _check(L, self.r._h, rc, "render_forward_device")
         return self.ldr, self.raw
+
+    def forward_loss(self, target: torch.Tensor) -> torch.Tensor:
+        """forward() with the L2 loss of every camera against `target`
+        (packed (P, 3) or (P, 4), alpha ignored) computed by the
+        post-process: dL/dI lands in self.dldi; returns the per-camera
+        losses as a float64 device tensor (compute_l2_grad /
+        compute_l2_loss, python/losses.py:10-45)."""
+        t = target.contiguous()
+        if t.dtype != torch.float32 or t.dim() != 2 or t.shape[0] != self.pixels or t.shape[1] not in (3, 4):
+            raise ValueError(f"target must be float32 ({self.pixels}, 3 or 4)")
+        L = self.r._lib
+        rc = L.pale_render_forward_loss_device(self.r._h, len(self.cams), self._cams.ctypes.data_as(N.u32p),
+                                               C.c_void_p(t.data_ptr()), t.shape[1],
+                                               C.c_void_p(self.ldr.data_ptr()), C.c_void_p(self.raw.data_ptr()),
+                                               C.c_void_p(self.dldi.data_ptr()), C.c_void_p(self.loss.data_ptr()),
+                                               self._stream())
+        _check(L, self.r._h, rc, "render_forward_loss_device")
+        return self.loss
 
     def backward(self, dldi: Optional[torch.Tensor] = None):
         """Adjoint pass with packed dL/dI (P, 4) (alpha ignored); gradients
@@ -78,10 +97,16 @@ class DeviceFrame:
         return self.r.stats()
 
 
-def l2_grad_(dldi: torch.Tensor, ldr: torch.Tensor, target_rgb: torch.Tensor) -> torch.Tensor:
-    """dL/dI of L = 1/2 mean((I - T)^2) over the RGB channels
-    (compute_l2_grad, python/losses.py:28-45), written into dldi (P, 4)."""
-    n = target_rgb.numel()
+def l2_grad_(dldi: torch.Tensor, ldr: torch.Tensor, target_rgb: torch.Tensor,
+             sizes: Optional[Sequence[tuple]] = None) -> torch.Tensor:
+    """dL/dI of L = 1/2 mean((I - T)^2) over the RGB values of each camera
+    (compute_l2_grad, python/losses.py:28-45, applied per camera as
+    training.py:634-657 does), written into dldi (P, 4) with torch ops.
+    `sizes` lists the cameras' (W, H) in packing order (one camera if None);
+    DeviceFrame.forward_loss does the same inside the post-process."""
     torch.sub(ldr[:, :3], target_rgb, out=dldi[:, :3])
-    dldi[:, :3].div_(n)
+    off = 0
+    for w, h in (sizes or [(target_rgb.shape[0], 1)]):
+        dldi[off:off + w * h, :3].div_(3 * w * h)
+        off += w * h
     return dldi

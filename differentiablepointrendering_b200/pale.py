@@ -118,6 +118,50 @@ class Renderer:
             off += n
         return out
 
+    def render_forward_loss(self, targets: Dict[str, np.ndarray]):
+        """render_forward of the cameras named in `targets` ({cam: (H,W,3)
+        or (H,W,4) float32, alpha ignored}) with the training loop's L2
+        loss computed by the post-process (compute_l2_grad /
+        compute_l2_loss, python/losses.py:10-45): returns (images as
+        render_forward, {cam: dL/dI (H,W,3) float32}, {cam: loss})."""
+        idx = [i for i, n in enumerate(self._names) if n in targets]
+        if len(idx) != len(targets):
+            raise RuntimeError(f"unknown camera in targets: {sorted(set(targets) - set(self._names))}")
+        chans = {np.asarray(targets[self._names[i]]).shape[-1] for i in idx}
+        if len(chans) > 1 or not chans <= {3, 4}:
+            raise RuntimeError("target images must all be (H,W,3) or all (H,W,4)")
+        ch = chans.pop() if chans else 3
+        parts = []
+        for i in idx:
+            w, h = self._sizes[i]
+            t = np.asarray(targets[self._names[i]], np.float32)
+            if t.shape != (h, w, ch):
+                raise RuntimeError(f"target for {self._names[i]} must have shape {(h, w, ch)}, got {t.shape}")
+            parts.append(t.reshape(-1))
+        tgt = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(ch, np.float32))
+        pix = sum(self._sizes[i][0] * self._sizes[i][1] for i in idx)
+        ldr = np.empty(max(1, pix) * 4, np.float32)
+        raw = np.empty(max(1, pix) * 4, np.float32)
+        dldi = np.empty(max(1, pix) * 4, np.float32)
+        loss = np.zeros(max(1, len(idx)), np.float64)
+        cams = N.cams_array(idx)
+        rc = self._lib.pale_render_forward_loss(self._h, len(idx), cams.ctypes.data_as(N.u32p),
+                                                tgt.ctypes.data_as(N.f32p), ch, ldr.ctypes.data_as(N.f32p),
+                                                raw.ctypes.data_as(N.f32p), dldi.ctypes.data_as(N.f32p),
+                                                loss.ctypes.data_as(C.POINTER(C.c_double)))
+        _check(self._lib, self._h, rc, "render_forward_loss")
+        images, grads, losses, off = {}, {}, {}, 0
+        for k, i in enumerate(idx):
+            w, h = self._sizes[i]
+            n = w * h * 4
+            name = self._names[i]
+            images[name] = ldr[off:off + n].reshape(h, w, 4).copy()
+            images[name + "_raw"] = raw[off:off + n].reshape(h, w, 4).copy()
+            grads[name] = dldi[off:off + n].reshape(h, w, 4)[..., :3].copy()
+            losses[name] = float(loss[k])
+            off += n
+        return images, grads, losses
+
     # ---------------------------------------------------------- backward
     def render_backward(self, targetRgb32f: Dict[str, np.ndarray]) -> Tuple[dict, dict]:
         """Adjoint pass with dL/dI images {cam: (H,W,3) float32}; returns

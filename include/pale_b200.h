@@ -222,6 +222,28 @@ int pale_render_backward(pale_handle *h, uint32_t num_selected,
                          const uint32_t *camera_indices, const float *dldi,
                          pale_points *grads, float *debug_opacity);
 
+/* Forward pass plus the training loop's L2 image loss (compute_l2_grad and
+ * compute_l2_loss, python/losses.py:10-45, per camera as
+ * python/training.py:625-657 applies them): with the LDR image I of each
+ * selected camera and the target T (RGB, packed like the images with
+ * `channels` = 3 or 4 floats per pixel, alpha ignored), the post-process
+ * writes dL/dI = (I - T) / (3 W H) (packed float4 per pixel, alpha 0) and
+ * loss[c] = 0.5 mean((I - T)^2) over the camera's RGB values (double).
+ * Host buffers; every output may be NULL. */
+int pale_render_forward_loss(pale_handle *h, uint32_t num_selected,
+                             const uint32_t *camera_indices,
+                             const float *target, uint32_t channels,
+                             float *ldr, float *raw, float *dldi,
+                             double *loss);
+
+/* Same with DEVICE pointers, enqueued on `stream` (NULL = the default
+ * stream) without waiting; d_ldr, d_raw, d_dldi and d_loss may be NULL. */
+int pale_render_forward_loss_device(pale_handle *h, uint32_t num_selected,
+                                    const uint32_t *camera_indices,
+                                    const float *d_target, uint32_t channels,
+                                    float *d_ldr, float *d_raw, float *d_dldi,
+                                    double *d_loss, void *stream);
+
 /* Same adjoint pass with DEVICE pointers for dL/dI and the gradient fields,
  * enqueued on `stream` (NULL = the default stream) without waiting. */
 int pale_render_backward_device(pale_handle *h, uint32_t num_selected,

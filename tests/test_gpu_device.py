@@ -30,7 +30,7 @@ def test_device_frame_matches_host_api(gpu, side_stream):
         stream = torch.cuda.Stream() if side_stream else torch.cuda.current_stream(dev)
         with torch.cuda.stream(stream):
             frame.forward()
-            l2_grad_(frame.dldi, frame.ldr, target)
+            l2_grad_(frame.dldi, frame.ldr, target, frame.sizes)
             frame.backward()
             ldr = frame.ldr.clone()
             grads = frame.grads["opacity"].clone()
@@ -40,7 +40,7 @@ def test_device_frame_matches_host_api(gpu, side_stream):
         for name, (w, h) in zip(r.get_camera_names(), frame.sizes):
             img = host[name]
             np.testing.assert_array_equal(ldr[off:off + w * h].view(h, w, 4).cpu().numpy(), img)
-            dl[name] = ((img[..., :3] - 0.25) / (frame.pixels * 3)).astype(np.float32)
+            dl[name] = ((img[..., :3] - 0.25) / (w * h * 3)).astype(np.float32)
             off += w * h
         g, _ = r.render_backward(dl)
         np.testing.assert_allclose(grads.cpu().numpy(), g["opacity"], rtol=1e-4, atol=1e-9)

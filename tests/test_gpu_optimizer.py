@@ -152,7 +152,7 @@ def test_device_training_loop_moves_opacity_towards_target(gpu):
     loss falls and the opacities rise."""
     import torch
 
-    from differentiablepointrendering_b200.device import DeviceFrame, l2_grad_
+    from differentiablepointrendering_b200.device import DeviceFrame
 
     pts = make_surfels(4000, 77)
     target_pts = {k: v.copy() for k, v in pts.items()}
@@ -174,9 +174,7 @@ def test_device_training_loop_moves_opacity_towards_target(gpu):
         cfg = {"optimizer_type": "adam", "learning_rate_opacity": 0.05}
         losses = []
         for _ in range(12):
-            f.forward()
-            losses.append(float(((f.ldr[:, :3] - target) ** 2).mean()))
-            l2_grad_(f.dldi, f.ldr, target)
+            losses.append(float(f.forward_loss(target).sum()))
             f.backward()
             f.step(cfg)
         torch.cuda.synchronize()
