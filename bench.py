@@ -134,7 +134,7 @@ def kernel_bytes(sf: dict, sb: dict) -> dict:
     fwd_q = sf["gather_queries"]
     adj_q = sb["gather_queries"]
     return {
-        "k_cg_trace": seg(sf["gather_segments"], sf["gather_node_visits"], sf["gather_surfel_tests"]),
+        "k_cg_round": seg(sf["gather_segments"], sf["gather_node_visits"], sf["gather_surfel_tests"]),
         "k_cg_lookup": look(fwd_q, sf["gather_photons_scanned"]),
         "k_adj_bounce": seg(sb["adjoint_segments"], sb["node_visits"], sb["surfel_tests"])
         + 96.0 * sb["adjoint_segments"],
@@ -143,7 +143,7 @@ def kernel_bytes(sf: dict, sb: dict) -> dict:
 
 
 def kernel_times(sf: dict, sb: dict) -> dict:
-    return {"k_cg_trace": (sf["trace_ms"], sf["trace_launches"]),
+    return {"k_cg_round": (sf["trace_ms"], sf["trace_launches"]),
             "k_cg_lookup": (sf["lookup_ms"], sf["lookup_launches"]),
             "k_adj_bounce": (sb["adjoint_bounce_ms"], sb["adjoint_bounce_launches"]),
             "k_transport": (sb["transport_ms"], sb["transport_launches"])}

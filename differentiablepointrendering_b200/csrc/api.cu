@@ -147,8 +147,9 @@ struct pale_handle {
   // camera-gather wavefront
   uint32_t path_cap = 0;
   KernelTimer timer;          // device time of the hot kernels of the last call
-  DBuf<RayRec> cg_paths;
-  DBuf<float4> cg_qrec;
+  DBuf<RayRec> cg_paths, cg_paths2;
+  DBuf<float4> cg_qrec, cg_info_b;
+  DBuf<uint4> cg_info_a;
   DBuf<uint32_t> cg_counts;
   DBuf<float4> cg_res, cg_fb;
   // run state, seeds, images, gradients
@@ -532,14 +533,16 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->job_count.alloc(2 * kMaxJobsPerBatch);
   h->job_start.alloc(2 * kMaxJobsPerBatch);
   // camera paths in flight: every pass of every pixel when that fits in
-  // 2^25 paths (4.3 GB of paths, lookup records and results), else chunks of whole
-  // passes
+  // 2^25 paths (3.2 GB of path queues, 8.6 GB of lookup records, 1 GB of
+  // per-entry state), else chunks of whole passes
   if (all_pix >= (1ull << 31)) throw ArgError("too many camera pixels");
   const uint64_t want = all_pix * std::max<uint32_t>(1u, st.gather_passes);
   h->path_cap = (uint32_t)std::max<uint64_t>(std::max<uint64_t>(all_pix, 1), std::min<uint64_t>(want, 1ull << 25));
-  h->cg_paths.alloc(h->path_cap); h->cg_qrec.alloc(4 * (size_t)h->path_cap); h->cg_res.alloc(h->path_cap);
+  h->cg_paths.alloc(h->path_cap); h->cg_paths2.alloc(h->path_cap);
+  h->cg_qrec.alloc(2 * (size_t)kGatherHits * h->path_cap); h->cg_res.alloc(h->path_cap);
+  h->cg_info_a.alloc(h->path_cap); h->cg_info_b.alloc(h->path_cap);
   h->cg_fb.alloc(std::max<uint64_t>(all_pix, 1));
-  h->cg_counts.alloc(kMaxLayers + 2);
+  h->cg_counts.alloc(2 * (kMaxLayers + 2));
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   CK(cudaStreamSynchronize(s));
 }
@@ -728,8 +731,11 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.rng_mode = st.rng_mode;
   F.exposure = st.exposure;
   F.gamma = st.gamma;
-  F.paths = h->cg_paths.p;
+  F.paths[0] = h->cg_paths.p;
+  F.paths[1] = h->cg_paths2.p;
   F.qrec = h->cg_qrec.p;
+  F.info_a = h->cg_info_a.p;
+  F.info_b = h->cg_info_b.p;
   F.counts = h->cg_counts.p;
   F.res = h->cg_res.p;
   F.fb = h->cg_fb.p;

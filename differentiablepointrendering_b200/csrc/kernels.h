@@ -162,11 +162,15 @@ struct FrameArgs {
   uint32_t gather_passes;
   uint32_t rng_mode;
   float exposure, gamma;
-  // wavefront buffers: path queue, lookup records (4 float4 each), queue
-  // length per layer (kMaxLayers + 2 words), per-path radiance, running
+  // wavefront buffers: path queues (ping-pong by round), lookup records (2
+  // float4 each, up to kGatherHits per queue entry), per-entry record range
+  // and end state, queue lengths per round (kMaxLayers + 2 words) followed
+  // by record counts per round (as many), per-path radiance, running
   // framebuffer
-  RayRec* paths;
+  RayRec* paths[2];
   float4* qrec;
+  uint4* info_a;
+  float4* info_b;
   uint32_t* counts;
   float4* res;
   float4* fb;
@@ -179,6 +183,12 @@ struct FrameArgs {
   uint32_t target_channels;
   float* dldi;
 };
+
+// Surfel layers collected per traversal of the camera gather.
+#ifndef PALE_GATHER_HITS
+#define PALE_GATHER_HITS 8
+#endif
+constexpr int kGatherHits = PALE_GATHER_HITS;
 
 // Per-camera L2 loss 0.5 mean((ldr - target)^2) over the RGB values of
 // each camera of a finished frame (needs a.ldr and a.target), summed in

@@ -335,14 +335,21 @@ __device__ __forceinline__ void primary_ray(const CameraRec& C, float px, float 
 // launchCameraGatherKernel (PrimalKernels.cpp:500-653) as a wavefront.  A
 // camera path is one (pixel, gather pass); it walks the surfel layers of its
 // ray front to back, compositing L += T*alpha*Lo, T *= 1 - alpha, until a
-// mesh (emitter or diffuse lookup) or a miss ends it.  Each layer is one
-// launch over the compacted queue of live paths, so the lanes of a warp all
-// trace and shade one layer instead of walking different numbers of layers.
-// The layer loop draws no random numbers, so queue order does not matter.
-// Each finished path writes its radiance to res[path]; k_cg_finalize then
-// adds the passes of a pixel in pass order, cur + fb, as the reference's
-// sequence of launches does, and applies launchPostProcessKernel
-// (PostprocessKernel.cpp:11-106).
+// mesh (emitter or diffuse lookup) or a miss ends it.  The reference traces
+// every layer from the root: the closest hit from the previous hit point
+// advanced by 1e-4.  Here one traversal per round collects the K closest
+// surfels and the round walks them in order, re-intersecting each from the
+// chained origin exactly as that layer's trace would (the first is that
+// trace's own hit; a surfel that is not hit from the chained origin, e.g.
+// within 1e-4 behind the previous layer, is passed over as the layered walk
+// passes over it); a round that used all K continues from the last one.
+// Every layer's photon lookup becomes a record; k_cg_lookup gives each
+// record a warp, and k_cg_compose adds a path's contributions in layer order,
+// so the sums are the layered walk's.  The walk draws no random numbers, so
+// queue order does not matter.  Each finished path writes its radiance to
+// res[path]; k_cg_finalize then adds the passes of a pixel in pass order,
+// cur + fb, as the reference's sequence of launches does, and applies
+// launchPostProcessKernel (PostprocessKernel.cpp:11-106).
 
 __device__ __forceinline__ uint32_t find_camera(const FrameArgs& A, uint32_t gp) {
   uint32_t ci = 0;
@@ -369,81 +376,156 @@ __global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1) {
   rec.o = make_float4(o.x, o.y, o.z, __uint_as_float(path));
   rec.d = make_float4(d.x, d.y, d.z, 1.0f);
   rec.t = make_float4(0.f, 0.f, 0.f, 0.f);
-  A.paths[path] = rec;
+  A.paths[0][path] = rec;
 }
 
-// Layer step 1: trace.  One lane per queue entry; entries whose path ended
-// in the previous layer's lookup carry path id kInvalid and are skipped.
-// Misses and emitter hits finish their path here; surfel hits and diffuse
-// mesh hits append a lookup record (warp-aggregated atomic on
-// counts[layer + 1]), whose index becomes the path's queue entry for the
-// next layer.
-// Lookup record (4 x float4): (hit position, path) (ray direction or mesh
-// normal, T) (radiance so far, alpha_geom) (surfel or material index, kind).
-enum : uint32_t { kQuerySurfel = 0, kQueryMesh = 1 };
+// Lookup record (2 x float4): (position, weight) (lookup normal, index |
+// kind << 30), weight = T * alpha for a surfel layer, T for the diffuse mesh
+// that ends a path.  k_cg_lookup overwrites the first float4 with the
+// layer's radiance contribution.  Unused slots of an entry's range are
+// kRecNone with zero contribution.
+enum : uint32_t { kRecSurfel = 0, kRecMesh = 1, kRecNone = 2 };
+constexpr uint32_t kRecIndexMask = 0x3FFFFFFFu;
 
-__global__ void __launch_bounds__(kBlock) k_cg_trace(FrameArgs A, uint32_t layer) {
+__device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float w, V3 nrm, uint32_t idx,
+                                           uint32_t kind) {
+  q[2 * (size_t)r] = make_float4(pos.x, pos.y, pos.z, w);
+  q[2 * (size_t)r + 1] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(idx | (kind << 30)));
+}
+
+// Round step 1: one lane per queue entry (a live path).
+template <int K>
+__global__ void __launch_bounds__(kBlock) k_cg_round(FrameArgs A, uint32_t round) {
   extern __shared__ BvhNode s_top[];
   stage_top_nodes(A.scene, s_top);
   const SceneView& S = A.scene;
-  const uint32_t n = A.counts[layer];
+  const uint32_t n = A.counts[round];
+  const RayRec* __restrict__ in = A.paths[round & 1];
+  RayRec* __restrict__ out = A.paths[(round + 1) & 1];
   const int lane = threadIdx.x & 31;
+  const float inf = __int_as_float(0x7f800000);
   TraceCounters ctr{0, 0};
   uint32_t segs = 0;
   for (uint32_t b = blockIdx.x * kBlock; b < n; b += gridDim.x * kBlock) {
     const uint32_t slot = b + threadIdx.x;
-    bool q = false;
-    float4 qa, qb, qc;
-    uint4 qd;
-    if (slot < n) {
-      const RayRec rec = A.paths[slot];
-      const uint32_t path = __float_as_uint(rec.o.w);
-      if (path != kInvalid) {
+    const bool live = slot < n;
+    RayRec rec{};
+    float tl[K];
+    uint32_t pl[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) pl[k] = 0;
+    uint32_t count = 0, nslots = 0;
+    Hit hm{};
+    V3 o{}, d{}, invw{}, dd{};
+    float best_m = inf;
+    if (live) {
+      rec = in[slot];
+      o = xyz(rec.o);
+      d = xyz(rec.d);
+      invw = safe_inv(d);
+      hm = intersect_meshes(S, o, d, invw, best_m);
+      if (S.has_pc &&
+          entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best_m),
+                  best_m)) {
+        dd = normalize(d);
+        const float limit = best_m < 3.0e38f ? best_m * 1.00001f + 1e-6f : inf;
+        count = surfel_khit<K>(S, s_top, o, dd, 1e-5f, limit, tl, pl, ctr, A.st);
+      }
+      nslots = count + (count < (uint32_t)K ? 1u : 0u);
+    }
+    // record range of this entry: warp scan of the slot counts, one atomic
+    uint32_t incl = nslots;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += v;
+    }
+    const uint32_t wtotal = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 0 && wtotal) base = atomicAdd(&A.counts[kMaxLayers + 2 + round], wtotal);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const uint32_t first = base + incl - nslots;
+
+    bool cont = false;
+    uint32_t flags = 0;
+    V3 c_em = v3(0.f, 0.f, 0.f);
+    V3 oc = o;
+    float T = rec.d.w;
+    uint32_t layer = __float_as_uint(rec.t.w);
+    uint32_t used = 0;
+    if (live) {
+      bool ended = false, mesh_first = false;
+      for (uint32_t i = 0; i < count && !ended; ++i) {
+        float th, a;
+        V3 x;
+        if (!surfel_hit(S.sf, pl[i], oc, dd, 1e-5f, inf, th, x, a)) continue;
+        // the mesh wins when it is nearer than this surfel from the chained origin
+        const float tw = dot(x - oc, d);
+        const float tm = hm.inst >= 0 ? dot(hm.pos - oc, d) : inf;
+        if (!(tw > 0.0f && tw < tm)) {
+          mesh_first = true;
+          break;
+        }
         ++segs;
-        const V3 d = xyz(rec.d);
-        const float T = rec.d.w;
-        V3 acc = xyz(rec.t);
-        const Hit h = intersect_scene(S, s_top, xyz(rec.o), d, ctr, A.st);
-        if (h.inst >= (int)S.mesh.instances) {
-          q = true;
-          qa = make_float4(h.pos.x, h.pos.y, h.pos.z, rec.o.w);
-          qb = make_float4(d.x, d.y, d.z, T);
-          qc = make_float4(acc.x, acc.y, acc.z, h.alpha);
-          qd = make_uint4(h.prim, kQuerySurfel, 0u, 0u);
-        } else if (h.inst >= 0) {
-          const uint32_t mi = __ldg(&S.mesh.material[h.inst]);
-          const float4 mat = __ldg(&S.mesh.materials[mi]);
-          if (mat.w > 0.f) {
-            V3 Le = scale(xyz(mat), mat.w);
-            Le = v3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
-            acc = acc + scale(Le, T);
-            A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
-          } else {
-            const V3 nrm = hit_normal(S, h);
-            q = true;
-            qa = make_float4(h.pos.x, h.pos.y, h.pos.z, rec.o.w);
-            qb = make_float4(nrm.x, nrm.y, nrm.z, T);
-            qc = make_float4(acc.x, acc.y, acc.z, 0.f);
-            qd = make_uint4(mi, kQueryMesh, 0u, 0u);
-          }
+        const float ae = __ldg(&S.sf.n[pl[i]]).w * a;
+        V3 nrm = xyz(__ldg(&S.sf.cn[pl[i]]));
+        if (dot(nrm, -d) < 0.0f) nrm = -nrm;
+        put_record(A.qrec, first + used, x, T * ae, nrm, pl[i], kRecSurfel);
+        ++used;
+        T *= (1.0f - ae);
+        if (layer + 1 >= (uint32_t)kMaxLayers) {
+          flag_error(A.st, kErrLayerCap);
+          ended = true;
+          break;
+        }
+        ++layer;
+        oc = x + scale(d, 1e-4f);
+      }
+      if (!ended) {
+        if (count == (uint32_t)K && !mesh_first) {
+          cont = true;   // more surfels may lie beyond the K-th
         } else {
-          A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
+          // the layer that ends the path, traced from the chained origin
+          ++segs;
+          float bm;
+          const Hit h2 = intersect_meshes(S, oc, d, invw, bm);
+          if (h2.inst >= 0) {
+            const uint32_t mi = __ldg(&S.mesh.material[h2.inst]);
+            const float4 mat = __ldg(&S.mesh.materials[mi]);
+            if (mat.w > 0.f) {
+              V3 Le = scale(xyz(mat), mat.w);
+              Le = v3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
+              c_em = scale(Le, T);
+              flags = 1;
+            } else {
+              put_record(A.qrec, first + used, h2.pos, T, hit_normal(S, h2), mi, kRecMesh);
+              ++used;
+            }
+          }
         }
       }
+      for (uint32_t r = used; r < nslots; ++r)
+        put_record(A.qrec, first + r, v3(0.f, 0.f, 0.f), 0.f, v3(0.f, 0.f, 0.f), 0u, kRecNone);
+      A.info_b[slot] = make_float4(c_em.x, c_em.y, c_em.z, 0.f);
     }
-    const unsigned ballot = __ballot_sync(0xffffffffu, q);
-    if (ballot) {
-      const int leader = __ffs(ballot) - 1;
-      uint32_t base = 0;
-      if (lane == leader) base = atomicAdd(&A.counts[layer + 1], (uint32_t)__popc(ballot));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (q) {
-        float4* r = A.qrec + 4 * (size_t)(base + __popc(ballot & ((1u << lane) - 1u)));
-        r[0] = qa;
-        r[1] = qb;
-        r[2] = qc;
-        r[3] = make_float4(__uint_as_float(qd.x), __uint_as_float(qd.y), 0.f, 0.f);
+    // next-round queue entries for the paths that continue
+    const unsigned cb = __ballot_sync(0xffffffffu, cont);
+    uint32_t nbase = 0;
+    if (cb) {
+      if (lane == __ffs(cb) - 1) nbase = atomicAdd(&A.counts[round + 1], (uint32_t)__popc(cb));
+      nbase = __shfl_sync(0xffffffffu, nbase, __ffs(cb) - 1);
+    }
+    if (live) {
+      uint32_t next = kInvalid;
+      if (cont) {
+        next = nbase + __popc(cb & ((1u << lane) - 1u));
+        RayRec nr;
+        nr.o = make_float4(oc.x, oc.y, oc.z, rec.o.w);
+        nr.d = make_float4(d.x, d.y, d.z, T);
+        nr.t = make_float4(0.f, 0.f, 0.f, __uint_as_float(layer));   // radiance added by k_cg_compose
+        out[next] = nr;
       }
+      A.info_a[slot] = make_uint4(first, nslots | (flags << 8), __float_as_uint(rec.o.w), next);
     }
   }
   warp_count(&A.st->gather_segments, segs);
@@ -453,78 +535,69 @@ __global__ void __launch_bounds__(kBlock) k_cg_trace(FrameArgs A, uint32_t layer
   warp_count(&A.st->gather_surfel_tests, ctr.tests);
 }
 
-// Layer step 2: one warp per lookup record (warps stride over the records,
-// so in deep layers, where few paths are left, every lookup has a warp of
-// its own).  Lane 0 then composites the hit: a surfel adds T*alpha*Lo and
-// passes the path on (record index = queue entry for the next layer); a
-// diffuse mesh hit adds T*Lo and ends the path.
-__global__ void __launch_bounds__(kBlock) k_cg_lookup(FrameArgs A, uint32_t layer) {
+// Round step 2: one warp per lookup record (warps stride over the records,
+// so in deep rounds every lookup has a warp of its own).  Lane 0 writes the
+// layer's contribution Lo * weight over the record's first float4.
+__global__ void __launch_bounds__(kBlock) k_cg_lookup(FrameArgs A, uint32_t round) {
   __shared__ float4 s_terms[kBlock];
   const SceneView& S = A.scene;
-  const uint32_t n = A.counts[layer + 1];
+  const uint32_t n = A.counts[kMaxLayers + 2 + round];
   const int lane = threadIdx.x & 31;
   float4* terms = s_terms + (threadIdx.x & ~31u);
   const uint32_t warps = gridDim.x * (kBlock / 32);
   uint32_t queries = 0, scanned = 0;
-  // lanes 0-15 hold the 16 floats of the next record, loaded one query ahead
+  // lanes 0-7 hold the 8 floats of the next record, loaded one record ahead
   uint32_t i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-  float pre = (i < n && lane < 16) ? reinterpret_cast<const float*>(A.qrec + 4 * (size_t)i)[lane] : 0.f;
+  float pre = (i < n && lane < 8) ? reinterpret_cast<const float*>(A.qrec + 2 * (size_t)i)[lane] : 0.f;
   for (; i < n; i += warps) {
     const float cur = pre;
-    if (i + warps < n && lane < 16) pre = reinterpret_cast<const float*>(A.qrec + 4 * (size_t)(i + warps))[lane];
+    if (i + warps < n && lane < 8) pre = reinterpret_cast<const float*>(A.qrec + 2 * (size_t)(i + warps))[lane];
     auto field = [&](int f) { return __shfl_sync(0xffffffffu, cur, f); };
-    const float4 qa = make_float4(field(0), field(1), field(2), field(3));
-    const float4 qb = make_float4(field(4), field(5), field(6), field(7));
-    const float4 qc = make_float4(field(8), field(9), field(10), field(11));
-    const float4 qd = make_float4(field(12), field(13), field(14), field(15));
-    const uint32_t idx = __float_as_uint(qd.x), kind = __float_as_uint(qd.y);
-    const V3 pos = xyz(qa);
-    V3 nrm = xyz(qb);
-    if (kind == kQuerySurfel) {
-      const V3 d = xyz(qb);
-      nrm = xyz(__ldg(&S.sf.cn[idx]));
-      if (dot(nrm, -d) < 0.0f) nrm = -nrm;
-    }
+    const float4 ra = make_float4(field(0), field(1), field(2), field(3));
+    const float4 rb = make_float4(field(4), field(5), field(6), field(7));
+    const uint32_t word = __float_as_uint(rb.w);
+    const uint32_t kind = word >> 30, idx = word & kRecIndexMask;
+    if (kind == kRecNone) continue;
     uint32_t cnt = 0;
-    const V3 E = gather_irradiance_warp(S.grid, pos, nrm, terms, cnt);
+    const V3 E = gather_irradiance_warp(S.grid, xyz(ra), xyz(rb), terms, cnt);
     if (lane == 0) {
       ++queries;
       scanned += cnt;
-      const uint32_t path = __float_as_uint(qa.w);
-      float T = qb.w;
-      V3 acc = xyz(qc);
-      RayRec next;
-      next.o = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
-      next.d = make_float4(0.f, 0.f, 0.f, 0.f);
-      next.t = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (kind == kQuerySurfel) {
-        const V3 d = xyz(qb);
+      V3 Lo;
+      if (kind == kRecSurfel) {
         const float4 al = __ldg(&S.sf.alb[idx]);
-        V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
-        float ae = __ldg(&S.sf.n[idx]).w * qc.w;
-        acc = acc + scale(Lo, T * ae);
-        T *= (1.0f - ae);
-        if (layer + 1 < (uint32_t)kMaxLayers) {
-          V3 no = pos + scale(d, 1e-4f);
-          next.o = make_float4(no.x, no.y, no.z, qa.w);
-          next.d = make_float4(d.x, d.y, d.z, T);
-          next.t = make_float4(acc.x, acc.y, acc.z, 0.f);
-        } else {
-          flag_error(A.st, kErrLayerCap);
-          A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
-        }
+        Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
       } else {
         const float4 mat = __ldg(&S.mesh.materials[idx]);
-        V3 Lo = mul(scale(xyz(mat), kInvPi), E);
-        acc = acc + scale(Lo, T);
-        A.res[path] = make_float4(acc.x, acc.y, acc.z, 0.f);
+        Lo = mul(scale(xyz(mat), kInvPi), E);
       }
-      A.paths[i] = next;
+      const V3 c = scale(Lo, ra.w);
+      A.qrec[2 * (size_t)i] = make_float4(c.x, c.y, c.z, 0.f);
     }
   }
   warp_count(&A.st->gather_queries, queries);
   warp_count(&A.st->photons_scanned, scanned);
   warp_count(&A.st->gather_photons_scanned, scanned);
+}
+
+// Round step 3: one lane per entry adds its layers' contributions in order
+// (then an emitter's), as the layered walk's acc = acc + c does, and hands
+// the sum to the path's next-round entry or to res[path].
+__global__ void k_cg_compose(FrameArgs A, uint32_t round) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= A.counts[round]) return;
+  const RayRec* __restrict__ in = A.paths[round & 1];
+  RayRec* __restrict__ out = A.paths[(round + 1) & 1];
+  const uint4 ia = A.info_a[e];
+  V3 acc = xyz(in[e].t);
+  const uint32_t nslots = ia.y & 0xFFu;
+  for (uint32_t r = 0; r < nslots; ++r) acc = acc + xyz(A.qrec[2 * (size_t)(ia.x + r)]);
+  if (ia.y & 0x100u) acc = acc + xyz(A.info_b[e]);
+  if (ia.w != kInvalid) {
+    out[ia.w].t = make_float4(acc.x, acc.y, acc.z, out[ia.w].t.w);
+  } else {
+    A.res[ia.z] = make_float4(acc.x, acc.y, acc.z, 0.f);
+  }
 }
 
 // fb += res/spp over passes [p0, p1) in pass order; the last chunk writes the
@@ -624,30 +697,32 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = top_smem(a.scene);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_cg_trace, kBlock, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_cg_round<kGatherHits>, kBlock, smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup, kBlock, 0);
   const uint32_t grid_t = (uint32_t)std::max(1, sms * std::max(1, per_sm_t));
   const uint32_t grid_l = (uint32_t)std::max(1, sms * std::max(1, per_sm_l));
   for (uint32_t p0 = 0; p0 < a.gather_passes; p0 += ppc) {
     const uint32_t p1 = std::min(a.gather_passes, p0 + ppc);
     const uint32_t n = (p1 - p0) * a.total_pixels;
-    cudaMemsetAsync(a.counts, 0, (kMaxLayers + 2) * sizeof(uint32_t), s);
+    cudaMemsetAsync(a.counts, 0, 2 * (kMaxLayers + 2) * sizeof(uint32_t), s);
     k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1); note_launch();
-    uint32_t layer = 0;
-    while (layer < (uint32_t)kMaxLayers) {
-      for (uint32_t group = 0; group < 16 && layer < (uint32_t)kMaxLayers; ++group, ++layer) {
+    // every round consumes at least one layer of each live path, so
+    // kMaxLayers rounds bound the walk (the layer cap ends longer ones)
+    uint32_t round = 0, live = n;
+    while (round < (uint32_t)kMaxLayers && live) {
+      for (uint32_t group = 0; group < 16 && round < (uint32_t)kMaxLayers; ++group, ++round) {
         if (a.timer) a.timer->begin(kTimeTrace, s);
-        k_cg_trace<<<grid_t, kBlock, smem, s>>>(a, layer); note_launch();
+        k_cg_round<kGatherHits><<<grid_t, kBlock, smem, s>>>(a, round); note_launch();
         if (a.timer) a.timer->end(s);
         if (a.timer) a.timer->begin(kTimeLookup, s);
-        k_cg_lookup<<<grid_l, kBlock, 0, s>>>(a, layer); note_launch();
+        k_cg_lookup<<<grid_l, kBlock, 0, s>>>(a, round); note_launch();
         if (a.timer) a.timer->end(s);
+        // queues only shrink, so `live` bounds the entries of every round of the group
+        k_cg_compose<<<blocks_for(live), kBlock, 0, s>>>(a, round); note_launch();
       }
-      // the host reads the queue length after each group of 16 layers
-      uint32_t left = 0;
-      cudaMemcpyAsync(&left, a.counts + layer, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+      // the host reads the queue length after each group of 16 rounds
+      cudaMemcpyAsync(&live, a.counts + round, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
       cudaStreamSynchronize(s);
-      if (left == 0) break;
     }
     k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1, p0 == 0, p1 == a.gather_passes); note_launch();
   }

@@ -193,6 +193,104 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode
   return hit;
 }
 
+// The K closest surfels with t in (tmin, limit) along (o, d), in increasing
+// t (ties keep the surfel found first): the traversal of surfel_closest
+// with the culling distance of the K-th hit found so far.  Returns the
+// number of hits (<= K); t_out/prim_out hold them in order.
+template <int K>
+__device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
+                                                float tmin, float limit, float (&t_out)[K], uint32_t (&prim_out)[K],
+                                                TraceCounters& ctr, RunState* st) {
+  if (S.node_count == 0) return 0;
+  const V3 inv = safe_inv(d);
+  uint32_t count = 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) t_out[k] = limit;
+  float best = limit;   // t_out[K - 1] once K hits are held
+  uint32_t stack_node[kStackDepth];
+  float stack_t[kStackDepth];
+  int sp = 0;
+  uint32_t node = 0;
+  const uint32_t visit_cap = 2u * S.node_count + 64u;
+  for (uint32_t visit = 0;; ++visit) {
+    float4 a, b, c;
+    uint4 w;
+    if (node >= S.node_count || visit > visit_cap) {
+      flag_error(st, kErrBounds);
+      break;
+    }
+    load_node(S, smem_top, node, a, b, c, w);
+    ctr.nodes++;
+    float e0 = w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
+    float e1 = w.y == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, b.z, b.w, c.x, c.y, c.z, c.w, best);
+    bool h0 = entered(e0, best), h1 = entered(e1, best);
+    uint32_t lw[2] = {w.x, w.y};
+    bool lh[2] = {h0 && (w.x & kLeafFlag) != 0, h1 && (w.y & kLeafFlag) != 0};
+    int first = (e1 < e0) ? 1 : 0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      int cidx = k == 0 ? first : 1 - first;
+      if (!lh[cidx]) continue;
+      uint32_t word = lw[cidx];
+      uint32_t f0 = word & 0x0FFFFFFFu, cnt = ((word >> 28) & 7u) + 1u;
+      if (f0 + cnt > S.sf.count) {
+        flag_error(st, kErrBounds);
+        continue;
+      }
+      for (uint32_t j = 0; j < cnt; ++j) {
+        float th, aa;
+        V3 xx;
+        ctr.tests++;
+        if (surfel_hit(S.sf, f0 + j, o, d, tmin, best, th, xx, aa)) {
+          // insert into the sorted list (static indices: stays in registers)
+          uint32_t pj = f0 + j;
+#pragma unroll
+          for (int q = 0; q < K; ++q) {
+            if (th < t_out[q]) {
+              const float tt = t_out[q];
+              const uint32_t pp = prim_out[q];
+              t_out[q] = th;
+              prim_out[q] = pj;
+              th = tt;
+              pj = pp;
+            }
+          }
+          count = count < (uint32_t)K ? count + 1 : count;
+          if (count == (uint32_t)K) best = t_out[K - 1];
+        }
+      }
+    }
+    h0 = h0 && !(w.x & kLeafFlag) && e0 <= best;
+    h1 = h1 && !(w.y & kLeafFlag) && e1 <= best;
+    if (h0 && h1) {
+      uint32_t nearN = e0 <= e1 ? w.x : w.y, farN = e0 <= e1 ? w.y : w.x;
+      float farT = e0 <= e1 ? e1 : e0;
+      if (sp < kStackDepth) {
+        stack_node[sp] = farN;
+        stack_t[sp] = farT;
+        ++sp;
+      } else {
+        flag_error(st, kErrStackOverflow);
+      }
+      node = nearN;
+      continue;
+    }
+    if (h0) { node = w.x; continue; }
+    if (h1) { node = w.y; continue; }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (stack_t[sp] <= best) {
+        node = stack_node[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  return count;
+}
+
 // The closest mesh hit, in object space per instance (intersectBLASMesh,
 // IntersectionKernels.h:37-105); `best` is the world distance of the hit
 // (+inf on a miss).
