@@ -189,6 +189,17 @@ struct FrameArgs {
 #define PALE_GATHER_HITS 8
 #endif
 constexpr int kGatherHits = PALE_GATHER_HITS;
+// Resident blocks per SM the traversal kernels are compiled for (their
+// register budget: 65536 / (kBlock * blocks)).
+#ifndef PALE_TRACE_MIN_BLOCKS
+#define PALE_TRACE_MIN_BLOCKS 4
+#endif
+constexpr int kTraceMinBlocks = PALE_TRACE_MIN_BLOCKS;
+// The same for the warp-per-lookup kernels (camera lookups, transport).
+#ifndef PALE_LOOKUP_MIN_BLOCKS
+#define PALE_LOOKUP_MIN_BLOCKS 4
+#endif
+constexpr int kLookupMinBlocks = PALE_LOOKUP_MIN_BLOCKS;
 
 // Per-camera L2 loss 0.5 mean((ldr - target)^2) over the RGB values of
 // each camera of a finished frame (needs a.ldr and a.target), summed in

@@ -395,7 +395,7 @@ __device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float 
 
 // Round step 1: one lane per queue entry (a live path).
 template <int K>
-__global__ void __launch_bounds__(kBlock) k_cg_round(FrameArgs A, uint32_t round) {
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs A, uint32_t round) {
   extern __shared__ BvhNode s_top[];
   stage_top_nodes(A.scene, s_top);
   const SceneView& S = A.scene;
@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_round(FrameArgs A, uint32_t round
 // Round step 2: one warp per lookup record (warps stride over the records,
 // so in deep rounds every lookup has a warp of its own).  Lane 0 writes the
 // layer's contribution Lo * weight over the record's first float4.
-__global__ void __launch_bounds__(kBlock) k_cg_lookup(FrameArgs A, uint32_t round) {
+__global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArgs A, uint32_t round) {
   __shared__ float4 s_terms[kBlock];
   const SceneView& S = A.scene;
   const uint32_t n = A.counts[kMaxLayers + 2 + round];
@@ -804,7 +804,7 @@ __global__ void __launch_bounds__(kMaxJobsPerBatch) k_job_scan(AdjointArgs A, ui
 }
 
 // launchAdjointIntersectKernel (AdjointKernels.cpp:87-386).
-__global__ void __launch_bounds__(kBlock) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index) {
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index) {
   extern __shared__ BvhNode s_top[];
   const uint32_t n_in = A.st->active[parity];
   if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
@@ -999,7 +999,7 @@ __device__ __forceinline__ AlphaGrad alpha_grad(const SurfelView& S, uint32_t k,
 // gradient event (warps stride over the event list): the warp does the
 // photon lookup of the event's end point together (gather_irradiance_warp)
 // and lane 0 adds the event's opacity-gradient term with one atomicAdd.
-__global__ void __launch_bounds__(kBlock) k_transport(AdjointArgs A) {
+__global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_transport(AdjointArgs A) {
   __shared__ float4 s_terms[kBlock];
   const uint32_t count = A.st->event_count;
   const SceneView& S = A.scene;
