@@ -141,6 +141,7 @@ struct pale_handle {
   DBuf<EventRec> ev_stage, ev_list;
   // adjoint batches
   uint32_t adj_cap = 0;
+  DBuf<uint32_t> adj_keys, adj_perm, adj_keys_tmp, adj_perm_tmp, adj_sort_temp;   // ray order of a bounce
   DBuf<AdjJob> d_jobs;
   DBuf<CameraRec> d_adj_cams;
   DBuf<uint32_t> job_count, job_start;
@@ -525,6 +526,9 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   const uint64_t adj_want = all_pix * std::max<uint32_t>(1u, st.adjoint_passes);
   h->adj_cap = (uint32_t)std::max<uint64_t>(max_pix, std::min<uint64_t>(adj_want, 1ull << 24));
   const size_t qa = std::max<size_t>(qc, h->adj_cap);
+  h->adj_keys.alloc(h->adj_cap); h->adj_perm.alloc(h->adj_cap);
+  h->adj_keys_tmp.alloc(h->adj_cap); h->adj_perm_tmp.alloc(h->adj_cap);
+  h->adj_sort_temp.alloc(radix_temp_words(h->adj_cap));
   h->q0.alloc(qa); h->q1.alloc(qa); h->qstage.alloc(qa); h->qflags.alloc(qa);
   h->tile_counts.alloc(qa / kBlock + 1); h->tile_offsets.alloc(qa / kBlock + 1);
   h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
@@ -813,6 +817,12 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.light0_valid = h->n_lights > 0;
   A.light0_area = h->light0_area;
   A.timer = &h->timer;
+  A.sort_keys = h->adj_keys.p;
+  A.perm = h->adj_perm.p;
+  A.sort_keys_tmp = h->adj_keys_tmp.p;
+  A.perm_tmp = h->adj_perm_tmp.p;
+  A.sort_temp = h->adj_sort_temp.p;
+  A.sort_capacity = h->adj_cap;
   // jobs in the reference's order (camera-major, then pass), packed into
   // batches of at most adj_cap paths and kMaxJobsPerBatch jobs
   std::vector<CameraRec> sel(nsel);

@@ -258,6 +258,16 @@ struct AdjointArgs {
   uint32_t light0_valid;
   float light0_area;
   KernelTimer* timer;      // host side, may be null
+  // Bounces after the first trace their rays in the order of a sort by
+  // (direction octant, origin Morton code): thread t takes queue slot
+  // perm[t].  Each ray keeps its slot for its random stream and its
+  // outputs, so the results do not depend on the order.  Null: slot order.
+  uint32_t* sort_keys;     // 4 arrays of the queue capacity: keys, perm,
+  uint32_t* perm;          //   and the sort's ping-pong copies
+  uint32_t* sort_keys_tmp;
+  uint32_t* perm_tmp;
+  uint32_t* sort_temp;     // radix_temp_words(queue capacity)
+  uint32_t sort_capacity;
 };
 
 void photon_emit(const PhotonArgs& a, cudaStream_t s);

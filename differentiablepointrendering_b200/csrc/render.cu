@@ -803,17 +803,59 @@ __global__ void __launch_bounds__(kMaxJobsPerBatch) k_job_scan(AdjointArgs A, ui
   cnt[j] = 0u;
 }
 
+// Sort key of a queued ray: direction octant (3 bits) over the Morton code
+// of its origin on a 512^3 lattice over the photon grid's box (27 bits).
+__device__ __forceinline__ uint32_t spread9(uint32_t v) {
+  v &= 0x1FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void k_adj_keys(AdjointArgs A, uint32_t parity) {
+  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
+  if (t >= A.st->active[parity]) return;
+  const RayRec ry = A.qb.q[parity][t];
+  const GridView& G = A.scene.grid;
+  uint32_t q[3];
+  const float o[3] = {ry.o.x, ry.o.y, ry.o.z}, lo[3] = {G.origin.x, G.origin.y, G.origin.z},
+              ext[3] = {G.cell.x * G.res[0], G.cell.y * G.res[1], G.cell.z * G.res[2]};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float f = (o[k] - lo[k]) / fmaxf(ext[k], 1e-30f) * 512.0f;
+    q[k] = (uint32_t)fminf(fmaxf(f, 0.0f), 511.0f);
+  }
+  const uint32_t oct = (ry.d.x < 0.f ? 1u : 0u) | (ry.d.y < 0.f ? 2u : 0u) | (ry.d.z < 0.f ? 4u : 0u);
+  A.sort_keys[t] = (oct << 27) | (spread9(q[0]) << 2) | (spread9(q[1]) << 1) | spread9(q[2]);
+  A.perm[t] = t;
+}
+
+// Per 256-slot tile of the input queue: survivors and events, for the
+// slot-ordered compaction.
+__global__ void k_adj_tile_counts(AdjointArgs A, uint32_t parity) {
+  const uint32_t n_in = A.st->active[parity];
+  if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
+  const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
+  const uint8_t f = slot < n_in ? A.qb.flags[slot] : 0;
+  const uint32_t ca = __syncthreads_count(f & 1), ce = __syncthreads_count(f & 2);
+  if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, ce);
+}
+
 // launchAdjointIntersectKernel (AdjointKernels.cpp:87-386).
-__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index) {
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index,
+                                                                        int sorted) {
   extern __shared__ BvhNode s_top[];
   const uint32_t n_in = A.st->active[parity];
   if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
   stage_top_nodes(A.scene, s_top);
-  const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
+  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
+  const uint32_t slot = (sorted && t < n_in) ? A.perm[t] : t;
   bool alive = false, has_ev = false;
   uint32_t job = kInvalid;
   TraceCounters ctr{0, 0};
-  if (slot < n_in) {
+  if (t < n_in) {
     const SceneView& S = A.scene;
     const RayRec ry = A.qb.q[parity][slot];
     const uint32_t jb = __float_as_uint(ry.d.w);
@@ -935,11 +977,9 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
     if (alive && (threadIdx.x & 31) == __ffs(peers) - 1)
       atomicAdd(&A.job_count[(size_t)(parity ^ 1u) * kMaxJobsPerBatch + job], (uint32_t)__popc(peers));
   }
-  warp_count(&A.st->adjoint_segments, slot < n_in ? 1u : 0u);
+  warp_count(&A.st->adjoint_segments, t < n_in ? 1u : 0u);
   warp_count(&A.st->node_visits, ctr.nodes);
   warp_count(&A.st->surfel_tests, ctr.tests);
-  uint32_t ca = __syncthreads_count(alive), ce = __syncthreads_count(has_ev);
-  if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, ce);
 }
 
 // Derivatives of eta * alpha_geom for the hit at x on surfel k along the
@@ -1125,9 +1165,17 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
   const uint32_t nb = blocks_for(npaths);
   if (nb == 0) return;
   const uint32_t parity = bounce & 1u;
+  // the first bounce traces camera rays in pixel order, already coherent
+  const int sorted = bounce > 0 && a.perm && npaths <= a.sort_capacity;
+  if (sorted) {
+    k_adj_keys<<<nb, kBlock, 0, s>>>(a, parity); note_launch();
+    radix_sort_pairs(a.sort_keys, a.perm, a.sort_keys_tmp, a.perm_tmp, &a.st->active[parity], npaths, 30,
+                     a.sort_temp, s);
+  }
   if (a.timer) a.timer->begin(kTimeAdjBounce, s);
-  k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce); note_launch();
+  k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce, sorted); note_launch();
   if (a.timer) a.timer->end(s);
+  k_adj_tile_counts<<<nb, kBlock, 0, s>>>(a, parity); note_launch();
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
   k_job_scan<<<1, kMaxJobsPerBatch, 0, s>>>(a, parity); note_launch();
   k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev); note_launch();
