@@ -631,14 +631,30 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
           }
         }
       }
-      // accepted terms packed in photon order
+      // accepted terms packed in photon order, one 32-float array per
+      // component; lane c adds component c four terms per shared load
       const unsigned m = __ballot_sync(0xffffffffu, in);
-      if (in) terms[__popc(m & ((1u << lane) - 1u))] = make_float4(tx, ty, tz, 0.f);
+      float* tb = reinterpret_cast<float*>(terms);
+      if (in) {
+        const int p = __popc(m & ((1u << lane) - 1u));
+        tb[p] = tx;
+        tb[32 + p] = ty;
+        tb[64 + p] = tz;
+      }
       __syncwarp();
       if (lane < 3) {
-        const float* t = reinterpret_cast<const float*>(terms) + lane;
+        const float4* t4 = reinterpret_cast<const float4*>(tb + 32 * lane);
         const int c = __popc(m);
-        for (int q = 0; q < c; ++q) acc = acc + t[4 * q];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          if (4 * q < c) {
+            const float4 v = t4[q];
+            acc = acc + v.x;
+            if (4 * q + 1 < c) acc = acc + v.y;
+            if (4 * q + 2 < c) acc = acc + v.z;
+            if (4 * q + 3 < c) acc = acc + v.w;
+          }
+        }
       }
       __syncwarp();
     }
