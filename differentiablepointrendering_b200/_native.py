@@ -256,6 +256,10 @@ def load_library() -> C.CDLL:
                                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "pale_optimizer_step": (C.c_int, [H, C.POINTER(PaleOptimizer), C.POINTER(PalePoints), C.c_void_p]),
         "pale_optimizer_reset": (C.c_int, [H]),
+        "pale_prune_by_opacity": (C.c_int, [H, C.c_float, C.c_uint32, C.c_double, C.c_uint32, u32p,
+                                            C.POINTER(C.c_int64)]),
+        "pale_densify_long_axis_split": (C.c_int, [H, C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                                   C.c_float, C.c_float, u32p, C.POINTER(C.c_int64)]),
         "pale_trace_rays": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, i32p, f32p, f32p, f32p]),
         "pale_trace_transmittance": (C.c_int, [H, C.c_uint32, f32p, f32p, i32p, f32p, f32p]),
         "pale_gather_irradiance": (C.c_int, [H, C.c_uint32, f32p, f32p, f32p]),
@@ -281,7 +285,8 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_get_points", "pale_get_order", "pale_apply_points", "pale_rebuild", "pale_trace_rays",
             "pale_trace_transmittance", "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
             "pale_get_stats", "pale_build_lbvh_noalloc", "pale_get_asset", "pale_optimizer_step",
-            "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device")
+            "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device",
+            "pale_prune_by_opacity", "pale_densify_long_axis_split")
 NOALLOC_MAX_SURFELS = 16384
 
 

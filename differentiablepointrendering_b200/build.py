@@ -13,7 +13,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = ("csrc/build.cu", "csrc/render.cu", "csrc/optim.cu", "csrc/api.cu")
+SOURCES = ("csrc/build.cu", "csrc/render.cu", "csrc/optim.cu", "csrc/density.cu", "csrc/api.cu")
 ARCH = ("-gencode", "arch=compute_100a,code=sm_100a")
 
 

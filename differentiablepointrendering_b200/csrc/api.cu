@@ -167,6 +167,9 @@ struct pale_handle {
   DBuf<uint32_t> opt_steps;
   uint64_t opt_gen = ~0ull, opt_t = 0;
   uint32_t opt_type = ~0u;
+  // density control scratch
+  DBuf<uint32_t> dc_keys, dc_vals, dc_keys_tmp, dc_vals_tmp, dc_sort_temp, dc_flags, dc_dst, dc_list, dc_word, dc_aux;
+  PointsBufs dc_points;
   pale_stats stats{};
   uint64_t launches_last = 0;  // kernels launched by the last render call
   int stats_pending = 0;   // a render ran without reading its run state yet
@@ -1248,6 +1251,154 @@ int pale_get_asset(pale_handle* h, pale_points* out) {
     use_stream(h, h->own_stream);
     out->count = h->np;
     download_points(h, h->asset, out);
+    return PALE_OK;
+  });
+}
+
+namespace {
+
+float host_key_to_float(uint32_t k) {
+  const uint32_t b = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+  float f;
+  std::memcpy(&f, &b, 4);
+  return f;
+}
+
+void density_scratch(pale_handle* h, uint32_t n) {
+  h->dc_keys.ensure(n); h->dc_vals.ensure(n); h->dc_keys_tmp.ensure(n); h->dc_vals_tmp.ensure(n);
+  h->dc_sort_temp.ensure(radix_temp_words(n)); h->dc_flags.ensure(n); h->dc_dst.ensure(n); h->dc_list.ensure(n);
+  h->dc_word.ensure(scan_temp_words(n));
+  h->dc_aux.ensure(4);
+}
+
+// Stable radix sort of (dc_keys, dc_vals) over n entries (four passes: the
+// result ends in dc_keys / dc_vals).
+void density_sort(pale_handle* h, uint32_t n, cudaStream_t s) {
+  CK(cudaMemcpyAsync(h->dc_aux.p, &n, 4, cudaMemcpyHostToDevice, s));
+  radix_sort_pairs(h->dc_keys.p, h->dc_vals.p, h->dc_keys_tmp.p, h->dc_vals_tmp.p, h->dc_aux.p, n, 32,
+                   h->dc_sort_temp.p, s);
+}
+
+// Exclusive scan of dc_flags into dc_dst; returns the number of flags set.
+uint32_t density_scan(pale_handle* h, uint32_t n, cudaStream_t s) {
+  uint32_t total = 0;
+  exclusive_scan(h->dc_flags.p, h->dc_dst.p, n, h->dc_word.p, h->dc_aux.p + 1, s);
+  CK(cudaMemcpyAsync(&total, h->dc_aux.p + 1, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return total;
+}
+
+// Replaces the asset by dc_points[0, m) and rebuilds.
+void density_commit(pale_handle* h, uint32_t m, cudaStream_t s) {
+  h->np = m;
+  h->asset.alloc(m);
+  copy_points(h, h->dc_points, h->asset, s);
+  build_from_device_asset(h);
+}
+
+void indices_to_host(pale_handle* h, const uint32_t* d_idx, uint32_t k, int64_t* out, bool sort, cudaStream_t s) {
+  std::vector<uint32_t> idx(k);
+  if (k) CK(cudaMemcpyAsync(idx.data(), d_idx, 4ull * k, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (sort) std::sort(idx.begin(), idx.end());
+  for (uint32_t j = 0; j < k; ++j) out[j] = idx[j];
+}
+
+}  // namespace
+
+int pale_prune_by_opacity(pale_handle* h, float min_opacity, uint32_t use_quantile, double max_fraction,
+                          uint32_t min_keep, uint32_t* removed_count, int64_t* removed) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    use_stream(h, h->own_stream);
+    cudaStream_t s = h->stream;
+    const uint32_t n = h->np;
+    if (removed_count) *removed_count = 0;
+    if (n == 0) return PALE_OK;
+    density_scratch(h, n);
+    opacity_sort_keys(h->asset.op.p, n, h->dc_keys.p, h->dc_vals.p, s);
+    density_sort(h, n, s);
+    float thr = min_opacity;
+    if (use_quantile) {
+      // np.quantile(opa, q) with the default "linear" method: virtual index
+      // (n - 1) q, the last value from n - 1 on, numpy's two-sided lerp
+      const double q = std::max(0.0, std::min(1.0, (double)min_opacity));
+      const double vi = (double)(n - 1) * q;
+      uint32_t lo = (uint32_t)std::floor(vi), hi = lo + 1;
+      const double g = vi - std::floor(vi);
+      if (vi >= (double)(n - 1)) lo = hi = n - 1;
+      uint32_t k2[2] = {0, 0};
+      CK(cudaMemcpyAsync(&k2[0], h->dc_keys.p + lo, 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&k2[1], h->dc_keys.p + hi, 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const float a = host_key_to_float(k2[0]), b = host_key_to_float(k2[1]);
+      const float diff = b - a;
+      const double t = g >= 0.5 ? (double)b - (double)diff * (1.0 - g) : (double)a + (double)diff * g;
+      thr = (float)t;
+    }
+    // opa <= threshold in float32, as numpy compares a float32 array with a Python float
+    count_le(h->asset.op.p, n, thr, h->dc_aux.p + 2, s);
+    uint32_t count = 0;
+    CK(cudaMemcpyAsync(&count, h->dc_aux.p + 2, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int64_t by_fraction = (int64_t)(max_fraction * (double)n);
+    const int64_t by_min = std::max<int64_t>(0, (int64_t)n - (int64_t)min_keep);
+    const int64_t max_prune = std::min(by_fraction, by_min);
+    if (count == 0 || max_prune <= 0) return PALE_OK;
+    // the candidates are the `count` lowest opacities, a prefix of the sort;
+    // above the cap the lowest max_prune of them (ties: lower index first)
+    const uint32_t k = (uint32_t)std::min<int64_t>(count, max_prune);
+    if (removed) indices_to_host(h, h->dc_vals.p, k, removed, true, s);
+    fill_u32(h->dc_flags.p, n, 1u, s);
+    mark_indices(h->dc_vals.p, k, n, h->dc_flags.p, 0u, s);
+    const uint32_t kept = density_scan(h, n, s);
+    h->dc_points.alloc(std::max(1u, kept));
+    compact_points(h->asset.view(), h->dc_flags.p, h->dc_dst.p, n, h->dc_points.view(), s);
+    density_commit(h, kept, s);
+    if (removed_count) *removed_count = k;
+    return PALE_OK;
+  });
+}
+
+int pale_densify_long_axis_split(pale_handle* h, const float* d_importance, int64_t max_new_points,
+                                 double split_distance, double minor_axis_shrink, double opacity_reduction,
+                                 float min_long_axis_scale, float grad_threshold, uint32_t* parent_count,
+                                 int64_t* parents_out) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    use_stream(h, h->own_stream);
+    cudaStream_t s = h->stream;
+    const uint32_t n = h->np;
+    if (parent_count) *parent_count = 0;
+    if (n == 0) return PALE_OK;
+    if (max_new_points >= 0 && max_new_points / 2 <= 0) return PALE_OK;
+    if ((uint64_t)n + 2ull * n >= (1ull << 28)) throw ArgError("at most 2^28 surfels are supported");
+    density_scratch(h, n);
+    split_candidates(h->asset.view(), n, d_importance, min_long_axis_scale, grad_threshold,
+                     d_importance && grad_threshold > 0.0f ? 1 : 0, h->dc_flags.p, h->dc_keys.p, h->dc_vals.p, s);
+    uint32_t np = density_scan(h, n, s);
+    if (np == 0) return PALE_OK;
+    if (max_new_points >= 0 && (int64_t)np > max_new_points / 2) {
+      // the budget binds: the highest scores (ties: lower index first)
+      np = (uint32_t)(max_new_points / 2);
+      density_sort(h, n, s);
+      fill_u32(h->dc_flags.p, n, 0u, s);
+      mark_indices(h->dc_vals.p, np, n, h->dc_flags.p, 1u, s);
+      density_scan(h, n, s);
+    }
+    // parents in increasing index order
+    flagged_list(h->dc_flags.p, h->dc_dst.p, n, h->dc_list.p, s);
+    if (parents_out) indices_to_host(h, h->dc_list.p, np, parents_out, false, s);
+    // survivors in order, then two children per parent
+    fill_u32(h->dc_flags.p, n, 1u, s);
+    mark_indices(h->dc_list.p, np, n, h->dc_flags.p, 0u, s);
+    const uint32_t kept = density_scan(h, n, s);
+    h->dc_points.alloc(kept + 2 * np);
+    compact_points(h->asset.view(), h->dc_flags.p, h->dc_dst.p, n, h->dc_points.view(), s);
+    split_children(h->asset.view(), h->dc_list.p, np, kept, h->dc_points.view(), split_distance, minor_axis_shrink,
+                   opacity_reduction, s);
+    density_commit(h, kept + 2 * np, s);
+    if (parent_count) *parent_count = np;
     return PALE_OK;
   });
 }

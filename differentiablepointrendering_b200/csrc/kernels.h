@@ -75,6 +75,19 @@ struct OptArgs {
 };
 void optimizer_step(const OptArgs& a, cudaStream_t s);
 
+// Density control helpers (density.cu).
+void opacity_sort_keys(const float* op, uint32_t n, uint32_t* keys, uint32_t* vals, cudaStream_t s);
+void count_le(const float* v, uint32_t n, float thr, uint32_t* count, cudaStream_t s);
+void fill_u32(uint32_t* a, uint32_t n, uint32_t value, cudaStream_t s);
+void mark_indices(const uint32_t* idx, uint32_t k, uint32_t n, uint32_t* flags, uint32_t value, cudaStream_t s);
+void compact_points(const PointsDev& src, const uint32_t* keep, const uint32_t* dst, uint32_t n, const PointsDev& out,
+                    cudaStream_t s);
+void flagged_list(const uint32_t* flag, const uint32_t* dst, uint32_t n, uint32_t* list, cudaStream_t s);
+void split_candidates(const PointsDev& a, uint32_t n, const float* importance, float min_long, float grad_threshold,
+                      int use_threshold, uint32_t* cand, uint32_t* keys, uint32_t* vals, cudaStream_t s);
+void split_children(const PointsDev& a, const uint32_t* parents, uint32_t np, uint32_t base, const PointsDev& out,
+                    double split, double shrink, double reduction, cudaStream_t s);
+
 // Device time of the hot kernels: a pair of CUDA events around every launch
 // of a timed kernel, summed per kernel after the stream is synchronised.
 // Host-side only (kernels receive the pointer inside their argument

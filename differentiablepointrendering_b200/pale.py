@@ -316,6 +316,62 @@ class Renderer:
         _check(self._lib, self._h, self._lib.pale_optimizer_step(self._h, C.byref(opt), g, s), "optimizer_step")
         self._asset_stale = True
 
+    # ------------------------------------------------------ density control
+    def prune_by_opacity(self, min_opacity: float, use_quantile: bool = True, max_fraction_to_prune: float = 0.3,
+                         min_points_to_keep: int = 1) -> np.ndarray:
+        """compute_prune_indices_by_opacity (density_control.py:199-263) on
+        the device asset, then remove_points + rebuild_bvh, in one call.
+        Returns the removed asset indices in increasing order (what
+        np.unique of the reference's indices gives)."""
+        n = self.num_points
+        out = np.zeros(max(1, n), np.int64)
+        cnt = C.c_uint32()
+        _check(self._lib, self._h,
+               self._lib.pale_prune_by_opacity(self._h, float(min_opacity), 1 if use_quantile else 0,
+                                               float(max_fraction_to_prune), int(min_points_to_keep), C.byref(cnt),
+                                               out.ctypes.data_as(C.POINTER(C.c_int64))), "prune_by_opacity")
+        if cnt.value:
+            self._asset_stale = True
+        return out[:cnt.value].copy()
+
+    def densify_long_axis_split(self, importance=None, max_new_points: Optional[int] = None,
+                                split_distance: float = 0.6, minor_axis_shrink: float = 0.85,
+                                opacity_reduction: float = 0.6, min_long_axis_scale: float = 0.0,
+                                grad_threshold: float = 0.0) -> np.ndarray:
+        """densify_points_long_axis_split (density_control.py:6-196) on the
+        device asset, then remove_points(parents) + add_points(children) +
+        rebuild_bvh.  `importance` (one score per surfel, asset order) may be
+        a CUDA tensor or a host array.  Returns the parent indices."""
+        n = self.num_points
+        keep = None
+        ptr = None
+        if importance is not None:
+            if hasattr(importance, "is_cuda") and importance.is_cuda:
+                keep = importance.detach().float().contiguous().reshape(-1)
+            else:
+                import torch
+                keep = torch.from_numpy(np.ascontiguousarray(np.asarray(importance, np.float32).reshape(-1))).cuda()
+            if keep.numel() != n:
+                raise ValueError(f"importance needs {n} scores, got {keep.numel()}")
+            ptr = C.c_void_p(keep.data_ptr())
+        budget = -1 if max_new_points is None else int(max_new_points)
+        if max_new_points is not None and int(max_new_points) // 2 <= 0:
+            return np.zeros(0, np.int64)
+        out = np.zeros(max(1, n), np.int64)
+        cnt = C.c_uint32()
+        if keep is not None:
+            import torch
+            torch.cuda.synchronize()
+        _check(self._lib, self._h,
+               self._lib.pale_densify_long_axis_split(self._h, ptr, budget, float(split_distance),
+                                                      float(minor_axis_shrink), float(opacity_reduction),
+                                                      float(min_long_axis_scale), float(grad_threshold), C.byref(cnt),
+                                                      out.ctypes.data_as(C.POINTER(C.c_int64))),
+               "densify_long_axis_split")
+        if cnt.value:
+            self._asset_stale = True
+        return out[:cnt.value].copy()
+
     def reset_optimizer(self):
         """Drops the device optimizer state (zero moments at the next step)."""
         _check(self._lib, self._h, self._lib.pale_optimizer_reset(self._h), "reset_optimizer")

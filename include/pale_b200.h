@@ -314,6 +314,43 @@ int pale_optimizer_step(pale_handle *h, const pale_optimizer *opt,
 /* Drops the optimizer state: the next step starts from zero moments. */
 int pale_optimizer_reset(pale_handle *h);
 
+/* Density control on the renderer's asset (the parameter order of the last
+ * apply / optimizer step), each followed by the BVH rebuild.
+ *
+ * pale_prune_by_opacity: compute_prune_indices_by_opacity
+ * (python/density_control.py:199-263) + remove_points
+ * (pale_bindings.cpp:1081-1189): with use_quantile the threshold is the
+ * `min_opacity` quantile of the opacities (numpy's default linear method),
+ * else min_opacity itself; surfels with opacity <= threshold are removed,
+ * at most min(floor(max_fraction * N), N - min_keep) of them, the lowest
+ * first (ties: lower index first; numpy's default argsort leaves ties in no
+ * defined order).  *removed_count gets their number and, when not NULL,
+ * removed[] (capacity: the point count) their indices in increasing order. */
+int pale_prune_by_opacity(pale_handle *h, float min_opacity, uint32_t use_quantile,
+                          double max_fraction, uint32_t min_keep,
+                          uint32_t *removed_count, int64_t *removed);
+
+/* pale_densify_long_axis_split: densify_points_long_axis_split
+ * (density_control.py:6-196) + remove_points(parents) + add_points(children)
+ * (pale_bindings.cpp:1081-1395).  Candidates have max(s_u, s_v) >=
+ * min_long_axis_scale and, with an importance array (DEVICE pointer, one
+ * score per surfel in asset order, may be NULL) and grad_threshold > 0, a
+ * score >= grad_threshold.  With max_new_points >= 0 at most
+ * max_new_points / 2 parents are split, the highest scores (importance,
+ * else the long-axis scale; ties: lower index first); max_new_points < 0
+ * sets no budget.  Each parent is replaced by two children offset by
+ * +-split_distance * 3 * s_long along its long tangent, with scales
+ * (s_long (1 - split_distance), s_short * minor_axis_shrink) and opacity
+ * clamp(opacity * opacity_reduction, 0, 1): the survivors keep their order
+ * and the children follow, parent by parent (+ then -).  *parent_count gets
+ * the number of parents and parents_out[] (capacity: the point count, may be
+ * NULL) their indices in increasing order. */
+int pale_densify_long_axis_split(pale_handle *h, const float *d_importance,
+                                 int64_t max_new_points, double split_distance,
+                                 double minor_axis_shrink, double opacity_reduction,
+                                 float min_long_axis_scale, float grad_threshold,
+                                 uint32_t *parent_count, int64_t *parents_out);
+
 /* Closest-hit queries against the scene (intersectScene in FirstHit mode,
  * IntersectionKernels.h:954-1097).  Host arrays of n rays; outputs:
  * instance (-1 = miss), primitive (surfel in BVH order or triangle id),
