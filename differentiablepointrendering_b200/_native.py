@@ -248,6 +248,7 @@ def load_library() -> C.CDLL:
         "pale_get_points": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_get_order": (C.c_int, [H, u32p]),
         "pale_apply_points": (C.c_int, [H, C.POINTER(PalePoints)]),
+        "pale_apply_points_device": (C.c_int, [H, C.POINTER(PalePoints), C.c_void_p]),
         "pale_rebuild": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_get_asset": (C.c_int, [H, C.POINTER(PalePoints)]),
         "pale_render_forward_loss": (C.c_int, [H, C.c_uint32, u32p, f32p, C.c_uint32, f32p, f32p, f32p,
@@ -286,7 +287,7 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_trace_transmittance", "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
             "pale_get_stats", "pale_build_lbvh_noalloc", "pale_get_asset", "pale_optimizer_step",
             "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device",
-            "pale_prune_by_opacity", "pale_densify_long_axis_split")
+            "pale_prune_by_opacity", "pale_densify_long_axis_split", "pale_apply_points_device")
 NOALLOC_MAX_SURFELS = 16384
 
 

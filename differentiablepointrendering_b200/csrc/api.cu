@@ -1230,6 +1230,34 @@ int pale_apply_points(pale_handle* h, const pale_points* p) {
   });
 }
 
+int pale_apply_points_device(pale_handle* h, const pale_points* p, void* stream) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    check_points(p, "pale_apply_points_device");
+    if (p->count != h->np) throw ArgError("apply_point_optimization expects consistent point count");
+    use_stream(h, caller_stream(stream));
+    cudaStream_t s = h->stream;
+    const size_t n = h->np;
+    if (!n) return PALE_OK;
+    PointsBufs& d = h->params;
+    auto cp = [&](float* dst, const float* src, size_t bytes) {
+      if (dst != src) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    };
+    cp(d.pos.p, p->position, 12 * n);
+    cp(d.tu.p, p->tangent_u, 12 * n);
+    cp(d.tv.p, p->tangent_v, 12 * n);
+    cp(d.sc.p, p->scale, 8 * n);
+    cp(d.alb.p, p->albedo, 12 * n);
+    cp(d.op.p, p->opacity, 4 * n);
+    cp(d.beta.p, p->beta, 4 * n);
+    derive_surfels(d.view(), h->np, SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p},
+                   s);
+    copy_points(h, d, h->asset, s);
+    CK(cudaGetLastError());
+    return PALE_OK;
+  });
+}
+
 int pale_rebuild(pale_handle* h, const pale_points* asset) {
   if (!h) return PALE_ERR_ARGUMENT;
   return guarded(h, [&]() {

@@ -263,6 +263,12 @@ int pale_get_order(pale_handle *h, uint32_t *order);
  * as they were).  params->count must equal the current count. */
 int pale_apply_points(pale_handle *h, const pale_points *params);
 
+/* Same with the seven fields as DEVICE pointers (BVH order; shape is
+ * ignored), enqueued on `stream` (NULL = the default stream) without
+ * waiting: the parameter tensors of a torch training loop go to the
+ * renderer without a host round trip. */
+int pale_apply_points_device(pale_handle *h, const pale_points *d_params, void *stream);
+
 /* Rebuilds the LBVH from an asset-order point set of any size (rebuild_bvh,
  * pale_bindings.cpp:1058-1079; also behind add_points / remove_points /
  * set_point_* which edit the asset and rebuild).  asset_points == NULL
