@@ -119,6 +119,7 @@ struct pale_handle {
   DBuf<int32_t> lc, rc;
   DBuf<float> box;
   DBuf<BvhNode> nodes;
+  DBuf<BvhNodeH> hnodes;   // traversal copy (half boxes) when PALE_HALF_NODES
   uint32_t node_count = 0, top = 0;
   float pc_lo[3] = {0, 0, 0}, pc_hi[3] = {0, 0, 0};
   // photon grid
@@ -195,7 +196,11 @@ struct pale_handle {
     s.mesh.materials = materials.p;
     s.mesh.instances = n_inst;
     s.sf = SurfelView{sf_pe.p, sf_n.p, sf_u.p, sf_v.p, sf_cn.p, sf_alb.p, np};
+#if PALE_HALF_NODES
+    s.nodes = hnodes.p;
+#else
     s.nodes = nodes.p;
+#endif
     s.node_count = np ? node_count : 0;
     s.top_nodes = np ? std::min(top, node_count) : 0;
     s.pc_lo = v3(pc_lo[0], pc_lo[1], pc_lo[2]);
@@ -275,7 +280,7 @@ void build_from_device_asset(pale_handle* h) {
   h->leaf_parent.ensure(n); h->visits.ensure(n); h->box.ensure(6 * (size_t)n);
   h->d_n.ensure(1);
   const uint32_t leaf = std::max(1u, std::min(8u, h->st.leaf_size ? h->st.leaf_size : 1u));
-  h->top = 256;
+  h->top = kTopNodes;
   h->node_count = (n <= leaf) ? 1 : h->top + (n - 1);
   if (n <= leaf) h->top = 0;
   h->nodes.ensure(h->node_count);
@@ -299,6 +304,10 @@ void build_from_device_asset(pale_handle* h) {
   A.err = &h->run.p->error;
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   lbvh_build(A, s);
+#if PALE_HALF_NODES
+  h->hnodes.ensure(h->node_count);
+  half_nodes(h->nodes.p, h->node_count, h->hnodes.p, s);
+#endif
   CK(cudaGetLastError());
   float b[12];
   uint32_t err = 0;

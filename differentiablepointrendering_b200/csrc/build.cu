@@ -603,6 +603,39 @@ void lbvh_build(const LbvhArgs& A, cudaStream_t s) {
   derive_surfels(A.params, n, A.derived, s);
 }
 
+namespace {
+__device__ __forceinline__ uint32_t pack_down(float a, float b) {
+  const __half2 h = __halves2half2(__float2half_rd(a), __float2half_rd(b));
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ uint32_t pack_up(float a, float b) {
+  const __half2 h = __halves2half2(__float2half_ru(a), __float2half_ru(b));
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+// mixed pair: first value a lower bound (down), second an upper bound (up)
+__device__ __forceinline__ uint32_t pack_down_up(float a, float b) {
+  const __half2 h = __halves2half2(__float2half_rd(a), __float2half_ru(b));
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__global__ void k_half_nodes(const BvhNode* __restrict__ in, uint32_t n, BvhNodeH* __restrict__ out) {
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  const BvhNode nd = in[i];
+  // a = c0.lo.xyz c0.hi.x, b = c0.hi.yz c1.lo.xy, c = c1.lo.z c1.hi.xyz
+  BvhNodeH h;
+  h.q0 = make_uint4(pack_down(nd.a.x, nd.a.y), pack_down_up(nd.a.z, nd.a.w), pack_up(nd.b.x, nd.b.y),
+                    pack_down(nd.b.z, nd.b.w));
+  h.q1 = make_uint4(pack_down_up(nd.c.x, nd.c.y), pack_up(nd.c.z, nd.c.w), nd.d.x, nd.d.y);
+  out[i] = h;
+}
+}  // namespace
+
+void half_nodes(const BvhNode* in, uint32_t n, BvhNodeH* out, cudaStream_t s) {
+  if (n == 0) return;
+  k_half_nodes<<<blocks_for(n), kBlock, 0, s>>>(in, n, out); note_launch();
+}
+
 void derive_surfels(const PointsDev& p, uint32_t n, const SurfelArrays& d, cudaStream_t s) {
   if (n == 0) return;
   k_derive<<<blocks_for(n), kBlock, 0, s>>>(p, n, d.pe, d.n, d.u, d.v, d.cn, d.alb); note_launch();

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace pale {
@@ -129,6 +130,25 @@ struct BvhNode {
 };
 static_assert(sizeof(BvhNode) == 64, "node layout");
 
+// Traversal copy of a node: the two child boxes in half precision rounded
+// outwards (lower corners down, upper corners up, so a box only grows and
+// no hit is lost) and the two child words, 32 B against BvhNode's 64 B.
+//   q0 = halves (c0.lo.x c0.lo.y) (c0.lo.z c0.hi.x) (c0.hi.y c0.hi.z) (c1.lo.x c1.lo.y)
+//   q1 = halves (c1.lo.z c1.hi.x) (c1.hi.y c1.hi.z), word0, word1
+struct BvhNodeH {
+  uint4 q0;
+  uint4 q1;
+};
+static_assert(sizeof(BvhNodeH) == 32, "node layout");
+#ifndef PALE_HALF_NODES
+#define PALE_HALF_NODES 1
+#endif
+#if PALE_HALF_NODES
+using TravNode = BvhNodeH;
+#else
+using TravNode = BvhNode;
+#endif
+
 // Surfel arrays in BVH (leaf) order.
 struct SurfelView {
   const float4* pe;    // position, 4*exp(beta)
@@ -177,7 +197,7 @@ struct GridView {
 struct SceneView {
   MeshView mesh;
   SurfelView sf;
-  const BvhNode* nodes;
+  const TravNode* nodes;   // traversal copy of the LBVH nodes
   uint32_t node_count;
   uint32_t top_nodes;      // nodes [0, top_nodes) are the shared-memory copy
   V3 pc_lo, pc_hi;         // box of the whole surfel cloud

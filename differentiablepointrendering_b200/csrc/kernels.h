@@ -52,6 +52,8 @@ size_t radix_temp_words(uint32_t n_max);
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp, const uint32_t* d_n,
                       uint32_t n_max, int bits, uint32_t* temp, cudaStream_t s);
 void lbvh_build(const LbvhArgs& a, cudaStream_t s);
+// The traversal copy of n nodes (BvhNodeH: boxes rounded outwards to half).
+void half_nodes(const BvhNode* in, uint32_t n, BvhNodeH* out, cudaStream_t s);
 void derive_surfels(const PointsDev& p, uint32_t n, const SurfelArrays& d, cudaStream_t s);
 
 // One optimizer step on the device (optim.cu), in BVH order like the
@@ -196,6 +198,13 @@ struct FrameArgs {
   uint32_t target_channels;
   float* dldi;
 };
+
+// LBVH nodes duplicated in breadth-first order at the front of the node
+// array and staged in shared memory by every traversal kernel.
+#ifndef PALE_TOP_NODES
+#define PALE_TOP_NODES 256
+#endif
+constexpr uint32_t kTopNodes = PALE_TOP_NODES;
 
 // Surfel layers collected per traversal of the camera gather.
 #ifndef PALE_GATHER_HITS

@@ -21,7 +21,7 @@ namespace pale {
 
 static inline uint32_t blocks_for(uint64_t n, int b = kBlock) { return (uint32_t)((n + b - 1) / b); }
 
-__device__ __forceinline__ void stage_top_nodes(const SceneView& S, BvhNode* smem) {
+__device__ __forceinline__ void stage_top_nodes(const SceneView& S, TravNode* smem) {
   for (uint32_t i = threadIdx.x; i < S.top_nodes; i += blockDim.x) smem[i] = S.nodes[i];
   __syncthreads();
 }
@@ -157,7 +157,7 @@ __global__ void k_photon_emit(PhotonArgs A) {
 
 // launchIntersectKernel for the photon pass (PrimalKernels.cpp:65-321).
 __global__ void __launch_bounds__(kBlock) k_photon_bounce(PhotonArgs A, uint32_t parity) {
-  extern __shared__ BvhNode s_top[];
+  extern __shared__ TravNode s_top[];
   const uint32_t n_in = A.st->active[parity];
   if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
   stage_top_nodes(A.scene, s_top);
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kBlock) k_photon_bounce(PhotonArgs A, uint32_t
   if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, cd);
 }
 
-static size_t top_smem(const SceneView& s) { return (size_t)s.top_nodes * sizeof(BvhNode); }
+static size_t top_smem(const SceneView& s) { return (size_t)s.top_nodes * sizeof(TravNode); }
 
 void photon_emit(const PhotonArgs& a, cudaStream_t s) {
   const uint32_t nb = blocks_for(a.photons_per_launch);
@@ -396,7 +396,7 @@ __device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float 
 // Round step 1: one lane per queue entry (a live path).
 template <int K>
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs A, uint32_t round) {
-  extern __shared__ BvhNode s_top[];
+  extern __shared__ TravNode s_top[];
   stage_top_nodes(A.scene, s_top);
   const SceneView& S = A.scene;
   const uint32_t n = A.counts[round];
@@ -846,7 +846,7 @@ __global__ void k_adj_tile_counts(AdjointArgs A, uint32_t parity) {
 // launchAdjointIntersectKernel (AdjointKernels.cpp:87-386).
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index,
                                                                         int sorted) {
-  extern __shared__ BvhNode s_top[];
+  extern __shared__ TravNode s_top[];
   const uint32_t n_in = A.st->active[parity];
   if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
   stage_top_nodes(A.scene, s_top);
@@ -1194,7 +1194,7 @@ __global__ void __launch_bounds__(kBlock) k_trace_rays(SceneView S, RunState* st
                                                        const float* __restrict__ o, const float* __restrict__ d,
                                                        int32_t* inst, int32_t* prim, float* t, float* alpha,
                                                        float* pos) {
-  extern __shared__ BvhNode s_top[];
+  extern __shared__ TravNode s_top[];
   stage_top_nodes(S, s_top);
   uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
@@ -1227,7 +1227,7 @@ __global__ void __launch_bounds__(kBlock) k_trace_transmittance(SceneView S, Run
                                                                 const float* __restrict__ o,
                                                                 const float* __restrict__ d, int32_t* inst,
                                                                 float* t, float* transmit) {
-  extern __shared__ BvhNode s_top[];
+  extern __shared__ TravNode s_top[];
   stage_top_nodes(S, s_top);
   uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;

@@ -94,7 +94,31 @@ __device__ __forceinline__ bool surfel_hit(const SurfelView& sf, uint32_t i, V3 
   return true;
 }
 
-__device__ __forceinline__ void load_node(const SceneView& S, const BvhNode* __restrict__ smem_top, uint32_t idx,
+#if PALE_HALF_NODES
+__device__ __forceinline__ float2 half_pair(uint32_t v) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&v));
+}
+
+__device__ __forceinline__ void load_node(const SceneView& S, const TravNode* __restrict__ smem_top, uint32_t idx,
+                                          float4& a, float4& b, float4& c, uint4& w) {
+  uint4 q0, q1;
+  if (idx < S.top_nodes) {
+    q0 = smem_top[idx].q0;
+    q1 = smem_top[idx].q1;
+  } else {
+    const BvhNodeH* nd = S.nodes + idx;
+    q0 = __ldg(&nd->q0);
+    q1 = __ldg(&nd->q1);
+  }
+  const float2 p0 = half_pair(q0.x), p1 = half_pair(q0.y), p2 = half_pair(q0.z), p3 = half_pair(q0.w);
+  const float2 p4 = half_pair(q1.x), p5 = half_pair(q1.y);
+  a = make_float4(p0.x, p0.y, p1.x, p1.y);
+  b = make_float4(p2.x, p2.y, p3.x, p3.y);
+  c = make_float4(p4.x, p4.y, p5.x, p5.y);
+  w = make_uint4(q1.z, q1.w, 0u, 0u);
+}
+#else
+__device__ __forceinline__ void load_node(const SceneView& S, const TravNode* __restrict__ smem_top, uint32_t idx,
                                           float4& a, float4& b, float4& c, uint4& w) {
   if (idx < S.top_nodes) {
     const BvhNode& nd = smem_top[idx];
@@ -104,12 +128,13 @@ __device__ __forceinline__ void load_node(const SceneView& S, const BvhNode* __r
     a = __ldg(&nd->a); b = __ldg(&nd->b); c = __ldg(&nd->c); w = __ldg(&nd->d);
   }
 }
+#endif
 
 // Closest surfel with t in (tmin, limit) along (o, d) (the surfel cloud's
 // transform is the identity, so this is intersectBLASPointCloudFirstHit,
 // IntersectionKernels.h:585-675, where tmin is rayEpsilon = 1e-5).  Returns
 // false on a miss.
-__device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
+__device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNode* __restrict__ smem_top, V3 o, V3 d,
                                                float tmin, float limit, uint32_t& prim, float& t, V3& x,
                                                float& alpha, TraceCounters& ctr, RunState* st) {
   if (S.node_count == 0) return false;
@@ -198,7 +223,7 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const BvhNode
 // with the culling distance of the K-th hit found so far.  Returns the
 // number of hits (<= K); t_out/prim_out hold them in order.
 template <int K>
-__device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
+__device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNode* __restrict__ smem_top, V3 o, V3 d,
                                                 float tmin, float limit, float (&t_out)[K], uint32_t (&prim_out)[K],
                                                 TraceCounters& ctr, RunState* st) {
   if (S.node_count == 0) return 0;
@@ -346,7 +371,7 @@ __device__ __forceinline__ Hit intersect_meshes(const SceneView& S, V3 o, V3 d, 
 
 // intersectScene, FirstHit mode: mesh instances, then the surfel cloud;
 // the closest world-space distance wins (:1060-1081).
-__device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode* __restrict__ smem_top, V3 o, V3 d,
+__device__ __forceinline__ Hit intersect_scene(const SceneView& S, const TravNode* __restrict__ smem_top, V3 o, V3 d,
                                                TraceCounters& ctr, RunState* st) {
   float best;
   const V3 invw = safe_inv(d);
@@ -384,7 +409,7 @@ __device__ __forceinline__ Hit intersect_scene(const SceneView& S, const BvhNode
 // T <= 0.001.  The cloud is skipped (T = 1) when its box starts beyond the
 // mesh hit, as the instance loop culls it.  `max_hits` bounds the walk (the
 // kernel flags kErrLayerCap when it is reached).
-__device__ __forceinline__ Hit intersect_scene_transmit(const SceneView& S, const BvhNode* __restrict__ smem_top,
+__device__ __forceinline__ Hit intersect_scene_transmit(const SceneView& S, const TravNode* __restrict__ smem_top,
                                                         V3 o, V3 d, float& T, uint32_t max_hits,
                                                         TraceCounters& ctr, RunState* st) {
   float best;

@@ -47,8 +47,9 @@ def test_lbvh_bit_exact(gpu, box, leaf):
     g = Renderer.from_scene(box, dict(SETTINGS, leaf_size=leaf))
     col = collected_asset_points(box)
     lo, hi = surfel_aabbs(col["position"], col["tangent_u"], col["tangent_v"], col["scale"])
-    codes_ref, order_ref, nodes_ref = lbvh_reference(col["position"], lo, hi, leaf_size=leaf, top=256)
     codes, nodes = g.get_bvh()
+    top = nodes.shape[0] - (g.num_points - 1)    # node count = staged top copies + Karras nodes
+    codes_ref, order_ref, nodes_ref = lbvh_reference(col["position"], lo, hi, leaf_size=leaf, top=top)
     order = g.get_point_order()
     g.close()
     assert np.array_equal(codes, codes_ref)
