@@ -625,17 +625,31 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
     const uint32_t excl = incl - len;
     const uint32_t seq = __shfl_sync(0xffffffffu, incl, 31);
     scanned += seq;
+    // the non-empty rows, compacted into lanes 0..nne-1 in row order (their
+    // starts are then strictly increasing); staged through the terms buffer
+    const unsigned nm = __ballot_sync(0xffffffffu, len > 0);
+    const int nne = __popc(nm);
+    uint32_t* cw = reinterpret_cast<uint32_t*>(terms);
+    if (len > 0) {
+      const int o = __popc(nm & ((1u << lane) - 1u));
+      cw[o] = j0;
+      cw[32 + o] = excl;
+    }
+    __syncwarp();
+    const uint32_t cj0 = lane < nne ? cw[lane] : 0u;
+    const uint32_t cex = lane < nne ? cw[32 + lane] : 0xFFFFFFFFu;
+    __syncwarp();
     for (uint32_t base = 0; base < seq; base += 32) {
       const uint32_t v = base + lane;
-      // row holding sequence index v: the last lane whose exclusive start <= v
-      int lo = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const uint32_t s = __shfl_sync(0xffffffffu, excl, lo + step);
-        if (lo + step < 32 && s <= v && (rb + lo + step) < rows) lo += step;
-      }
-      const uint32_t rj0 = __shfl_sync(0xffffffffu, j0, lo);
-      const uint32_t rex = __shfl_sync(0xffffffffu, excl, lo);
+      // row holding sequence index v: the non-empty rows starting at or
+      // before v are those starting before this round plus those starting
+      // in the round at lanes <= this one (one bit per row start)
+      const bool starts_here = lane < nne && cex >= base && cex - base < 32u;
+      const uint32_t smask = __reduce_or_sync(0xffffffffu, starts_here ? (1u << (cex - base)) : 0u);
+      const uint32_t before = __popc(__ballot_sync(0xffffffffu, lane < nne && cex < base));
+      const int ord = (int)before + __popc(smask & (0xFFFFFFFFu >> (31 - lane))) - 1;
+      const uint32_t rj0 = __shfl_sync(0xffffffffu, cj0, ord & 31);
+      const uint32_t rex = __shfl_sync(0xffffffffu, cex, ord & 31);
       float tx = 0.f, ty = 0.f, tz = 0.f;
       bool in = false;
       if (v < seq) {
