@@ -572,11 +572,32 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
   const int lane = threadIdx.x & 31;
   const float r = G.radius, r2 = r * r;
   const float invArea = 1.0f / (kPi * r2);
+  // window corners: lanes 0-5 each do one coordinate of world_to_cell(x -
+  // (r, r, r)) and world_to_cell(x + (r, r, r)), the same operations
+  int wc = 0;
+  if (lane < 6) {
+    const int a = lane % 3;
+    const float xa = a == 0 ? x.x : (a == 1 ? x.y : x.z);
+    const float oa = a == 0 ? G.origin.x : (a == 1 ? G.origin.y : G.origin.z);
+    const float ca = a == 0 ? G.cell.x : (a == 1 ? G.cell.y : G.cell.z);
+    const float p = lane < 3 ? xa - r : xa + r;
+    int v = (int)floorf((p - oa) / ca);
+    v = v < 0 ? 0 : v;
+    v = v > G.res[a] - 1 ? G.res[a] - 1 : v;
+    wc = v;
+  }
   int c0[3], c1[3];
-  world_to_cell(G, x - v3(r, r, r), c0);
-  world_to_cell(G, x + v3(r, r, r), c1);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    c0[a] = __shfl_sync(0xffffffffu, wc, a);
+    c1[a] = __shfl_sync(0xffffffffu, wc, 3 + a);
+  }
   const int ny = c1[1] - c0[1] + 1;
   const int rows = (c1[2] - c0[2] + 1) * ny;
+  // row k of the window is (z, y) = (k / ny, k % ny); (k + 1/2) / ny is at
+  // least 1/(2 ny) from an integer, far beyond float rounding
+  const float inv_ny = 1.0f / (float)ny;
+  const float inv_cx = 1.0f / G.cell.x;
   const uint32_t total_ph = __ldg(&G.cell_off[G.cells]);
   float acc = 0.f;   // lane c < 3: running sum of component c
   uint32_t scanned = 0;
@@ -585,7 +606,8 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
     const int k = rb + lane;
     uint32_t j0 = 0, len = 0;
     if (k < rows) {
-      const int cz = c0[2] + k / ny, cy = c0[1] + k % ny;
+      const int kz = (int)(((float)k + 0.5f) * inv_ny);
+      const int cz = c0[2] + kz, cy = c0[1] + (k - kz * ny);
       const uint32_t row = (uint32_t)((cz * G.res[1] + cy) * G.res[0]);
       // Clip the row to the sphere of radius r around x.  A photon binned
       // to cell c lies in [c, c + 1] cells from the origin up to rounding
@@ -602,8 +624,9 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
       const float rho2 = dy * dy + dz * dz;
       if (rho2 <= reach2) {
         const float w = sqrtf(reach2 - rho2) * 1.001f + 0.01f * G.cell.x;
-        int lo = (int)floorf(((x.x - w) - G.origin.x) / G.cell.x);
-        int hi = (int)floorf(((x.x + w) - G.origin.x) / G.cell.x);
+        // (a reciprocal is enough here: the 1% margin covers its rounding)
+        int lo = (int)floorf(((x.x - w) - G.origin.x) * inv_cx);
+        int hi = (int)floorf(((x.x + w) - G.origin.x) * inv_cx);
         lo = lo > c0[0] ? lo : c0[0];
         hi = hi < c1[0] ? hi : c1[0];
         if (lo <= hi) {
