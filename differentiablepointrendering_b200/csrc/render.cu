@@ -544,6 +544,7 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArg
   const uint32_t n = A.counts[kMaxLayers + 2 + round];
   const int lane = threadIdx.x & 31;
   float4* terms = s_terms + (threadIdx.x & ~31u);
+  const GatherConst GC = gather_const(S.grid);
   const uint32_t warps = gridDim.x * (kBlock / 32);
   uint32_t queries = 0, scanned = 0;
   // lanes 0-7 hold the 8 floats of the next record, loaded one record ahead
@@ -559,7 +560,7 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArg
     const uint32_t kind = word >> 30, idx = word & kRecIndexMask;
     if (kind == kRecNone) continue;
     uint32_t cnt = 0;
-    const V3 E = gather_irradiance_warp(S.grid, xyz(ra), xyz(rb), terms, cnt);
+    const V3 E = gather_irradiance_warp(S.grid, GC, xyz(ra), xyz(rb), terms, cnt);
     if (lane == 0) {
       ++queries;
       scanned += cnt;
@@ -1045,6 +1046,7 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_transport(AdjointA
   const SceneView& S = A.scene;
   const int lane = threadIdx.x & 31;
   float4* terms = s_terms + (threadIdx.x & ~31u);
+  const GatherConst GC = gather_const(S.grid);
   const uint32_t warps = gridDim.x * (kBlock / 32);
   uint32_t events = 0, queries = 0, scanned = 0;
   // lanes 0-23 hold the 24 words of the next event, loaded one event ahead
@@ -1069,7 +1071,7 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_transport(AdjointA
     const bool need = kind == kKindProjection || kind == kKindReflect || (kind == kKindNull && ev.d.z != kInvalid);
     V3 E = v3(0.f, 0.f, 0.f);
     uint32_t cnt = 0;
-    if (need) E = gather_irradiance_warp(S.grid, xyz(ev.a), xyz(ev.b), terms, cnt);
+    if (need) E = gather_irradiance_warp(S.grid, GC, xyz(ev.a), xyz(ev.b), terms, cnt);
     if (lane == 0) {
       ++events;
       if (need) {
@@ -1255,6 +1257,7 @@ __global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const bool in = i < n;
+  const GatherConst GC = gather_const(S.grid);
   V3 x = v3(0.f, 0.f, 0.f), nv = v3(0.f, 0.f, 0.f), e = v3(0.f, 0.f, 0.f);
   if (in) {
     x = v3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
@@ -1269,7 +1272,7 @@ __global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict
     const V3 qv = v3(__shfl_sync(0xffffffffu, nv.x, src), __shfl_sync(0xffffffffu, nv.y, src),
                      __shfl_sync(0xffffffffu, nv.z, src));
     uint32_t cnt = 0;
-    const V3 r = gather_irradiance_warp(S.grid, qx, qv, s_terms + (threadIdx.x & ~31u), cnt);
+    const V3 r = gather_irradiance_warp(S.grid, GC, qx, qv, s_terms + (threadIdx.x & ~31u), cnt);
     if (lane == src) e = r;
   }
   if (!in) return;

@@ -568,10 +568,33 @@ __device__ __forceinline__ void world_to_cell(const GridView& G, V3 p, int c[3])
 // reference's one-photon-at-a-time loop bit for bit.  `terms` is this
 // warp's 32 float4 of shared memory.
 // Returns the irradiance in every lane and the photons scanned in `count`.
-__device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3 n, float4* terms, uint32_t& count) {
+// Per-launch constants of the lookups: 1 / (pi r^2), 1 / cell, and the
+// T / D factor of the photon store (0 when nothing was deposited, so an
+// empty map gives zero irradiance).
+struct GatherConst {
+  float inv_area;
+  float inv_cx;
+  float scale;
+  uint32_t total_ph;   // photons in the sorted grid
+};
+
+__device__ __forceinline__ GatherConst gather_const(const GridView& G) {
+  GatherConst c;
+  const float r = G.radius, r2 = r * r;
+  c.inv_area = 1.0f / (kPi * r2);
+  c.inv_cx = 1.0f / G.cell.x;
+  const uint32_t T = *G.attempts;
+  const uint32_t D = (uint64_t)T < G.capacity ? T : (uint32_t)G.capacity;
+  c.scale = D == 0u ? 0.0f : (float)T / (float)D;
+  c.total_ph = __ldg(&G.cell_off[G.cells]);
+  return c;
+}
+
+__device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const GatherConst& GC, V3 x, V3 n,
+                                                     float4* terms, uint32_t& count) {
   const int lane = threadIdx.x & 31;
   const float r = G.radius, r2 = r * r;
-  const float invArea = 1.0f / (kPi * r2);
+  const float invArea = GC.inv_area;
   // window corners: lanes 0-5 each do one coordinate of world_to_cell(x -
   // (r, r, r)) and world_to_cell(x + (r, r, r)), the same operations
   int wc = 0;
@@ -597,8 +620,8 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
   // row k of the window is (z, y) = (k / ny, k % ny); (k + 1/2) / ny is at
   // least 1/(2 ny) from an integer, far beyond float rounding
   const float inv_ny = 1.0f / (float)ny;
-  const float inv_cx = 1.0f / G.cell.x;
-  const uint32_t total_ph = __ldg(&G.cell_off[G.cells]);
+  const float inv_cx = GC.inv_cx;
+  const uint32_t total_ph = GC.total_ph;
   float acc = 0.f;   // lane c < 3: running sum of component c
   uint32_t scanned = 0;
   for (int rb = 0; rb < rows; rb += 32) {
@@ -725,10 +748,7 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, V3 x, V3
   const float ex = __shfl_sync(0xffffffffu, acc, 0);
   const float ey = __shfl_sync(0xffffffffu, acc, 1);
   const float ez = __shfl_sync(0xffffffffu, acc, 2);
-  uint32_t T = *G.attempts;
-  uint32_t D = (uint64_t)T < G.capacity ? T : (uint32_t)G.capacity;
-  if (D == 0u) return v3(0.f, 0.f, 0.f);
-  float s = (float)T / (float)D;
+  const float s = GC.scale;
   return v3(ex * s, ey * s, ez * s);
 }
 
