@@ -619,7 +619,7 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const Ga
   const int rows = (c1[2] - c0[2] + 1) * ny;
   // row k of the window is (z, y) = (k / ny, k % ny); (k + 1/2) / ny is at
   // least 1/(2 ny) from an integer, far beyond float rounding
-  const float inv_ny = 1.0f / (float)ny;
+  const float inv_ny = __fdividef(1.0f, (float)ny);
   const float inv_cx = GC.inv_cx;
   const uint32_t total_ph = GC.total_ph;
   float acc = 0.f;   // lane c < 3: running sum of component c
@@ -646,7 +646,9 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const Ga
       if (cz < G.res[2] - 1) dz = fmaxf(dz, x.z - (G.origin.z + (float)(cz + 1) * G.cell.z + 0.01f * G.cell.z));
       const float rho2 = dy * dy + dz * dz;
       if (rho2 <= reach2) {
-        const float w = sqrtf(reach2 - rho2) * 1.001f + 0.01f * G.cell.x;
+        // (an approximate square root is enough: the 1.001 factor covers it)
+        const float q = fmaxf(reach2 - rho2, 1e-30f);
+        const float w = q * rsqrtf(q) * 1.001f + 0.01f * G.cell.x;
         // (a reciprocal is enough here: the 1% margin covers its rounding)
         int lo = (int)floorf(((x.x - w) - G.origin.x) * inv_cx);
         int hi = (int)floorf(((x.x + w) - G.origin.x) * inv_cx);
