@@ -95,7 +95,8 @@ struct pale_handle {
   // meshes
   uint32_t n_inst = 0, n_tris = 0;
   DBuf<float> o2w, w2o;
-  DBuf<float4> inst_box, tri, materials;
+  DBuf<float4> inst_box, tri, wtri, materials;
+  DBuf<uint2> wtri_range;
   DBuf<uint2> tri_range;
   DBuf<uint32_t> inst_mat;
   std::vector<float> h_inst_box;   // lo.xyz hi.xyz per instance
@@ -192,6 +193,8 @@ struct pale_handle {
     s.mesh.box = inst_box.p;
     s.mesh.tri_range = tri_range.p;
     s.mesh.tri = tri.p;
+    s.mesh.wtri = wtri.p;
+    s.mesh.wtri_range = wtri_range.p;
     s.mesh.material = inst_mat.p;
     s.mesh.materials = materials.p;
     s.mesh.instances = n_inst;
@@ -385,6 +388,24 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
     float* hb = &h->h_inst_box[6 * i];
     hb[0] = wl.x; hb[1] = wl.y; hb[2] = wl.z; hb[3] = wh.x; hb[4] = wh.y; hb[5] = wh.z;
   }
+  // world-space copies of every instance's triangles (the vertices of the
+  // mesh-hit normals, buildIntersectionNormal)
+  std::vector<float4> wtri;
+  std::vector<uint2> wrng(std::max(1u, h->n_inst));
+  for (uint32_t i = 0; i < h->n_inst; ++i) {
+    wrng[i] = make_uint2((uint32_t)(wtri.size() / 3), rng[i].y);
+    for (uint32_t k = 0; k < rng[i].y; ++k)
+      for (int c = 0; c < 3; ++c) {
+        const float4 v = tri[3 * (rng[i].x + k) + c];
+        const V3 pw = host_xform_point(d->instance_object_to_world + 16 * i, v3(v.x, v.y, v.z));
+        wtri.push_back(make_float4(pw.x, pw.y, pw.z, 0.f));
+      }
+  }
+  if (wtri.empty()) wtri.assign(3, make_float4(0.f, 0.f, 0.f, 0.f));
+  h->wtri.alloc(wtri.size());
+  h->wtri_range.alloc(wrng.size());
+  CK(cudaMemcpyAsync(h->wtri.p, wtri.data(), wtri.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->wtri_range.p, wrng.data(), wrng.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
   h->o2w.alloc(16 * (size_t)std::max(1u, h->n_inst));
   h->w2o.alloc(16 * (size_t)std::max(1u, h->n_inst));
   h->inst_box.alloc(box.size());

@@ -166,6 +166,9 @@ struct MeshView {
   const float4* box;       // per mesh instance: lo (xyz), hi (xyz) as 2 float4
   const uint2* tri_range;  // per mesh instance: first triangle, count
   const float4* tri;       // per triangle 3 float4 object-space vertices
+  const float4* wtri;      // per instance triangle 3 float4 world-space vertices,
+                           // xform_point(o2w, v) of the object-space ones
+  const uint2* wtri_range; // per mesh instance: first world triangle, count
   const uint32_t* material;  // per mesh instance
   const float4* materials;   // base colour rgb, power
   uint32_t instances;
@@ -256,6 +259,31 @@ __device__ __forceinline__ void warp_count(unsigned long long* ctr, uint32_t v) 
   int lane = threadIdx.x & 31;
   int leader = __ffs(mask) - 1;
   if (lane == leader && s) atomicAdd(ctr, (unsigned long long)s);
+}
+
+// Adds per-thread counts to three global counters with one atomic each per
+// block instead of per warp: same-address atomics serialise, and a kernel
+// with a block per 256 rays would issue millions.  Every thread of the
+// block must call it.
+__device__ __forceinline__ void block_count3(unsigned long long* ca, uint32_t va, unsigned long long* cb, uint32_t vb,
+                                             unsigned long long* cc, uint32_t vc) {
+  __shared__ unsigned long long s_cnt[3];
+  if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0ull;
+  __syncthreads();
+  const uint32_t a = __reduce_add_sync(0xffffffffu, va);
+  const uint32_t b = __reduce_add_sync(0xffffffffu, vb);
+  const uint32_t c = __reduce_add_sync(0xffffffffu, vc);
+  if ((threadIdx.x & 31) == 0) {
+    if (a) atomicAdd(&s_cnt[0], (unsigned long long)a);
+    if (b) atomicAdd(&s_cnt[1], (unsigned long long)b);
+    if (c) atomicAdd(&s_cnt[2], (unsigned long long)c);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_cnt[0] && ca) atomicAdd(ca, s_cnt[0]);
+    if (s_cnt[1] && cb) atomicAdd(cb, s_cnt[1]);
+    if (s_cnt[2] && cc) atomicAdd(cc, s_cnt[2]);
+  }
 }
 
 }  // namespace pale

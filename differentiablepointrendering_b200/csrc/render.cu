@@ -238,9 +238,8 @@ __global__ void __launch_bounds__(kBlock) k_photon_bounce(PhotonArgs A, uint32_t
     }
     A.qb.flags[slot] = (alive ? 1 : 0) | (dep ? 2 : 0);
   }
-  warp_count(&A.st->photon_segments, slot < n_in ? 1u : 0u);
-  warp_count(&A.st->node_visits, ctr.nodes);
-  warp_count(&A.st->surfel_tests, ctr.tests);
+  block_count3(&A.st->photon_segments, slot < n_in ? 1u : 0u, &A.st->node_visits, ctr.nodes, &A.st->surfel_tests,
+               ctr.tests);
   uint32_t ca = __syncthreads_count(alive), cd = __syncthreads_count(dep);
   if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, cd);
 }
@@ -978,9 +977,8 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
     if (alive && (threadIdx.x & 31) == __ffs(peers) - 1)
       atomicAdd(&A.job_count[(size_t)(parity ^ 1u) * kMaxJobsPerBatch + job], (uint32_t)__popc(peers));
   }
-  warp_count(&A.st->adjoint_segments, t < n_in ? 1u : 0u);
-  warp_count(&A.st->node_visits, ctr.nodes);
-  warp_count(&A.st->surfel_tests, ctr.tests);
+  block_count3(&A.st->adjoint_segments, t < n_in ? 1u : 0u, &A.st->node_visits, ctr.nodes, &A.st->surfel_tests,
+               ctr.tests);
 }
 
 // Derivatives of eta * alpha_geom for the hit at x on surfel k along the
@@ -1199,21 +1197,21 @@ __global__ void __launch_bounds__(kBlock) k_trace_rays(SceneView S, RunState* st
   extern __shared__ TravNode s_top[];
   stage_top_nodes(S, s_top);
   uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n) return;
   TraceCounters ctr{0, 0};
-  Hit h = intersect_scene(S, s_top, v3(o[3 * i], o[3 * i + 1], o[3 * i + 2]), v3(d[3 * i], d[3 * i + 1], d[3 * i + 2]),
-                          ctr, st);
-  inst[i] = h.inst;
-  prim[i] = h.inst >= 0 ? (int32_t)h.prim : -1;
-  t[i] = h.inst >= 0 ? h.t : 3.402823466e+38f;
-  alpha[i] = h.inst >= 0 ? h.alpha : 0.f;
-  if (pos) {
-    pos[3 * i] = h.pos.x;
-    pos[3 * i + 1] = h.pos.y;
-    pos[3 * i + 2] = h.pos.z;
+  if (i < n) {
+    Hit h = intersect_scene(S, s_top, v3(o[3 * i], o[3 * i + 1], o[3 * i + 2]),
+                            v3(d[3 * i], d[3 * i + 1], d[3 * i + 2]), ctr, st);
+    inst[i] = h.inst;
+    prim[i] = h.inst >= 0 ? (int32_t)h.prim : -1;
+    t[i] = h.inst >= 0 ? h.t : 3.402823466e+38f;
+    alpha[i] = h.inst >= 0 ? h.alpha : 0.f;
+    if (pos) {
+      pos[3 * i] = h.pos.x;
+      pos[3 * i + 1] = h.pos.y;
+      pos[3 * i + 2] = h.pos.z;
+    }
   }
-  atomicAdd(&st->node_visits, (unsigned long long)ctr.nodes);
-  atomicAdd(&st->surfel_tests, (unsigned long long)ctr.tests);
+  block_count3(&st->node_visits, ctr.nodes, &st->surfel_tests, ctr.tests, nullptr, 0u);
 }
 
 void trace_rays(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d, int32_t* inst,
@@ -1232,16 +1230,16 @@ __global__ void __launch_bounds__(kBlock) k_trace_transmittance(SceneView S, Run
   extern __shared__ TravNode s_top[];
   stage_top_nodes(S, s_top);
   uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n) return;
   TraceCounters ctr{0, 0};
-  float T = 1.0f;
-  Hit h = intersect_scene_transmit(S, s_top, v3(o[3 * i], o[3 * i + 1], o[3 * i + 2]),
-                                   v3(d[3 * i], d[3 * i + 1], d[3 * i + 2]), T, 1u << 16, ctr, st);
-  inst[i] = h.inst;
-  t[i] = h.inst >= 0 ? h.t : 3.402823466e+38f;
-  transmit[i] = T;
-  atomicAdd(&st->node_visits, (unsigned long long)ctr.nodes);
-  atomicAdd(&st->surfel_tests, (unsigned long long)ctr.tests);
+  if (i < n) {
+    float T = 1.0f;
+    Hit h = intersect_scene_transmit(S, s_top, v3(o[3 * i], o[3 * i + 1], o[3 * i + 2]),
+                                     v3(d[3 * i], d[3 * i + 1], d[3 * i + 2]), T, 1u << 16, ctr, st);
+    inst[i] = h.inst;
+    t[i] = h.inst >= 0 ? h.t : 3.402823466e+38f;
+    transmit[i] = T;
+  }
+  block_count3(&st->node_visits, ctr.nodes, &st->surfel_tests, ctr.tests, nullptr, 0u);
 }
 
 void trace_transmittance(const SceneView& sv, RunState* st, uint32_t n, const float* o, const float* d,

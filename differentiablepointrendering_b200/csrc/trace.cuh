@@ -316,6 +316,19 @@ __device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNo
   return count;
 }
 
+// A 4x4 instance matrix (16 floats, 64 B aligned) in four 16-byte loads.
+__device__ __forceinline__ void load_matrix(const float* M, float (&m)[16]) {
+  const float4* m4 = reinterpret_cast<const float4*>(M);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const float4 v = __ldg(&m4[r]);
+    m[4 * r] = v.x;
+    m[4 * r + 1] = v.y;
+    m[4 * r + 2] = v.z;
+    m[4 * r + 3] = v.w;
+  }
+}
+
 // The closest mesh hit, in object space per instance (intersectBLASMesh,
 // IntersectionKernels.h:37-105); `best` is the world distance of the hit
 // (+inf on a miss).
@@ -331,10 +344,8 @@ __device__ __forceinline__ Hit intersect_meshes(const SceneView& S, V3 o, V3 d, 
   for (uint32_t i = 0; i < M.instances; ++i) {
     const float4 lo = __ldg(&M.box[2 * i]), hi = __ldg(&M.box[2 * i + 1]);
     if (!entered(slab_entry(o, invw, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, best), best)) continue;
-    const float* W2O = M.w2o + 16 * i;
     float w2o[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) w2o[k] = __ldg(&W2O[k]);
+    load_matrix(M.w2o + 16 * i, w2o);
     V3 oo = xform_point(w2o, o);
     V3 dd = xform_dir(w2o, d);
     uint2 rg = __ldg(&M.tri_range[i]);
@@ -353,8 +364,7 @@ __device__ __forceinline__ Hit intersect_meshes(const SceneView& S, V3 o, V3 d, 
     }
     if (!any) continue;
     float o2w[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) o2w[k] = __ldg(&M.o2w[16 * i + k]);
+    load_matrix(M.o2w + 16 * i, o2w);
     V3 hw = xform_point(o2w, oo + scale(dd, bt));
     float tw = dot(hw - o, d);
     if (tw > 0.0f && tw < best) {
@@ -439,13 +449,10 @@ __device__ __forceinline__ Hit intersect_scene_transmit(const SceneView& S, cons
 // buildIntersectionNormal (KernelHelpers.h:480-503).
 __device__ __forceinline__ V3 hit_normal(const SceneView& S, const Hit& h) {
   if (h.inst < (int)S.mesh.instances) {
-    float o2w[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) o2w[k] = __ldg(&S.mesh.o2w[16 * h.inst + k]);
-    const float4* tv = S.mesh.tri + 3 * h.prim;
-    V3 p0 = xform_point(o2w, xyz(__ldg(&tv[0])));
-    V3 p1 = xform_point(o2w, xyz(__ldg(&tv[1])));
-    V3 p2 = xform_point(o2w, xyz(__ldg(&tv[2])));
+    // the world-space copy holds xform_point(o2w, v) of the triangle's vertices
+    const uint32_t k = h.prim - __ldg(&S.mesh.tri_range[h.inst]).x;
+    const float4* tv = S.mesh.wtri + 3 * (__ldg(&S.mesh.wtri_range[h.inst]).x + k);
+    const V3 p0 = xyz(__ldg(&tv[0])), p1 = xyz(__ldg(&tv[1])), p2 = xyz(__ldg(&tv[2]));
     return normalize(cross(p1 - p0, p2 - p0));
   }
   return xyz(__ldg(&S.sf.cn[h.prim]));
