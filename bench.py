@@ -214,6 +214,57 @@ def run_reference(args, rank: int, world: int):
 
 
 # ------------------------------------------------------------------- ours
+def plain_and_latency(r, frame, target, dev, batched_ms: float, steps: int = 2, requests: int = 20) -> dict:
+    """Beside the batched step: (1) the plain path, the same step with one
+    view per call (each call traces its photon map and runs its own camera
+    gather and adjoint, as render_forward/render_backward per camera do),
+    timed with CUDA events; (2) the latency of single-view gradient requests
+    (forward + L2 loss + adjoint of camera 0, host-synchronised each), wall
+    clock from submission to the result being ready."""
+    import numpy as np
+    import torch
+
+    from differentiablepointrendering_b200.device import DeviceFrame
+
+    frames, targets, off = [], [], 0
+    for i, (w, h) in enumerate(frame.sizes):
+        frames.append(DeviceFrame(r, cameras=[frame.cams[i]], device=dev))
+        targets.append(target[off:off + w * h].contiguous())
+        off += w * h
+
+    def plain_step():
+        for f, t in zip(frames, targets):
+            f.forward_loss(t)
+            f.backward()
+
+    plain_step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        plain_step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = a.elapsed_time(b) / steps
+    lat = []
+    for _ in range(requests):
+        t0 = time.perf_counter()
+        frames[0].forward_loss(targets[0])
+        frames[0].backward()
+        torch.cuda.synchronize()
+        lat.append((time.perf_counter() - t0) * 1e3)
+    lat = np.sort(np.array(lat))
+    w0, h0 = frame.sizes[0]
+    return {
+        "plain_per_view": {"ms_per_step": round(plain_ms, 3), "iters_per_s": round(1e3 / plain_ms, 4),
+                           "batched_speedup": round(plain_ms / batched_ms, 3), "steps": steps,
+                           "note": "same views, passes and seeds settings, one view per forward/adjoint call"},
+        "latency_ms": {"request": f"one {w0}x{h0} view: photon pass, gather, L2 loss, adjoint", "n": requests,
+                       "p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3)},
+    }
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import numpy as np
     import torch
@@ -326,6 +377,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if rank != 0:
         r.close()
         return
+    extra = {} if args.skip_extra else plain_and_latency(r, frame, target, dev, ms_per_step)
     peaks = read_peaks()
     hbm = peaks["hbm_gbs"] if peaks else 6650.0
     # per-kernel device time (events around every launch, stats step) and
@@ -364,6 +416,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "clocks": clk,
         "breakdown_ms": {"photon": round(sf["photon_ms"], 3), "gather": round(sf["gather_ms"], 3),
                          "adjoint": round(sb["backward_ms"], 3)},
+        **extra,
     }
     print(json.dumps(line), flush=True)
     r.close()
@@ -377,6 +430,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="box200k", choices=sorted(WORKLOADS))
     ap.add_argument("--skip-cpu", dest="skip_cpu", action="store_true")
+    ap.add_argument("--skip-extra", dest="skip_extra", action="store_true",
+                    help="skip the per-view and request-latency measurements")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
