@@ -35,6 +35,9 @@ WORKLOADS = {
     # the 10k-surfel, single-view workload
     "box10k": dict(n=10000, cams=1, res=256, photons=100000, bounces=4, forward_passes=1, spp=4,
                    adjoint_bounces=4, adjoint_spp=4, radius=0.02),
+    # the memory-bound case: 1M surfels, 32 views of 800x800, 64 passes, depth 8
+    "box1m-32view": dict(n=1000000, cams=32, res=800, photons=1000000, bounces=8, forward_passes=1, spp=64,
+                         adjoint_bounces=8, adjoint_spp=64, radius=0.01),
     # box200k's scene and photon map with one 256x256 view and 2 passes: the
     # case the per-kernel profiles are captured on (a few hundred MB resident)
     "box200k-1view": dict(n=200000, cams=1, res=256, photons=1000000, bounces=6, forward_passes=1, spp=2,
