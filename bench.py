@@ -425,6 +425,93 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     r.close()
 
 
+# ---------------------------------------------------------------- serving
+SERVING_SCENES = (   # name, surfels, views, resolution, passes, depth (log-uniform sizes, as the C5 spread)
+    ("s10k", 10000, 4, 128, 4, 4), ("s50k", 50000, 4, 256, 8, 5), ("s200k", 200000, 4, 512, 4, 6),
+    ("s1m", 1000000, 4, 256, 16, 8))
+
+
+def run_serving(args):
+    """Poisson stream of single-view requests (70% forward, 30% gradient)
+    over resident scenes of different sizes, served by serving.Server, and
+    the same stream served one request at a time in arrival order (the plain
+    path).  One JSON line: completed requests/s and p50/p99 latency of both."""
+    import numpy as np
+    import torch
+
+    from differentiablepointrendering_b200.build import build_library
+    from differentiablepointrendering_b200.scene import make_box_scene, make_surfels
+    from differentiablepointrendering_b200.serving import Request, Server
+
+    build_library()
+    rng = np.random.default_rng(17)
+    free, _ = torch.cuda.mem_get_info()
+    srv = Server(hbm_budget=min(150 << 30, int(free * 0.9)))
+    res = {}
+    for name, n, views, reso, spp, depth in SERVING_SCENES:
+        st = {"photons": 200000, "bounces": depth, "forward_passes": 1, "gather_passes": spp,
+              "adjoint_bounces": depth, "adjoint_passes": spp, "gather_radius": 0.01 if n >= 200000 else 0.02}
+        srv.add_scene(name, make_box_scene(n, cameras=views, resolution=reso, points=make_surfels(n, 1234)), st)
+        res[name] = (views, reso)
+    names = [s[0] for s in SERVING_SCENES]
+
+    def stream(rate, seconds):
+        t, out = 0.0, []
+        while t < seconds:
+            t += rng.exponential(1.0 / rate)
+            s = names[int(rng.integers(len(names)))]
+            views, reso = res[s]
+            grad = rng.uniform() < 0.3
+            tgt = rng.uniform(0, 1, (reso, reso, 3)).astype(np.float32) if grad else None
+            out.append((t, Request(s, int(rng.integers(views)), "gradient" if grad else "forward", tgt)))
+        return out
+
+    lines = []
+    for rate in args.rates:
+        reqs = stream(rate, args.seconds)
+        t0 = time.perf_counter()
+        for at, q in reqs:
+            delay = t0 + at - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            srv.submit(q)
+        for _, q in reqs:
+            q.done.wait(600)
+        span = max(q.t_done for _, q in reqs) - t0
+        lat = np.array([q.latency_ms for _, q in reqs])
+        # the plain path: the same arrivals, one request at a time in order
+        plain = []
+        clock = 0.0
+        for at, q in reqs:
+            p = Request(q.scene, q.camera, q.kind, q.target)
+            sc = srv.scenes[p.scene]
+            start = max(clock, at)
+            a = time.perf_counter()
+            if p.kind == "forward":
+                sc._forward([p.camera], [p])
+            else:
+                sc._gradient(p)
+            clock = start + (time.perf_counter() - a)
+            plain.append((clock - at) * 1e3)
+        plain = np.array(plain)
+        merged = [q.batch_views for _, q in reqs if q.kind == "forward"]
+        lines.append({"rate_per_s": rate, "requests": len(reqs),
+                      "served": {"p50_ms": round(float(np.percentile(lat, 50)), 2),
+                                 "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                                 "requests_per_s": round(len(reqs) / span, 2),
+                                 "mean_views_per_forward_call": round(float(np.mean(merged)), 2) if merged else 0},
+                      "plain": {"p50_ms": round(float(np.percentile(plain, 50)), 2),
+                                "p99_ms": round(float(np.percentile(plain, 99)), 2),
+                                "requests_per_s": round(len(reqs) / (clock + 1e-9), 2)}})
+    admitted = srv.admitted_bytes
+    srv.close()
+    print(json.dumps({"metric": "serving latency p50/p99 (ms) and requests/s", "impl": "ours",
+                      "scenes": [dict(zip(("name", "surfels", "views", "res", "passes", "depth"), s))
+                                 for s in SERVING_SCENES],
+                      "mix": "70% forward (LDR image of one view), 30% gradient (L2 loss + adjoint of one view)",
+                      "budget_bytes": srv.budget, "admitted_bytes": admitted, "runs": lines}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -435,7 +522,13 @@ def main():
     ap.add_argument("--skip-cpu", dest="skip_cpu", action="store_true")
     ap.add_argument("--skip-extra", dest="skip_extra", action="store_true",
                     help="skip the per-view and request-latency measurements")
+    ap.add_argument("--serving", action="store_true", help="serving benchmark (Poisson request stream)")
+    ap.add_argument("--rates", type=float, nargs="*", default=[5.0, 20.0, 50.0])
+    ap.add_argument("--seconds", type=float, default=6.0)
     args = ap.parse_args()
+    if args.serving:
+        run_serving(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -29,7 +29,7 @@ class PaleSettings(C.Structure):
                 ("q_null", C.c_float), ("q_reflect", C.c_float), ("q_transmit", C.c_float),
                 ("gather_radius", C.c_float), ("leaf_size", C.c_uint32), ("rng_mode", C.c_uint32),
                 ("debug_images", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float),
-                ("null_weight", C.c_uint32), ("gradients", C.c_uint32)]
+                ("null_weight", C.c_uint32), ("gradients", C.c_uint32), ("camera_seeds", C.c_uint32)]
 
 
 class PalePoints(C.Structure):
@@ -145,6 +145,9 @@ def settings_from_dict(d: Optional[dict]) -> PaleSettings:
             continue
         if k == "gradients":
             s.gradients = {"opacity": 0, "all": 1}.get(v, v) if isinstance(v, str) else int(v)
+            continue
+        if k == "camera_seeds":
+            s.camera_seeds = {"selection": 0, "camera": 1}.get(v, v) if isinstance(v, str) else int(v)
             continue
         if k not in SETTINGS_KEYS:
             raise KeyError(f"unknown renderer setting '{k}'")

@@ -704,13 +704,14 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   for (uint32_t i = 0; i < nsel; ++i) {
     sel[i] = h->cams[idx[i]];
     sel[i].pixel_offset = total;
-    sel[i].seed_slot = i;
+    sel[i].seed_slot = st.camera_seeds == PALE_CAMERA_SEEDS_CAMERA ? idx[i] : i;
     total += sel[i].w * sel[i].h;
   }
   h->d_cams.ensure(std::max<size_t>(1, nsel));
   if (nsel) CK(cudaMemcpyAsync(h->d_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
   // seed stream of submitPhotonMappingKernel: passes x (1 + bounces) + cameras
-  std::vector<uint32_t> seeds = mt_table(st.seed, (size_t)st.forward_passes * (1 + st.max_bounces) + nsel + 1);
+  const size_t cam_seeds = st.camera_seeds == PALE_CAMERA_SEEDS_CAMERA ? h->cams.size() : nsel;
+  std::vector<uint32_t> seeds = mt_table(st.seed, (size_t)st.forward_passes * (1 + st.max_bounces) + cam_seeds + 1);
   h->seeds_fwd.ensure(seeds.size());
   CK(cudaMemcpyAsync(h->seeds_fwd.p, seeds.data(), seeds.size() * 4, cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
@@ -1010,6 +1011,7 @@ int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale
     if (h->st.adjoint_bounces > 255) throw ArgError("at most 255 adjoint bounces are supported");
     if (h->st.null_weight > PALE_NULL_WEIGHT_UNBIASED) throw ArgError("null_weight must be reference or unbiased");
     if (h->st.gradients > PALE_GRADIENTS_ALL) throw ArgError("gradients must be opacity or all");
+    if (h->st.camera_seeds > PALE_CAMERA_SEEDS_CAMERA) throw ArgError("camera_seeds must be selection or camera");
     if (h->st.null_weight == PALE_NULL_WEIGHT_UNBIASED && !(h->st.q_null > 0.f))
       throw ArgError("unbiased null weighting needs q_null > 0");
     check_points(&desc->points, "pale_create");

@@ -60,6 +60,15 @@ typedef struct pale_handle pale_handle;
 #define PALE_GRADIENTS_OPACITY 0u
 #define PALE_GRADIENTS_ALL 1u
 
+/* Which seed of the camera-gather table a camera uses.  SELECTION is the
+ * reference's: the camera's position in the list a render call selects, so
+ * one camera rendered alone and inside a larger selection draws different
+ * samples.  CAMERA keys the seed by the camera's index in the scene, so a
+ * camera's image does not depend on which other cameras share the call
+ * (what a server that merges requests needs). */
+#define PALE_CAMERA_SEEDS_SELECTION 0u
+#define PALE_CAMERA_SEEDS_CAMERA 1u
+
 typedef struct pale_settings {
     uint32_t photons_per_launch;   /* "photons"          (default 1e6)       */
     uint32_t max_bounces;          /* "bounces"          (6)                 */
@@ -83,6 +92,7 @@ typedef struct pale_settings {
     float gamma;                   /* SensorGPU::gammaCorrection   (2.2)     */
     uint32_t null_weight;          /* PALE_NULL_WEIGHT_*                     */
     uint32_t gradients;            /* PALE_GRADIENTS_*                       */
+    uint32_t camera_seeds;         /* PALE_CAMERA_SEEDS_*                    */
 } pale_settings;
 
 /* Per-point parameter block (structure of arrays, float32).
