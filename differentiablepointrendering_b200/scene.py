@@ -368,19 +368,79 @@ _CUSTOM = ("x", "y", "z", "tu_x", "tu_y", "tu_z", "tv_x", "tv_y", "tv_z", "su", 
            "albedo_r", "albedo_g", "albedo_b", "opacity")
 
 
-def load_surfel_ply(path: str) -> Dict[str, np.ndarray]:
-    """Custom surfel schema of PLYPointLoader.ixx:156-161 (beta and shape
-    default to 0 when absent)."""
-    v = read_ply_vertices(path)
-    if not all(k in v for k in _CUSTOM):
-        raise RuntimeError(f"{path}: unsupported vertex schema")
+_SPLAT = ("x", "y", "z", "f_dc_0", "f_dc_1", "f_dc_2", "opacity", "scale_0", "scale_1",
+          "rot_0", "rot_1", "rot_2", "rot_3")
+
+
+def _norm_rows(a: np.ndarray) -> np.ndarray:
+    return a / np.sqrt(np.sum(a * a, axis=1, keepdims=True, dtype=np.float32))
+
+
+def canonical_frames(tu: np.ndarray, tv: np.ndarray):
+    """canonicalizeFrameFaceUp (PLYPointLoader.ixx:71-97): unit tangents,
+    Gram-Schmidt of the second against the first (the y axis, or x when the
+    first is near y, for a degenerate pair), and the second flipped so that
+    the normal tu x tv has z >= 0."""
+    tu = _norm_rows(tu.astype(np.float32))
+    tv = _norm_rows(tv.astype(np.float32))
+    ortho = tv - np.sum(tv * tu, axis=1, keepdims=True) * tu
+    bad = np.sum(ortho * ortho, axis=1) < np.float32(1e-6)
+    if bad.any():
+        alt = np.where((np.abs(tu[:, 1]) < 0.9)[:, None], np.array([0, 1, 0], np.float32),
+                       np.array([1, 0, 0], np.float32))
+        alt = alt - np.sum(alt * tu, axis=1, keepdims=True) * tu
+        ortho = np.where(bad[:, None], alt, ortho)
+    tv = _norm_rows(ortho)
+    flip = np.cross(tu, tv)[:, 2] < 0
+    tv = np.where(flip[:, None], -tv, tv)
+    return tu.astype(np.float32), tv.astype(np.float32)
+
+
+def _splat_points(v: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+    """The Gaussian-splat schema as surfels (PLYPointLoader.ixx:294-388):
+    radii 2 exp(scale_0/1), opacity sigmoid(opacity) (arguments clamped to
+    [-20, 20]), albedo 0.8 (the loader computes the DC colour but keeps a
+    constant albedo), tangents the first two columns of the normalised
+    rotation quaternion (w, x, y, z), then orthonormalised (the second
+    falls back to +y when it vanishes); beta and shape 0."""
     n = v["x"].shape[0]
-    st = lambda *ks: np.stack([v[k] for k in ks], 1)
-    return as_points(dict(position=st("x", "y", "z"), tangent_u=st("tu_x", "tu_y", "tu_z"),
-                          tangent_v=st("tv_x", "tv_y", "tv_z"), scale=st("su", "sv"),
-                          albedo=st("albedo_r", "albedo_g", "albedo_b"), opacity=v["opacity"],
-                          beta=v.get("beta", np.zeros(n, np.float32)),
-                          shape=v.get("shape", np.zeros(n, np.float32))))
+    f = lambda k: v[k].astype(np.float32)
+    c = lambda x: np.clip(x, np.float32(-20), np.float32(20))
+    q = np.stack([f("rot_0"), f("rot_1"), f("rot_2"), f("rot_3")], 1)
+    q = q / np.sqrt(np.sum(q * q, axis=1, keepdims=True, dtype=np.float32))
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    one, two = np.float32(1), np.float32(2)
+    tu = np.stack([one - two * (y * y + z * z), two * (x * y + w * z), two * (x * z - w * y)], 1)
+    tv = np.stack([two * (x * y - w * z), one - two * (x * x + z * z), two * (y * z + w * x)], 1)
+    lu = np.sum(tu * tu, axis=1, keepdims=True)
+    tu = np.where(lu > 0, tu / np.sqrt(np.where(lu > 0, lu, 1)), tu)
+    tv = tv - np.sum(tv * tu, axis=1, keepdims=True) * tu
+    lv = np.sum(tv * tv, axis=1, keepdims=True)
+    tv = np.where(lv > 0, tv / np.sqrt(np.where(lv > 0, lv, 1)), np.array([[0, 1, 0]], np.float32))
+    scale = np.stack([np.exp(c(f("scale_0"))), np.exp(c(f("scale_1")))], 1) * two
+    opacity = one / (one + np.exp(-c(f("opacity"))))
+    return as_points(dict(position=np.stack([f("x"), f("y"), f("z")], 1), tangent_u=tu, tangent_v=tv,
+                          scale=scale, albedo=np.full((n, 3), 0.8, np.float32), opacity=opacity,
+                          beta=np.zeros(n, np.float32), shape=np.zeros(n, np.float32)))
+
+
+def load_surfel_ply(path: str) -> Dict[str, np.ndarray]:
+    """PLYPointLoader (PLYPointLoader.ixx:144-390): the custom surfel schema
+    (:156-161; tangent frames canonicalised face up, albedo clamped to
+    [0, 1]; beta and shape default to 0 when absent) or the Gaussian-splat
+    schema (:163-167, converted as _splat_points describes)."""
+    v = read_ply_vertices(path)
+    if all(k in v for k in _CUSTOM):
+        n = v["x"].shape[0]
+        st = lambda *ks: np.stack([v[k] for k in ks], 1).astype(np.float32)
+        tu, tv = canonical_frames(st("tu_x", "tu_y", "tu_z"), st("tv_x", "tv_y", "tv_z"))
+        return as_points(dict(position=st("x", "y", "z"), tangent_u=tu, tangent_v=tv, scale=st("su", "sv"),
+                              albedo=np.clip(st("albedo_r", "albedo_g", "albedo_b"), 0, 1), opacity=v["opacity"],
+                              beta=v.get("beta", np.zeros(n, np.float32)),
+                              shape=v.get("shape", np.zeros(n, np.float32))))
+    if all(k in v for k in _SPLAT):
+        return _splat_points(v)
+    raise RuntimeError(f"{path}: unsupported vertex schema")
 
 
 def write_surfel_ply(path: str, points: Dict[str, np.ndarray]):
