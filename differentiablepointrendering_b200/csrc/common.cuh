@@ -140,6 +140,11 @@ struct BvhNodeH {
   uint4 q1;
 };
 static_assert(sizeof(BvhNodeH) == 32, "node layout");
+// Traversal stack entries per thread kept in shared memory (the rest local).
+#ifndef PALE_SMEM_STACK
+#define PALE_SMEM_STACK 8
+#endif
+
 #ifndef PALE_HALF_NODES
 #define PALE_HALF_NODES 1
 #endif

@@ -244,7 +244,11 @@ __global__ void __launch_bounds__(kBlock) k_photon_bounce(PhotonArgs A, uint32_t
   if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, cd);
 }
 
-static size_t top_smem(const SceneView& s) { return (size_t)s.top_nodes * sizeof(TravNode); }
+// Dynamic shared memory of a traversal kernel: the staged top nodes, then
+// PALE_SMEM_STACK stack entries (8 B) per thread of the block.
+static size_t top_smem(const SceneView& s) {
+  return (size_t)s.top_nodes * sizeof(TravNode) + (size_t)PALE_SMEM_STACK * kBlock * sizeof(uint2);
+}
 
 void photon_emit(const PhotonArgs& a, cudaStream_t s) {
   const uint32_t nb = blocks_for(a.photons_per_launch);

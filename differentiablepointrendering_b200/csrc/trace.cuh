@@ -130,6 +130,50 @@ __device__ __forceinline__ void load_node(const SceneView& S, const TravNode* __
 }
 #endif
 
+// The traversal stack of one thread: its first PALE_SMEM_STACK entries in
+// shared memory after the staged top nodes (entry k of thread t at
+// [k * blockDim.x + t], so a warp's accesses hit distinct banks), the rest
+// in a local array.  Traversal kernels size their dynamic shared memory for
+// it (top_smem).  The local part alone would be 512 B per thread, more than
+// L1 holds for four resident blocks, so pops would wait on L2.
+struct TravStack {
+#if PALE_SMEM_STACK > 0
+  uint2* sm;
+#endif
+  uint32_t node[kStackDepth - PALE_SMEM_STACK];
+  float t[kStackDepth - PALE_SMEM_STACK];
+  __device__ __forceinline__ TravStack(const TravNode* smem_top, uint32_t top_nodes) {
+#if PALE_SMEM_STACK > 0
+    sm = reinterpret_cast<uint2*>(const_cast<TravNode*>(smem_top) + top_nodes) + threadIdx.x;
+#else
+    (void)smem_top;
+    (void)top_nodes;
+#endif
+  }
+  __device__ __forceinline__ void push(int sp, uint32_t n, float tt) {
+#if PALE_SMEM_STACK > 0
+    if (sp < PALE_SMEM_STACK) {
+      sm[(size_t)sp * blockDim.x] = make_uint2(n, __float_as_uint(tt));
+      return;
+    }
+#endif
+    node[sp - PALE_SMEM_STACK] = n;
+    t[sp - PALE_SMEM_STACK] = tt;
+  }
+  __device__ __forceinline__ void get(int sp, uint32_t& n, float& tt) const {
+#if PALE_SMEM_STACK > 0
+    if (sp < PALE_SMEM_STACK) {
+      const uint2 e = sm[(size_t)sp * blockDim.x];
+      n = e.x;
+      tt = __uint_as_float(e.y);
+      return;
+    }
+#endif
+    n = node[sp - PALE_SMEM_STACK];
+    tt = t[sp - PALE_SMEM_STACK];
+  }
+};
+
 // Closest surfel with t in (tmin, limit) along (o, d) (the surfel cloud's
 // transform is the identity, so this is intersectBLASPointCloudFirstHit,
 // IntersectionKernels.h:585-675, where tmin is rayEpsilon = 1e-5).  Returns
@@ -141,8 +185,7 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
   const V3 inv = safe_inv(d);
   float best = limit;
   bool hit = false;
-  uint32_t stack_node[kStackDepth];
-  float stack_t[kStackDepth];
+  TravStack stk(smem_top, S.top_nodes);
   int sp = 0;
   uint32_t node = 0;
   // an acyclic tree visits each node at most once
@@ -192,8 +235,7 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
       uint32_t nearN = e0 <= e1 ? w.x : w.y, farN = e0 <= e1 ? w.y : w.x;
       float farT = e0 <= e1 ? e1 : e0;
       if (sp < kStackDepth) {
-        stack_node[sp] = farN;
-        stack_t[sp] = farT;
+        stk.push(sp, farN, farT);
         ++sp;
       } else {
         flag_error(st, kErrStackOverflow);
@@ -206,8 +248,11 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
     bool found = false;
     while (sp > 0) {
       --sp;
-      if (stack_t[sp] <= best) {
-        node = stack_node[sp];
+      uint32_t sn;
+      float st_t;
+      stk.get(sp, sn, st_t);
+      if (st_t <= best) {
+        node = sn;
         found = true;
         break;
       }
@@ -232,8 +277,7 @@ __device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNo
 #pragma unroll
   for (int k = 0; k < K; ++k) t_out[k] = limit;
   float best = limit;   // t_out[K - 1] once K hits are held
-  uint32_t stack_node[kStackDepth];
-  float stack_t[kStackDepth];
+  TravStack stk(smem_top, S.top_nodes);
   int sp = 0;
   uint32_t node = 0;
   const uint32_t visit_cap = 2u * S.node_count + 64u;
@@ -291,8 +335,7 @@ __device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNo
       uint32_t nearN = e0 <= e1 ? w.x : w.y, farN = e0 <= e1 ? w.y : w.x;
       float farT = e0 <= e1 ? e1 : e0;
       if (sp < kStackDepth) {
-        stack_node[sp] = farN;
-        stack_t[sp] = farT;
+        stk.push(sp, farN, farT);
         ++sp;
       } else {
         flag_error(st, kErrStackOverflow);
@@ -305,8 +348,11 @@ __device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNo
     bool found = false;
     while (sp > 0) {
       --sp;
-      if (stack_t[sp] <= best) {
-        node = stack_node[sp];
+      uint32_t sn;
+      float st_t;
+      stk.get(sp, sn, st_t);
+      if (st_t <= best) {
+        node = sn;
         found = true;
         break;
       }
