@@ -217,6 +217,12 @@ constexpr int kGatherHits = PALE_GATHER_HITS;
 #define PALE_TRACE_MIN_BLOCKS 4
 #endif
 constexpr int kTraceMinBlocks = PALE_TRACE_MIN_BLOCKS;
+// The camera-gather round kernel's own budget (its 8-hit list needs the
+// registers more than it needs the fourth block).
+#ifndef PALE_ROUND_MIN_BLOCKS
+#define PALE_ROUND_MIN_BLOCKS 3
+#endif
+constexpr int kRoundMinBlocks = PALE_ROUND_MIN_BLOCKS;
 // The same for the warp-per-lookup kernels (camera lookups, transport).
 #ifndef PALE_LOOKUP_MIN_BLOCKS
 #define PALE_LOOKUP_MIN_BLOCKS 4

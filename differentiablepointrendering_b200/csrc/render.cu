@@ -398,7 +398,7 @@ __device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float 
 
 // Round step 1: one lane per queue entry (a live path).
 template <int K>
-__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs A, uint32_t round) {
+__global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_round(FrameArgs A, uint32_t round) {
   extern __shared__ TravNode s_top[];
   stage_top_nodes(A.scene, s_top);
   const SceneView& S = A.scene;
