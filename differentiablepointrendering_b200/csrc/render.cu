@@ -861,16 +861,20 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
   TraceCounters ctr{0, 0};
   if (t < n_in) {
     const SceneView& S = A.scene;
-    const RayRec ry = A.qb.q[parity][slot];
-    const uint32_t jb = __float_as_uint(ry.d.w);
+    const float4 ro = A.qb.q[parity][slot].o, rd = A.qb.q[parity][slot].d;
+    const V3 o = xyz(ro), d = xyz(rd);
+    Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
+    // the rest of the ray and its random stream after the walk, so that
+    // they hold no registers during it
+    const float4 rt = A.qb.q[parity][slot].t;
+    const uint32_t jb = __float_as_uint(rd.w);
     job = jb >> 8;
     // the RNG key is the slot the ray holds in its own job's queue
     const uint32_t jslot = slot - A.job_start[(size_t)parity * kMaxJobsPerBatch + job];
     Rng r(per_item_seed(adjoint_base(A, job, 1u + bounce_index), jslot));
-    const V3 o = xyz(ry.o), d = xyz(ry.d), thr = xyz(ry.t);
-    const uint32_t path = __float_as_uint(ry.o.w), bounce = (jb & 0xFFu) + 1u;
-    const uint32_t pixel = __float_as_uint(ry.t.w);
-    Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
+    const V3 thr = xyz(rt);
+    const uint32_t path = __float_as_uint(ro.w), bounce = (jb & 0xFFu) + 1u;
+    const uint32_t pixel = __float_as_uint(rt.w);
     if (h.inst >= 0) {
       const bool is_mesh = h.inst < (int)S.mesh.instances;
       V3 nrm = hit_normal(S, h);

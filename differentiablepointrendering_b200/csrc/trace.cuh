@@ -94,6 +94,23 @@ __device__ __forceinline__ bool surfel_hit(const SurfelView& sf, uint32_t i, V3 
   return true;
 }
 
+// The hit point and alpha_geom of surfel i at distance th along (o, d):
+// the operations of surfel_hit after its distance test, so the values are
+// the ones it computed for that hit.
+__device__ __forceinline__ void surfel_eval(const SurfelView& sf, uint32_t i, V3 o, V3 d, float th, V3& x_out,
+                                            float& a_out) {
+  const float4 pe = __ldg(&sf.pe[i]);
+  const float4 u4 = __ldg(&sf.u[i]);
+  const float4 v4 = __ldg(&sf.v[i]);
+  V3 x = o + scale(d, th);
+  V3 r = x - xyz(pe);
+  float u = dot(xyz(u4), r) / u4.w;
+  float v = dot(xyz(v4), r) / v4.w;
+  float r2 = u * u + v * v;
+  a_out = powf(1.0f - r2, pe.w);
+  x_out = x;
+}
+
 #if PALE_HALF_NODES
 __device__ __forceinline__ float2 half_pair(uint32_t v) {
   return __half22float2(*reinterpret_cast<const __half2*>(&v));
@@ -220,12 +237,12 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
         float th, aa;
         V3 xx;
         ctr.tests++;
+        // only the distance and the surfel stay live in the walk; the hit
+        // point and alpha of the closest are evaluated after it
         if (surfel_hit(S.sf, f0 + j, o, d, tmin, best, th, xx, aa)) {
           best = th;
           hit = true;
           prim = f0 + j;
-          x = xx;
-          alpha = aa;
         }
       }
     }
@@ -259,7 +276,10 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
     }
     if (!found) break;
   }
-  if (hit) t = best;
+  if (hit) {
+    t = best;
+    surfel_eval(S.sf, prim, o, d, best, x, alpha);
+  }
   return hit;
 }
 
