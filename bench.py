@@ -129,6 +129,10 @@ class ClockSampler:
 # pending state; a gradient event is a 64 B record, its lookup and an 8 B
 # atomic read-modify-write.
 ROWS_PER_QUERY = 25
+FWD_COUNTERS = ("photon_segments", "photons_stored", "gather_segments", "gather_node_visits", "gather_surfel_tests",
+                "gather_queries", "gather_photons_scanned")
+ADJ_COUNTERS = ("adjoint_segments", "node_visits", "surfel_tests", "gradient_events", "gather_queries",
+                "photons_scanned")
 
 
 def kernel_bytes(sf: dict, sb: dict) -> dict:
@@ -419,6 +423,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "clocks": clk,
         "breakdown_ms": {"photon": round(sf["photon_ms"], 3), "gather": round(sf["gather_ms"], 3),
                          "adjoint": round(sb["backward_ms"], 3)},
+        # work of one step on this rank (device counters): the units behind
+        # the algorithmic bytes of each kernel
+        "counters": {"forward": {k: int(sf[k]) for k in FWD_COUNTERS},
+                     "adjoint": {k: int(sb[k]) for k in ADJ_COUNTERS}},
         **extra,
     }
     print(json.dumps(line), flush=True)

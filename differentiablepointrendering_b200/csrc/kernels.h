@@ -228,6 +228,12 @@ constexpr int kRoundMinBlocks = PALE_ROUND_MIN_BLOCKS;
 #define PALE_LOOKUP_MIN_BLOCKS 4
 #endif
 constexpr int kLookupMinBlocks = PALE_LOOKUP_MIN_BLOCKS;
+// The adjoint transport kernel: its event record and gradient terms spill
+// at 64 registers.
+#ifndef PALE_TRANSPORT_MIN_BLOCKS
+#define PALE_TRANSPORT_MIN_BLOCKS 3
+#endif
+constexpr int kTransportMinBlocks = PALE_TRANSPORT_MIN_BLOCKS;
 
 // Per-camera L2 loss 0.5 mean((ldr - target)^2) over the RGB values of
 // each camera of a finished frame (needs a.ldr and a.target), summed in

@@ -563,17 +563,18 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArg
     const uint32_t kind = word >> 30, idx = word & kRecIndexMask;
     if (kind == kRecNone) continue;
     uint32_t cnt = 0;
-    const V3 E = gather_irradiance_warp(S.grid, GC, xyz(ra), xyz(rb), terms, cnt);
+    // the surfel's albedo or the mesh material, loaded before the lookup
+    // so that its latency overlaps it
+    const V3 E = gather_irradiance_warp<false>(S.grid, GC, xyz(ra), xyz(rb), terms, cnt);
     if (lane == 0) {
+      const float4 refl = kind == kRecSurfel ? __ldg(&S.sf.alb[idx]) : __ldg(&S.mesh.materials[idx]);
       ++queries;
       scanned += cnt;
       V3 Lo;
       if (kind == kRecSurfel) {
-        const float4 al = __ldg(&S.sf.alb[idx]);
-        Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
+        Lo = mul(E, scale(scale(xyz(refl), refl.w), kInvPi));
       } else {
-        const float4 mat = __ldg(&S.mesh.materials[idx]);
-        Lo = mul(scale(xyz(mat), kInvPi), E);
+        Lo = mul(scale(xyz(refl), kInvPi), E);
       }
       const V3 c = scale(Lo, ra.w);
       A.qrec[2 * (size_t)i] = make_float4(c.x, c.y, c.z, 0.f);
@@ -1046,7 +1047,7 @@ __device__ __forceinline__ AlphaGrad alpha_grad(const SurfelView& S, uint32_t k,
 // gradient event (warps stride over the event list): the warp does the
 // photon lookup of the event's end point together (gather_irradiance_warp)
 // and lane 0 adds the event's opacity-gradient term with one atomicAdd.
-__global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_transport(AdjointArgs A) {
+__global__ void __launch_bounds__(kBlock, kTransportMinBlocks) k_transport(AdjointArgs A) {
   __shared__ float4 s_terms[kBlock];
   const uint32_t count = A.st->event_count;
   const SceneView& S = A.scene;
@@ -1077,7 +1078,7 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_transport(AdjointA
     const bool need = kind == kKindProjection || kind == kKindReflect || (kind == kKindNull && ev.d.z != kInvalid);
     V3 E = v3(0.f, 0.f, 0.f);
     uint32_t cnt = 0;
-    if (need) E = gather_irradiance_warp(S.grid, GC, xyz(ev.a), xyz(ev.b), terms, cnt);
+    if (need) E = gather_irradiance_warp<true>(S.grid, GC, xyz(ev.a), xyz(ev.b), terms, cnt);
     if (lane == 0) {
       ++events;
       if (need) {
@@ -1278,7 +1279,7 @@ __global__ void k_gather_points(SceneView S, uint32_t n, const float* __restrict
     const V3 qv = v3(__shfl_sync(0xffffffffu, nv.x, src), __shfl_sync(0xffffffffu, nv.y, src),
                      __shfl_sync(0xffffffffu, nv.z, src));
     uint32_t cnt = 0;
-    const V3 r = gather_irradiance_warp(S.grid, GC, qx, qv, s_terms + (threadIdx.x & ~31u), cnt);
+    const V3 r = gather_irradiance_warp<false>(S.grid, GC, qx, qv, s_terms + (threadIdx.x & ~31u), cnt);
     if (lane == src) e = r;
   }
   if (!in) return;

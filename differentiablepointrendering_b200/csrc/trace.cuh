@@ -663,6 +663,10 @@ __device__ __forceinline__ GatherConst gather_const(const GridView& G) {
   return c;
 }
 
+// kPipelined: each round's photon records are loaded one round ahead (the
+// adjoint's lookups, which wait on L2 more than they issue); camera
+// lookups, most of which end after one or two rounds, load them in place.
+template <bool kPipelined>
 __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const GatherConst& GC, V3 x, V3 n,
                                                      float4* terms, uint32_t& count) {
   const int lane = threadIdx.x & 31;
@@ -760,7 +764,9 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const Ga
     const uint32_t cj0 = lane < nne ? cw[lane] : 0u;
     const uint32_t cex = lane < nne ? cw[32 + lane] : 0xFFFFFFFFu;
     __syncwarp();
-    for (uint32_t base = 0; base < seq; base += 32) {
+    // The photon of sequence index base + lane: its three records at once
+    // (one memory round trip per round).
+    auto fetch = [&](uint32_t base, float4& pa, float4& pb, float& pc) {
       const uint32_t v = base + lane;
       // row holding sequence index v: the non-empty rows starting at or
       // before v are those starting before this round plus those starting
@@ -771,14 +777,28 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const Ga
       const int ord = (int)before + __popc(smask & (0xFFFFFFFFu >> (31 - lane))) - 1;
       const uint32_t rj0 = __shfl_sync(0xffffffffu, cj0, ord & 31);
       const uint32_t rex = __shfl_sync(0xffffffffu, cex, ord & 31);
+      if (v < seq) {
+        const uint32_t j = rj0 + (v - rex);
+        pa = __ldg(&G.pa[j]);
+        pb = __ldg(&G.pb[j]);
+        pc = __ldg(&G.pc[j]);
+      }
+    };
+    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+    float pc = 0.f;
+    if (kPipelined && seq > 0) fetch(0, pa, pb, pc);
+    for (uint32_t base = 0; base < seq; base += 32) {
+      float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
+      float nc = 0.f;
+      if (kPipelined) {
+        if (base + 32 < seq) fetch(base + 32, na, nb, nc);
+      } else {
+        fetch(base, pa, pb, pc);
+      }
+      const uint32_t v = base + lane;
       float tx = 0.f, ty = 0.f, tz = 0.f;
       bool in = false;
       if (v < seq) {
-        // all three records at once: one memory round trip per round
-        const uint32_t j = rj0 + (v - rex);
-        const float4 pa = __ldg(&G.pa[j]);
-        const float4 pb = __ldg(&G.pb[j]);
-        const float pc = __ldg(&G.pc[j]);
         const float dx = pa.x - x.x, dy = pa.y - x.y, dz = pa.z - x.z;
         const float d2 = dx * dx + dy * dy + dz * dz;
         if (d2 <= r2) {
@@ -817,6 +837,9 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const Ga
         }
       }
       __syncwarp();
+      pa = na;
+      pb = nb;
+      pc = nc;
     }
   }
   count += scanned;
