@@ -141,6 +141,8 @@ struct pale_handle {
   DBuf<float4> pend_a, pend_b;
   DBuf<uint4> pend_c;
   DBuf<EventRec> ev_stage, ev_list;
+  DBuf<float4> adj_hits;   // hit record per adjoint queue slot (2 float4)
+  DBuf<float4> adj_walkq;  // walk record per sorted position (2 float4)
   // adjoint batches
   uint32_t adj_cap = 0;
   DBuf<uint32_t> adj_keys, adj_perm, adj_keys_tmp, adj_perm_tmp, adj_sort_temp;   // ray order of a bounce
@@ -567,6 +569,8 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
   h->pend_a.alloc(qa); h->pend_b.alloc(qa); h->pend_c.alloc(qa);
   h->ev_stage.alloc(qa); h->ev_list.alloc(qa);
+  h->adj_hits.alloc(2 * qa);
+  h->adj_walkq.alloc(2 * qa);
   h->job_count.alloc(2 * kMaxJobsPerBatch);
   h->job_start.alloc(2 * kMaxJobsPerBatch);
   // camera paths in flight: every pass of every pixel when that fits in
@@ -857,6 +861,8 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.perm_tmp = h->adj_perm_tmp.p;
   A.sort_temp = h->adj_sort_temp.p;
   A.sort_capacity = h->adj_cap;
+  A.hits = h->adj_hits.p;
+  A.walkq = h->adj_walkq.p;
   // jobs in the reference's order (camera-major, then pass), packed into
   // batches of at most adj_cap paths and kMaxJobsPerBatch jobs
   std::vector<CameraRec> sel(nsel);

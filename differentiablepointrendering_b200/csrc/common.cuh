@@ -230,7 +230,7 @@ struct RunState {
   uint32_t photon_base;     // attempts before the current bounce
   uint32_t event_count;     // events of the current bounce
   uint32_t error;
-  uint32_t pad;
+  uint32_t walk_next;       // next ray of a persistent walk (sorted position)
   unsigned long long photon_segments;
   unsigned long long gather_segments;
   unsigned long long adjoint_segments;

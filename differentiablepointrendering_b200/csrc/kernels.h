@@ -228,6 +228,16 @@ constexpr int kRoundMinBlocks = PALE_ROUND_MIN_BLOCKS;
 #define PALE_LOOKUP_MIN_BLOCKS 4
 #endif
 constexpr int kLookupMinBlocks = PALE_LOOKUP_MIN_BLOCKS;
+// The adjoint's persistent surfel walk: lanes whose walk has ended take a
+// new ray every PALE_REFILL_STEPS node visits.
+#ifndef PALE_REFILL_STEPS
+#define PALE_REFILL_STEPS 16
+#endif
+constexpr int kRefillSteps = PALE_REFILL_STEPS;
+#ifndef PALE_WALK_MIN_BLOCKS
+#define PALE_WALK_MIN_BLOCKS 4
+#endif
+constexpr int kWalkMinBlocks = PALE_WALK_MIN_BLOCKS;
 // The adjoint transport kernel: its event record and gradient terms spill
 // at 64 registers.
 #ifndef PALE_TRANSPORT_MIN_BLOCKS
@@ -302,6 +312,14 @@ struct AdjointArgs {
   uint32_t* perm_tmp;
   uint32_t* sort_temp;     // radix_temp_words(queue capacity)
   uint32_t sort_capacity;
+  // Per sorted position t (the order the bounce traces its rays in): the
+  // closest mesh hit (2 float4: position and distance, +inf on a miss;
+  // alpha, instance bits, primitive bits), and the surfel walk's record
+  // (2 float4): (origin, walk limit or -1 when the ray does not enter the
+  // surfel cloud's box) (unit direction), whose second float4 the walk
+  // overwrites with its result (surfel bits, distance, 1 on a hit).
+  float4* hits;
+  float4* walkq;
 };
 
 void photon_emit(const PhotonArgs& a, cudaStream_t s);

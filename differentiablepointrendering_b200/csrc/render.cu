@@ -848,25 +848,127 @@ __global__ void k_adj_tile_counts(AdjointArgs A, uint32_t parity) {
   if (threadIdx.x == 0) A.qb.tile_counts[blockIdx.x] = make_uint2(ca, ce);
 }
 
-// launchAdjointIntersectKernel (AdjointKernels.cpp:87-386).
+// intersectScene of the adjoint bounce (AdjointKernels.cpp:87-386 traces
+// with it) in three steps: k_adj_mesh, k_adj_walk, and k_adj_bounce reading
+// their records.  Step 1: the mesh pass of every ray, one thread per ray in
+// the order of the bounce: the closest mesh hit, and the surfel walk's
+// record with its limit (the mesh distance plus intersect_scene's margin)
+// when the ray enters the surfel cloud's box before the mesh hit.
+__global__ void k_adj_mesh(AdjointArgs A, uint32_t parity, int sorted) {
+  const uint32_t n_in = A.st->active[parity];
+  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
+  if (t == 0) A.st->walk_next = 0u;
+  if (t >= n_in) return;
+  const uint32_t slot = sorted ? A.perm[t] : t;
+  const SceneView& S = A.scene;
+  const V3 o = xyz(A.qb.q[parity][slot].o), d = xyz(A.qb.q[parity][slot].d);
+  const V3 invw = safe_inv(d);
+  float best;
+  const Hit h = intersect_meshes(S, o, d, invw, best);
+  float limit = -1.0f;
+  if (S.has_pc && S.node_count > 0 &&
+      entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best), best))
+    limit = best < 3.0e38f ? best * 1.00001f + 1e-6f : __int_as_float(0x7f800000);
+  A.hits[2 * (size_t)t] = make_float4(h.pos.x, h.pos.y, h.pos.z, best);
+  A.hits[2 * (size_t)t + 1] = make_float4(h.alpha, __int_as_float(h.inst), __uint_as_float(h.prim), 0.0f);
+  const V3 dd = normalize(d);
+  A.walkq[2 * (size_t)t] = make_float4(o.x, o.y, o.z, limit);
+  A.walkq[2 * (size_t)t + 1] = make_float4(dd.x, dd.y, dd.z, 0.0f);
+}
+
+// Step 2: the closest-surfel walks (surfel_closest's) of the rays that
+// enter the cloud, on a persistent grid.  Each lane walks one ray at a
+// time; every kRefillSteps node visits the lanes whose walk has ended take
+// the next rays (one atomic per warp on a cursor over the bounce's order,
+// one load of the walk record each), so that a warp's lanes stay busy
+// while walks of very different lengths end.  A walk ends with one store of
+// its closest surfel and distance; the hits do not depend on the schedule.
+__global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs A, uint32_t parity) {
+  extern __shared__ TravNode s_top[];
+  stage_top_nodes(A.scene, s_top);
+  const SceneView& S = A.scene;
+  const uint32_t n_in = A.st->active[parity];
+  const int lane = threadIdx.x & 31;
+  TravStack stk(s_top, S.top_nodes);
+  ClosestWalk w;
+  TraceCounters ctr{0, 0};
+  uint32_t cur = kInvalid;   // sorted position of this lane's ray
+  bool more = true;          // uniform in the warp: the cursor has rays left
+  for (;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, cur == kInvalid);
+    if (need && more) {
+      const int leader = __ffs(need) - 1;
+      uint32_t b0 = 0;
+      if (lane == leader) b0 = atomicAdd(&A.st->walk_next, (uint32_t)__popc(need));
+      b0 = __shfl_sync(0xffffffffu, b0, leader);
+      if ((uint64_t)b0 + __popc(need) >= n_in) more = false;
+      if (cur == kInvalid) {
+        const uint32_t t = b0 + __popc(need & ((1u << lane) - 1u));
+        if (t < n_in) {
+          const float4 wa = A.walkq[2 * (size_t)t], wb = A.walkq[2 * (size_t)t + 1];
+          if (wa.w >= 0.0f) {
+            cur = t;
+            w.init(xyz(wa), xyz(wb), 1e-5f, wa.w);
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, cur != kInvalid)) {
+      if (!more) break;
+      continue;
+    }
+    for (int it = 0; it < kRefillSteps && cur != kInvalid; ++it) {
+      if (w.step(S, s_top, stk, ctr, A.st)) continue;
+      A.walkq[2 * (size_t)cur + 1] = make_float4(__uint_as_float(w.prim), w.best, w.hit ? 1.0f : 0.0f, 0.0f);
+      cur = kInvalid;
+    }
+  }
+  block_count3(&A.st->node_visits, ctr.nodes, &A.st->surfel_tests, ctr.tests, nullptr, 0u);
+}
+
+// Step 3, launchAdjointIntersectKernel (AdjointKernels.cpp:87-386) after
+// its intersection.  The hit is intersect_scene's: the walk's surfel when
+// its world distance is below the mesh hit's, else the mesh hit.
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index,
                                                                         int sorted) {
-  extern __shared__ TravNode s_top[];
   const uint32_t n_in = A.st->active[parity];
   if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
-  stage_top_nodes(A.scene, s_top);
   const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
   const uint32_t slot = (sorted && t < n_in) ? A.perm[t] : t;
   bool alive = false, has_ev = false;
   uint32_t job = kInvalid;
-  TraceCounters ctr{0, 0};
   if (t < n_in) {
     const SceneView& S = A.scene;
     const float4 ro = A.qb.q[parity][slot].o, rd = A.qb.q[parity][slot].d;
-    const V3 o = xyz(ro), d = xyz(rd);
-    Hit h = intersect_scene(S, s_top, o, d, ctr, A.st);
-    // the rest of the ray and its random stream after the walk, so that
-    // they hold no registers during it
+    const V3 d = xyz(rd);
+    Hit h;
+    {
+      const float4 ha = A.hits[2 * (size_t)t], hb = A.hits[2 * (size_t)t + 1];
+      h.pos = xyz(ha);
+      h.inst = __float_as_int(hb.y);
+      h.prim = __float_as_uint(hb.z);
+      h.alpha = hb.x;
+      h.t = h.inst >= 0 ? ha.w : 3.402823466e+38f;
+      const float best = ha.w;
+      if (A.walkq[2 * (size_t)t].w >= 0.0f) {
+        const float4 wr = A.walkq[2 * (size_t)t + 1];
+        if (wr.z != 0.0f) {
+          const V3 o = xyz(ro);
+          const uint32_t prim = __float_as_uint(wr.x);
+          V3 x;
+          float a;
+          surfel_eval(S.sf, prim, o, normalize(d), wr.y, x, a);
+          const float tw = dot(x - o, d);
+          if (tw > 0.0f && tw < best) {
+            h.inst = (int)S.mesh.instances;
+            h.t = tw;
+            h.pos = x;
+            h.prim = prim;
+            h.alpha = a;
+          }
+        }
+      }
+    }
     const float4 rt = A.qb.q[parity][slot].t;
     const uint32_t jb = __float_as_uint(rd.w);
     job = jb >> 8;
@@ -986,8 +1088,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
     if (alive && (threadIdx.x & 31) == __ffs(peers) - 1)
       atomicAdd(&A.job_count[(size_t)(parity ^ 1u) * kMaxJobsPerBatch + job], (uint32_t)__popc(peers));
   }
-  block_count3(&A.st->adjoint_segments, t < n_in ? 1u : 0u, &A.st->node_visits, ctr.nodes, &A.st->surfel_tests,
-               ctr.tests);
+  block_count3(&A.st->adjoint_segments, t < n_in ? 1u : 0u, nullptr, 0u, nullptr, 0u);
 }
 
 // Derivatives of eta * alpha_geom for the hit at x on surfel k along the
@@ -1181,17 +1282,23 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
     radix_sort_pairs(a.sort_keys, a.perm, a.sort_keys_tmp, a.perm_tmp, &a.st->active[parity], npaths, 30,
                      a.sort_temp, s);
   }
+  int dev = 0, sms = 148, per_sm = 1, per_sm_w = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = top_smem(a.scene);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_w, k_adj_walk, kBlock, smem);
+  // the walk's persistent grid: every SM filled once, no more blocks than rays need
+  const uint32_t grid_w = std::min<uint32_t>(nb, (uint32_t)std::max(1, sms * std::max(1, per_sm_w)));
   if (a.timer) a.timer->begin(kTimeAdjBounce, s);
-  k_adj_bounce<<<nb, kBlock, top_smem(a.scene), s>>>(a, parity, bounce, sorted); note_launch();
+  k_adj_mesh<<<nb, kBlock, 0, s>>>(a, parity, sorted); note_launch();
+  k_adj_walk<<<grid_w, kBlock, smem, s>>>(a, parity); note_launch();
+  k_adj_bounce<<<nb, kBlock, 0, s>>>(a, parity, bounce, sorted); note_launch();
   if (a.timer) a.timer->end(s);
   k_adj_tile_counts<<<nb, kBlock, 0, s>>>(a, parity); note_launch();
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
   k_job_scan<<<1, kMaxJobsPerBatch, 0, s>>>(a, parity); note_launch();
   k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev); note_launch();
   // one warp per event: a grid that fills every SM once
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport, kBlock, 0);
   if (a.timer) a.timer->begin(kTimeTransport, s);
   k_transport<<<(uint32_t)std::max(1, sms * std::max(1, per_sm)), kBlock, 0, s>>>(a); note_launch();

@@ -191,29 +191,39 @@ struct TravStack {
   }
 };
 
-// Closest surfel with t in (tmin, limit) along (o, d) (the surfel cloud's
-// transform is the identity, so this is intersectBLASPointCloudFirstHit,
-// IntersectionKernels.h:585-675, where tmin is rayEpsilon = 1e-5).  Returns
-// false on a miss.
-__device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNode* __restrict__ smem_top, V3 o, V3 d,
-                                               float tmin, float limit, uint32_t& prim, float& t, V3& x,
-                                               float& alpha, TraceCounters& ctr, RunState* st) {
-  if (S.node_count == 0) return false;
-  const V3 inv = safe_inv(d);
-  float best = limit;
-  bool hit = false;
-  TravStack stk(smem_top, S.top_nodes);
-  int sp = 0;
-  uint32_t node = 0;
-  // an acyclic tree visits each node at most once
-  const uint32_t visit_cap = 2u * S.node_count + 64u;
-  for (uint32_t visit = 0;; ++visit) {
-    float4 a, b, c;
-    uint4 w;
+// The closest-hit walk over the surfel LBVH, one node visit per step(), so
+// that a persistent kernel can hand a lane a new ray between steps.  After
+// init(), step() returns true while the walk goes on; `hit`, `prim` and
+// `best` then hold the closest surfel with t in (tmin, limit).
+struct ClosestWalk {
+  V3 o, d, inv;
+  float tmin, best;
+  uint32_t prim, node, visit;
+  int sp;
+  bool hit;
+  __device__ __forceinline__ void init(V3 o_, V3 d_, float tmin_, float limit) {
+    o = o_;
+    d = d_;
+    inv = safe_inv(d_);
+    tmin = tmin_;
+    best = limit;
+    prim = 0;
+    node = 0;
+    visit = 0;
+    sp = 0;
+    hit = false;
+  }
+  __device__ __forceinline__ bool step(const SceneView& S, const TravNode* __restrict__ smem_top, TravStack& stk,
+                                       TraceCounters& ctr, RunState* st) {
+    // an acyclic tree visits each node at most once
+    const uint32_t visit_cap = 2u * S.node_count + 64u;
     if (node >= S.node_count || visit > visit_cap) {
       flag_error(st, kErrBounds);
-      break;
+      return false;
     }
+    ++visit;
+    float4 a, b, c;
+    uint4 w;
     load_node(S, smem_top, node, a, b, c, w);
     ctr.nodes++;
     float e0 = w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
@@ -258,11 +268,10 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
         flag_error(st, kErrStackOverflow);
       }
       node = nearN;
-      continue;
+      return true;
     }
-    if (h0) { node = w.x; continue; }
-    if (h1) { node = w.y; continue; }
-    bool found = false;
+    if (h0) { node = w.x; return true; }
+    if (h1) { node = w.y; return true; }
     while (sp > 0) {
       --sp;
       uint32_t sn;
@@ -270,17 +279,32 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
       stk.get(sp, sn, st_t);
       if (st_t <= best) {
         node = sn;
-        found = true;
-        break;
+        return true;
       }
     }
-    if (!found) break;
+    return false;
   }
-  if (hit) {
-    t = best;
-    surfel_eval(S.sf, prim, o, d, best, x, alpha);
+};
+
+// Closest surfel with t in (tmin, limit) along (o, d) (the surfel cloud's
+// transform is the identity, so this is intersectBLASPointCloudFirstHit,
+// IntersectionKernels.h:585-675, where tmin is rayEpsilon = 1e-5).  Returns
+// false on a miss.
+__device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNode* __restrict__ smem_top, V3 o, V3 d,
+                                               float tmin, float limit, uint32_t& prim, float& t, V3& x,
+                                               float& alpha, TraceCounters& ctr, RunState* st) {
+  if (S.node_count == 0) return false;
+  TravStack stk(smem_top, S.top_nodes);
+  ClosestWalk w;
+  w.init(o, d, tmin, limit);
+  while (w.step(S, smem_top, stk, ctr, st)) {
   }
-  return hit;
+  if (w.hit) {
+    prim = w.prim;
+    t = w.best;
+    surfel_eval(S.sf, w.prim, o, d, w.best, x, alpha);
+  }
+  return w.hit;
 }
 
 // The K closest surfels with t in (tmin, limit) along (o, d), in increasing
