@@ -126,8 +126,10 @@ class ClockSampler:
 # 32 B per BVH node visited and 52 B per surfel test; a photon lookup reads
 # 36 B per photon scanned and 8 B (two cell offsets) per grid row of its
 # window (25 rows); the adjoint bounce also reads and writes its 48 B
-# pending state; a gradient event is a 64 B record, its lookup and an 8 B
-# atomic read-modify-write.
+# pending state, and its three kernels (mesh pass, persistent walk,
+# shading) pass 128 B of hit and walk records per ray between them (written
+# 64 B, read 48 + 16 B); a gradient event is a 64 B record, its lookup and
+# an 8 B atomic read-modify-write.
 ROWS_PER_QUERY = 25
 FWD_COUNTERS = ("photon_segments", "photons_stored", "gather_segments", "gather_node_visits", "gather_surfel_tests",
                 "gather_queries", "gather_photons_scanned")
@@ -144,7 +146,7 @@ def kernel_bytes(sf: dict, sb: dict) -> dict:
         "k_cg_round": seg(sf["gather_segments"], sf["gather_node_visits"], sf["gather_surfel_tests"]),
         "k_cg_lookup": look(fwd_q, sf["gather_photons_scanned"]),
         "k_adj_bounce": seg(sb["adjoint_segments"], sb["node_visits"], sb["surfel_tests"])
-        + 96.0 * sb["adjoint_segments"],
+        + (96.0 + 128.0) * sb["adjoint_segments"],
         "k_transport": 72.0 * sb["gradient_events"] + look(adj_q, sb["photons_scanned"]),
     }
 
