@@ -155,6 +155,8 @@ struct pale_handle {
   DBuf<RayRec> cg_paths, cg_paths2;
   DBuf<float4> cg_qrec, cg_info_b;
   DBuf<uint4> cg_info_a;
+  DBuf<float4> cg_mhit, cg_walk;   // per round entry: mesh hit, walk record
+  DBuf<uint32_t> cg_khit;          // per round entry: K-hit walk result
   DBuf<uint32_t> cg_counts;
   DBuf<float4> cg_res, cg_fb;
   // run state, seeds, images, gradients
@@ -582,6 +584,8 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->cg_paths.alloc(h->path_cap); h->cg_paths2.alloc(h->path_cap);
   h->cg_qrec.alloc(2 * (size_t)kGatherHits * h->path_cap); h->cg_res.alloc(h->path_cap);
   h->cg_info_a.alloc(h->path_cap); h->cg_info_b.alloc(h->path_cap);
+  h->cg_mhit.alloc(h->path_cap); h->cg_walk.alloc(2 * (size_t)h->path_cap);
+  h->cg_khit.alloc((size_t)kKHitWords * h->path_cap);
   h->cg_fb.alloc(std::max<uint64_t>(all_pix, 1));
   h->cg_counts.alloc(2 * (kMaxLayers + 2));
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
@@ -778,6 +782,9 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.qrec = h->cg_qrec.p;
   F.info_a = h->cg_info_a.p;
   F.info_b = h->cg_info_b.p;
+  F.mhit = h->cg_mhit.p;
+  F.walk = h->cg_walk.p;
+  F.khit = h->cg_khit.p;
   F.counts = h->cg_counts.p;
   F.res = h->cg_res.p;
   F.fb = h->cg_fb.p;

@@ -190,6 +190,14 @@ struct FrameArgs {
   float4* res;
   float4* fb;
   uint32_t path_capacity;  // >= total_pixels
+  // per queue entry of a round: the closest mesh hit (position, instance
+  // bits), the surfel walk's record (origin, limit or -1 when the path does
+  // not enter the surfel cloud's box) (unit direction), and the walk's
+  // result: the hit count and the surfels of the K closest hits
+  // (kKHitWords words)
+  float4* mhit;
+  float4* walk;
+  uint32_t* khit;
   KernelTimer* timer;      // host side, may be null
   // optional L2 image loss: target packed like the images with
   // target_channels floats per pixel; dL/dI (float4 per pixel) written by
@@ -211,6 +219,8 @@ constexpr uint32_t kTopNodes = PALE_TOP_NODES;
 #define PALE_GATHER_HITS 8
 #endif
 constexpr int kGatherHits = PALE_GATHER_HITS;
+// Words of a K-hit walk result: the count and K surfels, padded to uint4s.
+constexpr int kKHitWords = (kGatherHits + 4) / 4 * 4;
 // Resident blocks per SM the traversal kernels are compiled for (their
 // register budget: 65536 / (kBlock * blocks)).
 #ifndef PALE_TRACE_MIN_BLOCKS

@@ -397,42 +397,135 @@ __device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float 
 }
 
 // Round step 1: one lane per queue entry (a live path).
+// Round step 1a: the mesh pass of every queue entry (one thread per entry):
+// its closest mesh hit and its surfel walk's record, whose limit is the
+// mesh distance plus intersect_scene's margin.
+__global__ void k_cg_mesh(FrameArgs A, uint32_t round) {
+  const SceneView& S = A.scene;
+  const uint32_t n = A.counts[round];
+  if (blockIdx.x == 0 && threadIdx.x == 0) A.st->walk_next = 0u;
+  const RayRec* __restrict__ in = A.paths[round & 1];
+  for (uint32_t slot = blockIdx.x * kBlock + threadIdx.x; slot < n; slot += gridDim.x * kBlock) {
+    const V3 o = xyz(in[slot].o), d = xyz(in[slot].d);
+    const V3 invw = safe_inv(d);
+    float best_m;
+    const Hit hm = intersect_meshes(S, o, d, invw, best_m);
+    float limit = -1.0f;
+    if (S.has_pc && S.node_count > 0 &&
+        entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best_m),
+                best_m))
+      limit = best_m < 3.0e38f ? best_m * 1.00001f + 1e-6f : __int_as_float(0x7f800000);
+    A.mhit[slot] = make_float4(hm.pos.x, hm.pos.y, hm.pos.z, __int_as_float(hm.inst));
+    const V3 dd = normalize(d);
+    A.walk[2 * (size_t)slot] = make_float4(o.x, o.y, o.z, limit);
+    A.walk[2 * (size_t)slot + 1] = make_float4(dd.x, dd.y, dd.z, 0.0f);
+  }
+}
+
+// Round step 1b: the K-closest-surfel walks, on a persistent grid whose
+// lanes take the next queue entries every kRefillSteps node visits once
+// their walk has ended (as k_adj_walk does for the adjoint's closest hits).
+// A walk ends with one store of its hit count and surfels.
 template <int K>
-__global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_round(FrameArgs A, uint32_t round) {
+__global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_walk(FrameArgs A, uint32_t round) {
   extern __shared__ TravNode s_top[];
   stage_top_nodes(A.scene, s_top);
+  const SceneView& S = A.scene;
+  const uint32_t n = A.counts[round];
+  const int lane = threadIdx.x & 31;
+  TravStack stk(s_top, S.top_nodes);
+  KHitWalk<K> w;
+  TraceCounters ctr{0, 0};
+  uint32_t cur = kInvalid;   // queue entry of this lane's walk
+  bool more = true;          // uniform in the warp: the cursor has entries left
+  for (;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, cur == kInvalid);
+    if (need && more) {
+      const int leader = __ffs(need) - 1;
+      uint32_t b0 = 0;
+      if (lane == leader) b0 = atomicAdd(&A.st->walk_next, (uint32_t)__popc(need));
+      b0 = __shfl_sync(0xffffffffu, b0, leader);
+      if ((uint64_t)b0 + __popc(need) >= n) more = false;
+      if (cur == kInvalid) {
+        const uint32_t t = b0 + __popc(need & ((1u << lane) - 1u));
+        if (t < n) {
+          const float4 wa = A.walk[2 * (size_t)t], wb = A.walk[2 * (size_t)t + 1];
+          if (wa.w >= 0.0f) {
+            cur = t;
+            w.init(xyz(wa), xyz(wb), 1e-5f, wa.w);
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, cur != kInvalid)) {
+      if (!more) break;
+      continue;
+    }
+    for (int it = 0; it < kRefillSteps && cur != kInvalid; ++it) {
+      if (w.step(S, s_top, stk, ctr, A.st)) continue;
+      uint32_t rw[kKHitWords];
+      rw[0] = w.count;
+#pragma unroll
+      for (int k = 0; k < K; ++k) rw[1 + k] = w.prim_out[k];
+#pragma unroll
+      for (int k = K + 1; k < kKHitWords; ++k) rw[k] = 0u;
+      uint4* dst = reinterpret_cast<uint4*>(A.khit + (size_t)kKHitWords * cur);
+#pragma unroll
+      for (int q = 0; q < kKHitWords / 4; ++q) dst[q] = make_uint4(rw[4 * q], rw[4 * q + 1], rw[4 * q + 2], rw[4 * q + 3]);
+      cur = kInvalid;
+    }
+  }
+  warp_count(&A.st->node_visits, ctr.nodes);
+  warp_count(&A.st->surfel_tests, ctr.tests);
+  warp_count(&A.st->gather_node_visits, ctr.nodes);
+  warp_count(&A.st->gather_surfel_tests, ctr.tests);
+}
+
+// Round step 1c: the layers of each entry from its walk's hits, re-tested
+// from the chained origin, and the path's end.
+template <int K>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs A, uint32_t round) {
   const SceneView& S = A.scene;
   const uint32_t n = A.counts[round];
   const RayRec* __restrict__ in = A.paths[round & 1];
   RayRec* __restrict__ out = A.paths[(round + 1) & 1];
   const int lane = threadIdx.x & 31;
   const float inf = __int_as_float(0x7f800000);
-  TraceCounters ctr{0, 0};
   uint32_t segs = 0;
   for (uint32_t b = blockIdx.x * kBlock; b < n; b += gridDim.x * kBlock) {
     const uint32_t slot = b + threadIdx.x;
     const bool live = slot < n;
     RayRec rec{};
-    float tl[K];
     uint32_t pl[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) pl[k] = 0;
     uint32_t count = 0, nslots = 0;
     Hit hm{};
+    hm.inst = -1;
     V3 o{}, d{}, invw{}, dd{};
-    float best_m = inf;
     if (live) {
       rec = in[slot];
       o = xyz(rec.o);
       d = xyz(rec.d);
       invw = safe_inv(d);
-      hm = intersect_meshes(S, o, d, invw, best_m);
-      if (S.has_pc &&
-          entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best_m),
-                  best_m)) {
+      const float4 mh = A.mhit[slot];
+      hm.inst = __float_as_int(mh.w);
+      hm.pos = xyz(mh);
+      if (A.walk[2 * (size_t)slot].w >= 0.0f) {
         dd = normalize(d);
-        const float limit = best_m < 3.0e38f ? best_m * 1.00001f + 1e-6f : inf;
-        count = surfel_khit<K>(S, s_top, o, dd, 1e-5f, limit, tl, pl, ctr, A.st);
+        uint32_t rw[kKHitWords];
+        const uint4* src = reinterpret_cast<const uint4*>(A.khit + (size_t)kKHitWords * slot);
+#pragma unroll
+        for (int q = 0; q < kKHitWords / 4; ++q) {
+          const uint4 v = src[q];
+          rw[4 * q] = v.x;
+          rw[4 * q + 1] = v.y;
+          rw[4 * q + 2] = v.z;
+          rw[4 * q + 3] = v.w;
+        }
+        count = rw[0];
+#pragma unroll
+        for (int k = 0; k < K; ++k) pl[k] = rw[1 + k];
       }
       nslots = count + (count < (uint32_t)K ? 1u : 0u);
     }
@@ -532,10 +625,6 @@ __global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_round(FrameArgs 
     }
   }
   warp_count(&A.st->gather_segments, segs);
-  warp_count(&A.st->node_visits, ctr.nodes);
-  warp_count(&A.st->surfel_tests, ctr.tests);
-  warp_count(&A.st->gather_node_visits, ctr.nodes);
-  warp_count(&A.st->gather_surfel_tests, ctr.tests);
 }
 
 // Round step 2: one warp per lookup record (warps stride over the records,
@@ -698,13 +787,15 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
   }
   const uint32_t ppc = std::max<uint32_t>(1u, std::min(a.gather_passes, a.path_capacity / a.total_pixels));
   // persistent grids: every SM filled once
-  int dev = 0, sms = 148, per_sm_t = 1, per_sm_l = 1;
+  int dev = 0, sms = 148, per_sm_t = 1, per_sm_l = 1, per_sm_r = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = top_smem(a.scene);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_cg_round<kGatherHits>, kBlock, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_cg_walk<kGatherHits>, kBlock, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_cg_round<kGatherHits>, kBlock, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup, kBlock, 0);
   const uint32_t grid_t = (uint32_t)std::max(1, sms * std::max(1, per_sm_t));
+  const uint32_t grid_r = (uint32_t)std::max(1, sms * std::max(1, per_sm_r));
   const uint32_t grid_l = (uint32_t)std::max(1, sms * std::max(1, per_sm_l));
   for (uint32_t p0 = 0; p0 < a.gather_passes; p0 += ppc) {
     const uint32_t p1 = std::min(a.gather_passes, p0 + ppc);
@@ -717,7 +808,9 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
     while (round < (uint32_t)kMaxLayers && live) {
       for (uint32_t group = 0; group < 16 && round < (uint32_t)kMaxLayers; ++group, ++round) {
         if (a.timer) a.timer->begin(kTimeTrace, s);
-        k_cg_round<kGatherHits><<<grid_t, kBlock, smem, s>>>(a, round); note_launch();
+        k_cg_mesh<<<grid_r, kBlock, 0, s>>>(a, round); note_launch();
+        k_cg_walk<kGatherHits><<<grid_t, kBlock, smem, s>>>(a, round); note_launch();
+        k_cg_round<kGatherHits><<<grid_r, kBlock, 0, s>>>(a, round); note_launch();
         if (a.timer) a.timer->end(s);
         if (a.timer) a.timer->begin(kTimeLookup, s);
         k_cg_lookup<<<grid_l, kBlock, 0, s>>>(a, round); note_launch();

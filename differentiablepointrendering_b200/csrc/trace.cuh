@@ -308,30 +308,44 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
 }
 
 // The K closest surfels with t in (tmin, limit) along (o, d), in increasing
-// t (ties keep the surfel found first): the traversal of surfel_closest
-// with the culling distance of the K-th hit found so far.  Returns the
-// number of hits (<= K); t_out/prim_out hold them in order.
+// t (ties keep the surfel found first): the traversal of ClosestWalk with
+// the culling distance of the K-th hit found so far, one node visit per
+// step().  After init(), step() returns true while the walk goes on;
+// `count` (<= K) and t_out/prim_out then hold the hits in order.
 template <int K>
-__device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNode* __restrict__ smem_top, V3 o, V3 d,
-                                                float tmin, float limit, float (&t_out)[K], uint32_t (&prim_out)[K],
-                                                TraceCounters& ctr, RunState* st) {
-  if (S.node_count == 0) return 0;
-  const V3 inv = safe_inv(d);
-  uint32_t count = 0;
+struct KHitWalk {
+  V3 o, d, inv;
+  float tmin, best;   // best: t_out[K - 1] once K hits are held
+  uint32_t node, visit, count;
+  int sp;
+  float t_out[K];
+  uint32_t prim_out[K];
+  __device__ __forceinline__ void init(V3 o_, V3 d_, float tmin_, float limit) {
+    o = o_;
+    d = d_;
+    inv = safe_inv(d_);
+    tmin = tmin_;
+    best = limit;
+    node = 0;
+    visit = 0;
+    count = 0;
+    sp = 0;
 #pragma unroll
-  for (int k = 0; k < K; ++k) t_out[k] = limit;
-  float best = limit;   // t_out[K - 1] once K hits are held
-  TravStack stk(smem_top, S.top_nodes);
-  int sp = 0;
-  uint32_t node = 0;
-  const uint32_t visit_cap = 2u * S.node_count + 64u;
-  for (uint32_t visit = 0;; ++visit) {
-    float4 a, b, c;
-    uint4 w;
+    for (int k = 0; k < K; ++k) {
+      t_out[k] = limit;
+      prim_out[k] = 0;
+    }
+  }
+  __device__ __forceinline__ bool step(const SceneView& S, const TravNode* __restrict__ smem_top, TravStack& stk,
+                                       TraceCounters& ctr, RunState* st) {
+    const uint32_t visit_cap = 2u * S.node_count + 64u;
     if (node >= S.node_count || visit > visit_cap) {
       flag_error(st, kErrBounds);
-      break;
+      return false;
     }
+    ++visit;
+    float4 a, b, c;
+    uint4 w;
     load_node(S, smem_top, node, a, b, c, w);
     ctr.nodes++;
     float e0 = w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
@@ -385,11 +399,10 @@ __device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNo
         flag_error(st, kErrStackOverflow);
       }
       node = nearN;
-      continue;
+      return true;
     }
-    if (h0) { node = w.x; continue; }
-    if (h1) { node = w.y; continue; }
-    bool found = false;
+    if (h0) { node = w.x; return true; }
+    if (h1) { node = w.y; return true; }
     while (sp > 0) {
       --sp;
       uint32_t sn;
@@ -397,14 +410,12 @@ __device__ __forceinline__ uint32_t surfel_khit(const SceneView& S, const TravNo
       stk.get(sp, sn, st_t);
       if (st_t <= best) {
         node = sn;
-        found = true;
-        break;
+        return true;
       }
     }
-    if (!found) break;
+    return false;
   }
-  return count;
-}
+};
 
 // A 4x4 instance matrix (16 floats, 64 B aligned) in four 16-byte loads.
 __device__ __forceinline__ void load_matrix(const float* M, float (&m)[16]) {
