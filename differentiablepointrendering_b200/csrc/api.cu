@@ -141,7 +141,7 @@ struct pale_handle {
   DBuf<float4> pend_a, pend_b;
   DBuf<uint4> pend_c;
   DBuf<EventRec> ev_stage, ev_list;
-  DBuf<float4> adj_hits;   // hit record per adjoint queue slot (2 float4)
+  DBuf<float4> adj_hits;   // hit record per adjoint queue slot (3 float4)
   DBuf<float4> adj_walkq;  // walk record per sorted position (2 float4)
   // adjoint batches
   uint32_t adj_cap = 0;
@@ -571,7 +571,7 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
   h->pend_a.alloc(qa); h->pend_b.alloc(qa); h->pend_c.alloc(qa);
   h->ev_stage.alloc(qa); h->ev_list.alloc(qa);
-  h->adj_hits.alloc(2 * qa);
+  h->adj_hits.alloc(3 * qa);
   h->adj_walkq.alloc(2 * qa);
   h->job_count.alloc(2 * kMaxJobsPerBatch);
   h->job_start.alloc(2 * kMaxJobsPerBatch);

@@ -322,12 +322,13 @@ struct AdjointArgs {
   uint32_t* perm_tmp;
   uint32_t* sort_temp;     // radix_temp_words(queue capacity)
   uint32_t sort_capacity;
-  // Per sorted position t (the order the bounce traces its rays in): the
-  // closest mesh hit (2 float4: position and distance, +inf on a miss;
-  // alpha, instance bits, primitive bits), and the surfel walk's record
-  // (2 float4): (origin, walk limit or -1 when the ray does not enter the
-  // surfel cloud's box) (unit direction), whose second float4 the walk
-  // overwrites with its result (surfel bits, distance, 1 on a hit).
+  // Per queue slot, 3 float4: the closest mesh hit (position and distance,
+  // +inf on a miss; alpha, instance bits, primitive bits) and the surfel
+  // walk's result (surfel bits, distance, 1 on a hit), which the mesh pass
+  // sets to no hit.  Per sorted position t (the order the walk takes the
+  // rays in), the walk's record, 2 float4: (origin, walk limit or -1 when
+  // the ray does not enter the surfel cloud's box) (unit direction, slot
+  // bits).
   float4* hits;
   float4* walkq;
 };

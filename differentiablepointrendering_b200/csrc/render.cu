@@ -962,11 +962,12 @@ __global__ void k_adj_mesh(AdjointArgs A, uint32_t parity, int sorted) {
   if (S.has_pc && S.node_count > 0 &&
       entered(slab_entry(o, invw, S.pc_lo.x, S.pc_lo.y, S.pc_lo.z, S.pc_hi.x, S.pc_hi.y, S.pc_hi.z, best), best))
     limit = best < 3.0e38f ? best * 1.00001f + 1e-6f : __int_as_float(0x7f800000);
-  A.hits[2 * (size_t)t] = make_float4(h.pos.x, h.pos.y, h.pos.z, best);
-  A.hits[2 * (size_t)t + 1] = make_float4(h.alpha, __int_as_float(h.inst), __uint_as_float(h.prim), 0.0f);
+  A.hits[3 * (size_t)slot] = make_float4(h.pos.x, h.pos.y, h.pos.z, best);
+  A.hits[3 * (size_t)slot + 1] = make_float4(h.alpha, __int_as_float(h.inst), __uint_as_float(h.prim), 0.0f);
+  A.hits[3 * (size_t)slot + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const V3 dd = normalize(d);
   A.walkq[2 * (size_t)t] = make_float4(o.x, o.y, o.z, limit);
-  A.walkq[2 * (size_t)t + 1] = make_float4(dd.x, dd.y, dd.z, 0.0f);
+  A.walkq[2 * (size_t)t + 1] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(slot));
 }
 
 // Step 2: the closest-surfel walks (surfel_closest's) of the rays that
@@ -974,8 +975,9 @@ __global__ void k_adj_mesh(AdjointArgs A, uint32_t parity, int sorted) {
 // time; every kRefillSteps node visits the lanes whose walk has ended take
 // the next rays (one atomic per warp on a cursor over the bounce's order,
 // one load of the walk record each), so that a warp's lanes stay busy
-// while walks of very different lengths end.  A walk ends with one store of
-// its closest surfel and distance; the hits do not depend on the schedule.
+// while walks of very different lengths end.  A walk that finds a surfel
+// ends with one store of it and its distance in the ray's hit record; the
+// hits do not depend on the schedule.
 __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs A, uint32_t parity) {
   extern __shared__ TravNode s_top[];
   stage_top_nodes(A.scene, s_top);
@@ -985,7 +987,7 @@ __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs
   TravStack stk(s_top, S.top_nodes);
   ClosestWalk w;
   TraceCounters ctr{0, 0};
-  uint32_t cur = kInvalid;   // sorted position of this lane's ray
+  uint32_t cur = kInvalid;   // queue slot of this lane's ray
   bool more = true;          // uniform in the warp: the cursor has rays left
   for (;;) {
     const unsigned need = __ballot_sync(0xffffffffu, cur == kInvalid);
@@ -1000,7 +1002,7 @@ __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs
         if (t < n_in) {
           const float4 wa = A.walkq[2 * (size_t)t], wb = A.walkq[2 * (size_t)t + 1];
           if (wa.w >= 0.0f) {
-            cur = t;
+            cur = __float_as_uint(wb.w);
             w.init(xyz(wa), xyz(wb), 1e-5f, wa.w);
           }
         }
@@ -1012,7 +1014,7 @@ __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs
     }
     for (int it = 0; it < kRefillSteps && cur != kInvalid; ++it) {
       if (w.step(S, s_top, stk, ctr, A.st)) continue;
-      A.walkq[2 * (size_t)cur + 1] = make_float4(__uint_as_float(w.prim), w.best, w.hit ? 1.0f : 0.0f, 0.0f);
+      if (w.hit) A.hits[3 * (size_t)cur + 2] = make_float4(__uint_as_float(w.prim), w.best, 1.0f, 0.0f);
       cur = kInvalid;
     }
   }
@@ -1020,14 +1022,14 @@ __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs
 }
 
 // Step 3, launchAdjointIntersectKernel (AdjointKernels.cpp:87-386) after
-// its intersection.  The hit is intersect_scene's: the walk's surfel when
-// its world distance is below the mesh hit's, else the mesh hit.
-__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index,
-                                                                        int sorted) {
+// its intersection, in slot order (every access coalesced; the sorted
+// order only serves the walks).  The hit is intersect_scene's: the walk's
+// surfel when its world distance is below the mesh hit's, else the mesh hit.
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index) {
   const uint32_t n_in = A.st->active[parity];
   if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
   const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
-  const uint32_t slot = (sorted && t < n_in) ? A.perm[t] : t;
+  const uint32_t slot = t;
   bool alive = false, has_ev = false;
   uint32_t job = kInvalid;
   if (t < n_in) {
@@ -1036,15 +1038,15 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
     const V3 d = xyz(rd);
     Hit h;
     {
-      const float4 ha = A.hits[2 * (size_t)t], hb = A.hits[2 * (size_t)t + 1];
+      const float4 ha = A.hits[3 * (size_t)slot], hb = A.hits[3 * (size_t)slot + 1];
+      const float4 wr = A.hits[3 * (size_t)slot + 2];
       h.pos = xyz(ha);
       h.inst = __float_as_int(hb.y);
       h.prim = __float_as_uint(hb.z);
       h.alpha = hb.x;
       h.t = h.inst >= 0 ? ha.w : 3.402823466e+38f;
       const float best = ha.w;
-      if (A.walkq[2 * (size_t)t].w >= 0.0f) {
-        const float4 wr = A.walkq[2 * (size_t)t + 1];
+      {
         if (wr.z != 0.0f) {
           const V3 o = xyz(ro);
           const uint32_t prim = __float_as_uint(wr.x);
@@ -1385,7 +1387,7 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
   if (a.timer) a.timer->begin(kTimeAdjBounce, s);
   k_adj_mesh<<<nb, kBlock, 0, s>>>(a, parity, sorted); note_launch();
   k_adj_walk<<<grid_w, kBlock, smem, s>>>(a, parity); note_launch();
-  k_adj_bounce<<<nb, kBlock, 0, s>>>(a, parity, bounce, sorted); note_launch();
+  k_adj_bounce<<<nb, kBlock, 0, s>>>(a, parity, bounce); note_launch();
   if (a.timer) a.timer->end(s);
   k_adj_tile_counts<<<nb, kBlock, 0, s>>>(a, parity); note_launch();
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
