@@ -221,14 +221,15 @@ constexpr uint32_t kTopNodes = PALE_TOP_NODES;
 constexpr int kGatherHits = PALE_GATHER_HITS;
 // Words of a K-hit walk result: the count and K surfels, padded to uint4s.
 constexpr int kKHitWords = (kGatherHits + 4) / 4 * 4;
-// Resident blocks per SM the traversal kernels are compiled for (their
-// register budget: 65536 / (kBlock * blocks)).
+// Resident blocks per SM the record kernels around the walks (camera
+// layer records, adjoint shading) are compiled for (their register budget:
+// 65536 / (kBlock * blocks)).
 #ifndef PALE_TRACE_MIN_BLOCKS
 #define PALE_TRACE_MIN_BLOCKS 4
 #endif
 constexpr int kTraceMinBlocks = PALE_TRACE_MIN_BLOCKS;
-// The camera-gather round kernel's own budget (its 8-hit list needs the
-// registers more than it needs the fourth block).
+// The camera gather's 8-hit walk (its hit list needs the registers more
+// than it needs the fourth block).
 #ifndef PALE_ROUND_MIN_BLOCKS
 #define PALE_ROUND_MIN_BLOCKS 3
 #endif
@@ -238,8 +239,9 @@ constexpr int kRoundMinBlocks = PALE_ROUND_MIN_BLOCKS;
 #define PALE_LOOKUP_MIN_BLOCKS 4
 #endif
 constexpr int kLookupMinBlocks = PALE_LOOKUP_MIN_BLOCKS;
-// The adjoint's persistent surfel walk: lanes whose walk has ended take a
-// new ray every PALE_REFILL_STEPS node visits.
+// The persistent walks (adjoint closest hit, camera 8 hits): lanes whose
+// walk has ended take a new ray every PALE_REFILL_STEPS node visits;
+// PALE_WALK_MIN_BLOCKS is the adjoint walk's register budget.
 #ifndef PALE_REFILL_STEPS
 #define PALE_REFILL_STEPS 16
 #endif
