@@ -1028,11 +1028,10 @@ __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointArgs A, uint32_t parity, uint32_t bounce_index) {
   const uint32_t n_in = A.st->active[parity];
   if ((uint64_t)blockIdx.x * kBlock >= n_in) return;
-  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
-  const uint32_t slot = t;
+  const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
   bool alive = false, has_ev = false;
   uint32_t job = kInvalid;
-  if (t < n_in) {
+  if (slot < n_in) {
     const SceneView& S = A.scene;
     const float4 ro = A.qb.q[parity][slot].o, rd = A.qb.q[parity][slot].d;
     const V3 d = xyz(rd);
@@ -1046,21 +1045,19 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
       h.alpha = hb.x;
       h.t = h.inst >= 0 ? ha.w : 3.402823466e+38f;
       const float best = ha.w;
-      {
-        if (wr.z != 0.0f) {
-          const V3 o = xyz(ro);
-          const uint32_t prim = __float_as_uint(wr.x);
-          V3 x;
-          float a;
-          surfel_eval(S.sf, prim, o, normalize(d), wr.y, x, a);
-          const float tw = dot(x - o, d);
-          if (tw > 0.0f && tw < best) {
-            h.inst = (int)S.mesh.instances;
-            h.t = tw;
-            h.pos = x;
-            h.prim = prim;
-            h.alpha = a;
-          }
+      if (wr.z != 0.0f) {
+        const V3 o = xyz(ro);
+        const uint32_t prim = __float_as_uint(wr.x);
+        V3 x;
+        float a;
+        surfel_eval(S.sf, prim, o, normalize(d), wr.y, x, a);
+        const float tw = dot(x - o, d);
+        if (tw > 0.0f && tw < best) {
+          h.inst = (int)S.mesh.instances;
+          h.t = tw;
+          h.pos = x;
+          h.prim = prim;
+          h.alpha = a;
         }
       }
     }
@@ -1183,7 +1180,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
     if (alive && (threadIdx.x & 31) == __ffs(peers) - 1)
       atomicAdd(&A.job_count[(size_t)(parity ^ 1u) * kMaxJobsPerBatch + job], (uint32_t)__popc(peers));
   }
-  block_count3(&A.st->adjoint_segments, t < n_in ? 1u : 0u, nullptr, 0u, nullptr, 0u);
+  block_count3(&A.st->adjoint_segments, slot < n_in ? 1u : 0u, nullptr, 0u, nullptr, 0u);
 }
 
 // Derivatives of eta * alpha_geom for the hit at x on surfel k along the
