@@ -1,7 +1,7 @@
 """One process per GPU: how the views are split and the gradients summed.
 
 The renders of different views are independent given the surfels and the
-photon map (SURVEY: views x passes x pixels shard freely).  Every rank holds
+photon map (views, passes and pixels shard freely).  Every rank holds
 the same surfels, traces the same counter-keyed photons (so the photon maps
 are bit-identical without an exchange) and renders its own views; the only
 exchange is the sum of the per-surfel gradient arrays.
