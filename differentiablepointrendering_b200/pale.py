@@ -30,6 +30,32 @@ def _check(lib, h, rc: int, what: str):
         raise RuntimeError(f"{what} failed ({rc}): {msg}")
 
 
+def _split_rgba(buf: np.ndarray, sizes) -> list:
+    """(H, W, 4) views of consecutive cameras' pixels in one packed float32
+    buffer; `sizes` holds (W, H) per camera."""
+    out, off = [], 0
+    for w, h in sizes:
+        n = w * h * 4
+        out.append(buf[off:off + n].reshape(h, w, 4))
+        off += n
+    return out
+
+
+def _pack_rgba(rgbs) -> tuple:
+    """One packed float32 buffer of (H, W, 3) images with alpha 1 (the
+    layout the C-ABI reads), and its (H, W, 4) view per image; a 4-float
+    zero buffer and no views when there are no images."""
+    n = sum(a.shape[0] * a.shape[1] for a in rgbs) * 4
+    if n == 0:
+        return np.zeros(4, np.float32), []
+    buf = np.empty(n, np.float32)
+    views = _split_rgba(buf, [(a.shape[1], a.shape[0]) for a in rgbs])
+    for v, a in zip(views, rgbs):
+        v[..., :3] = a
+        v[..., 3] = 1.0
+    return buf, views
+
+
 class Renderer:
     """Adjoint photon-mapping renderer for beta surfels on one B200.
 
@@ -150,16 +176,16 @@ class Renderer:
                                                 raw.ctypes.data_as(N.f32p), dldi.ctypes.data_as(N.f32p),
                                                 loss.ctypes.data_as(C.POINTER(C.c_double)))
         _check(self._lib, self._h, rc, "render_forward_loss")
-        images, grads, losses, off = {}, {}, {}, 0
-        for k, i in enumerate(idx):
-            w, h = self._sizes[i]
-            n = w * h * 4
+        # the images are views of this call's buffers (no further copy)
+        sizes = [self._sizes[i] for i in idx]
+        images, grads, losses = {}, {}, {}
+        for k, (i, l4, r4, d4) in enumerate(zip(idx, _split_rgba(ldr, sizes), _split_rgba(raw, sizes),
+                                                _split_rgba(dldi, sizes))):
             name = self._names[i]
-            images[name] = ldr[off:off + n].reshape(h, w, 4).copy()
-            images[name + "_raw"] = raw[off:off + n].reshape(h, w, 4).copy()
-            grads[name] = dldi[off:off + n].reshape(h, w, 4)[..., :3].copy()
+            images[name] = l4
+            images[name + "_raw"] = r4
+            grads[name] = np.ascontiguousarray(d4[..., :3])
             losses[name] = float(loss[k])
-            off += n
         return images, grads, losses
 
     # ---------------------------------------------------------- backward
@@ -181,22 +207,20 @@ class Renderer:
             if w != sw or h != sh:
                 raise RuntimeError(f"render_backward: resolution mismatch for camera '{name}': target image is "
                                    f"{w}x{h}, but sensor is {sw}x{sh}")
-            rgb = np.ascontiguousarray(arr).view(np.float32).reshape(h, w, 3)
-            rgba = np.ones((h, w, 4), np.float32)
-            rgba[..., :3] = rgb
             idx.append(i)
-            imgs.append(rgba)
+            imgs.append(np.ascontiguousarray(arr).view(np.float32).reshape(h, w, 3))
+        # one packed RGBA buffer; the returned adjoint sources are its views
+        dldi, imgs = _pack_rgba(imgs)
         n = self.num_points
         grads = N.PointsHolder(n=n)
         pix = sum(im.size for im in imgs)
-        dldi = np.concatenate([im.reshape(-1) for im in imgs]) if imgs else np.zeros(4, np.float32)
         dbg = np.zeros(max(4, pix), np.float32) if self._settings.debug_images else None
         cams = N.cams_array(idx)
         rc = self._lib.pale_render_backward(self._h, len(idx), cams.ctypes.data_as(N.u32p),
                                             dldi.ctypes.data_as(N.f32p), C.byref(grads.struct),
                                             dbg.ctypes.data_as(N.f32p) if dbg is not None else None)
         _check(self._lib, self._h, rc, "render_backward")
-        g = {k: grads.arrays[k].copy() for k in POINT_FIELDS}
+        g = {k: grads.arrays[k] for k in POINT_FIELDS}   # this call's own arrays
         images = {"adjoint_source": {self._names[i]: im for i, im in zip(idx, imgs)}}
         if self._settings.debug_images:
             dbg_out, off = {}, 0
