@@ -2016,6 +2016,30 @@ int orc_get_photons(orc_scene *s, uint32_t *count, float *pos, float *pw, float 
     }
     return 0;
 }
+_Static_assert(sizeof(point_t) == 19 * 4, "point record");
+_Static_assert(sizeof(node_t) == 10 * 4, "node record");
+_Static_assert(sizeof(light_t) == 8 * 4, "light record");
+
+int orc_export_scene(const orc_scene *s, orc_export *e) {
+    memset(e, 0, sizeof(*e));
+    e->np = s->np; e->points = (const float *)s->pts; e->order = s->order;
+    e->nnodes = s->nnodes; e->nodes = s->nodes;
+    e->nv = s->nv; e->verts = s->verts; e->nt = s->nt; e->tris = s->tris;
+    e->nm = s->nm; e->mranges = s->mranges; e->nmat = s->nmat; e->mats = s->mats;
+    e->ninst = s->ninst; e->inst_mesh = s->inst_mesh; e->inst_mat = s->inst_mat;
+    e->o2w = s->o2w; e->w2o = s->w2o;
+    e->nlights = s->nlights; e->lights = s->lights; e->tri_cdf = s->tri_cdf; e->tri_global = s->tri_global;
+    e->ncam = s->ncam; e->cam_inv_view = s->cam_inv_view; e->cam_forward = s->cam_forward;
+    e->cam_fovy = s->cam_fovy; e->cam_size = s->cam_size; e->cam_names = s->cam_names;
+    e->radius = s->r;
+    e->cell[0] = s->cell.x; e->cell[1] = s->cell.y; e->cell[2] = s->cell.z;
+    e->origin[0] = s->origin.x; e->origin[1] = s->origin.y; e->origin[2] = s->origin.z;
+    for (int a = 0; a < 3; ++a) e->res[a] = s->res[a];
+    e->ncells = s->ncells;
+    e->photon_capacity = s->cap;
+    return s->bvh_kind == 0 ? 0 : 1;
+}
+
 int orc_get_stats(const orc_scene *s, orc_stats *out) {
     *out = s->stats;
     return 0;

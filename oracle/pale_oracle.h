@@ -94,6 +94,33 @@ int orc_get_photons(orc_scene *s, uint32_t *count, float *pos, float *pw, float 
                     uint32_t *cell_id, uint32_t *sorted, float *grid_info);
 int orc_get_stats(const orc_scene *s, orc_stats *out);
 
+/* The built scene as plain arrays, for the harness that runs the
+ * reference's own kernel code on it (oracle/ref_driver.cpp).  Pointers
+ * point into the scene and stay valid until the next rebuild.  Layouts:
+ *   points: 19 floats per surfel in BVH order (position[3], tangent_u[3],
+ *           tangent_v[3], scale[2], albedo[3], alpha_t, alpha_r, opacity,
+ *           beta, shape) after the reference's collection (unit tangents,
+ *           clamped albedo/opacity, alpha_r = 1, alpha_t = 0);
+ *   nodes:  10 words per node of the median-split BVH (lo[3], hi[3] as
+ *           floats; left, right as int32 (-1 for a leaf), first, count as
+ *           uint32; children of a node are consecutive);
+ *   lights: 8 words per light (mesh instance, first CDF entry, triangle
+ *           count as uint32; color[3], power, world area as floats) with
+ *           per-triangle inclusive CDF values and global triangle ids. */
+typedef struct orc_export {
+    uint32_t np; const float *points; const uint32_t *order;
+    uint32_t nnodes; const void *nodes;
+    uint32_t nv; const float *verts; uint32_t nt; const uint32_t *tris;
+    uint32_t nm; const uint32_t *mranges; uint32_t nmat; const float *mats;
+    uint32_t ninst; const uint32_t *inst_mesh, *inst_mat; const float *o2w, *w2o;
+    uint32_t nlights; const void *lights; const float *tri_cdf; const uint32_t *tri_global;
+    uint32_t ncam; const float *cam_inv_view, *cam_forward, *cam_fovy; const uint32_t *cam_size;
+    const char *cam_names;
+    float radius, cell[3], origin[3]; int32_t res[3]; uint32_t ncells;
+    uint64_t photon_capacity;
+} orc_export;
+int orc_export_scene(const orc_scene *s, orc_export *e);
+
 /* LBVH restatement on raw arrays (no scene): positions and per-surfel
  * boxes in BVH-input order -> Morton codes / order by sorted position and
  * 16-word traversal nodes.  Returns the node count. */
