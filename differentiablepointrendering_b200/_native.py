@@ -274,6 +274,7 @@ def load_library() -> C.CDLL:
         "pale_build_lbvh_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                               C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),
+        "pale_lbvh_node_count": (C.c_uint32, [C.c_uint32, C.c_uint32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -290,7 +291,8 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_trace_transmittance", "pale_gather_irradiance", "pale_load_photons", "pale_get_photons", "pale_get_bvh",
             "pale_get_stats", "pale_build_lbvh_noalloc", "pale_get_asset", "pale_optimizer_step",
             "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device",
-            "pale_prune_by_opacity", "pale_densify_long_axis_split", "pale_apply_points_device")
+            "pale_prune_by_opacity", "pale_densify_long_axis_split", "pale_apply_points_device",
+            "pale_lbvh_node_count")
 NOALLOC_MAX_SURFELS = 16384
 
 

@@ -676,7 +676,10 @@ std::mutex g_scratch_mu;
 void* g_scratch_addr[128] = {};
 
 // Device address of g_lbvh_scratch on the current device, looked up once
-// per device (the host-side symbol is not a device address).
+// per device (the host-side symbol is not a device address).  The cached
+// address belongs to the device's primary context: after cudaDeviceReset
+// the module is loaded again and the address must not be reused, so a
+// process that resets a device must not call this entry point afterwards.
 cudaError_t scratch_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -696,6 +699,12 @@ cudaError_t scratch_address(void** out) {
 
 }  // namespace pale
 
+extern "C" uint32_t pale_lbvh_node_count(uint32_t n, uint32_t leaf_size) {
+  const uint32_t leaf = leaf_size < 1 ? 1u : (leaf_size > 8 ? 8u : leaf_size);
+  if (n == 0) return 0;
+  return n <= leaf ? 1u : pale::kTopNodes + n - 1;
+}
+
 extern "C" int pale_build_lbvh_noalloc(const float* d_position, const float* d_tangent_u, const float* d_tangent_v,
                                        const float* d_scale, uint32_t n, uint32_t leaf_size, uint32_t* d_codes,
                                        uint32_t* d_order, float* d_nodes, uint32_t* d_status, void* stream) {
@@ -705,7 +714,14 @@ extern "C" int pale_build_lbvh_noalloc(const float* d_position, const float* d_t
                      std::to_string(kNoAllocMax));
     return PALE_ERR_ARGUMENT;
   }
-  if (n == 0) return PALE_OK;
+  if (n == 0) {
+    // nothing to build; a caller-supplied status word still reads 0
+    if (d_status && cudaMemsetAsync(d_status, 0, 4, (cudaStream_t)stream) != cudaSuccess) {
+      set_thread_error("pale_build_lbvh_noalloc: clearing the status word failed");
+      return PALE_ERR_CUDA;
+    }
+    return PALE_OK;
+  }
   if (!d_position || !d_tangent_u || !d_tangent_v || !d_scale || !d_codes || !d_order || !d_nodes) {
     set_thread_error("pale_build_lbvh_noalloc: null device pointer");
     return PALE_ERR_ARGUMENT;
@@ -749,7 +765,7 @@ extern "C" int pale_build_lbvh_noalloc(const float* d_position, const float* d_t
   PointsDev col{f_col, f_col + 3 * N, f_col + 6 * N, f_col + 9 * N, f_col + 11 * N, f_col + 14 * N, f_col + 15 * N,
                 f_col + 16 * N};
   const uint32_t leaf = leaf_size < 1 ? 1u : (leaf_size > 8 ? 8u : leaf_size);
-  const uint32_t top = 256;
+  const uint32_t top = kTopNodes;   // the same staged top as pale_create's build
   // zero what must start at zero: the error word and the refit counters
   cudaMemsetAsync(err, 0, 4, s);
   cudaMemsetAsync(f_dummy, 0, 12ull * N, s);

@@ -418,6 +418,14 @@ int pale_get_stats(pale_handle *h, pale_stats *stats);
 /* Largest surfel count pale_build_lbvh_noalloc accepts. */
 #define PALE_NOALLOC_MAX_SURFELS 16384u
 
+/* Node count of the LBVH over n surfels with the given leaf size (0 is
+ * taken as 1): 0 for n = 0, 1 when n <= leaf_size, else T + n - 1 with T
+ * the number of top nodes the library stages in shared memory (256 unless
+ * it was built with another -DPALE_TOP_NODES).  The size of the nodes
+ * buffer pale_build_lbvh_noalloc needs, and pale_get_bvh's node_count.
+ * Host only; no counterpart in the reference. */
+uint32_t pale_lbvh_node_count(uint32_t n, uint32_t leaf_size);
+
 /* LBVH build that allocates nothing.  No counterpart in the reference (its
  * BVH is built on the CPU); it serves callers that cannot allocate device
  * memory around the call: code running while a CUDA graph is captured
@@ -428,18 +436,20 @@ int pale_get_stats(pale_handle *h, pale_stats *stats);
  * Inputs (device, asset order, n <= PALE_NOALLOC_MAX_SURFELS): position n*3,
  * tangent_u n*3, tangent_v n*3, scale n*2.  Outputs (device, caller owned):
  * codes[n] and order[n] by sorted position, nodes as 16 floats per node
- * (1 node when n <= leaf_size, else 256 + n - 1), and optionally the
- * error flags in *d_status (0 = ok).  The result equals the LBVH that
- * pale_create / pale_rebuild build (see pale_get_bvh, pale_get_order).
+ * (pale_lbvh_node_count(n, leaf_size) nodes), and optionally the error
+ * flags in *d_status (0 = ok; also cleared to 0 when n = 0).  The result
+ * equals the LBVH that pale_create / pale_rebuild build (see pale_get_bvh,
+ * pale_get_order).
  *
- * Temporaries live in one fixed device array of about 2.6 MB that every
- * GPU loading the library holds until exit.  The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress), so make the
- * first call on each device outside any stream capture.  All calls share
- * the array: calls that overlap on the GPU race.  Work is enqueued on
- * `stream` (a cudaStream_t, NULL = default stream) without synchronising.
- * Returns PALE_ERR_ARGUMENT (with pale_last_error(NULL) text) when n is
- * above the maximum. */
+ * Temporaries live in one fixed device array of 2,731,904 bytes (2.6 MiB)
+ * that every GPU loading the library holds until exit.  The first call on
+ * a device looks up that array's device address (cudaGetSymbolAddress), so
+ * make the first call on each device outside any stream capture; the
+ * address is kept for the life of the process, so do not call this entry
+ * point after cudaDeviceReset.  All calls share the array: calls that
+ * overlap on the GPU race.  Work is enqueued on `stream` (a cudaStream_t,
+ * NULL = default stream) without synchronising.  Returns PALE_ERR_ARGUMENT
+ * (with pale_last_error(NULL) text) when n is above the maximum. */
 int pale_build_lbvh_noalloc(const float *d_position, const float *d_tangent_u,
                             const float *d_tangent_v, const float *d_scale,
                             uint32_t n, uint32_t leaf_size, uint32_t *d_codes,
