@@ -45,20 +45,19 @@ WORKLOADS = {
 }
 
 METRIC = "fwd+adjoint Mrays/s"
+L2_POLICY = "GPU arm: a 256 MB buffer (> 126 MB L2) zeroed between timed steps"
+
+
+def config_for(name: str, w: dict) -> dict:
+    """The bench line's config: the workload and the L2 policy, the same in
+    both arms."""
+    return {"workload": name, **w, "l2": L2_POLICY}
 
 
 def settings_for(w: dict) -> dict:
     return {"photons": w["photons"], "bounces": w["bounces"], "forward_passes": w["forward_passes"],
             "gather_passes": w["spp"], "adjoint_bounces": w["adjoint_bounces"], "adjoint_passes": w["adjoint_spp"],
             "gather_radius": w["radius"], "seed": 42, "rng_mode": "decorrelated"}
-
-
-def sample_settings(w: dict) -> dict:
-    """Bounded CPU sample of a workload: same scene, photon count / 4,
-    one camera at half resolution, one gather and one adjoint pass."""
-    s = settings_for(w)
-    s.update(photons=max(1000, w["photons"] // 4), gather_passes=1, adjoint_passes=1)
-    return s
 
 
 # ---------------------------------------------------------------- clocks
@@ -173,35 +172,70 @@ def read_traffic(kernel: str):
         return None
 
 
-def cpu_sample_run(w: dict, steps: int = 1):
-    """The CPU oracle (the reference's algorithm restated in C, all host
-    threads) on a bounded sample of the workload; returns (Mrays/s, secs,
-    description)."""
+def cpu_reference_run(w: dict, steps: int = 1, warmup: int = 0):
+    """The reference's own kernel code on the host cores, on the workload's
+    configuration: oracle/_ref/libpale_ref.so (the reference's unmodified
+    PrimalKernels.cpp / AdjointKernels.cpp / PostprocessKernel.cpp for the
+    CPU, every host thread) on the same scene, cameras, resolution, photon
+    count, radius and depths.  A step traces the full photon pass and grid,
+    then one gather pass and one adjoint pass of every camera; the
+    reference draws one seed per camera for all of its gather passes and
+    replays its one adjoint seed in every pass (SyclBridge.cpp:145,
+    AdjointKernels.cpp:27, 94), so the other passes of a full step are
+    repeats of these, and the step's time and ray count are the photon part
+    plus passes x the one-pass parts.  Falls back to the C oracle port when
+    the reference's kernels were not built.  Returns (Mrays/s, seconds
+    timed, description, kind, steps)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle_lib import OracleRenderer
-    from differentiablepointrendering_b200.scene import make_box_scene, jitter_target, make_surfels
     import numpy as np
+    from differentiablepointrendering_b200.scene import make_box_scene, make_surfels
+    import ref_lib
 
-    res = max(32, w["res"] // 2)
-    pts = make_surfels(w["n"], 1234)
-    scene = make_box_scene(w["n"], cameras=1, resolution=res, points=pts)
-    st = sample_settings(w)
-    o = OracleRenderer(scene, st)
-    tgt = np.zeros((res, res, 3), np.float32)
-    total_rays, total_t = 0, 0.0
-    for _ in range(steps):
+    threads = os.cpu_count() or 1
+    scene = make_box_scene(w["n"], cameras=w["cams"], resolution=w["res"], points=make_surfels(w["n"], 1234))
+    st = settings_for(w)
+    st.update(gather_passes=1, adjoint_passes=1, rng_mode="reference")
+    if ref_lib.available():
+        kind = "reference"
+        r = ref_lib.ReferenceRenderer(scene, st, threads=threads)
+        gather_segments = r.count_gather_segments()
+    else:
+        from oracle_lib import OracleRenderer
+        kind = "port"
+        r = OracleRenderer(scene, st, threads=threads)
+        gather_segments = None
+    total_rays, total_s = 0.0, 0.0
+    for k in range(warmup + steps):
         t0 = time.perf_counter()
-        img = o.render_forward()
-        s1 = o.stats()
-        raw = img["camera0"][..., :3]
-        o.render_backward({"camera0": ((raw - tgt) / raw.size).astype(np.float32)})
-        s2 = o.stats()
-        total_t += time.perf_counter() - t0
-        total_rays += s1["photon_segments"] + s1["gather_segments"] + s2["adjoint_segments"]
-    o.close()
-    desc = (f"CPU oracle, same {w['n']}-surfel scene, 1 camera at {res}x{res}, {st['photons']} photons, "
-            f"1 gather + 1 adjoint pass, depth {w['bounces']}/{w['adjoint_bounces']}")
-    return total_rays / total_t / 1e6, total_t, desc
+        img = r.render_forward()
+        t1 = time.perf_counter()
+        dl = {c: ((img[c][..., :3] - 0.5) / (3 * img[c][..., 0].size)).astype(np.float32)
+              for c in scene.camera_names}
+        if kind == "reference":
+            r.render_backward_opacity(dl)
+            t2 = time.perf_counter()
+            photon_ms, gather_ms, adjoint_ms = r.times_ms()
+            photon_segments, adjoint_segments = r.segments()
+            step_s = (photon_ms + w["spp"] * gather_ms + w["adjoint_spp"] * adjoint_ms) / 1e3
+            rays = photon_segments + w["spp"] * gather_segments + w["adjoint_spp"] * adjoint_segments
+        else:
+            sf = r.stats()
+            r.render_backward(dl)
+            t2 = time.perf_counter()
+            sb = r.stats()
+            step_s = (sf["photon_ms"] + w["spp"] * sf["gather_ms"] + w["adjoint_spp"] * sb["backward_ms"]) / 1e3
+            rays = sf["photon_segments"] + w["spp"] * sf["gather_segments"] + w["adjoint_spp"] * sb["adjoint_segments"]
+        if k >= warmup:
+            total_rays += rays
+            total_s += step_s
+    r.close()
+    what = "the reference's kernel sources compiled for the CPU" if kind == "reference" else "the C oracle port"
+    desc = (f"{what}, {threads} threads, {w['n']} surfels, {w['cams']} cameras at {w['res']}x{w['res']}, "
+            f"{w['photons']} photons, depth {w['bounces']}/{w['adjoint_bounces']}, radius {w['radius']}: per step "
+            f"the photon pass and grid plus 1 of the {w['spp']} gather and 1 of the {w['adjoint_spp']} adjoint passes "
+            f"of every camera, timed; the full step = photon part + passes x one-pass time (the reference repeats "
+            f"the same seeds in every pass); {steps} timed steps after {warmup} warm-up")
+    return total_rays / total_s / 1e6, total_s, desc, kind, steps
 
 
 # -------------------------------------------------------------- reference
@@ -209,16 +243,15 @@ def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
     w = WORKLOADS[args.workload]
-    cores = os.cpu_count()
-    value, secs, desc = cpu_sample_run(w, steps=max(1, args.steps))
+    steps, warmup = max(1, min(args.steps, 3)), min(args.warmup, 1)
+    value, secs, desc, kind, ran = cpu_reference_run(w, steps=steps, warmup=warmup)
     line = {"metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, **w},
-            "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores, "kind": "port",
+            "steps": ran, "warmup": warmup, "requested_steps": args.steps, "requested_warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_for(args.workload, w),
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": os.cpu_count(), "kind": kind,
                              "sample": desc},
-            "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference needs AdaptiveCpp SYCL, absent here; its algorithm runs as the C oracle port"}
+            "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -403,14 +436,17 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     top = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
     achieved = kernels[top]["achieved_gbs"]
     traffic = read_traffic(top)
-    cpu_val, cpu_secs, cpu_desc = cpu_sample_run(w, steps=1) if not args.skip_cpu else (None, 0, "skipped")
+    if args.skip_cpu:
+        cpu_val, cpu_desc, cpu_kind = None, "skipped", None
+    else:
+        cpu_val, _, cpu_desc, cpu_kind, _ = cpu_reference_run(w, steps=1, warmup=0)
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, **w, "iters_per_s": round(1e3 / ms_per_step, 4),
-                   "rays_per_step_per_gpu": int(rays), "l2": "256 MB buffer zeroed between timed steps",
-                   "parallelism": f"views sharded over {world} GPU(s), gradients all-reduced"},
+        "config": config_for(args.workload, w),
+        "iters_per_s": round(1e3 / ms_per_step, 4), "rays_per_step_per_gpu": int(rays),
+        "parallelism": f"views sharded over {world} GPU(s), gradients all-reduced",
         "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "gpu_launches": launches * args.steps,
@@ -421,7 +457,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "launch_ms": kernels[top]["launch_ms"], "launches_per_step": kernels[top]["launches"]},
         "kernels": kernels,
         "cpu_baseline": {"value": round(cpu_val, 4) if cpu_val else None, "unit": "Mrays/s",
-                         "cores": os.cpu_count(), "kind": "port", "sample": cpu_desc},
+                         "cores": os.cpu_count(), "kind": cpu_kind, "sample": cpu_desc},
         "clocks": clk,
         "breakdown_ms": {"photon": round(sf["photon_ms"], 3), "gather": round(sf["gather_ms"], 3),
                          "adjoint": round(sb["backward_ms"], 3)},

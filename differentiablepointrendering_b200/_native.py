@@ -29,7 +29,8 @@ class PaleSettings(C.Structure):
                 ("q_null", C.c_float), ("q_reflect", C.c_float), ("q_transmit", C.c_float),
                 ("gather_radius", C.c_float), ("leaf_size", C.c_uint32), ("rng_mode", C.c_uint32),
                 ("debug_images", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float),
-                ("null_weight", C.c_uint32), ("gradients", C.c_uint32), ("camera_seeds", C.c_uint32)]
+                ("null_weight", C.c_uint32), ("gradients", C.c_uint32), ("camera_seeds", C.c_uint32),
+                ("gather_batch_paths", C.c_uint32), ("adjoint_batch_paths", C.c_uint32)]
 
 
 class PalePoints(C.Structure):
@@ -119,6 +120,7 @@ SETTINGS_KEYS = {
     "rr_start": "rr_start", "q_null": "q_null", "q_reflect": "q_reflect", "q_transmit": "q_transmit",
     "gather_radius": "gather_radius", "leaf_size": "leaf_size", "debug_images": "debug_images",
     "exposure": "exposure", "gamma": "gamma",
+    "gather_batch_paths": "gather_batch_paths", "adjoint_batch_paths": "adjoint_batch_paths",
 }
 IGNORED_KEYS = ("logging", "depth_distort_weight", "normal_consistency_weight")
 

@@ -561,7 +561,8 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   // adjoint batches: the (camera, pass) jobs of a backward call trace
   // together, up to 2^24 paths (about 5.4 GB of queues and events)
   const uint64_t adj_want = all_pix * std::max<uint32_t>(1u, st.adjoint_passes);
-  h->adj_cap = (uint32_t)std::max<uint64_t>(max_pix, std::min<uint64_t>(adj_want, 1ull << 24));
+  const uint64_t adj_limit = st.adjoint_batch_paths ? st.adjoint_batch_paths : (1ull << 24);
+  h->adj_cap = (uint32_t)std::max<uint64_t>(max_pix, std::min<uint64_t>(adj_want, adj_limit));
   const size_t qa = std::max<size_t>(qc, h->adj_cap);
   h->adj_keys.alloc(h->adj_cap); h->adj_perm.alloc(h->adj_cap);
   h->adj_keys_tmp.alloc(h->adj_cap); h->adj_perm_tmp.alloc(h->adj_cap);
@@ -580,7 +581,8 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   // per-entry state), else chunks of whole passes
   if (all_pix >= (1ull << 31)) throw ArgError("too many camera pixels");
   const uint64_t want = all_pix * std::max<uint32_t>(1u, st.gather_passes);
-  h->path_cap = (uint32_t)std::max<uint64_t>(std::max<uint64_t>(all_pix, 1), std::min<uint64_t>(want, 1ull << 25));
+  const uint64_t cg_limit = st.gather_batch_paths ? st.gather_batch_paths : (1ull << 25);
+  h->path_cap = (uint32_t)std::max<uint64_t>(std::max<uint64_t>(all_pix, 1), std::min<uint64_t>(want, cg_limit));
   h->cg_paths.alloc(h->path_cap); h->cg_paths2.alloc(h->path_cap);
   h->cg_qrec.alloc(2 * (size_t)kGatherHits * h->path_cap); h->cg_res.alloc(h->path_cap);
   h->cg_info_a.alloc(h->path_cap); h->cg_info_b.alloc(h->path_cap);

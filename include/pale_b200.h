@@ -93,6 +93,11 @@ typedef struct pale_settings {
     uint32_t null_weight;          /* PALE_NULL_WEIGHT_*                     */
     uint32_t gradients;            /* PALE_GRADIENTS_*                       */
     uint32_t camera_seeds;         /* PALE_CAMERA_SEEDS_*                    */
+    uint32_t gather_batch_paths;   /* camera paths in flight per gather chunk
+                                      (0 = 2^25; at least every pixel once)  */
+    uint32_t adjoint_batch_paths;  /* adjoint paths per batch of (camera,
+                                      pass) jobs (0 = 2^24; at least the
+                                      largest camera's pixels)               */
 } pale_settings;
 
 /* Per-point parameter block (structure of arrays, float32).

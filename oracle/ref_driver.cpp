@@ -33,6 +33,7 @@
 // range whose untouched pages read as zero, so that entry is a black,
 // non-emissive material: the meaning the C oracle and the CUDA renderer give
 // it.  No reference source is edited.
+#include <omp.h>
 #include <sys/mman.h>
 
 #include <sycl/sycl.hpp>
@@ -117,8 +118,10 @@ struct ref_scene {
   std::vector<float3> gradPosition, gradTanU, gradTanV, gradAlbedo;
   std::vector<float2> gradScale;
   std::vector<float> gradBeta, gradShape;
-  // segment counts of the last call (host-visible queue sizes)
+  // segment counts of the last call (host-visible queue sizes) and the
+  // wall time of its parts
   uint64_t photonSegments = 0, adjointSegments = 0;
+  double photonMs = 0, gatherMs = 0, adjointMs = 0;
 };
 
 namespace {
@@ -493,6 +496,7 @@ RenderPackage make_package(ref_scene* s, SensorSet& ss) {
 // and the grid; with `gather` also the per-camera gather and the
 // post-process.  Returns the seed stream where the camera seeds start.
 std::mt19937_64 photon_mapping(ref_scene* s, RenderPackage& pkg, bool gather) {
+  const double t0 = omp_get_wtime();
   std::mt19937_64 seedGen(pkg.random.seed);
   pkg.queue.fill(pkg.intermediates.map.photonCountDevicePtr, 0u, 1).wait();
   s->photonSegments = 0;
@@ -520,6 +524,9 @@ std::mt19937_64 photon_mapping(ref_scene* s, RenderPackage& pkg, bool gather) {
   pkg.queue.memcpy(&photonMapCount, pkg.intermediates.map.photonCountDevicePtr, sizeof(uint32_t)).wait();
   const uint32_t photonCount = std::min(photonMapCount, pkg.intermediates.map.photonCapacity);
   buildPhotonCellRangesAndOrdering(pkg.queue, pkg.intermediates.map, photonCount);
+  const double t1 = omp_get_wtime();
+  s->photonMs = (t1 - t0) * 1e3;
+  s->gatherMs = 0;
   if (gather) {
     for (size_t cameraIndex = 0; cameraIndex < pkg.numSensors; ++cameraIndex) {
       pkg.random.number = seedGen();
@@ -527,6 +534,7 @@ std::mt19937_64 photon_mapping(ref_scene* s, RenderPackage& pkg, bool gather) {
       pkg.queue.wait();
     }
     launchPostProcessKernel(pkg);
+    s->gatherMs = (omp_get_wtime() - t1) * 1e3;
   }
   return seedGen;
 }
@@ -674,6 +682,7 @@ int ref_render_backward(ref_scene* s, uint32_t nsel, const uint32_t* cams, const
   pkg.gradients.numPoints = n;
 
   // submitAdjointKernel (SyclBridge.cpp:169-294)
+  const double t0 = omp_get_wtime();
   std::mt19937_64 seedGen(pkg.random.seed);
   s->adjointSegments = 0;
   pkg.queue.fill(pkg.intermediates.countPrimary, 0u, 1).wait();
@@ -714,6 +723,7 @@ int ref_render_backward(ref_scene* s, uint32_t nsel, const uint32_t* cams, const
       }
     }
   }
+  s->adjointMs = (omp_get_wtime() - t0) * 1e3;
   if (grad_opacity && n) std::memcpy(grad_opacity, s->gradOpacity.data(), n * sizeof(float));
   return 0;
 }
@@ -740,6 +750,14 @@ int ref_get_photons(const ref_scene* s, uint32_t* count, float* pos, float* powe
 void ref_get_segments(const ref_scene* s, uint64_t* photon, uint64_t* adjoint) {
   if (photon) *photon = s->photonSegments;
   if (adjoint) *adjoint = s->adjointSegments;
+}
+
+// Wall time of the last calls: photon pass + grid, camera gather +
+// post-process (last forward), adjoint pass (last backward).
+void ref_get_times(const ref_scene* s, double* photon_ms, double* gather_ms, double* adjoint_ms) {
+  if (photon_ms) *photon_ms = s->photonMs;
+  if (gather_ms) *gather_ms = s->gatherMs;
+  if (adjoint_ms) *adjoint_ms = s->adjointMs;
 }
 
 }  // extern "C"

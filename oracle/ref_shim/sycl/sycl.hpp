@@ -16,8 +16,8 @@
 //     when sycl_shim_set_threads(n > 1) asked for it (timing only; the
 //     atomic appends then interleave as on a real device).
 //   * parallel_for over an nd_range runs each work group's items as fibers
-//     that yield at item.barrier(), groups one after another on the calling
-//     thread, so group barriers have their SYCL meaning.
+//     that yield at item.barrier(), so group barriers have their SYCL
+//     meaning; groups run one after another on each thread of the team.
 // Device memory is host memory; atomic_ref wraps std::atomic_ref.
 #pragma once
 
@@ -359,6 +359,7 @@ struct nd_range {
 // fiber runtime of the nd_range executor (oracle/ref_shim/sycl_shim.cpp)
 namespace sycl_shim {
 void group_barrier();
+int current_thread();
 void run_nd_range(size_t groups, size_t local, const std::function<void(size_t, size_t)>& body);
 void run_range(size_t n, const std::function<void(size_t)>& body);
 }  // namespace sycl_shim
@@ -381,17 +382,19 @@ struct nd_item {
 
 class handler;
 
-// Work-group local memory.  Groups of one launch run one after another,
-// so one array per accessor serves every group; copies of the accessor
-// (the kernel lambda captures it by value) share it.
+// Work-group local memory: one array per thread of the team (groups run
+// one after another on each thread); copies of the accessor (the kernel
+// lambda captures it by value) share them.
 template <typename T, int D = 1>
 class local_accessor {
  public:
-  local_accessor(range<D> r, handler&) : buf_(std::make_shared<std::vector<T>>(r[0])) {}
-  T& operator[](size_t i) const { return (*buf_)[i]; }
+  local_accessor(range<D> r, handler&)
+      : buf_(std::make_shared<std::vector<std::vector<T>>>(static_cast<size_t>(sycl_shim_threads()),
+                                                           std::vector<T>(r[0]))) {}
+  T& operator[](size_t i) const { return (*buf_)[static_cast<size_t>(sycl_shim::current_thread())][i]; }
 
  private:
-  std::shared_ptr<std::vector<T>> buf_;
+  std::shared_ptr<std::vector<std::vector<T>>> buf_;
 };
 
 class event {

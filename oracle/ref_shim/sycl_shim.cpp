@@ -9,6 +9,9 @@
 // a fiber with its own small stack; the group's fibers run round robin, and
 // a fiber that reaches item.barrier() switches back to the scheduler, so
 // every item of the group reaches the barrier before any item passes it.
+// Groups run one after another on each thread of the team, every thread
+// with its own fibers (one contiguous block of stacks, so that a round over
+// the group stays in cache) and its own work-group local memory.
 // On x86-64 the switch is a few instructions that save the callee-saved
 // registers and the stack pointer; elsewhere it falls back to ucontext.
 #include <sycl/sycl.hpp>
@@ -75,7 +78,7 @@ sycl_shim_switch:
 
 namespace {
 
-constexpr size_t kStackBytes = 64 * 1024;
+constexpr size_t kStackBytes = 16 * 1024;
 
 struct Fiber {
   char* stack = nullptr;
@@ -90,6 +93,7 @@ struct Fiber {
 
 struct Group {
   std::vector<Fiber> fibers;
+  std::vector<char> stacks;
 #if defined(__x86_64__)
   void* sched_sp = nullptr;
 #else
@@ -163,14 +167,19 @@ void group_barrier() {
   to_scheduler();
 }
 
-void run_nd_range(size_t groups, size_t local, const std::function<void(size_t, size_t)>& body) {
+namespace {
+
+void run_groups(size_t first, size_t last, size_t stride, size_t local,
+                const std::function<void(size_t, size_t)>& body) {
   Group g;
   g.body = &body;
   g.fibers.resize(local);
-  for (auto& f : g.fibers) f.stack = static_cast<char*>(std::malloc(kStackBytes));
+  g.stacks.resize(local * kStackBytes + 64);
+  char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(g.stacks.data()) + 63) & ~uintptr_t(63));
+  for (size_t l = 0; l < local; ++l) g.fibers[l].stack = base + l * kStackBytes;
   Group* saved = t_group;
   t_group = &g;
-  for (size_t gi = 0; gi < groups; ++gi) {
+  for (size_t gi = first; gi < last; gi += stride) {
     g.group = gi;
     for (size_t l = 0; l < local; ++l) {
       g.fibers[l].local = l;
@@ -194,7 +203,21 @@ void run_nd_range(size_t groups, size_t local, const std::function<void(size_t, 
     }
   }
   t_group = saved;
-  for (auto& f : g.fibers) std::free(f.stack);
+}
+
+}  // namespace
+
+int current_thread() { return omp_in_parallel() ? omp_get_thread_num() : 0; }
+
+void run_nd_range(size_t groups, size_t local, const std::function<void(size_t, size_t)>& body) {
+  if (g_threads <= 1 || groups < 2) {
+    run_groups(0, groups, 1, local, body);
+    return;
+  }
+  const int team = static_cast<int>(std::min<size_t>(groups, static_cast<size_t>(g_threads)));
+#pragma omp parallel num_threads(team)
+  run_groups(static_cast<size_t>(omp_get_thread_num()), groups, static_cast<size_t>(omp_get_num_threads()), local,
+             body);
 }
 
 }  // namespace sycl_shim

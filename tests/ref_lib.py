@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
             "ref_render_backward": (C.c_int, [P, C.c_uint32, u32p, f32p, f32p]),
             "ref_get_photons": (C.c_int, [P, u32p, f32p, f32p, f32p, u32p, u32p]),
             "ref_get_segments": (None, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+            "ref_get_times": (None, [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -167,3 +168,9 @@ class ReferenceRenderer:
         a, b = C.c_uint64(), C.c_uint64()
         self.L.ref_get_segments(self.h, C.byref(a), C.byref(b))
         return int(a.value), int(b.value)
+
+    def times_ms(self):
+        """(photon pass + grid, camera gather + post-process, adjoint) of the last calls."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self.L.ref_get_times(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return float(a.value), float(b.value), float(c.value)
