@@ -255,6 +255,159 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- batched
+# C4: four box scenes of 50k-500k surfels with cameras on a 16-position ring
+# at 256-1024 pixels; an iteration draws 64 views (scene, ring position,
+# resolution, passes 1/4/16/32) and runs their forward (with the L2 loss)
+# and adjoint.  The batched form renders all 64 views as one camera-gather
+# wavefront and one adjoint wavefront over the four scenes (device.ViewBatch),
+# each scene tracing its photon map once; the plain forms run one view per
+# call (its scene's photon map traced again in every call), and one pass per
+# call as the reference's launch loop does (SyclBridge.cpp:136-146, 181-226).
+C4 = dict(scenes=(50000, 100000, 250000, 500000), ring=16, resolutions=(256, 512, 768, 1024), spp=(1, 4, 16, 32),
+          views=64, photons=1000000, bounces=6, radius=0.01)
+C4_TUNE = dict(leaf_size=(1, 2, 4, 8), walk_block=(256, 128, 64), adjoint_batch_paths=(1 << 22, 1 << 20, 1 << 18))
+
+
+def c4_settings(knobs: dict) -> dict:
+    st = {"photons": C4["photons"], "bounces": C4["bounces"], "forward_passes": 1, "gather_passes": max(C4["spp"]),
+          "adjoint_bounces": C4["bounces"], "adjoint_passes": max(C4["spp"]), "gather_radius": C4["radius"],
+          "seed": 42, "rng_mode": "decorrelated", "camera_seeds": "camera"}
+    st.update(knobs)
+    return st
+
+
+def c4_views(rng, count: int):
+    nres = len(C4["resolutions"])
+    out = []
+    for _ in range(count):
+        sc = int(rng.integers(len(C4["scenes"])))
+        cam = int(rng.integers(C4["ring"])) * nres + int(rng.integers(nres))
+        out.append((sc, cam, int(C4["spp"][int(rng.integers(len(C4["spp"])))]), 0))
+    return out
+
+
+class C4Run:
+    """The four C4 renderers with one set of knobs, and timed iterations."""
+
+    def __init__(self, knobs: dict, dev):
+        from differentiablepointrendering_b200.pale import Renderer
+        from differentiablepointrendering_b200.scene import make_box_scene, make_surfels
+
+        self.dev = dev
+        self.knobs = dict(knobs)
+        st = c4_settings(knobs)
+        self.renderers = []
+        for n in C4["scenes"]:
+            sc = make_box_scene(n, cameras=C4["ring"], resolutions=C4["resolutions"], points=make_surfels(n, 1234))
+            self.renderers.append(Renderer.from_scene(sc, st))
+
+    def close(self):
+        for r in self.renderers:
+            r.close()
+
+    def _event_ms(self, fn, reps: int = 1) -> float:
+        import torch
+
+        stream = torch.cuda.current_stream(self.dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def batched_ms(self, views) -> float:
+        import torch
+        from differentiablepointrendering_b200.device import ViewBatch
+
+        vb = ViewBatch(self.renderers, views, device=self.dev)
+        tgt = torch.zeros(vb.pixels, 3, dtype=torch.float32, device=self.dev)
+
+        def it():
+            vb.forward_loss(tgt)
+            vb.backward()
+
+        it()   # warm-up (wavefront buffers grow on the first call)
+        return self._event_ms(it)
+
+    def plain_ms(self, views, per_pass: bool) -> float:
+        import torch
+        from differentiablepointrendering_b200.device import ViewBatch
+
+        calls = []
+        for sc, cam, spp, depth in views:
+            if per_pass:
+                one = ViewBatch([self.renderers[sc]], [(0, cam, 1, depth)], device=self.dev)
+                calls.append((one, spp))
+            else:
+                calls.append((ViewBatch([self.renderers[sc]], [(0, cam, spp, depth)], device=self.dev), 1))
+        tgts = [torch.zeros(vb.pixels, 3, dtype=torch.float32, device=self.dev) for vb, _ in calls]
+
+        def it():
+            for (vb, reps), t in zip(calls, tgts):
+                vb.forward_loss(t)                        # the view's photon map, first pass
+                for _ in range(reps - 1):
+                    vb.forward_loss(t, trace_photons=False)   # further gather passes
+                for _ in range(reps):
+                    vb.backward()
+
+        calls[0][0].forward_loss(tgts[0])
+        calls[0][0].backward()
+        return self._event_ms(it)
+
+
+def c4_measure(dev, tune: bool = True, iterations: int = 1) -> dict:
+    """Autotuner + batched and plain C4 iterations.  The autotuner is a
+    coordinate descent over the leaf size, the walk block size and the
+    adjoint queue depth (adjoint_batch_paths), one batched iteration of a
+    16-view sample per candidate; the chosen knobs then time `iterations`
+    iterations of 64 drawn views (seed 7) batched, one view per call and one
+    pass per call."""
+    import numpy as np
+
+    knobs = {"leaf_size": 1, "walk_block": 256, "adjoint_batch_paths": 1 << 24}
+    trials = []
+    if tune:
+        sample = c4_views(np.random.default_rng(3), 16)
+        best = None
+        for key in ("leaf_size", "walk_block", "adjoint_batch_paths"):
+            for v in C4_TUNE[key]:
+                cand = dict(knobs, **{key: v})
+                run = C4Run(cand, dev)
+                try:
+                    ms = run.batched_ms(sample)
+                finally:
+                    run.close()
+                trials.append({**cand, "ms": round(ms, 2)})
+                if best is None or ms < best[0]:
+                    best = (ms, cand)
+            knobs = dict(best[1])
+    rng = np.random.default_rng(7)
+    run = C4Run(knobs, dev)
+    try:
+        res = {"batched_ms": [], "plain_per_view_ms": [], "plain_per_pass_ms": []}
+        for _ in range(iterations):
+            views = c4_views(rng, C4["views"])
+            res["batched_ms"].append(run.batched_ms(views))
+            res["plain_per_view_ms"].append(run.plain_ms(views, per_pass=False))
+            res["plain_per_pass_ms"].append(run.plain_ms(views, per_pass=True))
+    finally:
+        run.close()
+    b = float(np.mean(res["batched_ms"]))
+    pv = float(np.mean(res["plain_per_view_ms"]))
+    pp = float(np.mean(res["plain_per_pass_ms"]))
+    return {"workload": "c4", "scenes": list(C4["scenes"]), "views_per_iteration": C4["views"],
+            "resolutions": list(C4["resolutions"]), "passes": list(C4["spp"]), "photons": C4["photons"],
+            "depth": C4["bounces"], "iterations": iterations, "knobs": knobs, "autotune": trials,
+            "batched_iters_per_s": round(1e3 / b, 4), "plain_per_view_iters_per_s": round(1e3 / pv, 4),
+            "plain_per_pass_iters_per_s": round(1e3 / pp, 4),
+            "speedup_vs_plain_per_view": round(pv / b, 3), "speedup_vs_plain_per_pass": round(pp / b, 3),
+            "ms": {"batched": round(b, 2), "plain_per_view": round(pv, 2), "plain_per_pass": round(pp, 2)}}
+
+
 # ------------------------------------------------------------------- ours
 def plain_and_latency(r, frame, target, dev, batched_ms: float, steps: int = 2, requests: int = 20) -> dict:
     """Beside the batched step: (1) the plain path, the same step with one
@@ -314,7 +467,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     from differentiablepointrendering_b200.build import build_library
     from differentiablepointrendering_b200.device import DeviceFrame
-    from differentiablepointrendering_b200.multigpu import reduce_gradients, view_offset
+    from differentiablepointrendering_b200.multigpu import reduce_gradients, shard_cameras
     from differentiablepointrendering_b200.pale import Renderer
     from differentiablepointrendering_b200.scene import jitter_target, make_box_scene, make_surfels
 
@@ -322,15 +475,18 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.set_device(local_rank)
     dev = torch.device(f"cuda:{local_rank}")
     w = WORKLOADS[args.workload]
-    st = settings_for(w)
+    # weak scaling: one scene with cams x N cameras on the ring, split round
+    # robin over the ranks (rank r renders cameras r, r + N, ...: cams each);
+    # camera-keyed seeds make a camera's work independent of the split
+    st = dict(settings_for(w), camera_seeds="camera", gradients=args.gradients)
     pts = make_surfels(w["n"], 1234)
-    offset = view_offset(rank, world)      # rank r renders views rotated by r/N of the spacing
-    scene = make_box_scene(w["n"], cameras=w["cams"], resolution=w["res"], points=pts, ring_offset=offset)
+    scene = make_box_scene(w["n"], cameras=w["cams"] * world, resolution=w["res"], points=pts)
+    mine = shard_cameras(list(range(w["cams"] * world)), rank, world)
     tscene = scene.with_points(jitter_target(pts, 5678))
 
     # target images (renders of the jittered cloud), resident on the device
     tr = Renderer.from_scene(tscene, st)
-    tf = DeviceFrame(tr, device=dev)
+    tf = DeviceFrame(tr, cameras=mine, device=dev)
     tf.forward()
     target = tf.ldr[:, :3].clone()
     torch.cuda.synchronize()
@@ -338,7 +494,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     tr.close()
 
     r = Renderer.from_scene(scene, st)
-    frame = DeviceFrame(r, device=dev)
+    frame = DeviceFrame(r, cameras=mine, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -387,7 +543,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     value = float(total_rays.item()) / (ms_per_step / 1e3) / 1e6
 
     # ---- end to end through the public API with host buffers
-    cams = r.get_camera_names()
+    cams = [r.get_camera_names()[i] for i in mine]
     tgt_np = {}
     for i, name in enumerate(cams):
         ww, hh = frame.sizes[i]
@@ -420,6 +576,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         r.close()
         return
     extra = {} if args.skip_extra else plain_and_latency(r, frame, target, dev, ms_per_step)
+    if not args.skip_extra and world == 1:
+        r.close()      # frees box200k's buffers for the C4 scenes
+        extra["c4"] = c4_measure(dev, tune=not args.no_tune)
     peaks = read_peaks()
     hbm = peaks["hbm_gbs"] if peaks else 6650.0
     # per-kernel device time (events around every launch, stats step) and
@@ -445,8 +604,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_for(args.workload, w),
+        "gradients": args.gradients,
         "iters_per_s": round(1e3 / ms_per_step, 4), "rays_per_step_per_gpu": int(rays),
-        "parallelism": f"views sharded over {world} GPU(s), gradients all-reduced",
+        "parallelism": f"{w['cams'] * world} ring cameras split round robin over {world} GPU(s), gradients all-reduced",
         "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "gpu_launches": launches * args.steps,
@@ -468,7 +628,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         **extra,
     }
     print(json.dumps(line), flush=True)
-    r.close()
+    if args.skip_extra or world > 1:
+        r.close()
 
 
 # ---------------------------------------------------------------- serving
@@ -566,8 +727,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="box200k", choices=sorted(WORKLOADS))
     ap.add_argument("--skip-cpu", dest="skip_cpu", action="store_true")
+    ap.add_argument("--gradients", default="opacity", choices=("opacity", "all"),
+                    help="gradient groups of the adjoint: the reference's opacity, or all seven")
     ap.add_argument("--skip-extra", dest="skip_extra", action="store_true",
                     help="skip the per-view and request-latency measurements")
+    ap.add_argument("--no-tune", dest="no_tune", action="store_true", help="C4 without the autotuner")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (Poisson request stream)")
     ap.add_argument("--rates", type=float, nargs="*", default=[5.0, 20.0, 50.0])
     ap.add_argument("--seconds", type=float, default=6.0)

@@ -30,7 +30,12 @@ class PaleSettings(C.Structure):
                 ("gather_radius", C.c_float), ("leaf_size", C.c_uint32), ("rng_mode", C.c_uint32),
                 ("debug_images", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float),
                 ("null_weight", C.c_uint32), ("gradients", C.c_uint32), ("camera_seeds", C.c_uint32),
-                ("gather_batch_paths", C.c_uint32), ("adjoint_batch_paths", C.c_uint32)]
+                ("gather_batch_paths", C.c_uint32), ("adjoint_batch_paths", C.c_uint32),
+                ("walk_block", C.c_uint32)]
+
+
+class PaleView(C.Structure):
+    _fields_ = [("scene", C.c_uint32), ("camera", C.c_uint32), ("passes", C.c_uint32), ("depth", C.c_uint32)]
 
 
 class PalePoints(C.Structure):
@@ -121,6 +126,7 @@ SETTINGS_KEYS = {
     "gather_radius": "gather_radius", "leaf_size": "leaf_size", "debug_images": "debug_images",
     "exposure": "exposure", "gamma": "gamma",
     "gather_batch_paths": "gather_batch_paths", "adjoint_batch_paths": "adjoint_batch_paths",
+    "walk_block": "walk_block",
 }
 IGNORED_KEYS = ("logging", "depth_distort_weight", "normal_consistency_weight")
 
@@ -277,6 +283,12 @@ def load_library() -> C.CDLL:
                                               C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),
         "pale_lbvh_node_count": (C.c_uint32, [C.c_uint32, C.c_uint32]),
+        "pale_render_views_loss_device": (C.c_int, [C.c_uint32, C.POINTER(C.c_void_p), C.c_int, C.c_uint32,
+                                                    C.POINTER(PaleView), C.c_void_p, C.c_uint32, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "pale_render_views_backward_device": (C.c_int, [C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
+                                                        C.POINTER(PaleView), C.c_void_p, C.POINTER(PalePoints),
+                                                        C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -294,7 +306,7 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_get_stats", "pale_build_lbvh_noalloc", "pale_get_asset", "pale_optimizer_step",
             "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device",
             "pale_prune_by_opacity", "pale_densify_long_axis_split", "pale_apply_points_device",
-            "pale_lbvh_node_count")
+            "pale_lbvh_node_count", "pale_render_views_loss_device", "pale_render_views_backward_device")
 NOALLOC_MAX_SURFELS = 16384
 
 

@@ -111,6 +111,7 @@ struct pale_handle {
   std::vector<CameraRec> cams;
   std::vector<std::string> cam_names;
   DBuf<CameraRec> d_cams;
+  DBuf<uint32_t> d_view_start;   // per view: first camera path of the current gather chunk
   // surfels
   uint32_t np = 0;
   PointsBufs asset, collected, params;
@@ -342,6 +343,59 @@ void alloc_photon_store(pale_handle* h, uint64_t cap) {
 // Host restatement of toWorldPoint with the device's operation order.
 V3 host_xform_point(const float* M, V3 p) { return xform_point(M, p); }
 
+// Ray queues (ping-pong, staging, flags, per-tile counts) of at least n
+// slots: the photon passes need photons_per_launch, the adjoint its batch.
+void size_queues(pale_handle* h, size_t n) {
+  if (h->q0.n >= n) return;
+  h->q0.alloc(n); h->q1.alloc(n); h->qstage.alloc(n); h->qflags.alloc(n);
+  h->tile_counts.alloc(n / kBlock + 1); h->tile_offsets.alloc(n / kBlock + 1);
+}
+
+// The wavefront buffers of camera-gather and adjoint calls whose views hold
+// all_pix pixels, the largest view max_pix (grown, never shrunk):
+// - adjoint: the (view, pass) jobs of a call trace together, up to 2^24
+//   paths per batch (about 5.4 GB of queues and events), or the
+//   adjoint_batch_paths setting;
+// - camera gather: every pass of every pixel in flight when that fits in
+//   2^25 paths (3.2 GB of path queues, 8.6 GB of lookup records, 1 GB of
+//   per-entry state), or the gather_batch_paths setting, else chunks of
+//   whole passes; at least every pixel once.
+void size_wavefronts(pale_handle* h, uint64_t all_pix, uint32_t max_pix) {
+  const pale_settings& st = h->st;
+  if (all_pix >= (1ull << 31)) throw ArgError("too many camera pixels");
+  if (max_pix >= (1u << 24)) throw ArgError("a view of 2^24 pixels or more");
+  const size_t qc = h->qcap;
+  const uint64_t adj_want = all_pix * std::max<uint32_t>(1u, st.adjoint_passes);
+  const uint64_t adj_limit = std::min<uint64_t>(st.adjoint_batch_paths ? st.adjoint_batch_paths : (1ull << 24),
+                                                (1ull << 24));
+  const uint32_t adj_cap = (uint32_t)std::max<uint64_t>(max_pix, std::min<uint64_t>(adj_want, adj_limit));
+  if (adj_cap > h->adj_cap) {
+    h->adj_cap = adj_cap;
+    const size_t qa = std::max<size_t>(qc, h->adj_cap);
+    h->adj_keys.alloc(h->adj_cap); h->adj_perm.alloc(h->adj_cap);
+    h->adj_keys_tmp.alloc(h->adj_cap); h->adj_perm_tmp.alloc(h->adj_cap);
+    h->adj_sort_temp.alloc(radix_temp_words(h->adj_cap));
+    size_queues(h, qa);
+    h->pend_a.alloc(qa); h->pend_b.alloc(qa); h->pend_c.alloc(qa);
+    h->ev_stage.alloc(qa); h->ev_list.alloc(qa);
+    h->adj_hits.alloc(3 * qa);
+    h->adj_walkq.alloc(2 * qa);
+  }
+  const uint64_t want = all_pix * std::max<uint32_t>(1u, st.gather_passes);
+  const uint64_t cg_limit = st.gather_batch_paths ? st.gather_batch_paths : (1ull << 25);
+  const uint32_t path_cap =
+      (uint32_t)std::max<uint64_t>(std::max<uint64_t>(all_pix, 1), std::min<uint64_t>(want, cg_limit));
+  if (path_cap > h->path_cap) {
+    h->path_cap = path_cap;
+    h->cg_paths.alloc(h->path_cap); h->cg_paths2.alloc(h->path_cap);
+    h->cg_qrec.alloc(2 * (size_t)kGatherHits * h->path_cap); h->cg_res.alloc(h->path_cap);
+    h->cg_info_a.alloc(h->path_cap); h->cg_info_b.alloc(h->path_cap);
+    h->cg_mhit.alloc(h->path_cap); h->cg_walk.alloc(2 * (size_t)h->path_cap);
+    h->cg_khit.alloc((size_t)kKHitWords * h->path_cap);
+  }
+  h->cg_fb.ensure(std::max<uint64_t>(all_pix, 1));
+}
+
 void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   cudaStream_t s = h->stream;
   h->run.alloc(1);
@@ -558,38 +612,15 @@ void setup_scene(pale_handle* h, const pale_scene_desc* d) {
   // ---- queues: next power of two >= max(photons per launch, pixels)
   h->qcap = next_pow2(std::max(std::max(st.photons_per_launch, max_pix), 256u));
   const size_t qc = h->qcap;
-  // adjoint batches: the (camera, pass) jobs of a backward call trace
-  // together, up to 2^24 paths (about 5.4 GB of queues and events)
-  const uint64_t adj_want = all_pix * std::max<uint32_t>(1u, st.adjoint_passes);
-  const uint64_t adj_limit = st.adjoint_batch_paths ? st.adjoint_batch_paths : (1ull << 24);
-  h->adj_cap = (uint32_t)std::max<uint64_t>(max_pix, std::min<uint64_t>(adj_want, adj_limit));
-  const size_t qa = std::max<size_t>(qc, h->adj_cap);
-  h->adj_keys.alloc(h->adj_cap); h->adj_perm.alloc(h->adj_cap);
-  h->adj_keys_tmp.alloc(h->adj_cap); h->adj_perm_tmp.alloc(h->adj_cap);
-  h->adj_sort_temp.alloc(radix_temp_words(h->adj_cap));
-  h->q0.alloc(qa); h->q1.alloc(qa); h->qstage.alloc(qa); h->qflags.alloc(qa);
-  h->tile_counts.alloc(qa / kBlock + 1); h->tile_offsets.alloc(qa / kBlock + 1);
   h->ph_sa.alloc(qc); h->ph_sb.alloc(qc); h->ph_sc.alloc(qc);
-  h->pend_a.alloc(qa); h->pend_b.alloc(qa); h->pend_c.alloc(qa);
-  h->ev_stage.alloc(qa); h->ev_list.alloc(qa);
-  h->adj_hits.alloc(3 * qa);
-  h->adj_walkq.alloc(2 * qa);
   h->job_count.alloc(2 * kMaxJobsPerBatch);
   h->job_start.alloc(2 * kMaxJobsPerBatch);
-  // camera paths in flight: every pass of every pixel when that fits in
-  // 2^25 paths (3.2 GB of path queues, 8.6 GB of lookup records, 1 GB of
-  // per-entry state), else chunks of whole passes
-  if (all_pix >= (1ull << 31)) throw ArgError("too many camera pixels");
-  const uint64_t want = all_pix * std::max<uint32_t>(1u, st.gather_passes);
-  const uint64_t cg_limit = st.gather_batch_paths ? st.gather_batch_paths : (1ull << 25);
-  h->path_cap = (uint32_t)std::max<uint64_t>(std::max<uint64_t>(all_pix, 1), std::min<uint64_t>(want, cg_limit));
-  h->cg_paths.alloc(h->path_cap); h->cg_paths2.alloc(h->path_cap);
-  h->cg_qrec.alloc(2 * (size_t)kGatherHits * h->path_cap); h->cg_res.alloc(h->path_cap);
-  h->cg_info_a.alloc(h->path_cap); h->cg_info_b.alloc(h->path_cap);
-  h->cg_mhit.alloc(h->path_cap); h->cg_walk.alloc(2 * (size_t)h->path_cap);
-  h->cg_khit.alloc((size_t)kKHitWords * h->path_cap);
-  h->cg_fb.alloc(std::max<uint64_t>(all_pix, 1));
   h->cg_counts.alloc(2 * (kMaxLayers + 2));
+  // the photon queues now; the camera-gather and adjoint wavefronts when a
+  // call first renders through this handle (size_wavefronts), so that a
+  // scene that only lends its data to batched calls holds none
+  size_queues(h, qc);
+  (void)all_pix;
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   CK(cudaStreamSynchronize(s));
 }
@@ -698,37 +729,75 @@ struct LossReq {
   double* loss;    // may be null
 };
 
-// Forward render into the handle's packed device images.
-// trace_photons false: the camera gather alone, from the current photon
-// map (the last forward's or loaded photons), with the camera seeds the
-// last forward used.
-uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr, bool sync,
-                 bool trace_photons = true, const LossReq* lq = nullptr) {
-  cudaStream_t s = h->stream;
-  h->timer.used = 0;
-  const uint64_t launches0 = launches_issued();
-  const pale_settings& st = h->st;
-  validate_cams(h, nsel, idx);
-  std::vector<CameraRec> sel(nsel);
-  uint32_t total = 0;
-  for (uint32_t i = 0; i < nsel; ++i) {
-    sel[i] = h->cams[idx[i]];
-    sel[i].pixel_offset = total;
-    sel[i].seed_slot = st.camera_seeds == PALE_CAMERA_SEEDS_CAMERA ? idx[i] : i;
-    total += sel[i].w * sel[i].h;
+// One view of a render call: a camera of one of the call's scenes, with its
+// passes (gather and adjoint) and adjoint bounces.
+struct ViewReq {
+  uint32_t scene;    // index into the call's scene list
+  uint32_t cam;      // camera index in that scene
+  uint32_t passes;
+  uint32_t depth;
+};
+
+// The views of a one-scene call: the selected cameras with the scene's
+// gather passes (forward) or adjoint passes (adjoint) and its bounces.
+std::vector<ViewReq> all_passes(pale_handle* h, uint32_t nsel, const uint32_t* idx, bool adjoint) {
+  std::vector<ViewReq> v(nsel);
+  const uint32_t passes = adjoint ? h->st.adjoint_passes : h->st.gather_passes;
+  for (uint32_t i = 0; i < nsel; ++i) v[i] = ViewReq{0u, idx[i], passes, h->st.adjoint_bounces};
+  return v;
+}
+
+// adjoint: the views' passes are adjoint passes (at most the scene's
+// adjoint_passes), else gather passes (at most its gather_passes).
+void check_views(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views, bool adjoint) {
+  if (scenes.empty() || scenes.size() > kMaxScenes) throw ArgError("a call renders 1 to 8 scenes");
+  for (size_t k = 0; k < scenes.size(); ++k) {
+    if (!scenes[k]) throw ArgError("null scene handle");
+    for (size_t j = 0; j < k; ++j)
+      if (scenes[j] == scenes[k]) throw ArgError("a scene appears twice in the scene list");
   }
-  h->d_cams.ensure(std::max<size_t>(1, nsel));
-  if (nsel) CK(cudaMemcpyAsync(h->d_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
-  // seed stream of submitPhotonMappingKernel: passes x (1 + bounces) + cameras
-  const size_t cam_seeds = st.camera_seeds == PALE_CAMERA_SEEDS_CAMERA ? h->cams.size() : nsel;
-  std::vector<uint32_t> seeds = mt_table(st.seed, (size_t)st.forward_passes * (1 + st.max_bounces) + cam_seeds + 1);
+  for (const ViewReq& v : views) {
+    if (v.scene >= scenes.size()) throw ArgError("view scene index out of range");
+    pale_handle* h = scenes[v.scene];
+    if (v.cam >= h->cams.size()) throw ArgError("camera index out of range");
+    if (v.passes == 0 || v.passes > (adjoint ? h->st.adjoint_passes : h->st.gather_passes))
+      throw ArgError(adjoint ? "view passes must be 1 .. the scene's adjoint_passes"
+                             : "view passes must be 1 .. the scene's gather_passes");
+    if (v.depth > h->st.adjoint_bounces) throw ArgError("view depth above the scene's adjoint bounces");
+  }
+}
+
+// The camera seeds a scene's forward render uses: one per camera of the
+// scene (camera_seeds = camera) or one per view of the scene in the call
+// (the reference's order of the selection).
+std::vector<uint32_t> seed_slots(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views) {
+  std::vector<uint32_t> slot(views.size()), rank(scenes.size(), 0u);
+  for (size_t i = 0; i < views.size(); ++i) {
+    const uint32_t k = views[i].scene;
+    slot[i] = scenes[k]->st.camera_seeds == PALE_CAMERA_SEEDS_CAMERA ? views[i].cam : rank[k];
+    ++rank[k];
+  }
+  return slot;
+}
+
+// The seed table of a scene's forward render (submitPhotonMappingKernel's
+// stream: passes x (1 + bounces) photon seeds, then the camera seeds).
+void forward_seeds(pale_handle* h, size_t cam_words) {
+  const pale_settings& st = h->st;
+  const size_t words = std::max<size_t>(cam_words, h->cams.size());
+  std::vector<uint32_t> seeds = mt_table(st.seed, (size_t)st.forward_passes * (1 + st.max_bounces) + words + 1);
   h->seeds_fwd.ensure(seeds.size());
-  CK(cudaMemcpyAsync(h->seeds_fwd.p, seeds.data(), seeds.size() * 4, cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
-  CK(cudaEventRecord(h->ev0, s));
-  SceneView sv = h->view();
+  CK(cudaMemcpyAsync(h->seeds_fwd.p, seeds.data(), seeds.size() * 4, cudaMemcpyHostToDevice, h->stream));
+}
+
+// The photon passes and the photon grid of scene h on its stream
+// (submitPhotonMappingKernel, SyclBridge.cpp:82-138); the seed cursor
+// where the camera seeds start is kept in h->cam_cursor.
+void trace_photon_map(pale_handle* h) {
+  cudaStream_t s = h->stream;
+  const pale_settings& st = h->st;
   PhotonArgs P{};
-  P.scene = sv;
+  P.scene = h->view();
   P.st = h->run.p;
   P.seeds = h->seeds_fwd.p;
   P.qb = QueueBufs{{h->q0.p, h->q1.p}, h->qstage.p, h->qflags.p, h->tile_counts.p, h->tile_offsets.p, h->qcap};
@@ -740,45 +809,110 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   P.q_reflect = st.q_reflect;
   P.q_transmit = st.q_transmit;
   if (st.photons_per_launch > h->qcap) throw ArgError("photons per launch exceed the queue capacity");
-  uint32_t* cursor = &h->run.p->seed_cursor;
-  if (!trace_photons) {
-    CK(cudaMemcpyAsync(cursor, h->cam_cursor.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-  } else {
-    for (uint32_t pass = 0; pass < st.forward_passes; ++pass) {
-      photon_emit(P, s);
-      for (uint32_t b = 0; b < st.max_bounces; ++b) photon_bounce(P, b & 1u, s);
+  for (uint32_t pass = 0; pass < st.forward_passes; ++pass) {
+    photon_emit(P, s);
+    for (uint32_t b = 0; b < st.max_bounces; ++b) photon_bounce(P, b & 1u, s);
+  }
+  GridBufs G{};
+  G.cell_id = h->g_cell_id.p;
+  G.sorted = h->g_sorted.p;
+  G.keys_tmp = h->g_keys.p;
+  G.vals_tmp = h->g_vals_tmp.p;
+  G.sort_temp = h->g_sort_temp.p;
+  G.cell_count = h->g_cell_count.p;
+  G.cell_off = h->g_cell_off.p;
+  G.scan_temp = h->g_scan_temp.p;
+  G.pa = h->g_pa.p;
+  G.pb = h->g_pb.p;
+  G.pc = h->g_pc.p;
+  G.d_stored = h->g_stored.p;
+  G.d_attempts = h->g_attempts.p;
+  grid_build(P.scene, h->run.p, P.ps, G, h->cells, h->key_bits, s);
+  CK(cudaMemcpyAsync(h->cam_cursor.p, &h->run.p->seed_cursor, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+}
+
+// The scene table of a call: every scene's view, with the same number of
+// LBVH top nodes staged per scene (256 shared among them).
+SceneTable scene_table(const std::vector<pale_handle*>& scenes) {
+  SceneTable T{};
+  T.n = (uint32_t)scenes.size();
+  uint32_t staged = kTopNodes / T.n;
+  for (uint32_t k = 0; k < T.n; ++k) {
+    T.s[k] = scenes[k]->view();
+    staged = std::min(staged, T.s[k].top_nodes);
+  }
+  for (uint32_t k = 0; k < T.n; ++k) T.s[k].top_nodes = staged;
+  T.staged = staged;
+  return T;
+}
+
+// The views' camera records, packed in call order.
+std::vector<CameraRec> view_records(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views,
+                                    uint32_t& total, uint32_t& max_pix) {
+  const std::vector<uint32_t> slots = seed_slots(scenes, views);
+  std::vector<CameraRec> sel(views.size());
+  total = 0;
+  max_pix = 0;
+  for (size_t i = 0; i < views.size(); ++i) {
+    const ViewReq& v = views[i];
+    sel[i] = scenes[v.scene]->cams[v.cam];
+    sel[i].pixel_offset = total;
+    sel[i].seed_slot = slots[i];
+    sel[i].passes = v.passes;
+    sel[i].scene = v.scene;
+    sel[i].depth = v.depth ? v.depth : scenes[v.scene]->st.adjoint_bounces;
+    total += sel[i].w * sel[i].h;
+    max_pix = std::max(max_pix, sel[i].w * sel[i].h);
+  }
+  return sel;
+}
+
+// The forward render of `views` into packed device images, on the stream
+// of scenes[0], whose wavefront buffers the call uses; the other scenes
+// lend their scene data (surfels, LBVH, meshes, photon grid).  With
+// trace_photons every scene first traces its photon map; without, the
+// camera gather runs on the current photon maps (the last forward's or
+// loaded photons) with the camera seeds the last forward used.
+uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views, float* d_raw,
+                      float* d_ldr, bool sync, bool trace_photons, const LossReq* lq) {
+  pale_handle* h = scenes[0];
+  cudaStream_t s = h->stream;
+  h->timer.used = 0;
+  const uint64_t launches0 = launches_issued();
+  check_views(scenes, views, false);
+  uint32_t total = 0, max_pix = 0;
+  std::vector<CameraRec> sel = view_records(scenes, views, total, max_pix);
+  size_wavefronts(h, total, max_pix);
+  const uint32_t nsel = (uint32_t)sel.size();
+  h->d_cams.ensure(std::max<size_t>(1, nsel));
+  h->d_view_start.ensure(std::max<size_t>(1, nsel));
+  if (nsel) CK(cudaMemcpyAsync(h->d_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
+  for (size_t k = 0; k < scenes.size(); ++k) {
+    pale_handle* sk = scenes[k];
+    forward_seeds(sk, views.size());
+    if (trace_photons) {
+      CK(cudaMemsetAsync(sk->run.p, 0, sizeof(RunState), s));
+      if (k == 0) CK(cudaEventRecord(h->ev0, s));
+      trace_photon_map(sk);
     }
-    GridBufs G{};
-    G.cell_id = h->g_cell_id.p;
-    G.sorted = h->g_sorted.p;
-    G.keys_tmp = h->g_keys.p;
-    G.vals_tmp = h->g_vals_tmp.p;
-    G.sort_temp = h->g_sort_temp.p;
-    G.cell_count = h->g_cell_count.p;
-    G.cell_off = h->g_cell_off.p;
-    G.scan_temp = h->g_scan_temp.p;
-    G.pa = h->g_pa.p;
-    G.pb = h->g_pb.p;
-    G.pc = h->g_pc.p;
-    G.d_stored = h->g_stored.p;
-    G.d_attempts = h->g_attempts.p;
-    grid_build(sv, h->run.p, P.ps, G, h->cells, h->key_bits, s);
-    CK(cudaMemcpyAsync(h->cam_cursor.p, cursor, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  }
+  if (!trace_photons) {
+    CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+    CK(cudaEventRecord(h->ev0, s));
   }
   CK(cudaEventRecord(h->ev1, s));
   FrameArgs F{};
-  F.scene = sv;
+  F.scenes = scene_table(scenes);
+  for (size_t k = 0; k < scenes.size(); ++k) F.sseeds[k] = SceneSeeds{scenes[k]->seeds_fwd.p, scenes[k]->cam_cursor.p};
   F.st = h->run.p;
-  F.seeds = h->seeds_fwd.p;
   F.cams = h->d_cams.p;
   F.ncams = nsel;
   F.total_pixels = total;
   F.raw = d_raw;
   F.ldr = d_ldr;
-  F.gather_passes = st.gather_passes;
-  F.rng_mode = st.rng_mode;
-  F.exposure = st.exposure;
-  F.gamma = st.gamma;
+  F.rng_mode = h->st.rng_mode;
+  F.exposure = h->st.exposure;
+  F.gamma = h->st.gamma;
   F.paths[0] = h->cg_paths.p;
   F.paths[1] = h->cg_paths2.p;
   F.qrec = h->cg_qrec.p;
@@ -791,13 +925,14 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   F.res = h->cg_res.p;
   F.fb = h->cg_fb.p;
   F.path_capacity = h->path_cap;
+  F.walk_block = h->st.walk_block;
   F.timer = &h->timer;
   if (lq) {
     F.target = lq->target;
     F.target_channels = lq->channels;
     F.dldi = lq->dldi;
   }
-  camera_gather(F, s);
+  camera_gather(F, sel, h->d_view_start.p, s);
   if (lq && lq->loss) {
     h->loss_part.ensure((size_t)std::max(1u, nsel) * kLossChunks);
     image_loss(F, h->loss_part.p, lq->loss, s);
@@ -809,6 +944,12 @@ uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_ra
   h->stats_pending = 1;
   if (sync) copy_stats(h);
   return total;
+}
+
+uint32_t forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, float* d_raw, float* d_ldr, bool sync,
+                 bool trace_photons = true, const LossReq* lq = nullptr) {
+  validate_cams(h, nsel, idx);
+  return render_views({h}, all_passes(h, nsel, idx, false), d_raw, d_ldr, sync, trace_photons, lq);
 }
 
 void zero_grads(pale_handle* h, cudaStream_t s) {
@@ -825,23 +966,47 @@ void zero_grads(pale_handle* h, cudaStream_t s) {
   CK(cudaMemsetAsync(g.shape.p, 0, 4 * n, s));
 }
 
-// Adjoint pass reading packed dL/dI at d_dldi (device).
-void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi, float* d_dbg, bool sync) {
+// The adjoint pass of `views` reading packed dL/dI at d_dldi (device), on
+// the stream and with the wavefront buffers of scenes[0]; each scene's
+// gradients accumulate in its own arrays (BVH order).  All scenes share
+// the rng mode, the null weighting and the gradient groups of scenes[0].
+void adjoint_views(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views, const float* d_dldi,
+                   float* d_dbg, bool sync) {
+  pale_handle* h = scenes[0];
   cudaStream_t s = h->stream;
   h->timer.used = 0;
   const uint64_t launches0 = launches_issued();
   const pale_settings& st = h->st;
-  validate_cams(h, nsel, idx);
-  std::vector<uint32_t> seeds =
-      mt_table(st.rng_mode == PALE_RNG_DECORRELATED ? st.seed : 42ull,
-               (size_t)nsel * st.adjoint_passes * (1 + st.adjoint_bounces) + 1);
+  check_views(scenes, views, true);
+  uint32_t total = 0, max_pix = 0;
+  std::vector<CameraRec> sel = view_records(scenes, views, total, max_pix);
+  size_wavefronts(h, total, max_pix);
+  // decorrelated seeds: per scene one block of (1 + bounces) per (camera,
+  // pass), camera-major with the scene's passes as the stride; a camera is
+  // its position among the scene's views in the call, or with camera_seeds
+  // = camera its scene index, so that its gradient does not depend on which
+  // other cameras the call holds.  The scenes' tables are concatenated.
+  std::vector<uint32_t> seeds;
+  std::vector<size_t> seed_base(scenes.size());
+  std::vector<uint32_t> nviews(scenes.size(), 0u);
+  for (const ViewReq& v : views) ++nviews[v.scene];
+  for (size_t k = 0; k < scenes.size(); ++k) {
+    const pale_settings& sk = scenes[k]->st;
+    const bool by_camera = sk.camera_seeds == PALE_CAMERA_SEEDS_CAMERA;
+    const size_t seed_cams = by_camera ? scenes[k]->cams.size() : nviews[k];
+    std::vector<uint32_t> t = mt_table(st.rng_mode == PALE_RNG_DECORRELATED ? sk.seed : 42ull,
+                                       seed_cams * sk.adjoint_passes * (1 + sk.adjoint_bounces) + 1);
+    seed_base[k] = seeds.size();
+    seeds.insert(seeds.end(), t.begin(), t.end());
+  }
   h->seeds_adj.ensure(seeds.size());
   CK(cudaMemcpyAsync(h->seeds_adj.p, seeds.data(), seeds.size() * 4, cudaMemcpyHostToDevice, s));
-  zero_grads(h, s);
+  for (pale_handle* sk : scenes) zero_grads(sk, s);
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   CK(cudaEventRecord(h->ev0, s));
   AdjointArgs A{};
-  A.scene = h->view();
+  A.scenes = scene_table(scenes);
+  for (size_t k = 0; k < scenes.size(); ++k) A.sgrads[k] = SceneGrads{scenes[k]->grads.op.p, scenes[k]->grads.view()};
   A.st = h->run.p;
   A.seeds = h->seeds_adj.p;
   A.qb = QueueBufs{{h->q0.p, h->q1.p}, h->qstage.p, h->qflags.p, h->tile_counts.p, h->tile_offsets.p,
@@ -849,15 +1014,12 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.pend = PendingBufs{h->pend_a.p, h->pend_b.p, h->pend_c.p};
   A.ev = EventBufs{h->ev_stage.p, h->ev_list.p};
   A.dldi = d_dldi;
-  A.grad_opacity = h->grads.op.p;
-  A.grads = h->grads.view();
   A.all_grads = st.gradients == PALE_GRADIENTS_ALL;
   A.debug_opacity = d_dbg;
   A.rr_start = st.rr_start;
   A.q_null = st.q_null;
   A.q_reflect = st.q_reflect;
   A.q_transmit = st.q_transmit;
-  A.inv_spp = 1.0f / (float)st.adjoint_passes;
   A.fixed_seed = st.random_number;
   A.rng_mode = st.rng_mode;
   A.null_scale = st.null_weight == PALE_NULL_WEIGHT_UNBIASED ? 1.0f / st.q_null : 1.0f;
@@ -872,36 +1034,35 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   A.sort_capacity = h->adj_cap;
   A.hits = h->adj_hits.p;
   A.walkq = h->adj_walkq.p;
-  // jobs in the reference's order (camera-major, then pass), packed into
+  A.walk_block = st.walk_block;
+  // jobs in the reference's order (view-major, then pass), packed into
   // batches of at most adj_cap paths and kMaxJobsPerBatch jobs
-  std::vector<CameraRec> sel(nsel);
-  uint32_t offset = 0;
-  for (uint32_t i = 0; i < nsel; ++i) {
-    sel[i] = h->cams[idx[i]];
-    sel[i].pixel_offset = offset;
-    if (sel[i].w * sel[i].h > h->adj_cap) throw ArgError("camera larger than the queue capacity");
-    offset += sel[i].w * sel[i].h;
-  }
+  const std::vector<uint32_t> slots = seed_slots(scenes, views);
   std::vector<AdjJob> jobs;
   std::vector<std::pair<uint32_t, uint32_t>> batches;  // (first job, paths)
-  uint32_t in_batch = 0, first = 0;
-  for (uint32_t i = 0; i < nsel; ++i) {
+  uint32_t in_batch = 0, first = 0, max_depth = 0;
+  for (uint32_t i = 0; i < (uint32_t)sel.size(); ++i) {
     const uint32_t npix = sel[i].w * sel[i].h;
-    for (uint32_t spp = 0; spp < st.adjoint_passes; ++spp) {
+    const pale_settings& sk = scenes[sel[i].scene]->st;
+    const uint32_t stride = 1u + sk.adjoint_bounces;
+    max_depth = std::max(max_depth, sel[i].depth);
+    for (uint32_t spp = 0; spp < sel[i].passes; ++spp) {
       const uint32_t j = (uint32_t)jobs.size();
       if (in_batch + npix > h->adj_cap || j - first == kMaxJobsPerBatch) {
         batches.emplace_back(first, in_batch);
         first = j;
         in_batch = 0;
       }
-      jobs.push_back(AdjJob{i, in_batch, npix, (i * st.adjoint_passes + spp) * (1u + st.adjoint_bounces)});
+      const size_t seed_index = seed_base[sel[i].scene] + ((size_t)slots[i] * sk.adjoint_passes + spp) * stride;
+      jobs.push_back(AdjJob{i, in_batch, npix, (uint32_t)seed_index});
       in_batch += npix;
     }
   }
   if (!jobs.empty()) batches.emplace_back(first, in_batch);
-  h->d_adj_cams.ensure(std::max<size_t>(1, nsel));
+  h->d_adj_cams.ensure(std::max<size_t>(1, sel.size()));
   h->d_jobs.ensure(std::max<size_t>(1, jobs.size()));
-  if (nsel) CK(cudaMemcpyAsync(h->d_adj_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
+  if (!sel.empty())
+    CK(cudaMemcpyAsync(h->d_adj_cams.p, sel.data(), sel.size() * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
   if (!jobs.empty())
     CK(cudaMemcpyAsync(h->d_jobs.p, jobs.data(), jobs.size() * sizeof(AdjJob), cudaMemcpyHostToDevice, s));
   A.cams = h->d_adj_cams.p;
@@ -914,7 +1075,7 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
     A.njobs = j1 - j0;
     const uint32_t npaths = batches[bi].second;
     adjoint_raygen(A, npaths, s);
-    for (uint32_t b = 0; b < st.adjoint_bounces; ++b) adjoint_bounce(A, b, npaths, s);
+    for (uint32_t b = 0; b < max_depth; ++b) adjoint_bounce(A, b, npaths, s);
   }
   CK(cudaEventRecord(h->ev1, s));
   CK(cudaGetLastError());
@@ -922,6 +1083,11 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   h->timed = 2;
   h->stats_pending = 1;
   if (sync) copy_stats(h);
+}
+
+void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi, float* d_dbg, bool sync) {
+  validate_cams(h, nsel, idx);
+  adjoint_views({h}, all_passes(h, nsel, idx, true), d_dldi, d_dbg, sync);
 }
 
 void download_points(pale_handle* h, const PointsBufs& src, pale_points* out) {
@@ -1027,6 +1193,8 @@ int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale
     if (h->st.null_weight > PALE_NULL_WEIGHT_UNBIASED) throw ArgError("null_weight must be reference or unbiased");
     if (h->st.gradients > PALE_GRADIENTS_ALL) throw ArgError("gradients must be opacity or all");
     if (h->st.camera_seeds > PALE_CAMERA_SEEDS_CAMERA) throw ArgError("camera_seeds must be selection or camera");
+    if (h->st.walk_block != 0 && h->st.walk_block != 64 && h->st.walk_block != 128 && h->st.walk_block != 256)
+      throw ArgError("walk_block must be 64, 128 or 256");
     if (h->st.null_weight == PALE_NULL_WEIGHT_UNBIASED && !(h->st.q_null > 0.f))
       throw ArgError("unbiased null weighting needs q_null > 0");
     check_points(&desc->points, "pale_create");
@@ -1228,6 +1396,80 @@ int pale_render_backward_device(pale_handle* h, uint32_t nsel, const uint32_t* i
       cp(d_grads->beta, h->grads.beta.p, 4 * n);
       cp(d_grads->shape, h->grads.shape.p, 4 * n);
     }
+    return PALE_OK;
+  });
+}
+
+namespace {
+std::vector<pale_handle*> scene_list(uint32_t n, pale_handle* const* scenes) {
+  if (!scenes || n == 0 || n > kMaxScenes) throw ArgError("a call renders 1 to 8 scenes");
+  return std::vector<pale_handle*>(scenes, scenes + n);
+}
+
+std::vector<ViewReq> view_list(uint32_t n, const pale_view* views) {
+  if (n && !views) throw ArgError("view list is null");
+  std::vector<ViewReq> v(n);
+  for (uint32_t i = 0; i < n; ++i) v[i] = ViewReq{views[i].scene, views[i].camera, views[i].passes, views[i].depth};
+  return v;
+}
+
+void copy_grads_out(pale_handle* h, pale_points* d_grads, cudaStream_t s) {
+  const size_t n = h->np;
+  auto cp = [&](float* dst, const float* src, size_t bytes) {
+    if (dst && n) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+  };
+  cp(d_grads->position, h->grads.pos.p, 12 * n);
+  cp(d_grads->tangent_u, h->grads.tu.p, 12 * n);
+  cp(d_grads->tangent_v, h->grads.tv.p, 12 * n);
+  cp(d_grads->scale, h->grads.sc.p, 8 * n);
+  cp(d_grads->albedo, h->grads.alb.p, 12 * n);
+  cp(d_grads->opacity, h->grads.op.p, 4 * n);
+  cp(d_grads->beta, h->grads.beta.p, 4 * n);
+  cp(d_grads->shape, h->grads.shape.p, 4 * n);
+}
+}  // namespace
+
+int pale_render_views_loss_device(uint32_t num_scenes, pale_handle* const* scenes, int trace_photons,
+                                  uint32_t num_views, const pale_view* views, const float* d_target,
+                                  uint32_t channels, float* d_ldr, float* d_raw, float* d_dldi, double* d_loss,
+                                  void* stream) {
+  if (!scenes || num_scenes == 0 || !scenes[0]) return fail(nullptr, PALE_ERR_ARGUMENT, "no scenes");
+  pale_handle* h = scenes[0];
+  return guarded(h, [&]() {
+    std::vector<pale_handle*> sc = scene_list(num_scenes, scenes);
+    std::vector<ViewReq> vw = view_list(num_views, views);
+    check_views(sc, vw, false);
+    if ((d_dldi || d_loss) && !d_target && num_views) throw ArgError("target image is null");
+    if (d_target && channels != 3 && channels != 4) throw ArgError("target images need 3 or 4 channels");
+    size_t pix = 0;
+    for (const ViewReq& v : vw) pix += (size_t)sc[v.scene]->cams[v.cam].w * sc[v.scene]->cams[v.cam].h;
+    const cudaStream_t s = caller_stream(stream);
+    for (pale_handle* sk : sc) use_stream(sk, s);
+    h->img_raw.ensure(4 * std::max<size_t>(1, pix));
+    if (!d_ldr && (d_loss || d_dldi)) {
+      h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
+      d_ldr = h->img_ldr.p;
+    }
+    LossReq lq{d_target, channels, d_dldi, d_loss};
+    render_views(sc, vw, d_raw ? d_raw : h->img_raw.p, d_ldr, false, trace_photons != 0, d_target ? &lq : nullptr);
+    return PALE_OK;
+  });
+}
+
+int pale_render_views_backward_device(uint32_t num_scenes, pale_handle* const* scenes, uint32_t num_views,
+                                      const pale_view* views, const float* d_dldi, pale_points* d_grads,
+                                      void* stream) {
+  if (!scenes || num_scenes == 0 || !scenes[0]) return fail(nullptr, PALE_ERR_ARGUMENT, "no scenes");
+  pale_handle* h = scenes[0];
+  return guarded(h, [&]() {
+    std::vector<pale_handle*> sc = scene_list(num_scenes, scenes);
+    std::vector<ViewReq> vw = view_list(num_views, views);
+    if (num_views && !d_dldi) throw ArgError("dL/dI is null");
+    const cudaStream_t s = caller_stream(stream);
+    for (pale_handle* sk : sc) use_stream(sk, s);
+    adjoint_views(sc, vw, d_dldi, nullptr, false);
+    if (d_grads)
+      for (size_t k = 0; k < sc.size(); ++k) copy_grads_out(sc[k], &d_grads[k], s);
     return PALE_OK;
   });
 }

@@ -252,7 +252,10 @@ struct CameraRec {
   uint32_t w, h;
   uint32_t pixel_offset;   // first pixel of this camera in the packed images
   uint32_t seed_slot;      // seed index relative to the cursor
-  uint32_t pad[2];
+  uint32_t passes;         // gather / adjoint passes of this view
+  uint32_t scene;          // index of the view's scene in the call's scene table
+  uint32_t depth;          // adjoint bounces of this view
+  uint32_t pad[3];
 };
 
 __device__ __forceinline__ void flag_error(RunState* st, uint32_t bit) { atomicOr(&st->error, bit); }

@@ -165,16 +165,49 @@ struct EventBufs {
   EventRec* list;         // compacted, slot order
 };
 
-struct FrameArgs {
-  SceneView scene;
-  RunState* st;
+// The scenes of one render call.  A call renders views (a camera of a scene
+// and its number of passes); the views of every scene trace as one
+// wavefront, each path finding its scene's surfels, LBVH, meshes and photon
+// grid through the view's scene index.  The first `staged` LBVH nodes of
+// every scene are staged in shared memory by the traversal kernels, scene
+// k's at [k * staged, (k + 1) * staged), and each table entry's top_nodes
+// is that count.
+constexpr uint32_t kMaxScenes = 8;
+
+struct SceneTable {
+  SceneView s[kMaxScenes];
+  uint32_t n;
+  uint32_t staged;
+};
+
+// Where the camera seeds of a scene's forward render start: the scene's
+// seed table and the device word holding the cursor position after its
+// photon passes.
+struct SceneSeeds {
   const uint32_t* seeds;
-  const CameraRec* cams;
+  const uint32_t* cursor;
+};
+
+// Gradient arrays of a scene (BVH order).
+struct SceneGrads {
+  float* opacity;
+  PointsDev all;          // all seven groups, written when all_grads
+};
+
+struct FrameArgs {
+  SceneTable scenes;
+  SceneSeeds sseeds[kMaxScenes];
+  RunState* st;
+  const CameraRec* cams;  // the views, in packing order (pixel_offset increasing)
   uint32_t ncams;
   uint32_t total_pixels;
   float* raw;             // packed H*W*4 per camera
   float* ldr;
-  uint32_t gather_passes;
+  // paths of the current chunk: view v's passes [p0, min(p1, passes)) at
+  // paths view_start[v] + (pass - p0) * pixels + pixel; non-decreasing, a
+  // view without a pass in the chunk has an empty range
+  const uint32_t* view_start;
+  uint32_t walk_block;     // threads per block of the persistent walks (host side)
   uint32_t rng_mode;
   float exposure, gamma;
   // wavefront buffers: path queues (ping-pong by round), lookup records (2
@@ -242,6 +275,13 @@ constexpr int kLookupMinBlocks = PALE_LOOKUP_MIN_BLOCKS;
 // The persistent walks (adjoint closest hit, camera 8 hits): lanes whose
 // walk has ended take a new ray every PALE_REFILL_STEPS node visits;
 // PALE_WALK_MIN_BLOCKS is the adjoint walk's register budget.
+// A persistent walk's lanes standing at leaves test them together once at
+// least PALE_LEAF_BATCH lanes of the warp do (or every walking lane).
+#ifndef PALE_LEAF_BATCH
+#define PALE_LEAF_BATCH 8
+#endif
+constexpr int kLeafBatch = PALE_LEAF_BATCH;
+
 #ifndef PALE_REFILL_STEPS
 #define PALE_REFILL_STEPS 16
 #endif
@@ -289,15 +329,14 @@ struct AdjJob {
 constexpr uint32_t kMaxJobsPerBatch = 1024;
 
 struct AdjointArgs {
-  SceneView scene;
+  SceneTable scenes;
+  SceneGrads sgrads[kMaxScenes];
   RunState* st;
   const uint32_t* seeds;
   QueueBufs qb;
   PendingBufs pend;
   EventBufs ev;
   const float* dldi;       // packed H*W*4 per camera
-  float* grad_opacity;
-  PointsDev grads;         // all seven groups (BVH order), written when all_grads
   uint32_t all_grads;
   float* debug_opacity;    // packed H*W*4 per camera or null
   const CameraRec* cams;   // selected cameras, packed pixel offsets
@@ -307,7 +346,6 @@ struct AdjointArgs {
   uint32_t* job_start;     // [2][kMaxJobsPerBatch] queue start per job
   uint32_t rr_start;
   float q_null, q_reflect, q_transmit;
-  float inv_spp;
   uint32_t fixed_seed;     // reference mode: settings.random.number
   uint32_t rng_mode;
   float null_scale;        // NullTransmittance weight: 1 or 1 / q_null
@@ -333,13 +371,17 @@ struct AdjointArgs {
   // bits).
   float4* hits;
   float4* walkq;
+  uint32_t walk_block;     // threads per block of the persistent walks (host side)
 };
 
 void photon_emit(const PhotonArgs& a, cudaStream_t s);
 void photon_bounce(const PhotonArgs& a, uint32_t parity, cudaStream_t s);
 void grid_build(const SceneView& sv, RunState* st, const PhotonStore& ps, const GridBufs& g, uint32_t cells,
                 int key_bits, cudaStream_t s);
-void camera_gather(const FrameArgs& a, cudaStream_t s);
+// The camera gather of the views `views` (host copy of a.cams; every view
+// passes >= 1); d_view_start holds views.size() words of device scratch.
+void camera_gather(const FrameArgs& a, const std::vector<CameraRec>& views, uint32_t* d_view_start,
+                   cudaStream_t s);
 void adjoint_raygen(const AdjointArgs& a, uint32_t npaths, cudaStream_t s);
 void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cudaStream_t s);
 

@@ -26,6 +26,29 @@ __device__ __forceinline__ void stage_top_nodes(const SceneView& S, TravNode* sm
   __syncthreads();
 }
 
+// The staged top nodes of every scene of a call: scene k's first
+// T.staged nodes at smem[k * T.staged].
+__device__ __forceinline__ void stage_top_nodes(const SceneTable& T, TravNode* smem) {
+  const uint32_t total = T.n * T.staged;
+  for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+    const uint32_t k = i / T.staged;
+    smem[i] = T.s[k].nodes[i - k * T.staged];
+  }
+  __syncthreads();
+}
+
+// The view (index into the call's cameras) that holds packed pixel gp:
+// the last camera whose pixel_offset is <= gp.
+__device__ __forceinline__ uint32_t view_of_pixel(const CameraRec* __restrict__ cams, uint32_t ncams, uint32_t gp) {
+  uint32_t lo = 0, hi = ncams - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (cams[mid].pixel_offset <= gp) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 __device__ __forceinline__ RayRec make_ray(V3 o, V3 d, V3 thr, uint32_t path, uint32_t bounce, uint32_t pixel) {
   RayRec r;
   r.o = make_float4(o.x, o.y, o.z, __uint_as_float(path));
@@ -249,6 +272,25 @@ __global__ void __launch_bounds__(kBlock) k_photon_bounce(PhotonArgs A, uint32_t
 static size_t top_smem(const SceneView& s) {
   return (size_t)s.top_nodes * sizeof(TravNode) + (size_t)PALE_SMEM_STACK * kBlock * sizeof(uint2);
 }
+static size_t top_smem(const SceneTable& t, int threads = kBlock) {
+  return (size_t)t.n * t.staged * sizeof(TravNode) + (size_t)PALE_SMEM_STACK * threads * sizeof(uint2);
+}
+
+// Launch of a persistent walk kernel with the block size `threads` (64,
+// 128 or 256): one resident wave of blocks (occupancy x SMs), at most
+// `limit` blocks of 256-thread equivalents.
+template <typename KernelT, typename Args>
+static void launch_walk(KernelT kernel, int threads, const Args& a, uint32_t arg, size_t smem, uint32_t limit,
+                        cudaStream_t s) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  const uint64_t grid = std::min<uint64_t>((uint64_t)limit * (kBlock / threads),
+                                           (uint64_t)std::max(1, sms * std::max(1, per_sm)));
+  kernel<<<(uint32_t)std::max<uint64_t>(1, grid), threads, smem, s>>>(a, arg);
+  note_launch();
+}
 
 void photon_emit(const PhotonArgs& a, cudaStream_t s) {
   const uint32_t nb = blocks_for(a.photons_per_launch);
@@ -355,21 +397,36 @@ __device__ __forceinline__ void primary_ray(const CameraRec& C, float px, float 
 // launchPostProcessKernel (PostprocessKernel.cpp:11-106).
 
 __device__ __forceinline__ uint32_t find_camera(const FrameArgs& A, uint32_t gp) {
-  uint32_t ci = 0;
-  while (ci + 1 < A.ncams && A.cams[ci + 1].pixel_offset <= gp) ++ci;
-  return ci;
+  return view_of_pixel(A.cams, A.ncams, gp);
 }
 
-// Primary rays of passes [p0, p1): path = (pass - p0) * total_pixels + gp.
-__global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1) {
-  const uint32_t n = (p1 - p0) * A.total_pixels;
+// The view of chunk path `path`: the last view whose first path of the
+// chunk is <= path.  view_start is non-decreasing; a view without a pass in
+// the chunk has an empty range (its start is the next view's), so the last
+// view at or below `path` is the one that holds it.
+__device__ __forceinline__ uint32_t view_of_path(const FrameArgs& A, uint32_t path) {
+  uint32_t lo = 0, hi = A.ncams - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (A.view_start[mid] <= path) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Primary rays of the chunk of passes [p0, p1): view v's pass p at paths
+// view_start[v] + (p - p0) * pixels(v) + pixel.
+__global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1, uint32_t n) {
   const uint32_t path = blockIdx.x * kBlock + threadIdx.x;
   if (path == 0) A.counts[0] = n;
   if (path >= n) return;
-  const uint32_t pass = p0 + path / A.total_pixels, gp = path % A.total_pixels;
-  const CameraRec& C = A.cams[find_camera(A, gp)];
-  const uint32_t pix = gp - C.pixel_offset;
-  const uint64_t cseed = A.seeds[A.st->seed_cursor + C.seed_slot];
+  const uint32_t v = view_of_path(A, path);
+  const CameraRec& C = A.cams[v];
+  const uint32_t npix = C.w * C.h;
+  const uint32_t local = path - A.view_start[v];
+  const uint32_t pass = p0 + local / npix, pix = local % npix;
+  const SceneSeeds& SS = A.sseeds[C.scene];
+  const uint64_t cseed = SS.seeds[*SS.cursor + C.seed_slot];
   const uint64_t base = A.rng_mode == 1 ? per_item_seed(cseed, pass) : cseed;
   Rng r(per_item_seed(base, pix));
   float jx = r.next_float() - 0.5f, jy = r.next_float() - 0.5f;
@@ -387,13 +444,15 @@ __global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1) {
 // that ends a path.  k_cg_lookup overwrites the first float4 with the
 // layer's radiance contribution.  Unused slots of an entry's range are
 // kRecNone with zero contribution.
+// The index word also holds the record's scene: index (27 bits) | scene
+// << 27 | kind << 30.
 enum : uint32_t { kRecSurfel = 0, kRecMesh = 1, kRecNone = 2 };
-constexpr uint32_t kRecIndexMask = 0x3FFFFFFFu;
+constexpr uint32_t kRecIndexMask = 0x07FFFFFFu;
 
 __device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float w, V3 nrm, uint32_t idx,
-                                           uint32_t kind) {
+                                           uint32_t kind, uint32_t sid) {
   q[2 * (size_t)r] = make_float4(pos.x, pos.y, pos.z, w);
-  q[2 * (size_t)r + 1] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(idx | (kind << 30)));
+  q[2 * (size_t)r + 1] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(idx | (sid << 27) | (kind << 30)));
 }
 
 // Round step 1: one lane per queue entry (a live path).
@@ -401,12 +460,14 @@ __device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float 
 // its closest mesh hit and its surfel walk's record, whose limit is the
 // mesh distance plus intersect_scene's margin.
 __global__ void k_cg_mesh(FrameArgs A, uint32_t round) {
-  const SceneView& S = A.scene;
   const uint32_t n = A.counts[round];
   if (blockIdx.x == 0 && threadIdx.x == 0) A.st->walk_next = 0u;
   const RayRec* __restrict__ in = A.paths[round & 1];
   for (uint32_t slot = blockIdx.x * kBlock + threadIdx.x; slot < n; slot += gridDim.x * kBlock) {
-    const V3 o = xyz(in[slot].o), d = xyz(in[slot].d);
+    const float4 ro = in[slot].o;
+    const uint32_t sid = A.cams[view_of_path(A, __float_as_uint(ro.w))].scene;
+    const SceneView& S = A.scenes.s[sid];
+    const V3 o = xyz(ro), d = xyz(in[slot].d);
     const V3 invw = safe_inv(d);
     float best_m;
     const Hit hm = intersect_meshes(S, o, d, invw, best_m);
@@ -418,7 +479,7 @@ __global__ void k_cg_mesh(FrameArgs A, uint32_t round) {
     A.mhit[slot] = make_float4(hm.pos.x, hm.pos.y, hm.pos.z, __int_as_float(hm.inst));
     const V3 dd = normalize(d);
     A.walk[2 * (size_t)slot] = make_float4(o.x, o.y, o.z, limit);
-    A.walk[2 * (size_t)slot + 1] = make_float4(dd.x, dd.y, dd.z, 0.0f);
+    A.walk[2 * (size_t)slot + 1] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(sid));
   }
 }
 
@@ -426,16 +487,23 @@ __global__ void k_cg_mesh(FrameArgs A, uint32_t round) {
 // lanes take the next queue entries every kRefillSteps node visits once
 // their walk has ended (as k_adj_walk does for the adjoint's closest hits).
 // A walk ends with one store of its hit count and surfels.
-template <int K>
-__global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_walk(FrameArgs A, uint32_t round) {
+// kMulti: the call renders several scenes (each lane's scene from its walk
+// record); a one-scene call reads the table's first entry, whose fields the
+// compiler takes straight from the kernel parameters.
+// kThreads: threads per block (the autotuner's choice of 64, 128 or 256);
+// the register budget per thread stays the one of kRoundMinBlocks blocks
+// of kBlock threads.
+template <int K, bool kMulti, int kThreads>
+__global__ void __launch_bounds__(kThreads, kRoundMinBlocks * (kBlock / kThreads))
+    k_cg_walk(FrameArgs A, uint32_t round) {
   extern __shared__ TravNode s_top[];
-  stage_top_nodes(A.scene, s_top);
-  const SceneView& S = A.scene;
+  stage_top_nodes(A.scenes, s_top);
   const uint32_t n = A.counts[round];
   const int lane = threadIdx.x & 31;
-  TravStack stk(s_top, S.top_nodes);
+  TravStack stk(s_top, A.scenes.n * A.scenes.staged);
   KHitWalk<K> w;
   TraceCounters ctr{0, 0};
+  uint32_t sid = 0;          // scene of this lane's walk
   uint32_t cur = kInvalid;   // queue entry of this lane's walk
   bool more = true;          // uniform in the warp: the cursor has entries left
   for (;;) {
@@ -452,6 +520,7 @@ __global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_walk(FrameArgs A
           const float4 wa = A.walk[2 * (size_t)t], wb = A.walk[2 * (size_t)t + 1];
           if (wa.w >= 0.0f) {
             cur = t;
+            if (kMulti) sid = __float_as_uint(wb.w);
             w.init(xyz(wa), xyz(wb), 1e-5f, wa.w);
           }
         }
@@ -461,8 +530,12 @@ __global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_walk(FrameArgs A
       if (!more) break;
       continue;
     }
-    for (int it = 0; it < kRefillSteps && cur != kInvalid; ++it) {
-      if (w.step(S, s_top, stk, ctr, A.st)) continue;
+    for (int it = 0; it < kRefillSteps; ++it) {
+      if (!__any_sync(0xffffffffu, cur != kInvalid)) break;
+      const uint32_t sc = kMulti ? sid : 0u;
+      if (warp_step(w, cur != kInvalid, A.scenes.s[sc], s_top + sc * A.scenes.staged, stk, ctr, A.st) ||
+          cur == kInvalid)
+        continue;
       uint32_t rw[kKHitWords];
       rw[0] = w.count;
 #pragma unroll
@@ -485,7 +558,6 @@ __global__ void __launch_bounds__(kBlock, kRoundMinBlocks) k_cg_walk(FrameArgs A
 // from the chained origin, and the path's end.
 template <int K>
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs A, uint32_t round) {
-  const SceneView& S = A.scene;
   const uint32_t n = A.counts[round];
   const RayRec* __restrict__ in = A.paths[round & 1];
   RayRec* __restrict__ out = A.paths[(round + 1) & 1];
@@ -503,8 +575,10 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
     Hit hm{};
     hm.inst = -1;
     V3 o{}, d{}, invw{}, dd{};
+    uint32_t sid = 0;
     if (live) {
       rec = in[slot];
+      sid = __float_as_uint(A.walk[2 * (size_t)slot + 1].w);
       o = xyz(rec.o);
       d = xyz(rec.d);
       invw = safe_inv(d);
@@ -549,6 +623,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
     float T = rec.d.w;
     uint32_t layer = __float_as_uint(rec.t.w);
     uint32_t used = 0;
+    const SceneView& S = A.scenes.s[sid];
     if (live) {
       bool ended = false, mesh_first = false;
       for (uint32_t i = 0; i < count && !ended; ++i) {
@@ -566,7 +641,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
         const float ae = __ldg(&S.sf.n[pl[i]]).w * a;
         V3 nrm = xyz(__ldg(&S.sf.cn[pl[i]]));
         if (dot(nrm, -d) < 0.0f) nrm = -nrm;
-        put_record(A.qrec, first + used, x, T * ae, nrm, pl[i], kRecSurfel);
+        put_record(A.qrec, first + used, x, T * ae, nrm, pl[i], kRecSurfel, sid);
         ++used;
         T *= (1.0f - ae);
         if (layer + 1 >= (uint32_t)kMaxLayers) {
@@ -594,14 +669,14 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
               c_em = scale(Le, T);
               flags = 1;
             } else {
-              put_record(A.qrec, first + used, h2.pos, T, hit_normal(S, h2), mi, kRecMesh);
+              put_record(A.qrec, first + used, h2.pos, T, hit_normal(S, h2), mi, kRecMesh, sid);
               ++used;
             }
           }
         }
       }
       for (uint32_t r = used; r < nslots; ++r)
-        put_record(A.qrec, first + r, v3(0.f, 0.f, 0.f), 0.f, v3(0.f, 0.f, 0.f), 0u, kRecNone);
+        put_record(A.qrec, first + r, v3(0.f, 0.f, 0.f), 0.f, v3(0.f, 0.f, 0.f), 0u, kRecNone, 0u);
       A.info_b[slot] = make_float4(c_em.x, c_em.y, c_em.z, 0.f);
     }
     // next-round queue entries for the paths that continue
@@ -630,13 +705,15 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
 // Round step 2: one warp per lookup record (warps stride over the records,
 // so in deep rounds every lookup has a warp of its own).  Lane 0 writes the
 // layer's contribution Lo * weight over the record's first float4.
+template <bool kMulti>
 __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArgs A, uint32_t round) {
   __shared__ float4 s_terms[kBlock];
-  const SceneView& S = A.scene;
+  __shared__ GatherConst s_gc[kMaxScenes];
+  if (threadIdx.x < A.scenes.n) s_gc[threadIdx.x] = gather_const(A.scenes.s[threadIdx.x].grid);
+  __syncthreads();
   const uint32_t n = A.counts[kMaxLayers + 2 + round];
   const int lane = threadIdx.x & 31;
   float4* terms = s_terms + (threadIdx.x & ~31u);
-  const GatherConst GC = gather_const(S.grid);
   const uint32_t warps = gridDim.x * (kBlock / 32);
   uint32_t queries = 0, scanned = 0;
   // lanes 0-7 hold the 8 floats of the next record, loaded one record ahead
@@ -649,12 +726,11 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArg
     const float4 ra = make_float4(field(0), field(1), field(2), field(3));
     const float4 rb = make_float4(field(4), field(5), field(6), field(7));
     const uint32_t word = __float_as_uint(rb.w);
-    const uint32_t kind = word >> 30, idx = word & kRecIndexMask;
+    const uint32_t kind = word >> 30, idx = word & kRecIndexMask, sid = kMulti ? (word >> 27) & 7u : 0u;
     if (kind == kRecNone) continue;
+    const SceneView& S = A.scenes.s[sid];
     uint32_t cnt = 0;
-    // the surfel's albedo or the mesh material, loaded before the lookup
-    // so that its latency overlaps it
-    const V3 E = gather_irradiance_warp<false>(S.grid, GC, xyz(ra), xyz(rb), terms, cnt);
+    const V3 E = gather_irradiance_warp<false>(S.grid, s_gc[sid], xyz(ra), xyz(rb), terms, cnt);
     if (lane == 0) {
       const float4 refl = kind == kRecSurfel ? __ldg(&S.sf.alb[idx]) : __ldg(&S.mesh.materials[idx]);
       ++queries;
@@ -694,16 +770,24 @@ __global__ void k_cg_compose(FrameArgs A, uint32_t round) {
   }
 }
 
-// fb += res/spp over passes [p0, p1) in pass order; the last chunk writes the
-// RAW image and the post-processed LDR image.
-__global__ void k_cg_finalize(FrameArgs A, uint32_t p0, uint32_t p1, int first, int last) {
+// fb += res/passes over the view's passes of the chunk [p0, p1), in pass
+// order; the chunk that holds a view's last pass writes its RAW image and
+// the post-processed LDR image.
+__global__ void k_cg_finalize(FrameArgs A, uint32_t p0, uint32_t p1) {
   const uint32_t gp = blockIdx.x * kBlock + threadIdx.x;
   if (gp >= A.total_pixels) return;
-  float4 f = first ? make_float4(0.f, 0.f, 0.f, 0.f) : A.fb[gp];
+  const uint32_t v = find_camera(A, gp);
+  const CameraRec& C = A.cams[v];
+  const uint32_t P = C.passes;
+  if (P == 0 || p0 >= P) return;                    // finished in an earlier chunk
+  const uint32_t npix = C.w * C.h, pix = gp - C.pixel_offset;
+  const uint32_t q1 = p1 < P ? p1 : P;
+  const bool last = q1 == P;
+  float4 f = p0 == 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : A.fb[gp];
   float fb[4] = {f.x, f.y, f.z, f.w};
-  const float inv = 1.f / (float)A.gather_passes;
-  for (uint32_t p = p0; p < p1; ++p) {
-    const float4 a = A.res[(size_t)(p - p0) * A.total_pixels + gp];
+  const float inv = 1.f / (float)P;
+  for (uint32_t p = p0; p < q1; ++p) {
+    const float4 a = A.res[(size_t)A.view_start[v] + (size_t)(p - p0) * npix + pix];
     float cur[4] = {a.x * inv, a.y * inv, a.z * inv, 1.0f * inv};
 #pragma unroll
     for (int k = 0; k < 4; ++k) fb[k] = cur[k] + fb[k];
@@ -728,7 +812,6 @@ __global__ void k_cg_finalize(FrameArgs A, uint32_t p0, uint32_t p1, int first, 
     if (A.dldi) {
       // compute_l2_grad (python/losses.py:27-45) per camera: the residual
       // over the camera's number of RGB values, in float32
-      const CameraRec& C = A.cams[find_camera(A, gp)];
       const float size = (float)(3u * C.w * C.h);
       const float* t = A.target + (size_t)A.target_channels * gp;
       *reinterpret_cast<float4*>(A.dldi + o4) =
@@ -779,29 +862,47 @@ void image_loss(const FrameArgs& a, double* partials, double* loss, cudaStream_t
   k_loss_final<<<(a.ncams + 63) / 64, 64, 0, s>>>(a, partials, kLossChunks, loss); note_launch();
 }
 
-void camera_gather(const FrameArgs& a, cudaStream_t s) {
-  if (a.total_pixels == 0) return;
-  if (a.gather_passes == 0) {
-    k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, 0, 0, 1, 1); note_launch();
-    return;
-  }
-  const uint32_t ppc = std::max<uint32_t>(1u, std::min(a.gather_passes, a.path_capacity / a.total_pixels));
+template <bool kMulti>
+static void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>& views, uint32_t* d_view_start,
+                               cudaStream_t s) {
+  FrameArgs a = a0;
+  a.view_start = d_view_start;
+  uint32_t max_passes = 0;
+  for (const CameraRec& v : views) max_passes = std::max(max_passes, v.passes);
+  // paths of the chunk of passes [p0, p1): every view's passes in it
+  auto chunk_paths = [&](uint32_t p0, uint32_t p1) {
+    uint64_t n = 0;
+    for (const CameraRec& v : views) {
+      const uint32_t q1 = std::min(p1, v.passes);
+      if (q1 > p0) n += (uint64_t)v.w * v.h * (q1 - p0);
+    }
+    return n;
+  };
   // persistent grids: every SM filled once
-  int dev = 0, sms = 148, per_sm_t = 1, per_sm_l = 1, per_sm_r = 1;
+  int dev = 0, sms = 148, per_sm_l = 1, per_sm_r = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t smem = top_smem(a.scene);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_cg_walk<kGatherHits>, kBlock, smem);
+  const int wt = a.walk_block == 64 || a.walk_block == 128 ? (int)a.walk_block : kBlock;
+  const size_t smem = top_smem(a.scenes, wt);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_cg_round<kGatherHits>, kBlock, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup, kBlock, 0);
-  const uint32_t grid_t = (uint32_t)std::max(1, sms * std::max(1, per_sm_t));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup<kMulti>, kBlock, 0);
   const uint32_t grid_r = (uint32_t)std::max(1, sms * std::max(1, per_sm_r));
   const uint32_t grid_l = (uint32_t)std::max(1, sms * std::max(1, per_sm_l));
-  for (uint32_t p0 = 0; p0 < a.gather_passes; p0 += ppc) {
-    const uint32_t p1 = std::min(a.gather_passes, p0 + ppc);
-    const uint32_t n = (p1 - p0) * a.total_pixels;
+  std::vector<uint32_t> starts(views.size());
+  for (uint32_t p0 = 0, p1 = 0; p0 < max_passes; p0 = p1) {
+    // chunks of whole passes: as many as the path capacity holds (one at least)
+    p1 = p0 + 1;
+    while (p1 < max_passes && chunk_paths(p0, p1 + 1) <= a.path_capacity) ++p1;
+    uint64_t acc = 0;
+    for (size_t v = 0; v < views.size(); ++v) {
+      starts[v] = (uint32_t)acc;
+      const uint32_t q1 = std::min(p1, views[v].passes);
+      if (q1 > p0) acc += (uint64_t)views[v].w * views[v].h * (q1 - p0);
+    }
+    const uint32_t n = (uint32_t)acc;
+    cudaMemcpyAsync(d_view_start, starts.data(), starts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(a.counts, 0, 2 * (kMaxLayers + 2) * sizeof(uint32_t), s);
-    k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1); note_launch();
+    k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1, n); note_launch();
     // every round consumes at least one layer of each live path, so
     // kMaxLayers rounds bound the walk (the layer cap ends longer ones)
     uint32_t round = 0, live = n;
@@ -809,11 +910,13 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
       for (uint32_t group = 0; group < 16 && round < (uint32_t)kMaxLayers; ++group, ++round) {
         if (a.timer) a.timer->begin(kTimeTrace, s);
         k_cg_mesh<<<grid_r, kBlock, 0, s>>>(a, round); note_launch();
-        k_cg_walk<kGatherHits><<<grid_t, kBlock, smem, s>>>(a, round); note_launch();
+        if (wt == 64) launch_walk(k_cg_walk<kGatherHits, kMulti, 64>, 64, a, round, smem, ~0u, s);
+        else if (wt == 128) launch_walk(k_cg_walk<kGatherHits, kMulti, 128>, 128, a, round, smem, ~0u, s);
+        else launch_walk(k_cg_walk<kGatherHits, kMulti, 256>, 256, a, round, smem, ~0u, s);
         k_cg_round<kGatherHits><<<grid_r, kBlock, 0, s>>>(a, round); note_launch();
         if (a.timer) a.timer->end(s);
         if (a.timer) a.timer->begin(kTimeLookup, s);
-        k_cg_lookup<<<grid_l, kBlock, 0, s>>>(a, round); note_launch();
+        k_cg_lookup<kMulti><<<grid_l, kBlock, 0, s>>>(a, round); note_launch();
         if (a.timer) a.timer->end(s);
         // queues only shrink, so `live` bounds the entries of every round of the group
         k_cg_compose<<<blocks_for(live), kBlock, 0, s>>>(a, round); note_launch();
@@ -822,8 +925,15 @@ void camera_gather(const FrameArgs& a, cudaStream_t s) {
       cudaMemcpyAsync(&live, a.counts + round, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
       cudaStreamSynchronize(s);
     }
-    k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1, p0 == 0, p1 == a.gather_passes); note_launch();
+    k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1); note_launch();
   }
+}
+
+void camera_gather(const FrameArgs& a, const std::vector<CameraRec>& views, uint32_t* d_view_start,
+                   cudaStream_t s) {
+  if (a.total_pixels == 0 || views.empty()) return;
+  if (a.scenes.n > 1) camera_gather_impl<true>(a, views, d_view_start, s);
+  else camera_gather_impl<false>(a, views, d_view_start, s);
 }
 
 // ------------------------------------------------------------- adjoint
@@ -912,11 +1022,15 @@ __device__ __forceinline__ uint32_t spread9(uint32_t v) {
   return v;
 }
 
+// Sort key of a ray: (direction octant, 27-bit Morton code of the origin in
+// its scene's grid box); with several scenes, (scene, octant, 24-bit Morton
+// code), so that the rays of one scene stay together.
 __global__ void k_adj_keys(AdjointArgs A, uint32_t parity) {
   const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
   if (t >= A.st->active[parity]) return;
   const RayRec ry = A.qb.q[parity][t];
-  const GridView& G = A.scene.grid;
+  const uint32_t sid = A.cams[A.jobs[__float_as_uint(ry.d.w) >> 8].cam].scene;
+  const GridView& G = A.scenes.s[sid].grid;
   uint32_t q[3];
   const float o[3] = {ry.o.x, ry.o.y, ry.o.z}, lo[3] = {G.origin.x, G.origin.y, G.origin.z},
               ext[3] = {G.cell.x * G.res[0], G.cell.y * G.res[1], G.cell.z * G.res[2]};
@@ -926,7 +1040,8 @@ __global__ void k_adj_keys(AdjointArgs A, uint32_t parity) {
     q[k] = (uint32_t)fminf(fmaxf(f, 0.0f), 511.0f);
   }
   const uint32_t oct = (ry.d.x < 0.f ? 1u : 0u) | (ry.d.y < 0.f ? 2u : 0u) | (ry.d.z < 0.f ? 4u : 0u);
-  A.sort_keys[t] = (oct << 27) | (spread9(q[0]) << 2) | (spread9(q[1]) << 1) | spread9(q[2]);
+  const uint32_t morton = (spread9(q[0]) << 2) | (spread9(q[1]) << 1) | spread9(q[2]);
+  A.sort_keys[t] = A.scenes.n > 1 ? (sid << 27) | (oct << 24) | (morton >> 3) : (oct << 27) | morton;
   A.perm[t] = t;
 }
 
@@ -953,8 +1068,10 @@ __global__ void k_adj_mesh(AdjointArgs A, uint32_t parity, int sorted) {
   if (t == 0) A.st->walk_next = 0u;
   if (t >= n_in) return;
   const uint32_t slot = sorted ? A.perm[t] : t;
-  const SceneView& S = A.scene;
-  const V3 o = xyz(A.qb.q[parity][slot].o), d = xyz(A.qb.q[parity][slot].d);
+  const float4 rd = A.qb.q[parity][slot].d;
+  const uint32_t sid = A.cams[A.jobs[__float_as_uint(rd.w) >> 8].cam].scene;
+  const SceneView& S = A.scenes.s[sid];
+  const V3 o = xyz(A.qb.q[parity][slot].o), d = xyz(rd);
   const V3 invw = safe_inv(d);
   float best;
   const Hit h = intersect_meshes(S, o, d, invw, best);
@@ -966,8 +1083,9 @@ __global__ void k_adj_mesh(AdjointArgs A, uint32_t parity, int sorted) {
   A.hits[3 * (size_t)slot + 1] = make_float4(h.alpha, __int_as_float(h.inst), __uint_as_float(h.prim), 0.0f);
   A.hits[3 * (size_t)slot + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const V3 dd = normalize(d);
+  // the slot (below 2^24) with the scene in the top bits
   A.walkq[2 * (size_t)t] = make_float4(o.x, o.y, o.z, limit);
-  A.walkq[2 * (size_t)t + 1] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(slot));
+  A.walkq[2 * (size_t)t + 1] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(slot | (sid << 24)));
 }
 
 // Step 2: the closest-surfel walks (surfel_closest's) of the rays that
@@ -978,15 +1096,17 @@ __global__ void k_adj_mesh(AdjointArgs A, uint32_t parity, int sorted) {
 // while walks of very different lengths end.  A walk that finds a surfel
 // ends with one store of it and its distance in the ray's hit record; the
 // hits do not depend on the schedule.
-__global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs A, uint32_t parity) {
+template <bool kMulti, int kThreads>
+__global__ void __launch_bounds__(kThreads, kWalkMinBlocks * (kBlock / kThreads))
+    k_adj_walk(AdjointArgs A, uint32_t parity) {
   extern __shared__ TravNode s_top[];
-  stage_top_nodes(A.scene, s_top);
-  const SceneView& S = A.scene;
+  stage_top_nodes(A.scenes, s_top);
   const uint32_t n_in = A.st->active[parity];
   const int lane = threadIdx.x & 31;
-  TravStack stk(s_top, S.top_nodes);
+  TravStack stk(s_top, A.scenes.n * A.scenes.staged);
   ClosestWalk w;
   TraceCounters ctr{0, 0};
+  uint32_t sid = 0;          // scene of this lane's ray
   uint32_t cur = kInvalid;   // queue slot of this lane's ray
   bool more = true;          // uniform in the warp: the cursor has rays left
   for (;;) {
@@ -1002,7 +1122,9 @@ __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs
         if (t < n_in) {
           const float4 wa = A.walkq[2 * (size_t)t], wb = A.walkq[2 * (size_t)t + 1];
           if (wa.w >= 0.0f) {
-            cur = __float_as_uint(wb.w);
+            const uint32_t word = __float_as_uint(wb.w);
+            cur = word & 0x00FFFFFFu;
+            if (kMulti) sid = word >> 24;
             w.init(xyz(wa), xyz(wb), 1e-5f, wa.w);
           }
         }
@@ -1012,8 +1134,12 @@ __global__ void __launch_bounds__(kBlock, kWalkMinBlocks) k_adj_walk(AdjointArgs
       if (!more) break;
       continue;
     }
-    for (int it = 0; it < kRefillSteps && cur != kInvalid; ++it) {
-      if (w.step(S, s_top, stk, ctr, A.st)) continue;
+    for (int it = 0; it < kRefillSteps; ++it) {
+      if (!__any_sync(0xffffffffu, cur != kInvalid)) break;
+      const uint32_t sc = kMulti ? sid : 0u;
+      if (warp_step(w, cur != kInvalid, A.scenes.s[sc], s_top + sc * A.scenes.staged, stk, ctr, A.st) ||
+          cur == kInvalid)
+        continue;
       if (w.hit) A.hits[3 * (size_t)cur + 2] = make_float4(__uint_as_float(w.prim), w.best, 1.0f, 0.0f);
       cur = kInvalid;
     }
@@ -1032,8 +1158,8 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
   bool alive = false, has_ev = false;
   uint32_t job = kInvalid;
   if (slot < n_in) {
-    const SceneView& S = A.scene;
     const float4 ro = A.qb.q[parity][slot].o, rd = A.qb.q[parity][slot].d;
+    const SceneView& S = A.scenes.s[A.cams[A.jobs[__float_as_uint(rd.w) >> 8].cam].scene];
     const V3 d = xyz(rd);
     Hit h;
     {
@@ -1097,7 +1223,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
         else if (is_mesh) mat = __ldg(&S.mesh.material[h.inst]);
         ev.a = f4(h.pos, refl ? h.alpha : pa.w);
         ev.b = f4(on, refl ? pdf : endcos);
-        ev.c = f4(pthr, 0.f);
+        ev.c = f4(pthr, __uint_as_float(job));
         ev.d = make_uint4(pkind, refl ? h.prim : pc.x, mat, pc.z);
         // the target surfel's hit: the endpoint (reflect) or the pending
         // null surfel, on the same line (a null continuation keeps d)
@@ -1149,7 +1275,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
           if (alive && bounce_index == 0) {
             ev.a = f4(h.pos, h.alpha);
             ev.b = f4(on, 0.f);
-            ev.c = f4(divs(thr, A.q_reflect), 0.f);
+            ev.c = f4(divs(thr, A.q_reflect), __uint_as_float(job));
             ev.d = make_uint4(kKindProjection, h.prim, kInvalid, pixel);
             ev.e = f4(h.pos, 0.f);
             ev.f = f4(normalize(d), 0.f);
@@ -1168,6 +1294,8 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_adj_bounce(AdjointA
           alive = russian_roulette(r, bounce, nt, A.rr_start);
         }
       }
+      // a view's rays end after its own number of bounces
+      if (alive && bounce >= A.cams[A.jobs[job].cam].depth) alive = false;
       if (alive) A.qb.stage[slot] = make_ray(no, nd, nt, path, bounce | (job << 8), pixel);
       if (has_ev) A.ev.stage[slot] = ev;
     }
@@ -1236,64 +1364,95 @@ __device__ __forceinline__ AlphaGrad alpha_grad(const SurfelView& S, uint32_t k,
   return g;
 }
 
-// launchAdjointTransportKernel (AdjointKernels.cpp:389-509).  One warp per
-// gradient event (warps stride over the event list): the warp does the
-// photon lookup of the event's end point together (gather_irradiance_warp)
-// and lane 0 adds the event's opacity-gradient term with one atomicAdd.
+// launchAdjointTransportKernel (AdjointKernels.cpp:389-509).  A warp takes
+// the events of a tile of 32 (warps stride over the tiles), lane i the
+// i-th: every lane loads its own event record (one coalesced load), the
+// warp does the photon lookups of the tile's events one after another
+// (gather_irradiance_warp, each lookup's 32 photon rounds spread over the
+// lanes) and the lane of each event keeps its irradiance; then every lane
+// evaluates its own event's terms (the opacity term as the reference
+// computes it; with gradients = "all" also the other six groups) at the
+// same time.  Events with the same target surfel are added up inside the
+// warp before they reach memory (__match_any_sync groups the lanes by
+// scene and target; the lowest lane of a group sums the group's terms in lane order
+// from shared memory), and each group's terms go out with one atomicAdd
+// per component, the components of one group spread over lanes.
+constexpr int kTransportTerms = 16;   // opacity, beta, position 3, tangent_u 3, tangent_v 3, scale 2, albedo 3 - 1
+
 __global__ void __launch_bounds__(kBlock, kTransportMinBlocks) k_transport(AdjointArgs A) {
-  __shared__ float4 s_terms[kBlock];
+  __shared__ float4 s_terms[kBlock];                        // per warp: the lookups' row compaction
+  __shared__ float s_val[kBlock / 32][kTransportTerms + 1][33];   // per warp: the lanes' terms
+  __shared__ GatherConst s_gc[kMaxScenes];
+  if (threadIdx.x < A.scenes.n) s_gc[threadIdx.x] = gather_const(A.scenes.s[threadIdx.x].grid);
+  __syncthreads();
   const uint32_t count = A.st->event_count;
-  const SceneView& S = A.scene;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float4* terms = s_terms + (threadIdx.x & ~31u);
-  const GatherConst GC = gather_const(S.grid);
   const uint32_t warps = gridDim.x * (kBlock / 32);
+  const uint32_t tiles = (count + 31u) / 32u;
+  const int nterms = A.all_grads ? kTransportTerms + 1 : 1;
   uint32_t events = 0, queries = 0, scanned = 0;
-  // lanes 0-23 hold the 24 words of the next event, loaded one event ahead
-  constexpr int kWords = sizeof(EventRec) / 4;
-  uint32_t e = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-  float pre = (e < count && lane < kWords) ? reinterpret_cast<const float*>(A.ev.list + e)[lane] : 0.f;
-  for (; e < count; e += warps) {
-    const float cur = pre;
-    if (e + warps < count && lane < kWords) pre = reinterpret_cast<const float*>(A.ev.list + e + warps)[lane];
-    auto field = [&](int f) { return __shfl_sync(0xffffffffu, cur, f); };
+  for (uint32_t tile = blockIdx.x * (kBlock / 32) + wid; tile < tiles; tile += warps) {
+    const uint32_t e = tile * 32u + lane;
+    const bool valid = e < count;
+    // the lookup's point and normal and the event's kind and indices now;
+    // the throughput (and the alpha-gradient point) after the lookups
+    const EventRec* src = A.ev.list + (valid ? e : 0u);
     EventRec ev;
-    ev.a = make_float4(field(0), field(1), field(2), field(3));
-    ev.b = make_float4(field(4), field(5), field(6), field(7));
-    ev.c = make_float4(field(8), field(9), field(10), field(11));
-    ev.d = make_uint4(__float_as_uint(field(12)), __float_as_uint(field(13)), __float_as_uint(field(14)),
-                      __float_as_uint(field(15)));
-    ev.e = make_float4(field(16), field(17), field(18), field(19));
-    ev.f = make_float4(field(20), field(21), field(22), field(23));
+    uint32_t sid = 0, passes = 1;   // the event's scene and its view's passes
+    if (valid) {
+      ev.a = src->a;
+      ev.b = src->b;
+      ev.d = src->d;
+      const CameraRec& C = A.cams[A.jobs[__float_as_uint(src->c.w)].cam];
+      sid = C.scene;
+      passes = C.passes;
+    } else {
+      ev.a = ev.b = make_float4(0.f, 0.f, 0.f, 0.f);
+      ev.d = make_uint4(kInvalid, kInvalid, kInvalid, 0u);
+    }
     const uint32_t kind = ev.d.x;
     // a null event ending on a surfel has no material (the reference reads
     // materials[0xFFFFFFFF], AdjointKernels.cpp:446-447): no contribution
-    const bool need = kind == kKindProjection || kind == kKindReflect || (kind == kKindNull && ev.d.z != kInvalid);
+    const bool need =
+        valid && (kind == kKindProjection || kind == kKindReflect || (kind == kKindNull && ev.d.z != kInvalid));
     V3 E = v3(0.f, 0.f, 0.f);
-    uint32_t cnt = 0;
-    if (need) E = gather_irradiance_warp<true>(S.grid, GC, xyz(ev.a), xyz(ev.b), terms, cnt);
-    if (lane == 0) {
-      ++events;
-      if (need) {
-        ++queries;
+    for (unsigned m = __ballot_sync(0xffffffffu, need); m; m &= m - 1u) {
+      const int j = __ffs(m) - 1;
+      const V3 xj = v3(__shfl_sync(0xffffffffu, ev.a.x, j), __shfl_sync(0xffffffffu, ev.a.y, j),
+                       __shfl_sync(0xffffffffu, ev.a.z, j));
+      const V3 nj = v3(__shfl_sync(0xffffffffu, ev.b.x, j), __shfl_sync(0xffffffffu, ev.b.y, j),
+                       __shfl_sync(0xffffffffu, ev.b.z, j));
+      const uint32_t sj = __shfl_sync(0xffffffffu, sid, j);
+      uint32_t cnt = 0;
+      const V3 Ej = gather_irradiance_warp<true>(A.scenes.s[sj].grid, s_gc[sj], xj, nj, terms, cnt);
+      if (lane == j) {
+        E = Ej;
         scanned += cnt;
+        ++queries;
       }
-      const V3 thr = xyz(ev.c);
-      float g = 0.f;       // opacity term, as the reference computes it
-      float W = 0.f;       // the event's weight: g = W * alpha_geom
-      V3 dalb = v3(0.f, 0.f, 0.f);
-      uint32_t target = kInvalid;
+    }
+    // this lane's event
+    const SceneView& S = A.scenes.s[sid];
+    const float inv_spp = 1.0f / (float)passes;
+    float g = 0.f;        // opacity term, as the reference computes it
+    float W = 0.f;        // the event's weight: g = W * alpha_geom
+    V3 dalb = v3(0.f, 0.f, 0.f);
+    uint32_t target = kInvalid;
+    if (valid) {
+      ++events;
+      const V3 thr = xyz(src->c);
       if (kind == kKindProjection) {
         target = ev.d.y;
         const float4 al = __ldg(&S.sf.alb[target < S.sf.count ? target : 0u]);
         V3 fr = scale(scale(xyz(al), al.w), kInvPi);
         V3 Lo = mul(fr, E);
-        g = vsum(mul(scale(thr, ev.a.w), Lo)) * A.inv_spp;
+        g = vsum(mul(scale(thr, ev.a.w), Lo)) * inv_spp;
         if (A.all_grads && target < S.sf.count) {
-          W = vsum(mul(thr, Lo)) * A.inv_spp;
+          W = vsum(mul(thr, Lo)) * inv_spp;
           // d/d albedo of eta alpha_geom (alpha_r albedo / pi) E, per channel
           const float eta = __ldg(&S.sf.n[target]).w;
-          dalb = scale(mul(thr, E), eta * ev.a.w * al.w * kInvPi * A.inv_spp);
+          dalb = scale(mul(thr, E), eta * ev.a.w * al.w * kInvPi * inv_spp);
         }
       } else if (kind == kKindNull) {
         target = ev.d.y;
@@ -1306,49 +1465,85 @@ __global__ void __launch_bounds__(kBlock, kTransportMinBlocks) k_transport(Adjoi
             Le = scale(scale(xyz(mat), mat.w / (kPi * area)), ev.b.w);
           }
           V3 Lo = Le + Lr;
-          g = vsum(mul(scale(thr, -ev.a.w * A.null_scale), Lo)) * A.inv_spp;
-          if (A.all_grads) W = -vsum(mul(thr, Lo)) * A.null_scale * A.inv_spp;
+          g = vsum(mul(scale(thr, -ev.a.w * A.null_scale), Lo)) * inv_spp;
+          if (A.all_grads) W = -vsum(mul(thr, Lo)) * A.null_scale * inv_spp;
         }
       } else if (kind == kKindReflect) {
         target = ev.d.y;
         const float4 mat = __ldg(&S.mesh.materials[ev.d.z]);
         V3 Lo = scale(mul(E, xyz(mat)), kInvPi);
         V3 p = divs(thr, ev.b.w);
-        g = vsum(scale(mul(p, Lo), ev.a.w)) * A.inv_spp;
-        if (A.all_grads) W = vsum(mul(p, Lo)) * A.inv_spp;
+        g = vsum(scale(mul(p, Lo), ev.a.w)) * inv_spp;
+        if (A.all_grads) W = vsum(mul(p, Lo)) * inv_spp;
       }
       if (target != kInvalid && target >= S.sf.count) {
         flag_error(A.st, kErrBounds);
-      } else if (target != kInvalid) {
-        atomicAdd(&A.grad_opacity[target], g);
-        if (A.all_grads && W != 0.f) {
-          const AlphaGrad ag = alpha_grad(S.sf, target, xyz(ev.e), xyz(ev.f));
-          const PointsDev& G = A.grads;
-          atomicAdd(&G.beta[target], W * ag.beta);
-          atomicAdd(&G.position[3 * target + 0], W * ag.pos.x);
-          atomicAdd(&G.position[3 * target + 1], W * ag.pos.y);
-          atomicAdd(&G.position[3 * target + 2], W * ag.pos.z);
-          atomicAdd(&G.tangent_u[3 * target + 0], W * ag.tu.x);
-          atomicAdd(&G.tangent_u[3 * target + 1], W * ag.tu.y);
-          atomicAdd(&G.tangent_u[3 * target + 2], W * ag.tu.z);
-          atomicAdd(&G.tangent_v[3 * target + 0], W * ag.tv.x);
-          atomicAdd(&G.tangent_v[3 * target + 1], W * ag.tv.y);
-          atomicAdd(&G.tangent_v[3 * target + 2], W * ag.tv.z);
-          atomicAdd(&G.scale[2 * target + 0], W * ag.su);
-          atomicAdd(&G.scale[2 * target + 1], W * ag.sv);
+        target = kInvalid;
+      }
+      if (target != kInvalid && A.debug_opacity) {
+        float* px = A.debug_opacity + 4 * (size_t)ev.d.w;
+        atomicAdd(px + 0, g);
+        atomicAdd(px + 1, g);
+        atomicAdd(px + 2, g);
+        px[3] = 1.0f;
+      }
+    }
+    // the lane's terms, in the order of kTransportTerms
+    float (*val)[33] = s_val[wid];
+    val[0][lane] = g;
+    if (A.all_grads) {
+      AlphaGrad ag{};
+      if (target != kInvalid && W != 0.f) ag = alpha_grad(S.sf, target, xyz(src->e), xyz(src->f));
+      const bool w0 = target != kInvalid && W != 0.f;
+      val[1][lane] = w0 ? W * ag.beta : 0.f;
+      val[2][lane] = w0 ? W * ag.pos.x : 0.f;
+      val[3][lane] = w0 ? W * ag.pos.y : 0.f;
+      val[4][lane] = w0 ? W * ag.pos.z : 0.f;
+      val[5][lane] = w0 ? W * ag.tu.x : 0.f;
+      val[6][lane] = w0 ? W * ag.tu.y : 0.f;
+      val[7][lane] = w0 ? W * ag.tu.z : 0.f;
+      val[8][lane] = w0 ? W * ag.tv.x : 0.f;
+      val[9][lane] = w0 ? W * ag.tv.y : 0.f;
+      val[10][lane] = w0 ? W * ag.tv.z : 0.f;
+      val[11][lane] = w0 ? W * ag.su : 0.f;
+      val[12][lane] = w0 ? W * ag.sv : 0.f;
+      val[13][lane] = dalb.x;
+      val[14][lane] = dalb.y;
+      val[15][lane] = dalb.z;
+      val[16][lane] = 0.f;
+    }
+    __syncwarp();
+    // same-target lanes form a group; its lowest lane sums the group's terms
+    const unsigned grp = __match_any_sync(0xffffffffu, ((unsigned long long)sid << 32) | target);
+    const bool leader = target != kInvalid && lane == __ffs(grp) - 1;
+    if (leader && __popc(grp) > 1) {
+      for (int c = 0; c < nterms; ++c) {
+        float acc = 0.f;
+        for (unsigned r = grp; r; r &= r - 1u) acc += val[c][__ffs(r) - 1];
+        val[c][lane] = acc;
+      }
+    }
+    __syncwarp();
+    // one atomicAdd per component of each group: the group leaders in turn,
+    // the components over lanes
+    for (unsigned lm = __ballot_sync(0xffffffffu, leader); lm; lm &= lm - 1u) {
+      const int L = __ffs(lm) - 1;
+      const uint32_t t = __shfl_sync(0xffffffffu, target, L);
+      const SceneGrads& G = A.sgrads[__shfl_sync(0xffffffffu, sid, L)];
+      if (lane < nterms) {
+        const float v = val[lane][L];
+        float* dst = nullptr;
+        switch (lane) {
+          case 0: dst = G.opacity + t; break;
+          case 1: dst = G.all.beta + t; break;
+          case 2: case 3: case 4: dst = G.all.position + 3 * (size_t)t + (lane - 2); break;
+          case 5: case 6: case 7: dst = G.all.tangent_u + 3 * (size_t)t + (lane - 5); break;
+          case 8: case 9: case 10: dst = G.all.tangent_v + 3 * (size_t)t + (lane - 8); break;
+          case 11: case 12: dst = G.all.scale + 2 * (size_t)t + (lane - 11); break;
+          case 13: case 14: case 15: dst = G.all.albedo + 3 * (size_t)t + (lane - 13); break;
+          default: break;
         }
-        if (A.all_grads && kind == kKindProjection) {
-          atomicAdd(&A.grads.albedo[3 * target + 0], dalb.x);
-          atomicAdd(&A.grads.albedo[3 * target + 1], dalb.y);
-          atomicAdd(&A.grads.albedo[3 * target + 2], dalb.z);
-        }
-        if (A.debug_opacity) {
-          float* px = A.debug_opacity + 4 * (size_t)ev.d.w;
-          atomicAdd(px + 0, g);
-          atomicAdd(px + 1, g);
-          atomicAdd(px + 2, g);
-          px[3] = 1.0f;
-        }
+        if (dst && (lane == 0 || v != 0.f)) atomicAdd(dst, v);
       }
     }
     __syncwarp();
@@ -1374,23 +1569,31 @@ void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cuda
     radix_sort_pairs(a.sort_keys, a.perm, a.sort_keys_tmp, a.perm_tmp, &a.st->active[parity], npaths, 30,
                      a.sort_temp, s);
   }
-  int dev = 0, sms = 148, per_sm = 1, per_sm_w = 1;
+  int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t smem = top_smem(a.scene);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_w, k_adj_walk, kBlock, smem);
-  // the walk's persistent grid: every SM filled once, no more blocks than rays need
-  const uint32_t grid_w = std::min<uint32_t>(nb, (uint32_t)std::max(1, sms * std::max(1, per_sm_w)));
+  const bool multi = a.scenes.n > 1;
+  const int wt = a.walk_block == 64 || a.walk_block == 128 ? (int)a.walk_block : kBlock;
+  const size_t smem = top_smem(a.scenes, wt);
   if (a.timer) a.timer->begin(kTimeAdjBounce, s);
   k_adj_mesh<<<nb, kBlock, 0, s>>>(a, parity, sorted); note_launch();
-  k_adj_walk<<<grid_w, kBlock, smem, s>>>(a, parity); note_launch();
+  // the walk's persistent grid: every SM filled once, no more blocks than rays need
+  if (multi) {
+    if (wt == 64) launch_walk(k_adj_walk<true, 64>, 64, a, parity, smem, nb, s);
+    else if (wt == 128) launch_walk(k_adj_walk<true, 128>, 128, a, parity, smem, nb, s);
+    else launch_walk(k_adj_walk<true, 256>, 256, a, parity, smem, nb, s);
+  } else {
+    if (wt == 64) launch_walk(k_adj_walk<false, 64>, 64, a, parity, smem, nb, s);
+    else if (wt == 128) launch_walk(k_adj_walk<false, 128>, 128, a, parity, smem, nb, s);
+    else launch_walk(k_adj_walk<false, 256>, 256, a, parity, smem, nb, s);
+  }
   k_adj_bounce<<<nb, kBlock, 0, s>>>(a, parity, bounce); note_launch();
   if (a.timer) a.timer->end(s);
   k_adj_tile_counts<<<nb, kBlock, 0, s>>>(a, parity); note_launch();
   k_queue_scan<<<1, 1024, 0, s>>>(a.st, a.qb.tile_counts, a.qb.tile_offsets, parity, 0, 0, 1, 0); note_launch();
   k_job_scan<<<1, kMaxJobsPerBatch, 0, s>>>(a, parity); note_launch();
   k_queue_scatter<1><<<nb, kBlock, 0, s>>>(a.st, a.qb, parity, 0, 0, PhotonStore{}, a.ev); note_launch();
-  // one warp per event: a grid that fills every SM once
+  // a warp per tile of 32 events: a grid that fills every SM once
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport, kBlock, 0);
   if (a.timer) a.timer->begin(kTimeTransport, s);
   k_transport<<<(uint32_t)std::max(1, sms * std::max(1, per_sm)), kBlock, 0, s>>>(a); note_launch();

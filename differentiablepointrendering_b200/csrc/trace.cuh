@@ -191,30 +191,67 @@ struct TravStack {
   }
 };
 
-// The closest-hit walk over the surfel LBVH, one node visit per step(), so
-// that a persistent kernel can hand a lane a new ray between steps.  After
-// init(), step() returns true while the walk goes on; `hit`, `prim` and
-// `best` then hold the closest surfel with t in (tmin, limit).
-struct ClosestWalk {
+// One walk over the surfel LBVH, one step() at a time, so that a persistent
+// kernel can hand a lane a new ray between steps.  A walk's position is a
+// child word with its entry distance: an inner node (a step loads it, tests
+// its two child boxes, continues with the nearer child hit and pushes the
+// farther) or a leaf (a step tests its surfels).  Leaves go through the same
+// near-to-far order and stack as inner nodes, so that a warp can run the
+// steps of its lanes that stand at leaves together, apart from the inner
+// visits (at_leaf()): the surfel test and the node visit are long and
+// different code, and a lane that tested its leaf inside the node visit
+// kept the other lanes of its warp waiting.  `Leaf` is the walk's leaf
+// test (a closest hit, or the K closest hits).
+template <class Leaf>
+struct WalkBase {
   V3 o, d, inv;
-  float tmin, best;
-  uint32_t prim, node, visit;
+  float tmin;
+  uint32_t node, visit;
+  float node_t;
   int sp;
-  bool hit;
-  __device__ __forceinline__ void init(V3 o_, V3 d_, float tmin_, float limit) {
+  __device__ __forceinline__ void start(V3 o_, V3 d_, float tmin_) {
     o = o_;
     d = d_;
     inv = safe_inv(d_);
     tmin = tmin_;
-    best = limit;
-    prim = 0;
-    node = 0;
+    node = 0;        // the root, an inner node
+    node_t = 0.0f;
     visit = 0;
     sp = 0;
-    hit = false;
+  }
+  __device__ __forceinline__ bool at_leaf() const { return (node & kLeafFlag) != 0u; }
+  // the next position from the stack whose box the ray can still enter
+  __device__ __forceinline__ bool pop(const TravStack& stk, float best) {
+    while (sp > 0) {
+      --sp;
+      uint32_t sn;
+      float st_t;
+      stk.get(sp, sn, st_t);
+      if (st_t <= best) {
+        node = sn;
+        node_t = st_t;
+        return true;
+      }
+    }
+    return false;
   }
   __device__ __forceinline__ bool step(const SceneView& S, const TravNode* __restrict__ smem_top, TravStack& stk,
                                        TraceCounters& ctr, RunState* st) {
+    Leaf& self = *static_cast<Leaf*>(this);
+    if (at_leaf()) {
+      if (node_t <= self.best) {
+        const uint32_t f0 = node & 0x0FFFFFFFu, cnt = ((node >> 28) & 7u) + 1u;
+        if (f0 + cnt > S.sf.count) {
+          flag_error(st, kErrBounds);
+        } else {
+          for (uint32_t j = 0; j < cnt; ++j) {
+            ctr.tests++;
+            self.test(S.sf, f0 + j);
+          }
+        }
+      }
+      return pop(stk, self.best);
+    }
     // an acyclic tree visits each node at most once
     const uint32_t visit_cap = 2u * S.node_count + 64u;
     if (node >= S.node_count || visit > visit_cap) {
@@ -226,63 +263,61 @@ struct ClosestWalk {
     uint4 w;
     load_node(S, smem_top, node, a, b, c, w);
     ctr.nodes++;
-    float e0 = w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
-    float e1 = w.y == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, b.z, b.w, c.x, c.y, c.z, c.w, best);
-    bool h0 = entered(e0, best), h1 = entered(e1, best);
-    // leaves: test their surfels now, nearer leaf first
-    uint32_t lw[2] = {w.x, w.y};
-    bool lh[2] = {h0 && (w.x & kLeafFlag) != 0, h1 && (w.y & kLeafFlag) != 0};
-    int first = (e1 < e0) ? 1 : 0;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      int cidx = k == 0 ? first : 1 - first;
-      if (!lh[cidx]) continue;
-      uint32_t word = lw[cidx];
-      uint32_t f0 = word & 0x0FFFFFFFu, cnt = ((word >> 28) & 7u) + 1u;
-      if (f0 + cnt > S.sf.count) {
-        flag_error(st, kErrBounds);
-        continue;
-      }
-      for (uint32_t j = 0; j < cnt; ++j) {
-        float th, aa;
-        V3 xx;
-        ctr.tests++;
-        // only the distance and the surfel stay live in the walk; the hit
-        // point and alpha of the closest are evaluated after it
-        if (surfel_hit(S.sf, f0 + j, o, d, tmin, best, th, xx, aa)) {
-          best = th;
-          hit = true;
-          prim = f0 + j;
-        }
-      }
-    }
-    h0 = h0 && !(w.x & kLeafFlag) && e0 <= best;
-    h1 = h1 && !(w.y & kLeafFlag) && e1 <= best;
+    const float best = self.best;
+    const float e0 =
+        w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
+    const float e1 =
+        w.y == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, b.z, b.w, c.x, c.y, c.z, c.w, best);
+    const bool h0 = entered(e0, best), h1 = entered(e1, best);
     if (h0 && h1) {
-      uint32_t nearN = e0 <= e1 ? w.x : w.y, farN = e0 <= e1 ? w.y : w.x;
-      float farT = e0 <= e1 ? e1 : e0;
+      const bool first0 = e0 <= e1;
       if (sp < kStackDepth) {
-        stk.push(sp, farN, farT);
+        stk.push(sp, first0 ? w.y : w.x, first0 ? e1 : e0);
         ++sp;
       } else {
         flag_error(st, kErrStackOverflow);
       }
-      node = nearN;
+      node = first0 ? w.x : w.y;
+      node_t = first0 ? e0 : e1;
       return true;
     }
-    if (h0) { node = w.x; return true; }
-    if (h1) { node = w.y; return true; }
-    while (sp > 0) {
-      --sp;
-      uint32_t sn;
-      float st_t;
-      stk.get(sp, sn, st_t);
-      if (st_t <= best) {
-        node = sn;
-        return true;
-      }
+    if (h0) {
+      node = w.x;
+      node_t = e0;
+      return true;
     }
-    return false;
+    if (h1) {
+      node = w.y;
+      node_t = e1;
+      return true;
+    }
+    return pop(stk, best);
+  }
+};
+
+// Closest surfel with t in (tmin, limit): after start(), step() returns
+// true while the walk goes on; `hit`, `prim` and `best` then hold the
+// closest surfel.
+struct ClosestWalk : WalkBase<ClosestWalk> {
+  float best;
+  uint32_t prim;
+  bool hit;
+  __device__ __forceinline__ void init(V3 o_, V3 d_, float tmin_, float limit) {
+    start(o_, d_, tmin_);
+    best = limit;
+    prim = 0;
+    hit = false;
+  }
+  __device__ __forceinline__ void test(const SurfelView& sf, uint32_t i) {
+    float th, aa;
+    V3 xx;
+    // only the distance and the surfel stay live in the walk; the hit point
+    // and alpha of the closest are evaluated after it
+    if (surfel_hit(sf, i, o, d, tmin, best, th, xx, aa)) {
+      best = th;
+      hit = true;
+      prim = i;
+    }
   }
 };
 
@@ -308,114 +343,64 @@ __device__ __forceinline__ bool surfel_closest(const SceneView& S, const TravNod
 }
 
 // The K closest surfels with t in (tmin, limit) along (o, d), in increasing
-// t (ties keep the surfel found first): the traversal of ClosestWalk with
-// the culling distance of the K-th hit found so far, one node visit per
-// step().  After init(), step() returns true while the walk goes on;
-// `count` (<= K) and t_out/prim_out then hold the hits in order.
+// t (ties keep the surfel found first), with the culling distance of the
+// K-th hit found so far.  After init(), step() returns true while the walk
+// goes on; `count` (<= K) and t_out/prim_out then hold the hits in order.
 template <int K>
-struct KHitWalk {
-  V3 o, d, inv;
-  float tmin, best;   // best: t_out[K - 1] once K hits are held
-  uint32_t node, visit, count;
-  int sp;
+struct KHitWalk : WalkBase<KHitWalk<K>> {
+  float best;   // t_out[K - 1] once K hits are held
+  uint32_t count;
   float t_out[K];
   uint32_t prim_out[K];
   __device__ __forceinline__ void init(V3 o_, V3 d_, float tmin_, float limit) {
-    o = o_;
-    d = d_;
-    inv = safe_inv(d_);
-    tmin = tmin_;
+    this->start(o_, d_, tmin_);
     best = limit;
-    node = 0;
-    visit = 0;
     count = 0;
-    sp = 0;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       t_out[k] = limit;
       prim_out[k] = 0;
     }
   }
-  __device__ __forceinline__ bool step(const SceneView& S, const TravNode* __restrict__ smem_top, TravStack& stk,
-                                       TraceCounters& ctr, RunState* st) {
-    const uint32_t visit_cap = 2u * S.node_count + 64u;
-    if (node >= S.node_count || visit > visit_cap) {
-      flag_error(st, kErrBounds);
-      return false;
-    }
-    ++visit;
-    float4 a, b, c;
-    uint4 w;
-    load_node(S, smem_top, node, a, b, c, w);
-    ctr.nodes++;
-    float e0 = w.x == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, a.x, a.y, a.z, a.w, b.x, b.y, best);
-    float e1 = w.y == kEmptyChild ? __int_as_float(0x7f800000) : slab_entry(o, inv, b.z, b.w, c.x, c.y, c.z, c.w, best);
-    bool h0 = entered(e0, best), h1 = entered(e1, best);
-    uint32_t lw[2] = {w.x, w.y};
-    bool lh[2] = {h0 && (w.x & kLeafFlag) != 0, h1 && (w.y & kLeafFlag) != 0};
-    int first = (e1 < e0) ? 1 : 0;
+  __device__ __forceinline__ void test(const SurfelView& sf, uint32_t i) {
+    float th, aa;
+    V3 xx;
+    if (surfel_hit(sf, i, this->o, this->d, this->tmin, best, th, xx, aa)) {
+      // insert into the sorted list (static indices: stays in registers)
+      uint32_t pj = i;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      int cidx = k == 0 ? first : 1 - first;
-      if (!lh[cidx]) continue;
-      uint32_t word = lw[cidx];
-      uint32_t f0 = word & 0x0FFFFFFFu, cnt = ((word >> 28) & 7u) + 1u;
-      if (f0 + cnt > S.sf.count) {
-        flag_error(st, kErrBounds);
-        continue;
-      }
-      for (uint32_t j = 0; j < cnt; ++j) {
-        float th, aa;
-        V3 xx;
-        ctr.tests++;
-        if (surfel_hit(S.sf, f0 + j, o, d, tmin, best, th, xx, aa)) {
-          // insert into the sorted list (static indices: stays in registers)
-          uint32_t pj = f0 + j;
-#pragma unroll
-          for (int q = 0; q < K; ++q) {
-            if (th < t_out[q]) {
-              const float tt = t_out[q];
-              const uint32_t pp = prim_out[q];
-              t_out[q] = th;
-              prim_out[q] = pj;
-              th = tt;
-              pj = pp;
-            }
-          }
-          count = count < (uint32_t)K ? count + 1 : count;
-          if (count == (uint32_t)K) best = t_out[K - 1];
+      for (int q = 0; q < K; ++q) {
+        if (th < t_out[q]) {
+          const float tt = t_out[q];
+          const uint32_t pp = prim_out[q];
+          t_out[q] = th;
+          prim_out[q] = pj;
+          th = tt;
+          pj = pp;
         }
       }
+      count = count < (uint32_t)K ? count + 1 : count;
+      if (count == (uint32_t)K) best = t_out[K - 1];
     }
-    h0 = h0 && !(w.x & kLeafFlag) && e0 <= best;
-    h1 = h1 && !(w.y & kLeafFlag) && e1 <= best;
-    if (h0 && h1) {
-      uint32_t nearN = e0 <= e1 ? w.x : w.y, farN = e0 <= e1 ? w.y : w.x;
-      float farT = e0 <= e1 ? e1 : e0;
-      if (sp < kStackDepth) {
-        stk.push(sp, farN, farT);
-        ++sp;
-      } else {
-        flag_error(st, kErrStackOverflow);
-      }
-      node = nearN;
-      return true;
-    }
-    if (h0) { node = w.x; return true; }
-    if (h1) { node = w.y; return true; }
-    while (sp > 0) {
-      --sp;
-      uint32_t sn;
-      float st_t;
-      stk.get(sp, sn, st_t);
-      if (st_t <= best) {
-        node = sn;
-        return true;
-      }
-    }
-    return false;
   }
 };
+
+// One step of a persistent walk loop for the lanes of a warp: the lanes
+// whose walk stands at a leaf step together once at least kLeafBatch of
+// them (or all of the walking lanes) do, the other times the lanes at inner
+// nodes step.  Returns for this lane whether its walk goes on (a lane that
+// sat out the step keeps walking).  Every lane of the warp calls it.
+template <class W>
+__device__ __forceinline__ bool warp_step(W& w, bool walking, const SceneView& S,
+                                          const TravNode* __restrict__ smem_top, TravStack& stk, TraceCounters& ctr,
+                                          RunState* st) {
+  const bool lf = walking && w.at_leaf();
+  const unsigned ml = __ballot_sync(0xffffffffu, lf);
+  const unsigned ma = __ballot_sync(0xffffffffu, walking);
+  const bool leaf_phase = ml != 0u && (ml == ma || __popc(ml) >= kLeafBatch);
+  if (walking && lf == leaf_phase) return w.step(S, smem_top, stk, ctr, st);
+  return walking;
+}
 
 // A 4x4 instance matrix (16 floats, 64 B aligned) in four 16-byte loads.
 __device__ __forceinline__ void load_matrix(const float* M, float (&m)[16]) {
@@ -669,12 +654,13 @@ __device__ __forceinline__ void world_to_cell(const GridView& G, V3 p, int c[3])
 // (z, y) order visits the photons in the reference's cell-by-cell order.
 // The rows of the window are concatenated (a warp scan of their lengths),
 // and each round the 32 lanes test 32 consecutive photons of that sequence
-// with coalesced loads.  The sums keep the reference's order: the lanes
-// whose photon passes the radius and cosine tests write their three terms
-// to `terms`, packed in photon order (ballot ranks), and lanes 0, 1 and 2
-// add the x, y and z terms in sequence, so the result equals the
-// reference's one-photon-at-a-time loop bit for bit.  `terms` is this
-// warp's 32 float4 of shared memory.
+// with coalesced loads.  Every lane adds the power of the photons it
+// accepts (radius and cosine tests) into its own running sum, and the 32
+// sums are added by a butterfly of shuffles at the end: the same terms as
+// the reference's one-photon-at-a-time loop, summed in another order (the
+// result differs from it by float rounding, about 1e-7 relative; a photon
+// within a rounding error of the radius can fall on either side).  `terms`
+// is this warp's 32 float4 of shared memory (the row compaction).
 // Returns the irradiance in every lane and the photons scanned in `count`.
 // Per-launch constants of the lookups: 1 / (pi r^2), 1 / cell, and the
 // T / D factor of the photon store (0 when nothing was deposited, so an
@@ -734,7 +720,7 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const Ga
   const float inv_ny = __fdividef(1.0f, (float)ny);
   const float inv_cx = GC.inv_cx;
   const uint32_t total_ph = GC.total_ph;
-  float acc = 0.f;   // lane c < 3: running sum of component c
+  float ax = 0.f, ay = 0.f, az = 0.f;   // this lane's sums of the accepted terms
   uint32_t scanned = 0;
   for (int rb = 0; rb < rows; rb += 32) {
     // this lane's row: offsets and length
@@ -831,58 +817,30 @@ __device__ __forceinline__ V3 gather_irradiance_warp(const GridView& G, const Ga
         fetch(base, pa, pb, pc);
       }
       const uint32_t v = base + lane;
-      float tx = 0.f, ty = 0.f, tz = 0.f;
-      bool in = false;
       if (v < seq) {
         const float dx = pa.x - x.x, dy = pa.y - x.y, dz = pa.z - x.z;
-        const float d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 <= r2) {
-          const float cosine = n.x * (-pb.x) + n.y * (-pb.y) + n.z * (-pb.z);
-          if (!(cosine < 0.0f)) {
-            in = true;
-            tx = pa.w * invArea;
-            ty = pb.w * invArea;
-            tz = pc * invArea;
-          }
+        const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
+        const float cosine = -__fmaf_rn(n.z, pb.z, __fmaf_rn(n.y, pb.y, n.x * pb.x));
+        if (d2 <= r2 && !(cosine < 0.0f)) {
+          ax = __fmaf_rn(pa.w, invArea, ax);
+          ay = __fmaf_rn(pb.w, invArea, ay);
+          az = __fmaf_rn(pc, invArea, az);
         }
       }
-      // accepted terms packed in photon order, one 32-float array per
-      // component; lane c adds component c four terms per shared load
-      const unsigned m = __ballot_sync(0xffffffffu, in);
-      float* tb = reinterpret_cast<float*>(terms);
-      if (in) {
-        const int p = __popc(m & ((1u << lane) - 1u));
-        tb[p] = tx;
-        tb[32 + p] = ty;
-        tb[64 + p] = tz;
-      }
-      __syncwarp();
-      if (lane < 3) {
-        const float4* t4 = reinterpret_cast<const float4*>(tb + 32 * lane);
-        const int c = __popc(m);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          if (4 * q < c) {
-            const float4 v = t4[q];
-            acc = acc + v.x;
-            if (4 * q + 1 < c) acc = acc + v.y;
-            if (4 * q + 2 < c) acc = acc + v.z;
-            if (4 * q + 3 < c) acc = acc + v.w;
-          }
-        }
-      }
-      __syncwarp();
       pa = na;
       pb = nb;
       pc = nc;
     }
   }
   count += scanned;
-  const float ex = __shfl_sync(0xffffffffu, acc, 0);
-  const float ey = __shfl_sync(0xffffffffu, acc, 1);
-  const float ez = __shfl_sync(0xffffffffu, acc, 2);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    az += __shfl_xor_sync(0xffffffffu, az, o);
+  }
   const float s = GC.scale;
-  return v3(ex * s, ey * s, ez * s);
+  return v3(ax * s, ay * s, az * s);
 }
 
 }  // namespace pale

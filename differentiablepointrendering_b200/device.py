@@ -110,3 +110,89 @@ def l2_grad_(dldi: torch.Tensor, ldr: torch.Tensor, target_rgb: torch.Tensor,
         dldi[off:off + w * h, :3].div_(3 * w * h)
         off += w * h
     return dldi
+
+
+class ViewBatch:
+    """Views of several renderers (scenes) rendered together: the forward
+    pass of every view is ONE camera-gather wavefront and the adjoint ONE
+    wavefront of (view, pass) jobs, each path finding its scene through its
+    view.  A view is (scene index, camera index, passes, depth): passes from
+    1 to the scene's gather/adjoint passes, depth 0 (the scene's adjoint
+    bounces) or fewer bounces.  Images, dL/dI and targets are packed in view
+    order as DeviceFrame's; every call runs on the caller's CUDA stream with
+    the wavefront buffers of the first renderer."""
+
+    def __init__(self, renderers: Sequence[Renderer], views: Sequence[Sequence[int]], device=None):
+        if not renderers:
+            raise ValueError("no renderers")
+        self.renderers = list(renderers)
+        self.device = torch.device(device or f"cuda:{torch.cuda.current_device()}")
+        vs = []
+        for v in views:
+            s, c, p, d = (list(v) + [0, 0, 0, 0])[:4]
+            vs.append((int(s), int(c), int(p), int(d)))
+        self.views = vs
+        arr = (N.PaleView * max(1, len(vs)))()
+        for i, (s, c, p, d) in enumerate(vs):
+            if not 0 <= s < len(self.renderers):
+                raise ValueError(f"view {i}: scene {s} outside the {len(self.renderers)} renderers")
+            arr[i].scene, arr[i].camera, arr[i].passes, arr[i].depth = s, c, p, d
+        self._views = arr
+        self._scenes = (C.c_void_p * len(self.renderers))(*[r._h.value for r in self.renderers])
+        self.sizes = [self.renderers[s]._sizes[c] for s, c, _, _ in vs]
+        self.pixels = sum(w * h for w, h in self.sizes)
+        f = dict(dtype=torch.float32, device=self.device)
+        self.ldr = torch.zeros(max(1, self.pixels), 4, **f)
+        self.raw = torch.zeros(max(1, self.pixels), 4, **f)
+        self.dldi = torch.zeros(max(1, self.pixels), 4, **f)
+        self.loss = torch.zeros(max(1, len(vs)), dtype=torch.float64, device=self.device)
+        self.grads = []
+        self._gstructs = (N.PalePoints * len(self.renderers))()
+        for k, r in enumerate(self.renderers):
+            n = r.num_points
+            g = {key: torch.zeros((n, POINT_WIDTH[key]) if POINT_WIDTH[key] > 1 else (n,), **f) for key in POINT_FIELDS}
+            self.grads.append(g)
+            self._gstructs[k].count = n
+            for key in POINT_FIELDS:
+                setattr(self._gstructs[k], key, C.cast(C.c_void_p(g[key].data_ptr()), N.f32p))
+
+    def _stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def forward_loss(self, target: Optional[torch.Tensor] = None, trace_photons: bool = True):
+        """Forward render of every view (with the L2 loss against `target`,
+        packed (P, 3) or (P, 4), when given); returns the per-view losses
+        (float64 device tensor) or None."""
+        L = self.renderers[0]._lib
+        t = None
+        if target is not None:
+            t = target.contiguous()
+            if t.dtype != torch.float32 or t.dim() != 2 or t.shape[0] != self.pixels or t.shape[1] not in (3, 4):
+                raise ValueError(f"target must be float32 ({self.pixels}, 3 or 4)")
+        rc = L.pale_render_views_loss_device(
+            len(self.renderers), self._scenes, 1 if trace_photons else 0, len(self.views), self._views,
+            C.c_void_p(t.data_ptr()) if t is not None else None, t.shape[1] if t is not None else 0,
+            C.c_void_p(self.ldr.data_ptr()), C.c_void_p(self.raw.data_ptr()),
+            C.c_void_p(self.dldi.data_ptr()) if t is not None else None,
+            C.c_void_p(self.loss.data_ptr()) if t is not None else None, self._stream())
+        _check(L, self.renderers[0]._h, rc, "render_views_loss_device")
+        return self.loss if t is not None else None
+
+    def backward(self, dldi: Optional[torch.Tensor] = None):
+        """Adjoint pass of every view with packed dL/dI (P, 4) (default: the
+        last forward_loss's); returns one gradient dict per renderer (BVH
+        order)."""
+        d = self.dldi if dldi is None else dldi.contiguous()
+        L = self.renderers[0]._lib
+        rc = L.pale_render_views_backward_device(len(self.renderers), self._scenes, len(self.views), self._views,
+                                                 C.c_void_p(d.data_ptr()), self._gstructs, self._stream())
+        _check(L, self.renderers[0]._h, rc, "render_views_backward_device")
+        return self.grads
+
+    def split(self, packed: torch.Tensor) -> List[torch.Tensor]:
+        """Packed (P, 4) -> list of (H, W, 4) views, one per view."""
+        out, off = [], 0
+        for w, h in self.sizes:
+            out.append(packed[off:off + w * h].view(h, w, 4))
+            off += w * h
+        return out

@@ -6,19 +6,31 @@ the same surfels, traces the same counter-keyed photons (so the photon maps
 are bit-identical without an exchange) and renders its own views; the only
 exchange is the sum of the per-surfel gradient arrays.
 
-- view_offset(rank, world): rank r renders the ring of views rotated by
-  r / world of the camera spacing, so N ranks with C views each cover the
-  ring of N*C views evenly.
+- shard_cameras(names, rank, world): the cameras of one scene split round
+  robin over the ranks.  With the setting camera_seeds = "camera" a
+  camera's image and gradient do not depend on the other cameras of a call,
+  so the ranks' gradients, summed, equal one process rendering every camera.
+- view_offset(rank, world): rank r's ring of views rotated by r / world of
+  the camera spacing; N rings of C views interleave into the ring of N*C
+  views that shard_cameras splits the same way.
 - reduce_gradients(grads): sums the gradient arrays of all ranks in place
   with ONE all-reduce over a flat buffer (eight arrays per step would be
   eight latency-bound collectives).
 """
 from __future__ import annotations
 
-from typing import Dict, Optional
+from typing import Dict, List, Optional, Sequence
 
 import torch
 import torch.distributed as dist
+
+
+def shard_cameras(names: Sequence[str], rank: int, world: int) -> List[str]:
+    """The cameras rank `rank` of `world` renders: every world-th camera from
+    position `rank` (round robin, so the views of a ring spread evenly)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside a world of {world}")
+    return list(names)[rank::world]
 
 
 def view_offset(rank: int, world: int) -> float:

@@ -266,8 +266,13 @@ def ring_cameras(count: int, radius: float = 1.5, height: float = 0.0, offset: f
 
 def make_box_scene(n_surfels: int, cameras: int = 1, resolution: int = 256, fovy: float = 40.0,
                    seed: int = 1234, radiance: float = 15.0,
-                   points: Optional[Dict[str, np.ndarray]] = None, ring_offset: float = 0.0) -> SceneArrays:
+                   points: Optional[Dict[str, np.ndarray]] = None, ring_offset: float = 0.0,
+                   resolutions: Optional[Sequence[int]] = None) -> SceneArrays:
     """The synthetic box of the throughput workloads.
+
+    Cameras: `cameras` positions on the ring, each at `resolution`, or with
+    `resolutions` one camera per (position, resolution), camera index
+    position * len(resolutions) + k, named camera{position}_{resolution}.
 
     Walls are instances of the rectangle quad (front faces inward), albedo
     0.8 (floor, ceiling, back), 0.6/0.1/0.1 (x = -0.5) and 0.1/0.6/0.1
@@ -289,7 +294,11 @@ def make_box_scene(n_surfels: int, cameras: int = 1, resolution: int = 256, fovy
     B.add_instance(quad, green, trs((0.5, 0, 0), (0, 1, 0), -90.0, h), "right")
     B.add_instance(quad, light, trs((0, 0, 0.499), (1, 0, 0), 180.0, (0.125, 0.125, 1.0)), "light")
     for k, eye in enumerate(ring_cameras(cameras, offset=ring_offset)):
-        B.add_camera(f"camera{k}", eye, (0, 0, 0), (0, 0, 1), fovy, resolution, resolution)
+        if resolutions:
+            for res in resolutions:
+                B.add_camera(f"camera{k}_{res}", eye, (0, 0, 0), (0, 0, 1), fovy, res, res)
+        else:
+            B.add_camera(f"camera{k}", eye, (0, 0, 0), (0, 0, 1), fovy, resolution, resolution)
     if points is None:
         points = make_surfels(n_surfels, seed)
     return B.finish(points)

@@ -60,12 +60,14 @@ typedef struct pale_handle pale_handle;
 #define PALE_GRADIENTS_OPACITY 0u
 #define PALE_GRADIENTS_ALL 1u
 
-/* Which seed of the camera-gather table a camera uses.  SELECTION is the
- * reference's: the camera's position in the list a render call selects, so
- * one camera rendered alone and inside a larger selection draws different
- * samples.  CAMERA keys the seed by the camera's index in the scene, so a
- * camera's image does not depend on which other cameras share the call
- * (what a server that merges requests needs). */
+/* Which seeds a camera uses: its camera-gather seed and, with decorrelated
+ * seeds, its adjoint seeds.  SELECTION is the reference's: the camera's
+ * position in the list a render call selects, so one camera rendered alone
+ * and inside a larger selection draws different samples.  CAMERA keys the
+ * seeds by the camera's index in the scene, so a camera's image and
+ * gradient do not depend on which other cameras share the call (what a
+ * server that merges requests needs, and ranks that split the cameras of
+ * one scene). */
 #define PALE_CAMERA_SEEDS_SELECTION 0u
 #define PALE_CAMERA_SEEDS_CAMERA 1u
 
@@ -98,6 +100,8 @@ typedef struct pale_settings {
     uint32_t adjoint_batch_paths;  /* adjoint paths per batch of (camera,
                                       pass) jobs (0 = 2^24; at least the
                                       largest camera's pixels)               */
+    uint32_t walk_block;           /* threads per block of the persistent
+                                      BVH walks: 64, 128 or 256 (0 = 256)    */
 } pale_settings;
 
 /* Per-point parameter block (structure of arrays, float32).
@@ -265,6 +269,46 @@ int pale_render_backward_device(pale_handle *h, uint32_t num_selected,
                                 const uint32_t *camera_indices,
                                 const float *d_dldi, pale_points *d_grads,
                                 void *stream);
+
+/* One view of a batched render: a camera of one of the call's scenes with
+ * its own number of passes and adjoint bounces. */
+typedef struct pale_view {
+    uint32_t scene;    /* index into the call's scene list                      */
+    uint32_t camera;   /* camera index in that scene                            */
+    uint32_t passes;   /* gather passes in a forward call, adjoint passes in an
+                          adjoint call: 1 .. the scene's gather_passes /
+                          adjoint_passes                                        */
+    uint32_t depth;    /* adjoint bounces: 0 = the scene's adjoint_bounces, at
+                          most that                                             */
+} pale_view;
+
+/* Batched forward render with the L2 loss: the views of up to 8 scenes of
+ * uneven resolution, passes and depth as ONE camera-gather wavefront (every
+ * path finds its scene's surfels, LBVH, meshes and photon grid through its
+ * view).  No counterpart in the reference, which renders one camera and
+ * one pass per launch (SyclBridge.cpp:136-146).  With trace_photons every
+ * scene first traces its own photon map; without, the views use the
+ * current photon maps.  Images, dL/dI and losses are packed in view order
+ * like pale_render_forward_loss_device's (d_target likewise); d_ldr, d_raw,
+ * d_dldi and d_loss may be NULL.  Runs on `stream` (NULL = the default
+ * stream) with the wavefront buffers of scenes[0], without waiting; a
+ * camera's seeds follow the scenes' camera_seeds setting.  Errors are
+ * reported through scenes[0] (pale_last_error). */
+int pale_render_views_loss_device(uint32_t num_scenes, pale_handle *const *scenes,
+                                  int trace_photons, uint32_t num_views,
+                                  const pale_view *views, const float *d_target,
+                                  uint32_t channels, float *d_ldr, float *d_raw,
+                                  float *d_dldi, double *d_loss, void *stream);
+
+/* The adjoint pass of the same views as ONE wavefront of (view, pass) jobs:
+ * dL/dI packed in view order (DEVICE).  Each scene's gradients accumulate
+ * in its own arrays; d_grads is NULL or num_scenes entries of DEVICE
+ * pointers that receive them (BVH order, as pale_render_backward_device).
+ * The rng mode, null weighting and gradient groups are scenes[0]'s. */
+int pale_render_views_backward_device(uint32_t num_scenes, pale_handle *const *scenes,
+                                      uint32_t num_views, const pale_view *views,
+                                      const float *d_dldi, pale_points *d_grads,
+                                      void *stream);
 
 /* Current per-point parameters in BVH order (get_point_parameters,
  * pale_bindings.cpp:733-850). */

@@ -1447,7 +1447,8 @@ static void postprocess(const orc_scene *s, const float *raw, float *ldr, uint32
     }
 }
 
-static void gather_cameras(orc_scene *s, mt64_t mt, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw);
+static void gather_cameras(orc_scene *s, mt64_t mt, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                           float *ldr, float *raw);
 
 int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw) {
     apply_threads();
@@ -1460,7 +1461,7 @@ int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float 
     s->cam_mt = mt;
     s->cam_mt_valid = 1;
     double t1 = now_ms();
-    gather_cameras(s, mt, nsel, cams, ldr, raw);
+    gather_cameras(s, mt, nsel, cams, NULL, ldr, raw);
     double t2 = now_ms();
     s->stats.photon_ms = (float)(t1 - t0);
     s->stats.gather_ms = (float)(t2 - t1);
@@ -1477,22 +1478,31 @@ int orc_render_gather(orc_scene *s, uint32_t nsel, const uint32_t *cams, float *
     if (s->cam_mt_valid) mt = s->cam_mt;
     else mt_seed(&mt, s->st.seed);
     double t1 = now_ms();
-    gather_cameras(s, mt, nsel, cams, ldr, raw);
+    gather_cameras(s, mt, nsel, cams, NULL, ldr, raw);
     s->stats.gather_ms = (float)(now_ms() - t1);
     s->stats.forward_ms = s->stats.gather_ms;
     return 0;
 }
 
-static void gather_cameras(orc_scene *s, mt64_t mt, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw) {
+/* passes: per selected camera (a view's own number of gather passes), or
+ * NULL for the settings' gather_passes. */
+static void gather_cameras(orc_scene *s, mt64_t mt, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                           float *ldr, float *raw) {
     size_t off = 0;
+    /* camera seeds: one draw per selected camera in selection order (the
+     * reference), or one per scene camera, indexed by the camera */
+    const uint32_t nseed = s->st.camera_seeds == 1 ? s->ncam : nsel;
+    uint32_t *cam_seed = (uint32_t *)malloc((nseed ? nseed : 1) * sizeof(uint32_t));
+    for (uint32_t k = 0; k < nseed; ++k) cam_seed[k] = (uint32_t)mt_next(&mt);
     for (uint32_t ci = 0; ci < nsel; ++ci) {
         uint32_t cam = cams[ci];
         uint32_t W = s->cam_size[2 * cam], H = s->cam_size[2 * cam + 1], npix = W * H;
-        uint64_t cseed = (uint32_t)mt_next(&mt);
+        uint64_t cseed = cam_seed[s->st.camera_seeds == 1 ? cam : ci];
         float *fb = (float *)calloc((size_t)npix * 4, sizeof(float));
-        float spp = (float)s->st.gather_passes;
+        const uint32_t npass = passes ? passes[ci] : s->st.gather_passes;
+        float spp = (float)npass;
         uint64_t segs = 0, queries = 0, scanned = 0, nodes = 0, tests = 0;
-        for (uint32_t pass = 0; pass < s->st.gather_passes; ++pass) {
+        for (uint32_t pass = 0; pass < npass; ++pass) {
             uint64_t base = s->st.rng_mode == 1 ? orc_per_item_seed(cseed, pass) : cseed;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : segs, queries, scanned, nodes, tests)
             for (int64_t p = 0; p < (int64_t)npix; ++p) {
@@ -1518,6 +1528,7 @@ static void gather_cameras(orc_scene *s, mt64_t mt, uint32_t nsel, const uint32_
         off += (size_t)npix * 4;
         free(fb);
     }
+    free(cam_seed);
 }
 
 /* --------------------------------------------------------- adjoint pass */
@@ -1767,8 +1778,37 @@ static float transport_event(const orc_scene *s, const event_t *e, float invSpp,
     return 0.0f;
 }
 
+static int render_backward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                                 const uint32_t *depths, const float *dldi, orc_points *grads, float *debug_opacity);
+
 int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const float *dldi,
                         orc_points *grads, float *debug_opacity) {
+    return render_backward_views(s, nsel, cams, NULL, NULL, dldi, grads, debug_opacity);
+}
+
+int orc_render_forward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                             float *ldr, float *raw) {
+    apply_threads();
+    memset(&s->stats, 0, sizeof(s->stats));
+    mt64_t mt;
+    mt_seed(&mt, s->st.seed);
+    photon_pass(s, &mt);
+    build_grid(s);
+    s->cam_mt = mt;
+    s->cam_mt_valid = 1;
+    gather_cameras(s, mt, nsel, cams, passes, ldr, raw);
+    return 0;
+}
+
+int orc_render_backward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                              const uint32_t *depths, const float *dldi, orc_points *grads) {
+    return render_backward_views(s, nsel, cams, passes, depths, dldi, grads, NULL);
+}
+
+/* passes / depths: per selected camera (a view's own passes and adjoint
+ * bounces; depth 0 = the settings'), or NULL for the settings. */
+static int render_backward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                                 const uint32_t *depths, const float *dldi, orc_points *grads, float *debug_opacity) {
     apply_threads();
     memset(&s->stats, 0, sizeof(s->stats));
     double t0 = now_ms();
@@ -1778,10 +1818,18 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
      * tangent_v[3], scale[2], albedo[3] */
     const int all = st->gradients == 1;
     float *gall = all ? (float *)calloc((size_t)(s->np ? s->np : 1) * 15, sizeof(float)) : NULL;
+    /* adjoint seed table: per (camera, pass) one draw for the ray
+     * generation and one per bounce, camera-major; the camera is its
+     * position in the selection, or with camera_seeds its scene index */
     mt64_t mt;
     mt_seed(&mt, st->rng_mode == 1 ? st->seed : 42ull);
+    const uint32_t seed_cams = st->camera_seeds == 1 ? s->ncam : nsel;
+    const size_t per_job = (size_t)st->adjoint_bounces + 1;
+    const size_t nseeds = (size_t)seed_cams * st->adjoint_passes * per_job;
+    uint32_t *seed_tab = (uint32_t *)malloc((nseeds ? nseeds : 1) * sizeof(uint32_t));
+    for (size_t k = 0; k < nseeds; ++k) seed_tab[k] = (uint32_t)mt_next(&mt);
     size_t off = 0;
-    float invSpp = 1.0f / (float)st->adjoint_passes;
+
     for (uint32_t ci = 0; ci < nsel; ++ci) {
         uint32_t cam = cams[ci];
         uint32_t W = s->cam_size[2 * cam], H = s->cam_size[2 * cam + 1], npix = W * H;
@@ -1791,13 +1839,17 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
         pending_t *pend = (pending_t *)malloc(npix * sizeof(pending_t));
         float *dbg = debug_opacity ? debug_opacity + off : NULL;
         if (dbg) memset(dbg, 0, (size_t)npix * 4 * sizeof(float));
-        for (uint32_t spp = 0; spp < st->adjoint_passes; ++spp) {
+        const uint32_t npass = passes ? passes[ci] : st->adjoint_passes;
+        const uint32_t depth = depths && depths[ci] ? depths[ci] : st->adjoint_bounces;
+        const float invSpp = 1.0f / (float)npass;
+        for (uint32_t spp = 0; spp < npass; ++spp) {
             /* decorrelated mode: one seed for the ray generation and one per
                bounce of every pass, drawn whether or not the bounce has work */
-            uint32_t sspp = (uint32_t)mt_next(&mt);
+            const uint32_t *blk = seed_tab + ((size_t)(st->camera_seeds == 1 ? cam : ci) * st->adjoint_passes + spp) * per_job;
+            uint32_t sspp = blk[0];
             uint64_t rbase = st->rng_mode == 1 ? sspp : st->random_number;
             uint32_t *sbounce = (uint32_t *)malloc((st->adjoint_bounces + 1) * sizeof(uint32_t));
-            for (uint32_t b = 0; b < st->adjoint_bounces; ++b) sbounce[b] = (uint32_t)mt_next(&mt);
+            for (uint32_t b = 0; b < st->adjoint_bounces; ++b) sbounce[b] = blk[1 + b];
             /* launchRayGenAdjointKernel (AdjointKernels.cpp:15-84) */
             for (uint32_t p = 0; p < npix; ++p) {
                 rng_t r = rng_make(orc_per_item_seed(rbase, p));
@@ -1814,7 +1866,7 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
                 pend[p].inst = INVALID_U32;
             }
             uint32_t active = npix;
-            for (uint32_t b = 0; b < st->adjoint_bounces && active > 0; ++b) {
+            for (uint32_t b = 0; b < depth && active > 0; ++b) {
                 uint64_t bbase = st->rng_mode == 1 ? sbounce[b] : st->random_number;
                 s->stats.adjoint_segments += active;
                 uint64_t nodes = 0, tests = 0;
@@ -1922,6 +1974,7 @@ int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const
     }
     free(gop);
     free(gall);
+    free(seed_tab);
     s->stats.backward_ms = (float)(now_ms() - t0);
     return 0;
 }

@@ -40,6 +40,7 @@ typedef struct orc_settings {
     float exposure, gamma;
     uint32_t null_weight;   /* 0 reference, 1 unbiased (divide by q_null) */
     uint32_t gradients;     /* 0 opacity, 1 all seven groups */
+    uint32_t camera_seeds;  /* 0 by position in the selection, 1 by camera index */
 } orc_settings;
 
 typedef struct orc_points {
@@ -84,6 +85,13 @@ int orc_render_forward(orc_scene *s, uint32_t nsel, const uint32_t *cams, float 
 int orc_render_gather(orc_scene *s, uint32_t nsel, const uint32_t *cams, float *ldr, float *raw);
 int orc_render_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const float *dldi,
                         orc_points *grads, float *debug_opacity);
+/* The same with a number of passes per selected camera (and for the
+ * adjoint a number of bounces, 0 = the settings'), the views of a batched
+ * render. */
+int orc_render_forward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                             float *ldr, float *raw);
+int orc_render_backward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                              const uint32_t *depths, const float *dldi, orc_points *grads);
 int orc_trace_rays(orc_scene *s, uint32_t n, const float *o, const float *d, int32_t *inst,
                    int32_t *prim, float *t, float *alpha, float *hitpos);
 int orc_trace_transmittance(orc_scene *s, uint32_t n, const float *o, const float *d, int32_t *inst, float *t,

@@ -40,6 +40,9 @@ def lib() -> C.CDLL:
             "orc_render_forward": (C.c_int, [P, C.c_uint32, N.u32p, N.f32p, N.f32p]),
             "orc_render_gather": (C.c_int, [P, C.c_uint32, N.u32p, N.f32p, N.f32p]),
             "orc_render_backward": (C.c_int, [P, C.c_uint32, N.u32p, N.f32p, C.POINTER(N.PalePoints), N.f32p]),
+            "orc_render_forward_views": (C.c_int, [P, C.c_uint32, N.u32p, N.u32p, N.f32p, N.f32p]),
+            "orc_render_backward_views": (C.c_int, [P, C.c_uint32, N.u32p, N.u32p, N.u32p, N.f32p,
+                                                    C.POINTER(N.PalePoints)]),
             "orc_trace_rays": (C.c_int, [P, C.c_uint32, N.f32p, N.f32p, N.i32p, N.i32p, N.f32p, N.f32p, N.f32p]),
             "orc_trace_transmittance": (C.c_int, [P, C.c_uint32, N.f32p, N.f32p, N.i32p, N.f32p, N.f32p]),
             "orc_gather_irradiance": (C.c_int, [P, C.c_uint32, N.f32p, N.f32p, N.f32p]),
@@ -99,14 +102,16 @@ class OracleRenderer:
     def num_points(self) -> int:
         return int(self.L.orc_point_count(self.h))
 
-    def render_forward(self, camera_name: str = "") -> Dict[str, np.ndarray]:
+    def render_forward(self, camera_name="") -> Dict[str, np.ndarray]:
+        """One camera by name, a list of names, or every camera ("")."""
         return self._render(camera_name, self.L.orc_render_forward)
 
-    def render_gather(self, camera_name: str = "") -> Dict[str, np.ndarray]:
+    def render_gather(self, camera_name="") -> Dict[str, np.ndarray]:
         return self._render(camera_name, self.L.orc_render_gather)
 
     def _render(self, camera_name, fn) -> Dict[str, np.ndarray]:
-        idx = [i for i, n in enumerate(self.names) if (not camera_name or n == camera_name)]
+        want = [camera_name] if isinstance(camera_name, str) else list(camera_name)
+        idx = [i for i, n in enumerate(self.names) if (want == [""] or n in want)]
         pix = sum(self.sizes[i][0] * self.sizes[i][1] for i in idx)
         ldr = np.empty(max(1, pix) * 4, np.float32)
         raw = np.empty(max(1, pix) * 4, np.float32)
@@ -139,6 +144,40 @@ class OracleRenderer:
                                           fptr(dbg)) == 0
         g = {k: grads.arrays[k].copy() for k in POINT_FIELDS}
         return g, {"debug_opacity": dbg[:pix]}
+
+    def render_views(self, cams, passes):
+        """Forward render of cameras `cams` (indices) with passes[i] gather
+        passes each: {name: LDR, name + "_raw": RAW} per view."""
+        cams = np.asarray(cams, np.uint32)
+        ps = np.asarray(passes, np.uint32)
+        pix = sum(self.sizes[i][0] * self.sizes[i][1] for i in cams)
+        ldr = np.empty(max(1, pix) * 4, np.float32)
+        raw = np.empty(max(1, pix) * 4, np.float32)
+        assert self.L.orc_render_forward_views(self.h, len(cams), uptr(cams), uptr(ps), fptr(ldr), fptr(raw)) == 0
+        out, off = [], 0
+        for i in cams:
+            w, h = self.sizes[i]
+            n = w * h * 4
+            out.append((ldr[off:off + n].reshape(h, w, 4).copy(), raw[off:off + n].reshape(h, w, 4).copy()))
+            off += n
+        return out
+
+    def backward_views(self, cams, passes, depths, dldi_rgb):
+        """Adjoint of the views (passes and bounces per view, depth 0 = the
+        settings') with dL/dI images (H, W, 3) per view; gradient dict."""
+        cams = np.asarray(cams, np.uint32)
+        ps = np.asarray(passes, np.uint32)
+        ds = np.asarray(depths, np.uint32)
+        parts = []
+        for a in dldi_rgb:
+            rgba = np.ones(a.shape[:2] + (4,), np.float32)
+            rgba[..., :3] = a
+            parts.append(rgba.reshape(-1))
+        dl = np.concatenate(parts) if parts else np.zeros(4, np.float32)
+        grads = N.PointsHolder(n=self.num_points)
+        assert self.L.orc_render_backward_views(self.h, len(cams), uptr(cams), uptr(ps), uptr(ds), fptr(dl),
+                                                C.byref(grads.struct)) == 0
+        return {k: grads.arrays[k].copy() for k in POINT_FIELDS}
 
     def get_point_parameters(self):
         out = N.PointsHolder(n=self.num_points)
