@@ -633,90 +633,130 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
 
 # ---------------------------------------------------------------- serving
-SERVING_SCENES = (   # name, surfels, views, resolution, passes, depth (log-uniform sizes, as the C5 spread)
-    ("s10k", 10000, 4, 128, 4, 4), ("s50k", 50000, 4, 256, 8, 5), ("s200k", 200000, 4, 512, 4, 6),
-    ("s1m", 1000000, 4, 256, 16, 8))
+SERVING_SURFELS = tuple(int(round(10000 * 100 ** (k / 7))) for k in range(8))   # 10k .. 1M, log-uniform
+SERVING_RES = (128, 256, 512, 1024)
+SERVING_SPP = (1, 2, 4, 8, 16, 32, 64)
+SERVING_SETTINGS = {"photons": 1000000, "bounces": 8, "forward_passes": 1, "gather_passes": 64,
+                    "adjoint_bounces": 8, "adjoint_passes": 64, "gather_radius": 0.01}
+
+
+def serving_request(rng, names, kind=None, res=None, spp=None):
+    """One request of the serving mix: a scene of the eight, a camera of
+    resolution uniform in 128..1024 (squared), passes log-uniform in 1..64,
+    adjoint depth uniform in 4..8; 70% forward, 30% gradient."""
+    from differentiablepointrendering_b200.serving import Request
+
+    s = names[int(rng.integers(len(names)))]
+    k = int(rng.integers(len(SERVING_RES))) if res is None else SERVING_RES.index(res)
+    cam = int(rng.integers(2)) * len(SERVING_RES) + k
+    kind = kind or ("gradient" if rng.uniform() < 0.3 else "forward")
+    reso = SERVING_RES[k]
+    tgt = rng.uniform(0, 1, (reso, reso, 3)).astype("float32") if kind == "gradient" else None
+    passes = spp or SERVING_SPP[int(rng.integers(len(SERVING_SPP)))]
+    return Request(s, cam, kind, tgt, passes, int(rng.integers(4, 9)))
+
+
+def serve_stream(srv, reqs):
+    """Submits (arrival time, request) pairs at their times; the served
+    latencies, the span, and the same arrivals on the plain path (each
+    request alone, in arrival order, on a virtual clock)."""
+    import numpy as np
+
+    from differentiablepointrendering_b200.serving import Request
+
+    t0 = time.perf_counter()
+    for at, q in reqs:
+        delay = t0 + at - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        srv.submit(q)
+    for _, q in reqs:
+        q.done.wait(900)
+        if q.error:
+            raise RuntimeError(q.error)
+    span = max(q.t_done for _, q in reqs) - t0
+    served = np.array([q.latency_ms for _, q in reqs])
+    clock, plain, service = 0.0, [], []
+    for at, q in reqs:
+        p = srv.serve_one(Request(q.scene, q.camera, q.kind, q.target, q.passes, q.depth))
+        if p.error:
+            raise RuntimeError(p.error)
+        clock = max(clock, at) + (p.t_done - p.t_submit)
+        plain.append((clock - at) * 1e3)
+        service.append((p.t_done - p.t_submit) * 1e3)
+    return served, span, np.array(plain), clock, np.array(service)
+
+
+def _pcts(a):
+    import numpy as np
+
+    return {"p50_ms": round(float(np.percentile(a, 50)), 2), "p99_ms": round(float(np.percentile(a, 99)), 2)}
 
 
 def run_serving(args):
-    """Poisson stream of single-view requests (70% forward, 30% gradient)
-    over resident scenes of different sizes, served by serving.Server, and
-    the same stream served one request at a time in arrival order (the plain
-    path).  One JSON line: completed requests/s and p50/p99 latency of both."""
+    """The serving workload: eight resident box scenes of 10k..1M surfels
+    (log-uniform) admitted under a 150 GB HBM budget, and Poisson streams of
+    single-view requests (70% forward, 30% gradient; resolution 128..1024
+    squared, passes 1..64, depth 4..8) at each rate, served by
+    serving.Server in rounds and, for comparison, one request at a time in
+    arrival order (the plain path).  Then streams of 512x512 gradient
+    requests alone, for their p99 latency.  One JSON line."""
     import numpy as np
     import torch
 
     from differentiablepointrendering_b200.build import build_library
     from differentiablepointrendering_b200.scene import make_box_scene, make_surfels
-    from differentiablepointrendering_b200.serving import Request, Server
+    from differentiablepointrendering_b200.serving import Server
 
     build_library()
     rng = np.random.default_rng(17)
     free, _ = torch.cuda.mem_get_info()
-    srv = Server(hbm_budget=min(150 << 30, int(free * 0.9)))
-    res = {}
-    for name, n, views, reso, spp, depth in SERVING_SCENES:
-        st = {"photons": 200000, "bounces": depth, "forward_passes": 1, "gather_passes": spp,
-              "adjoint_bounces": depth, "adjoint_passes": spp, "gather_radius": 0.01 if n >= 200000 else 0.02}
-        srv.add_scene(name, make_box_scene(n, cameras=views, resolution=reso, points=make_surfels(n, 1234)), st)
-        res[name] = (views, reso)
-    names = [s[0] for s in SERVING_SCENES]
-
-    def stream(rate, seconds):
-        t, out = 0.0, []
-        while t < seconds:
-            t += rng.exponential(1.0 / rate)
-            s = names[int(rng.integers(len(names)))]
-            views, reso = res[s]
-            grad = rng.uniform() < 0.3
-            tgt = rng.uniform(0, 1, (reso, reso, 3)).astype(np.float32) if grad else None
-            out.append((t, Request(s, int(rng.integers(views)), "gradient" if grad else "forward", tgt)))
-        return out
-
-    lines = []
+    budget = min(150 * 10 ** 9, int(free * 0.9))
+    srv = Server(hbm_budget=budget, max_views=64, max_pixels=1 << 24, max_paths=args.round_paths)
+    names = []
+    t_admit = time.perf_counter()
+    for k, n in enumerate(SERVING_SURFELS):
+        name = f"box{n // 1000}k"
+        srv.add_scene(name, make_box_scene(n, cameras=2, resolutions=SERVING_RES,
+                                           points=make_surfels(n, 1234 + k)), SERVING_SETTINGS)
+        names.append(name)
+    t_admit = time.perf_counter() - t_admit
+    # warm-up: every scene once, both kinds, so the wavefront buffers exist
+    warm = [(0.0, serving_request(rng, names, kind, 1024, 1)) for kind in ("forward", "gradient")]
+    serve_stream(srv, warm)
+    runs = []
     for rate in args.rates:
-        reqs = stream(rate, args.seconds)
-        t0 = time.perf_counter()
-        for at, q in reqs:
-            delay = t0 + at - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            srv.submit(q)
-        for _, q in reqs:
-            q.done.wait(600)
-        span = max(q.t_done for _, q in reqs) - t0
-        lat = np.array([q.latency_ms for _, q in reqs])
-        # the plain path: the same arrivals, one request at a time in order
-        plain = []
-        clock = 0.0
-        for at, q in reqs:
-            p = Request(q.scene, q.camera, q.kind, q.target)
-            sc = srv.scenes[p.scene]
-            start = max(clock, at)
-            a = time.perf_counter()
-            if p.kind == "forward":
-                sc._forward([p.camera], [p])
-            else:
-                sc._gradient(p)
-            clock = start + (time.perf_counter() - a)
-            plain.append((clock - at) * 1e3)
-        plain = np.array(plain)
-        merged = [q.batch_views for _, q in reqs if q.kind == "forward"]
-        lines.append({"rate_per_s": rate, "requests": len(reqs),
-                      "served": {"p50_ms": round(float(np.percentile(lat, 50)), 2),
-                                 "p99_ms": round(float(np.percentile(lat, 99)), 2),
-                                 "requests_per_s": round(len(reqs) / span, 2),
-                                 "mean_views_per_forward_call": round(float(np.mean(merged)), 2) if merged else 0},
-                      "plain": {"p50_ms": round(float(np.percentile(plain, 50)), 2),
-                                "p99_ms": round(float(np.percentile(plain, 99)), 2),
-                                "requests_per_s": round(len(reqs) / (clock + 1e-9), 2)}})
+        count = max(8, min(args.requests, int(rate * args.seconds)))
+        t, reqs = 0.0, []
+        for _ in range(count):
+            t += rng.exponential(1.0 / rate)
+            reqs.append((t, serving_request(rng, names)))
+        served, span, plain, clock, service = serve_stream(srv, reqs)
+        views = [q.batch_views for _, q in reqs]
+        runs.append({"rate_per_s": rate, "requests": count,
+                     "served": dict(_pcts(served), requests_per_s=round(count / span, 2),
+                                    mean_views_per_round=round(float(np.mean(views)), 2),
+                                    max_views_per_round=int(max(views))),
+                     "plain": dict(_pcts(plain), requests_per_s=round(count / clock, 2),
+                                   service=_pcts(service))})
+    g512 = []
+    for spp in (1, 4, 16):
+        t, reqs = 0.0, []
+        for _ in range(args.requests_512):
+            t += rng.exponential(1.0 / args.rate_512)
+            reqs.append((t, serving_request(rng, names, "gradient", 512, spp)))
+        served, span, plain, clock, service = serve_stream(srv, reqs)
+        g512.append({"passes": spp, "rate_per_s": args.rate_512, "requests": len(reqs),
+                     "served": _pcts(served), "plain": _pcts(plain), "service_alone": _pcts(service)})
     admitted = srv.admitted_bytes
     srv.close()
-    print(json.dumps({"metric": "serving latency p50/p99 (ms) and requests/s", "impl": "ours",
-                      "scenes": [dict(zip(("name", "surfels", "views", "res", "passes", "depth"), s))
-                                 for s in SERVING_SCENES],
+    print(json.dumps({"metric": "serving latency p50/p99 (ms) and requests/s", "impl": "ours", "n_gpus": 1,
+                      "scenes": [{"name": m, "surfels": n} for m, n in zip(names, SERVING_SURFELS)],
+                      "scene_settings": SERVING_SETTINGS, "resolutions": SERVING_RES, "passes": SERVING_SPP,
+                      "depths": [4, 8], "round_paths": args.round_paths,
                       "mix": "70% forward (LDR image of one view), 30% gradient (L2 loss + adjoint of one view)",
-                      "budget_bytes": srv.budget, "admitted_bytes": admitted, "runs": lines}), flush=True)
+                      "budget_bytes": budget, "admitted_bytes": admitted, "admit_s": round(t_admit, 2),
+                      "runs": runs, "gradient_512": g512}), flush=True)
 
 
 def main():
@@ -732,12 +772,28 @@ def main():
     ap.add_argument("--skip-extra", dest="skip_extra", action="store_true",
                     help="skip the per-view and request-latency measurements")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true", help="C4 without the autotuner")
+    ap.add_argument("--c4", action="store_true", help="only the C4 batched-vs-plain measurement")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (Poisson request stream)")
-    ap.add_argument("--rates", type=float, nargs="*", default=[5.0, 20.0, 50.0])
-    ap.add_argument("--seconds", type=float, default=6.0)
+    ap.add_argument("--rates", type=float, nargs="*", default=[50.0, 200.0, 500.0, 2000.0])
+    ap.add_argument("--seconds", type=float, default=4.0, help="serving: stream length per rate")
+    ap.add_argument("--requests", type=int, default=200, help="serving: at most this many requests per rate")
+    ap.add_argument("--round-paths", dest="round_paths", type=int, default=1 << 26,
+                    help="serving: camera paths (pixels x passes) per round")
+    ap.add_argument("--rate-512", dest="rate_512", type=float, default=20.0)
+    ap.add_argument("--requests-512", dest="requests_512", type=int, default=40)
     args = ap.parse_args()
     if args.serving:
         run_serving(args)
+        return
+    if args.c4:
+        import torch
+        from differentiablepointrendering_b200.build import build_library
+
+        build_library()
+        dev = torch.device("cuda:0")
+        res = c4_measure(dev, tune=not args.no_tune, iterations=max(1, args.steps if args.steps < 5 else 1))
+        print(json.dumps({"metric": "C4 iters/s", "value": res["batched_iters_per_s"], "unit": "iters/s",
+                          "impl": "ours", "n_gpus": 1, "higher_is_better": True, **res}), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

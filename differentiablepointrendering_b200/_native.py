@@ -31,7 +31,8 @@ class PaleSettings(C.Structure):
                 ("debug_images", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float),
                 ("null_weight", C.c_uint32), ("gradients", C.c_uint32), ("camera_seeds", C.c_uint32),
                 ("gather_batch_paths", C.c_uint32), ("adjoint_batch_paths", C.c_uint32),
-                ("walk_block", C.c_uint32)]
+                ("walk_block", C.c_uint32), ("estimator", C.c_uint32), ("vertex_store", C.c_uint32),
+                ("vertex_store_bytes", C.c_uint64)]
 
 
 class PaleView(C.Structure):
@@ -60,7 +61,8 @@ class PaleStats(C.Structure):
         "gather_queries", "node_visits", "surfel_tests", "photons_scanned", "gather_node_visits",
         "gather_surfel_tests", "gather_photons_scanned", "kernel_launches")] + \
         [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms")] + \
-        [("timed_ms", C.c_float * 4), ("timed_launches", C.c_uint32 * 4)]
+        [("timed_ms", C.c_float * 4), ("timed_launches", C.c_uint32 * 4), ("vertex_bytes", C.c_uint64),
+         ("vertex_chunks_stored", C.c_uint32), ("vertex_chunks_replayed", C.c_uint32)]
 
     TIMED = ("trace", "lookup", "adjoint_bounce", "transport")
 
@@ -126,7 +128,7 @@ SETTINGS_KEYS = {
     "gather_radius": "gather_radius", "leaf_size": "leaf_size", "debug_images": "debug_images",
     "exposure": "exposure", "gamma": "gamma",
     "gather_batch_paths": "gather_batch_paths", "adjoint_batch_paths": "adjoint_batch_paths",
-    "walk_block": "walk_block",
+    "walk_block": "walk_block", "vertex_store_bytes": "vertex_store_bytes",
 }
 IGNORED_KEYS = ("logging", "depth_distort_weight", "normal_consistency_weight")
 
@@ -156,6 +158,12 @@ def settings_from_dict(d: Optional[dict]) -> PaleSettings:
             continue
         if k == "camera_seeds":
             s.camera_seeds = {"selection": 0, "camera": 1}.get(v, v) if isinstance(v, str) else int(v)
+            continue
+        if k == "estimator":
+            s.estimator = {"reference": 0, "gather": 1}.get(v, v) if isinstance(v, str) else int(v)
+            continue
+        if k == "vertices":
+            s.vertex_store = {"auto": 0, "checkpoint": 1, "replay": 2}.get(v, v) if isinstance(v, str) else int(v)
             continue
         if k not in SETTINGS_KEYS:
             raise KeyError(f"unknown renderer setting '{k}'")
@@ -283,6 +291,7 @@ def load_library() -> C.CDLL:
                                               C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),
         "pale_lbvh_node_count": (C.c_uint32, [C.c_uint32, C.c_uint32]),
+        "pale_trace_photon_map": (C.c_int, [C.c_void_p, C.c_void_p]),
         "pale_render_views_loss_device": (C.c_int, [C.c_uint32, C.POINTER(C.c_void_p), C.c_int, C.c_uint32,
                                                     C.POINTER(PaleView), C.c_void_p, C.c_uint32, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -306,7 +315,8 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_get_stats", "pale_build_lbvh_noalloc", "pale_get_asset", "pale_optimizer_step",
             "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device",
             "pale_prune_by_opacity", "pale_densify_long_axis_split", "pale_apply_points_device",
-            "pale_lbvh_node_count", "pale_render_views_loss_device", "pale_render_views_backward_device")
+            "pale_lbvh_node_count", "pale_render_views_loss_device", "pale_render_views_backward_device",
+            "pale_trace_photon_map")
 NOALLOC_MAX_SURFELS = 16384
 
 

@@ -167,6 +167,19 @@ struct pale_handle {
   DBuf<float> img_raw, img_ldr, dldi, dbg, target;
   DBuf<double> loss_part, loss;
   PointsBufs grads;
+  // gather estimator: the vertex store (chunks of the last forward that
+  // fit), the replay scratch (the largest chunk replayed), and what the
+  // last forward rendered: its views, scenes and their BVH and photon-map
+  // generations, which its backward must find unchanged
+  VertexPlan vplan;
+  std::vector<CameraRec> vviews;
+  std::vector<pale_handle*> vscenes;
+  std::vector<uint64_t> vgens;
+  DBuf<float4> vs_rec_xa, vs_rec_ew, vs_ent_d, vs_ent_l, sc_rec_xa, sc_rec_ew, sc_ent_d, sc_ent_l;
+  DBuf<uint4> vs_ent_b, sc_ent_b;
+  DBuf<uint32_t> vs_base, vs_overflow, vs_chunk_base;
+  uint64_t photon_gen = 0;     // photon maps traced or loaded so far
+  uint64_t params_gen = 0;     // surfel parameter writes so far
   uint64_t bvh_gen = 0;        // BVH builds so far
   uint64_t grads_gen = ~0ull;  // build the gradients belong to
   // optimizer state (BVH order; starts over after every build)
@@ -749,11 +762,14 @@ std::vector<ViewReq> all_passes(pale_handle* h, uint32_t nsel, const uint32_t* i
 
 // adjoint: the views' passes are adjoint passes (at most the scene's
 // adjoint_passes), else gather passes (at most its gather_passes).
-void check_views(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views, bool adjoint) {
+// allow_twice: one scene may fill several entries of the list (an adjoint
+// call whose entries have gradient arrays of their own).
+void check_views(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views, bool adjoint,
+                 bool allow_twice = false) {
   if (scenes.empty() || scenes.size() > kMaxScenes) throw ArgError("a call renders 1 to 8 scenes");
   for (size_t k = 0; k < scenes.size(); ++k) {
     if (!scenes[k]) throw ArgError("null scene handle");
-    for (size_t j = 0; j < k; ++j)
+    for (size_t j = 0; j < k && !allow_twice; ++j)
       if (scenes[j] == scenes[k]) throw ArgError("a scene appears twice in the scene list");
   }
   for (const ViewReq& v : views) {
@@ -829,6 +845,7 @@ void trace_photon_map(pale_handle* h) {
   G.d_attempts = h->g_attempts.p;
   grid_build(P.scene, h->run.p, P.ps, G, h->cells, h->key_bits, s);
   CK(cudaMemcpyAsync(h->cam_cursor.p, &h->run.p->seed_cursor, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  ++h->photon_gen;
 }
 
 // The scene table of a call: every scene's view, with the same number of
@@ -867,6 +884,78 @@ std::vector<CameraRec> view_records(const std::vector<pale_handle*>& scenes, con
   return sel;
 }
 
+// The camera gather's arguments for the views whose records are in
+// h->d_cams (h = scenes[0], whose wavefront buffers the gather uses).
+FrameArgs frame_args(const std::vector<pale_handle*>& scenes, uint32_t nsel, uint32_t total) {
+  pale_handle* h = scenes[0];
+  FrameArgs F{};
+  F.scenes = scene_table(scenes);
+  for (size_t k = 0; k < scenes.size(); ++k) F.sseeds[k] = SceneSeeds{scenes[k]->seeds_fwd.p, scenes[k]->cam_cursor.p};
+  F.st = h->run.p;
+  F.cams = h->d_cams.p;
+  F.ncams = nsel;
+  F.total_pixels = total;
+  F.rng_mode = h->st.rng_mode;
+  F.exposure = h->st.exposure;
+  F.gamma = h->st.gamma;
+  F.paths[0] = h->cg_paths.p;
+  F.paths[1] = h->cg_paths2.p;
+  F.qrec = h->cg_qrec.p;
+  F.info_a = h->cg_info_a.p;
+  F.info_b = h->cg_info_b.p;
+  F.mhit = h->cg_mhit.p;
+  F.walk = h->cg_walk.p;
+  F.khit = h->cg_khit.p;
+  F.counts = h->cg_counts.p;
+  F.res = h->cg_res.p;
+  F.fb = h->cg_fb.p;
+  F.path_capacity = h->path_cap;
+  F.walk_block = h->st.walk_block;
+  F.timer = &h->timer;
+  return F;
+}
+
+// Bytes of the vertex store per record slot and per entry slot.
+constexpr uint64_t kRecSlotBytes = 2 * sizeof(float4), kEntSlotBytes = 2 * sizeof(float4) + sizeof(uint4);
+
+// Before a forward with the gather estimator: the store grows to hold every
+// chunk of the previous forward (with 1/16 to spare), when the vertex_store
+// mode is "checkpoint", or "auto" and the bytes fit the budget
+// (vertex_store_bytes; 0 = half the device memory free now).  A training
+// loop renders the same views every iteration, so from its second
+// iteration on every chunk is kept.
+void vertex_store_grow(pale_handle* h) {
+  const pale_settings& st = h->st;
+  if (st.vertex_store == PALE_VERTICES_REPLAY) return;
+  uint64_t recs = 0, ents = 0;
+  for (const VertexChunk& c : h->vplan.chunks) {
+    recs += c.recs;
+    ents += c.ents;
+  }
+  recs += recs / 16 + 1024;
+  ents += ents / 16 + 1024;
+  if (recs <= h->vs_rec_xa.n && ents <= h->vs_ent_d.n) return;
+  if (recs >= (1ull << 32) || ents >= (1ull << 32)) return;   // slots are 32-bit: the chunks are replayed
+  const uint64_t bytes = recs * kRecSlotBytes + ents * kEntSlotBytes;
+  if (st.vertex_store == PALE_VERTICES_AUTO) {
+    uint64_t budget = st.vertex_store_bytes;
+    if (!budget) {
+      size_t free_b = 0, total_b = 0;
+      CK(cudaMemGetInfo(&free_b, &total_b));
+      budget = free_b / 2 + h->vs_rec_xa.n * kRecSlotBytes + h->vs_ent_d.n * kEntSlotBytes;
+    }
+    if (bytes > budget) return;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  h->vs_rec_xa.alloc(recs); h->vs_rec_ew.alloc(recs);
+  h->vs_ent_d.alloc(ents); h->vs_ent_b.alloc(ents); h->vs_ent_l.alloc(ents);
+}
+
+uint64_t vertex_bytes(const pale_handle* h) {
+  return h->vs_rec_xa.n * kRecSlotBytes + h->vs_ent_d.n * kEntSlotBytes + h->sc_rec_xa.n * kRecSlotBytes +
+         h->sc_ent_d.n * kEntSlotBytes;
+}
+
 // The forward render of `views` into packed device images, on the stream
 // of scenes[0], whose wavefront buffers the call uses; the other scenes
 // lend their scene data (surfels, LBVH, meshes, photon grid).  With
@@ -887,52 +976,58 @@ uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector
   h->d_cams.ensure(std::max<size_t>(1, nsel));
   h->d_view_start.ensure(std::max<size_t>(1, nsel));
   if (nsel) CK(cudaMemcpyAsync(h->d_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
+  // photon maps of the scenes that some view renders (a scene of the list
+  // without views, such as a handle that only lends its wavefront buffers,
+  // is left alone)
+  std::vector<char> used(scenes.size(), 0);
+  for (const ViewReq& v : views) used[v.scene] = 1;
+  CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+  CK(cudaEventRecord(h->ev0, s));
   for (size_t k = 0; k < scenes.size(); ++k) {
     pale_handle* sk = scenes[k];
+    if (!used[k]) continue;
     forward_seeds(sk, views.size());
     if (trace_photons) {
-      CK(cudaMemsetAsync(sk->run.p, 0, sizeof(RunState), s));
-      if (k == 0) CK(cudaEventRecord(h->ev0, s));
+      if (sk != h) CK(cudaMemsetAsync(sk->run.p, 0, sizeof(RunState), s));
       trace_photon_map(sk);
     }
   }
-  if (!trace_photons) {
-    CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
-    CK(cudaEventRecord(h->ev0, s));
-  }
   CK(cudaEventRecord(h->ev1, s));
-  FrameArgs F{};
-  F.scenes = scene_table(scenes);
-  for (size_t k = 0; k < scenes.size(); ++k) F.sseeds[k] = SceneSeeds{scenes[k]->seeds_fwd.p, scenes[k]->cam_cursor.p};
-  F.st = h->run.p;
-  F.cams = h->d_cams.p;
-  F.ncams = nsel;
-  F.total_pixels = total;
+  FrameArgs F = frame_args(scenes, nsel, total);
   F.raw = d_raw;
   F.ldr = d_ldr;
-  F.rng_mode = h->st.rng_mode;
-  F.exposure = h->st.exposure;
-  F.gamma = h->st.gamma;
-  F.paths[0] = h->cg_paths.p;
-  F.paths[1] = h->cg_paths2.p;
-  F.qrec = h->cg_qrec.p;
-  F.info_a = h->cg_info_a.p;
-  F.info_b = h->cg_info_b.p;
-  F.mhit = h->cg_mhit.p;
-  F.walk = h->cg_walk.p;
-  F.khit = h->cg_khit.p;
-  F.counts = h->cg_counts.p;
-  F.res = h->cg_res.p;
-  F.fb = h->cg_fb.p;
-  F.path_capacity = h->path_cap;
-  F.walk_block = h->st.walk_block;
-  F.timer = &h->timer;
   if (lq) {
     F.target = lq->target;
     F.target_channels = lq->channels;
     F.dldi = lq->dldi;
   }
-  camera_gather(F, sel, h->d_view_start.p, s);
+  VertexPlan* plan = nullptr;
+  if (h->st.estimator == PALE_ESTIMATOR_GATHER) {
+    // keep the path vertices: in the store while the chunks fit, else only
+    // their counts (the backward replays those chunks)
+    plan = &h->vplan;
+    vertex_store_grow(h);
+    const size_t nchunks = gather_chunks(sel, h->path_cap).size();
+    h->vs_base.ensure(2 * kVertexBases);
+    h->vs_overflow.ensure(1);
+    h->vs_chunk_base.ensure(std::max<size_t>(1, nchunks) * 2 * kVertexBases);
+    plan->d_chunk_base = h->vs_chunk_base.p;
+    plan->store = h->st.vertex_store != PALE_VERTICES_REPLAY && h->vs_rec_xa.p && h->vs_ent_d.p;
+    F.vs = VertexStore{h->vs_rec_xa.p, h->vs_rec_ew.p, h->vs_ent_d.p, h->vs_ent_b.p, h->vs_ent_l.p, h->vs_base.p,
+                       h->vs_overflow.p, (uint32_t)h->vs_rec_xa.n, (uint32_t)h->vs_ent_d.n, 0u, 0u, 0};
+    h->vviews.clear();   // valid again once the gather has run
+  }
+  camera_gather(F, sel, h->d_view_start.p, s, plan);
+  if (plan) {
+    h->vviews = sel;
+    h->vscenes = scenes;
+    h->vgens.clear();
+    for (pale_handle* sk : scenes) {
+      h->vgens.push_back(sk->bvh_gen);
+      h->vgens.push_back(sk->photon_gen);
+      h->vgens.push_back(sk->params_gen);
+    }
+  }
   if (lq && lq->loss) {
     h->loss_part.ensure((size_t)std::max(1u, nsel) * kLossChunks);
     image_loss(F, h->loss_part.p, lq->loss, s);
@@ -966,18 +1061,73 @@ void zero_grads(pale_handle* h, cudaStream_t s) {
   CK(cudaMemsetAsync(g.shape.p, 0, 4 * n, s));
 }
 
+// The gather estimator's backward: the derivative of the last forward
+// render of the same views (h = scenes[0] holds its vertex plan), swept
+// from the vertex store where its chunks were kept and replayed into the
+// scratch store where they were not.
+void gather_adjoint(const std::vector<pale_handle*>& scenes, const std::vector<CameraRec>& sel, uint32_t total,
+                    const float* d_dldi, const SceneGrads* grads, bool all) {
+  pale_handle* h = scenes[0];
+  cudaStream_t s = h->stream;
+  bool same = !h->vviews.empty() && h->vviews.size() == sel.size() && h->vscenes == scenes &&
+              std::memcmp(h->vviews.data(), sel.data(), sel.size() * sizeof(CameraRec)) == 0;
+  for (size_t k = 0; same && k < scenes.size(); ++k)
+    same = h->vgens[3 * k] == scenes[k]->bvh_gen && h->vgens[3 * k + 1] == scenes[k]->photon_gen &&
+           h->vgens[3 * k + 2] == scenes[k]->params_gen;
+  if (!same)
+    throw ArgError("the gather estimator differentiates the last forward render: render the same views, with "
+                   "the same points and photon maps, right before the backward");
+  const uint32_t nsel = (uint32_t)sel.size();
+  CK(cudaMemcpyAsync(h->d_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
+  FrameArgs F = frame_args(scenes, nsel, total);
+  F.view_start = h->d_view_start.p;
+  // the replay scratch: the largest chunk that was not stored
+  uint64_t recs = 0, ents = 0;
+  for (const VertexChunk& c : h->vplan.chunks)
+    if (!c.stored) {
+      recs = std::max<uint64_t>(recs, c.recs);
+      ents = std::max<uint64_t>(ents, c.ents);
+    }
+  if (recs) {
+    h->sc_rec_xa.ensure(recs); h->sc_rec_ew.ensure(recs);
+    h->sc_ent_d.ensure(ents); h->sc_ent_b.ensure(ents); h->sc_ent_l.ensure(ents);
+  }
+  h->vs_base.ensure(2 * kVertexBases);
+  h->vs_overflow.ensure(1);
+  F.vs = VertexStore{h->vs_rec_xa.p, h->vs_rec_ew.p, h->vs_ent_d.p, h->vs_ent_b.p, h->vs_ent_l.p, h->vs_base.p,
+                     h->vs_overflow.p, (uint32_t)h->vs_rec_xa.n, (uint32_t)h->vs_ent_d.n, 0u, 0u, 0};
+  VertexStore scratch{h->sc_rec_xa.p, h->sc_rec_ew.p, h->sc_ent_d.p, h->sc_ent_b.p, h->sc_ent_l.p, h->vs_base.p,
+                      h->vs_overflow.p, (uint32_t)h->sc_rec_xa.n, (uint32_t)h->sc_ent_d.n, 0u, 0u, 1};
+  SweepArgs W{};
+  W.dldi = d_dldi;
+  for (size_t k = 0; k < scenes.size(); ++k) W.grads[k] = grads[k];
+  W.all_grads = all ? 1 : 0;
+  gather_backward(F, sel, h->vplan, W, scratch, s);
+  uint32_t stored = 0;
+  for (const VertexChunk& c : h->vplan.chunks) stored += c.stored ? 1u : 0u;
+  h->stats.vertex_chunks_stored = stored;
+  h->stats.vertex_chunks_replayed = (uint32_t)h->vplan.chunks.size() - stored;
+  h->stats.vertex_bytes = vertex_bytes(h);
+}
+
 // The adjoint pass of `views` reading packed dL/dI at d_dldi (device), on
 // the stream and with the wavefront buffers of scenes[0]; each scene's
 // gradients accumulate in its own arrays (BVH order).  All scenes share
 // the rng mode, the null weighting and the gradient groups of scenes[0].
+// out: null, or per entry of `scenes` DEVICE gradient arrays (every field
+// but shape non-null) that the entry's gradients accumulate in, zeroed
+// first, instead of the scene's own arrays; then one scene may fill
+// several entries (one per request of a server).
 void adjoint_views(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views, const float* d_dldi,
-                   float* d_dbg, bool sync) {
+                   float* d_dbg, bool sync, const pale_points* out = nullptr) {
   pale_handle* h = scenes[0];
   cudaStream_t s = h->stream;
   h->timer.used = 0;
   const uint64_t launches0 = launches_issued();
   const pale_settings& st = h->st;
-  check_views(scenes, views, true);
+  // the gather estimator differentiates a forward render: its views carry
+  // gather passes
+  check_views(scenes, views, st.estimator != PALE_ESTIMATOR_GATHER, out != nullptr);
   uint32_t total = 0, max_pix = 0;
   std::vector<CameraRec> sel = view_records(scenes, views, total, max_pix);
   size_wavefronts(h, total, max_pix);
@@ -1001,12 +1151,39 @@ void adjoint_views(const std::vector<pale_handle*>& scenes, const std::vector<Vi
   }
   h->seeds_adj.ensure(seeds.size());
   CK(cudaMemcpyAsync(h->seeds_adj.p, seeds.data(), seeds.size() * 4, cudaMemcpyHostToDevice, s));
-  for (pale_handle* sk : scenes) zero_grads(sk, s);
+  AdjointArgs A{};
+  for (size_t k = 0; k < scenes.size(); ++k) {
+    pale_handle* sk = scenes[k];
+    if (!out) {
+      zero_grads(sk, s);
+      A.sgrads[k] = SceneGrads{sk->grads.op.p, sk->grads.view()};
+      continue;
+    }
+    const pale_points& g = out[k];
+    if (!g.position || !g.tangent_u || !g.tangent_v || !g.scale || !g.albedo || !g.opacity || !g.beta)
+      throw ArgError("gradient outputs need every field but shape");
+    const size_t n = sk->np;
+    for (float* f : {g.position, g.tangent_u, g.tangent_v, g.albedo}) CK(cudaMemsetAsync(f, 0, 12 * n, s));
+    CK(cudaMemsetAsync(g.scale, 0, 8 * n, s));
+    CK(cudaMemsetAsync(g.opacity, 0, 4 * n, s));
+    CK(cudaMemsetAsync(g.beta, 0, 4 * n, s));
+    if (g.shape) CK(cudaMemsetAsync(g.shape, 0, 4 * n, s));
+    PointsDev pd{g.position, g.tangent_u, g.tangent_v, g.scale, g.albedo, g.opacity, g.beta, g.shape};
+    A.sgrads[k] = SceneGrads{g.opacity, pd};
+  }
   CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
   CK(cudaEventRecord(h->ev0, s));
-  AdjointArgs A{};
+  if (st.estimator == PALE_ESTIMATOR_GATHER) {
+    gather_adjoint(scenes, sel, total, d_dldi, A.sgrads, st.gradients == PALE_GRADIENTS_ALL);
+    CK(cudaEventRecord(h->ev1, s));
+    CK(cudaGetLastError());
+    h->launches_last = launches_issued() - launches0;
+    h->timed = 2;
+    h->stats_pending = 1;
+    if (sync) copy_stats(h);
+    return;
+  }
   A.scenes = scene_table(scenes);
-  for (size_t k = 0; k < scenes.size(); ++k) A.sgrads[k] = SceneGrads{scenes[k]->grads.op.p, scenes[k]->grads.view()};
   A.st = h->run.p;
   A.seeds = h->seeds_adj.p;
   A.qb = QueueBufs{{h->q0.p, h->q1.p}, h->qstage.p, h->qflags.p, h->tile_counts.p, h->tile_offsets.p,
@@ -1087,7 +1264,7 @@ void adjoint_views(const std::vector<pale_handle*>& scenes, const std::vector<Vi
 
 void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d_dldi, float* d_dbg, bool sync) {
   validate_cams(h, nsel, idx);
-  adjoint_views({h}, all_passes(h, nsel, idx, true), d_dldi, d_dbg, sync);
+  adjoint_views({h}, all_passes(h, nsel, idx, h->st.estimator != PALE_ESTIMATOR_GATHER), d_dldi, d_dbg, sync);
 }
 
 void download_points(pale_handle* h, const PointsBufs& src, pale_points* out) {
@@ -1195,6 +1372,9 @@ int pale_create(const pale_scene_desc* desc, const pale_settings* settings, pale
     if (h->st.camera_seeds > PALE_CAMERA_SEEDS_CAMERA) throw ArgError("camera_seeds must be selection or camera");
     if (h->st.walk_block != 0 && h->st.walk_block != 64 && h->st.walk_block != 128 && h->st.walk_block != 256)
       throw ArgError("walk_block must be 64, 128 or 256");
+    if (h->st.estimator > PALE_ESTIMATOR_GATHER) throw ArgError("estimator must be 0 (reference) or 1 (gather)");
+    if (h->st.vertex_store > PALE_VERTICES_REPLAY)
+      throw ArgError("vertex_store must be 0 (auto), 1 (checkpoint) or 2 (replay)");
     if (h->st.null_weight == PALE_NULL_WEIGHT_UNBIASED && !(h->st.q_null > 0.f))
       throw ArgError("unbiased null weighting needs q_null > 0");
     check_points(&desc->points, "pale_create");
@@ -1413,20 +1593,6 @@ std::vector<ViewReq> view_list(uint32_t n, const pale_view* views) {
   return v;
 }
 
-void copy_grads_out(pale_handle* h, pale_points* d_grads, cudaStream_t s) {
-  const size_t n = h->np;
-  auto cp = [&](float* dst, const float* src, size_t bytes) {
-    if (dst && n) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
-  };
-  cp(d_grads->position, h->grads.pos.p, 12 * n);
-  cp(d_grads->tangent_u, h->grads.tu.p, 12 * n);
-  cp(d_grads->tangent_v, h->grads.tv.p, 12 * n);
-  cp(d_grads->scale, h->grads.sc.p, 8 * n);
-  cp(d_grads->albedo, h->grads.alb.p, 12 * n);
-  cp(d_grads->opacity, h->grads.op.p, 4 * n);
-  cp(d_grads->beta, h->grads.beta.p, 4 * n);
-  cp(d_grads->shape, h->grads.shape.p, 4 * n);
-}
 }  // namespace
 
 int pale_render_views_loss_device(uint32_t num_scenes, pale_handle* const* scenes, int trace_photons,
@@ -1456,6 +1622,18 @@ int pale_render_views_loss_device(uint32_t num_scenes, pale_handle* const* scene
   });
 }
 
+int pale_trace_photon_map(pale_handle* h, void* stream) {
+  if (!h) return PALE_ERR_ARGUMENT;
+  return guarded(h, [&]() {
+    use_stream(h, caller_stream(stream));
+    forward_seeds(h, h->cams.size());
+    CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), h->stream));
+    trace_photon_map(h);
+    CK(cudaGetLastError());
+    return PALE_OK;
+  });
+}
+
 int pale_render_views_backward_device(uint32_t num_scenes, pale_handle* const* scenes, uint32_t num_views,
                                       const pale_view* views, const float* d_dldi, pale_points* d_grads,
                                       void* stream) {
@@ -1467,9 +1645,7 @@ int pale_render_views_backward_device(uint32_t num_scenes, pale_handle* const* s
     if (num_views && !d_dldi) throw ArgError("dL/dI is null");
     const cudaStream_t s = caller_stream(stream);
     for (pale_handle* sk : sc) use_stream(sk, s);
-    adjoint_views(sc, vw, d_dldi, nullptr, false);
-    if (d_grads)
-      for (size_t k = 0; k < sc.size(); ++k) copy_grads_out(sc[k], &d_grads[k], s);
+    adjoint_views(sc, vw, d_dldi, nullptr, false, d_grads);
     return PALE_OK;
   });
 }
@@ -1512,6 +1688,7 @@ int pale_apply_points(pale_handle* h, const pale_points* p) {
     CK(cudaMemcpyAsync(d.beta.p, p->beta, 4 * n, cudaMemcpyHostToDevice, s));
     derive_surfels(d.view(), h->np, SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p},
                    s);
+    ++h->params_gen;
     copy_points(h, d, h->asset, s);   // the asset mirrors the written parameters
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
@@ -1541,6 +1718,7 @@ int pale_apply_points_device(pale_handle* h, const pale_points* p, void* stream)
     cp(d.beta.p, p->beta, 4 * n);
     derive_surfels(d.view(), h->np, SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p},
                    s);
+    ++h->params_gen;
     copy_points(h, d, h->asset, s);
     CK(cudaGetLastError());
     return PALE_OK;
@@ -1789,6 +1967,7 @@ int pale_optimizer_step(pale_handle* h, const pale_optimizer* o, const pale_poin
     optimizer_step(A, s);
     derive_surfels(h->params.view(), n,
                    SurfelArrays{h->sf_pe.p, h->sf_n.p, h->sf_u.p, h->sf_v.p, h->sf_cn.p, h->sf_alb.p}, s);
+    ++h->params_gen;
     CK(cudaGetLastError());
     return PALE_OK;
   });
@@ -1887,6 +2066,7 @@ int pale_load_photons(pale_handle* h, uint32_t n, const float* pos, const float*
     }
     PhotonStore ps{h->ph_a.p, h->ph_b.p, h->ph_c.p, h->ph_sa.p, h->ph_sb.p, h->ph_sc.p, h->photon_cap};
     load_photon_arrays(n, dP.p, dW.p, dD.p, ps, s);
+    ++h->photon_gen;
     CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
     CK(cudaMemcpyAsync(&h->run.p->photon_attempts, &n, 4, cudaMemcpyHostToDevice, s));
     GridBufs G{};

@@ -194,6 +194,29 @@ struct SceneGrads {
   PointsDev all;          // all seven groups, written when all_grads
 };
 
+// The camera gather's path vertices, for the gather estimator (the exact
+// derivative of the gathered image with the photon map held).  Every queue
+// entry of a round (a live camera path) and every lookup record of its
+// layers get a slot: records at base[r] + (the record's index in round r),
+// entries at base[kVertexBases + r] + (the entry's index in round r).  The
+// bases are kept whenever `base` is set (the record and entry counts of a
+// chunk); slots are written when `write` is set and dropped, with
+// *overflow set, past the capacities.
+constexpr uint32_t kVertexBases = kMaxLayers + 1;
+
+struct VertexStore {
+  float4* rec_xa;       // surfel layer: hit point, alpha_geom
+  float4* rec_ew;       // irradiance at the layer (or at the mesh that ends the path), index word
+  float4* ent_d;        // ray direction, transmittance in front of the entry's first layer
+  uint4* ent_b;         // first record, records | emitter << 8, next round's entry or kInvalid, path
+  float4* ent_l;        // emitter radiance (unattenuated); the sweep's radiance behind the entry's front
+  uint32_t* base;       // 2 * kVertexBases words
+  uint32_t* overflow;
+  uint32_t rec_cap, ent_cap;
+  uint32_t rec_start, ent_start;   // where the chunk's first round starts
+  int write;
+};
+
 struct FrameArgs {
   SceneTable scenes;
   SceneSeeds sseeds[kMaxScenes];
@@ -238,6 +261,8 @@ struct FrameArgs {
   const float* target;
   uint32_t target_channels;
   float* dldi;
+  // the gather estimator's vertex store (base null: not kept)
+  VertexStore vs;
 };
 
 // LBVH nodes duplicated in breadth-first order at the front of the node
@@ -381,7 +406,43 @@ void grid_build(const SceneView& sv, RunState* st, const PhotonStore& ps, const 
 // The camera gather of the views `views` (host copy of a.cams; every view
 // passes >= 1); d_view_start holds views.size() words of device scratch.
 void camera_gather(const FrameArgs& a, const std::vector<CameraRec>& views, uint32_t* d_view_start,
-                   cudaStream_t s);
+                   cudaStream_t s, struct VertexPlan* plan = nullptr);
+
+// The chunks of a camera gather: runs of whole passes [p0, p1) whose paths
+// (every view's passes in the run) fit the path capacity, one pass at least.
+std::vector<std::pair<uint32_t, uint32_t>> gather_chunks(const std::vector<CameraRec>& views, uint32_t path_capacity);
+
+// Host record of a camera gather kept for the gather estimator: per chunk
+// its passes, paths, rounds, where its slots start and how many it used,
+// whether they were stored, and its view_start table; d_chunk_base holds
+// each chunk's 2 * kVertexBases bases.
+struct VertexChunk {
+  uint32_t p0 = 0, p1 = 0, n = 0, rounds = 0;
+  uint32_t rec_start = 0, ent_start = 0, recs = 0, ents = 0;
+  bool stored = false;
+  std::vector<uint32_t> starts;
+};
+
+struct VertexPlan {
+  bool store = false;          // write the chunks' slots while they fit
+  std::vector<VertexChunk> chunks;
+  uint32_t* d_chunk_base = nullptr;   // chunks.size() * 2 * kVertexBases words
+};
+
+// The gather estimator's backward over the chunks of `plan`: each stored
+// chunk is swept from the store; any other is replayed (its rounds traced
+// again with the forward's seeds, its slots written from 0) and swept.
+// a: the forward's frame arguments with a.vs the store and a.view_start the
+// device table; scratch: the store replayed chunks are written to (big
+// enough for the largest chunk not stored).  The sweep reads dL/dI (float4
+// per packed pixel) and accumulates into the scenes' gradient arrays.
+struct SweepArgs {
+  const float* dldi;
+  SceneGrads grads[kMaxScenes];
+  int all_grads;
+};
+void gather_backward(const FrameArgs& a, const std::vector<CameraRec>& views, const VertexPlan& plan,
+                     const SweepArgs& w, const VertexStore& scratch, cudaStream_t s);
 void adjoint_raygen(const AdjointArgs& a, uint32_t npaths, cudaStream_t s);
 void adjoint_bounce(const AdjointArgs& a, uint32_t bounce, uint32_t npaths, cudaStream_t s);
 

@@ -419,6 +419,11 @@ __device__ __forceinline__ uint32_t view_of_path(const FrameArgs& A, uint32_t pa
 __global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1, uint32_t n) {
   const uint32_t path = blockIdx.x * kBlock + threadIdx.x;
   if (path == 0) A.counts[0] = n;
+  if (path == 0 && A.vs.base) {
+    A.vs.base[0] = A.vs.rec_start;
+    A.vs.base[kVertexBases] = A.vs.ent_start;
+    *A.vs.overflow = 0u;
+  }
   if (path >= n) return;
   const uint32_t v = view_of_path(A, path);
   const CameraRec& C = A.cams[v];
@@ -453,6 +458,28 @@ __device__ __forceinline__ void put_record(float4* q, uint32_t r, V3 pos, float 
                                            uint32_t kind, uint32_t sid) {
   q[2 * (size_t)r] = make_float4(pos.x, pos.y, pos.z, w);
   q[2 * (size_t)r + 1] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(idx | (sid << 27) | (kind << 30)));
+}
+
+// Vertex-store slot of record / entry `i` of round `round` (kInvalid when
+// the store is not written or the slot lies past its capacity).
+__device__ __forceinline__ uint32_t vs_rec_slot(const FrameArgs& A, uint32_t round, uint32_t i) {
+  if (!A.vs.write) return kInvalid;
+  const uint64_t g = (uint64_t)A.vs.base[round] + i;
+  if (g >= A.vs.rec_cap) {
+    atomicOr(A.vs.overflow, 1u);
+    return kInvalid;
+  }
+  return (uint32_t)g;
+}
+
+__device__ __forceinline__ uint32_t vs_ent_slot(const FrameArgs& A, uint32_t round, uint32_t i) {
+  if (!A.vs.write) return kInvalid;
+  const uint64_t g = (uint64_t)A.vs.base[kVertexBases + round] + i;
+  if (g >= A.vs.ent_cap) {
+    atomicOr(A.vs.overflow, 1u);
+    return kInvalid;
+  }
+  return (uint32_t)g;
 }
 
 // Round step 1: one lane per queue entry (a live path).
@@ -642,6 +669,8 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
         V3 nrm = xyz(__ldg(&S.sf.cn[pl[i]]));
         if (dot(nrm, -d) < 0.0f) nrm = -nrm;
         put_record(A.qrec, first + used, x, T * ae, nrm, pl[i], kRecSurfel, sid);
+        const uint32_t vr = vs_rec_slot(A, round, first + used);
+        if (vr != kInvalid) A.vs.rec_xa[vr] = make_float4(x.x, x.y, x.z, a);
         ++used;
         T *= (1.0f - ae);
         if (layer + 1 >= (uint32_t)kMaxLayers) {
@@ -668,6 +697,8 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
               Le = v3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
               c_em = scale(Le, T);
               flags = 1;
+              const uint32_t ve = vs_ent_slot(A, round, slot);
+              if (ve != kInvalid) A.vs.ent_l[ve] = make_float4(Le.x, Le.y, Le.z, 0.f);
             } else {
               put_record(A.qrec, first + used, h2.pos, T, hit_normal(S, h2), mi, kRecMesh, sid);
               ++used;
@@ -697,6 +728,14 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_cg_round(FrameArgs 
         out[next] = nr;
       }
       A.info_a[slot] = make_uint4(first, nslots | (flags << 8), __float_as_uint(rec.o.w), next);
+      const uint32_t ve = vs_ent_slot(A, round, slot);
+      if (ve != kInvalid) {
+        // the entry's first record and the next round's entry as store slots
+        const uint32_t rb = A.vs.base[round], eb = A.vs.base[kVertexBases + round];
+        A.vs.ent_d[ve] = rec.d;
+        A.vs.ent_b[ve] = make_uint4(rb + first, used | (flags << 8), next != kInvalid ? eb + n + next : kInvalid,
+                                    __float_as_uint(rec.o.w));
+      }
     }
   }
   warp_count(&A.st->gather_segments, segs);
@@ -743,6 +782,8 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArg
       }
       const V3 c = scale(Lo, ra.w);
       A.qrec[2 * (size_t)i] = make_float4(c.x, c.y, c.z, 0.f);
+      const uint32_t vr = vs_rec_slot(A, round, i);
+      if (vr != kInvalid) A.vs.rec_ew[vr] = make_float4(E.x, E.y, E.z, rb.w);
     }
   }
   warp_count(&A.st->gather_queries, queries);
@@ -755,6 +796,11 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArg
 // the sum to the path's next-round entry or to res[path].
 __global__ void k_cg_compose(FrameArgs A, uint32_t round) {
   const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e == 0 && A.vs.base) {
+    // the next round's slots follow this round's records and entries
+    A.vs.base[round + 1] = A.vs.base[round] + A.counts[kMaxLayers + 2 + round];
+    A.vs.base[kVertexBases + round + 1] = A.vs.base[kVertexBases + round] + A.counts[round];
+  }
   if (e >= A.counts[round]) return;
   const RayRec* __restrict__ in = A.paths[round & 1];
   RayRec* __restrict__ out = A.paths[(round + 1) & 1];
@@ -862,11 +908,7 @@ void image_loss(const FrameArgs& a, double* partials, double* loss, cudaStream_t
   k_loss_final<<<(a.ncams + 63) / 64, 64, 0, s>>>(a, partials, kLossChunks, loss); note_launch();
 }
 
-template <bool kMulti>
-static void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>& views, uint32_t* d_view_start,
-                               cudaStream_t s) {
-  FrameArgs a = a0;
-  a.view_start = d_view_start;
+std::vector<std::pair<uint32_t, uint32_t>> gather_chunks(const std::vector<CameraRec>& views, uint32_t path_capacity) {
   uint32_t max_passes = 0;
   for (const CameraRec& v : views) max_passes = std::max(max_passes, v.passes);
   // paths of the chunk of passes [p0, p1): every view's passes in it
@@ -878,62 +920,145 @@ static void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>
     }
     return n;
   };
+  std::vector<std::pair<uint32_t, uint32_t>> out;
+  for (uint32_t p0 = 0, p1 = 0; p0 < max_passes; p0 = p1) {
+    p1 = p0 + 1;
+    while (p1 < max_passes && chunk_paths(p0, p1 + 1) <= path_capacity) ++p1;
+    out.emplace_back(p0, p1);
+  }
+  return out;
+}
+
+namespace {
+
+// view_start of the chunk [p0, p1): each view's first path in it
+std::vector<uint32_t> chunk_starts(const std::vector<CameraRec>& views, uint32_t p0, uint32_t p1, uint32_t& n) {
+  std::vector<uint32_t> starts(views.size());
+  uint64_t acc = 0;
+  for (size_t v = 0; v < views.size(); ++v) {
+    starts[v] = (uint32_t)acc;
+    const uint32_t q1 = std::min(p1, views[v].passes);
+    if (q1 > p0) acc += (uint64_t)views[v].w * views[v].h * (q1 - p0);
+  }
+  n = (uint32_t)acc;
+  return starts;
+}
+
+// The launch shapes of the camera gather's kernels.
+struct GatherShape {
+  uint32_t grid_r = 1, grid_l = 1;
+  int wt = kBlock;
+  size_t smem = 0;
+};
+
+template <bool kMulti>
+GatherShape gather_shape(const FrameArgs& a) {
+  GatherShape g;
   // persistent grids: every SM filled once
   int dev = 0, sms = 148, per_sm_l = 1, per_sm_r = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int wt = a.walk_block == 64 || a.walk_block == 128 ? (int)a.walk_block : kBlock;
-  const size_t smem = top_smem(a.scenes, wt);
+  g.wt = a.walk_block == 64 || a.walk_block == 128 ? (int)a.walk_block : kBlock;
+  g.smem = top_smem(a.scenes, g.wt);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_cg_round<kGatherHits>, kBlock, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup<kMulti>, kBlock, 0);
-  const uint32_t grid_r = (uint32_t)std::max(1, sms * std::max(1, per_sm_r));
-  const uint32_t grid_l = (uint32_t)std::max(1, sms * std::max(1, per_sm_l));
-  std::vector<uint32_t> starts(views.size());
-  for (uint32_t p0 = 0, p1 = 0; p0 < max_passes; p0 = p1) {
-    // chunks of whole passes: as many as the path capacity holds (one at least)
-    p1 = p0 + 1;
-    while (p1 < max_passes && chunk_paths(p0, p1 + 1) <= a.path_capacity) ++p1;
-    uint64_t acc = 0;
-    for (size_t v = 0; v < views.size(); ++v) {
-      starts[v] = (uint32_t)acc;
-      const uint32_t q1 = std::min(p1, views[v].passes);
-      if (q1 > p0) acc += (uint64_t)views[v].w * views[v].h * (q1 - p0);
+  g.grid_r = (uint32_t)std::max(1, sms * std::max(1, per_sm_r));
+  g.grid_l = (uint32_t)std::max(1, sms * std::max(1, per_sm_l));
+  return g;
+}
+
+// The rounds of one chunk of n paths (its view_start already on the
+// device); returns the rounds run.
+template <bool kMulti>
+uint32_t gather_rounds(const FrameArgs& a, const GatherShape& g, uint32_t p0, uint32_t p1, uint32_t n,
+                       cudaStream_t s) {
+  cudaMemsetAsync(a.counts, 0, 2 * (kMaxLayers + 2) * sizeof(uint32_t), s);
+  k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1, n); note_launch();
+  // every round consumes at least one layer of each live path, so
+  // kMaxLayers rounds bound the walk (the layer cap ends longer ones)
+  uint32_t round = 0, live = n;
+  while (round < (uint32_t)kMaxLayers && live) {
+    for (uint32_t group = 0; group < 16 && round < (uint32_t)kMaxLayers; ++group, ++round) {
+      if (a.timer) a.timer->begin(kTimeTrace, s);
+      k_cg_mesh<<<g.grid_r, kBlock, 0, s>>>(a, round); note_launch();
+      if (g.wt == 64) launch_walk(k_cg_walk<kGatherHits, kMulti, 64>, 64, a, round, g.smem, ~0u, s);
+      else if (g.wt == 128) launch_walk(k_cg_walk<kGatherHits, kMulti, 128>, 128, a, round, g.smem, ~0u, s);
+      else launch_walk(k_cg_walk<kGatherHits, kMulti, 256>, 256, a, round, g.smem, ~0u, s);
+      k_cg_round<kGatherHits><<<g.grid_r, kBlock, 0, s>>>(a, round); note_launch();
+      if (a.timer) a.timer->end(s);
+      if (a.timer) a.timer->begin(kTimeLookup, s);
+      k_cg_lookup<kMulti><<<g.grid_l, kBlock, 0, s>>>(a, round); note_launch();
+      if (a.timer) a.timer->end(s);
+      // queues only shrink, so `live` bounds the entries of every round of the group
+      k_cg_compose<<<blocks_for(live), kBlock, 0, s>>>(a, round); note_launch();
     }
-    const uint32_t n = (uint32_t)acc;
+    // the host reads the queue length after each group of 16 rounds
+    cudaMemcpyAsync(&live, a.counts + round, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+  }
+  return round;
+}
+
+template <bool kMulti>
+void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>& views, uint32_t* d_view_start,
+                        cudaStream_t s, VertexPlan* plan) {
+  FrameArgs a = a0;
+  a.view_start = d_view_start;
+  const GatherShape g = gather_shape<kMulti>(a);
+  const auto chunks = gather_chunks(views, a.path_capacity);
+  if (plan) plan->chunks.assign(chunks.size(), VertexChunk{});
+  uint32_t rec_used = 0, ent_used = 0;   // stored slots so far
+  bool room = plan && plan->store;
+  for (size_t c = 0; c < chunks.size(); ++c) {
+    const uint32_t p0 = chunks[c].first, p1 = chunks[c].second;
+    uint32_t n = 0;
+    std::vector<uint32_t> starts = chunk_starts(views, p0, p1, n);
     cudaMemcpyAsync(d_view_start, starts.data(), starts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(a.counts, 0, 2 * (kMaxLayers + 2) * sizeof(uint32_t), s);
-    k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1, n); note_launch();
-    // every round consumes at least one layer of each live path, so
-    // kMaxLayers rounds bound the walk (the layer cap ends longer ones)
-    uint32_t round = 0, live = n;
-    while (round < (uint32_t)kMaxLayers && live) {
-      for (uint32_t group = 0; group < 16 && round < (uint32_t)kMaxLayers; ++group, ++round) {
-        if (a.timer) a.timer->begin(kTimeTrace, s);
-        k_cg_mesh<<<grid_r, kBlock, 0, s>>>(a, round); note_launch();
-        if (wt == 64) launch_walk(k_cg_walk<kGatherHits, kMulti, 64>, 64, a, round, smem, ~0u, s);
-        else if (wt == 128) launch_walk(k_cg_walk<kGatherHits, kMulti, 128>, 128, a, round, smem, ~0u, s);
-        else launch_walk(k_cg_walk<kGatherHits, kMulti, 256>, 256, a, round, smem, ~0u, s);
-        k_cg_round<kGatherHits><<<grid_r, kBlock, 0, s>>>(a, round); note_launch();
-        if (a.timer) a.timer->end(s);
-        if (a.timer) a.timer->begin(kTimeLookup, s);
-        k_cg_lookup<kMulti><<<grid_l, kBlock, 0, s>>>(a, round); note_launch();
-        if (a.timer) a.timer->end(s);
-        // queues only shrink, so `live` bounds the entries of every round of the group
-        k_cg_compose<<<blocks_for(live), kBlock, 0, s>>>(a, round); note_launch();
-      }
-      // the host reads the queue length after each group of 16 rounds
-      cudaMemcpyAsync(&live, a.counts + round, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (plan) {
+      // write the chunk after the stored ones while the store has room;
+      // otherwise only count its slots
+      a.vs.write = room ? 1 : 0;
+      a.vs.rec_start = room ? rec_used : 0u;
+      a.vs.ent_start = room ? ent_used : 0u;
+    }
+    const uint32_t rounds = gather_rounds<kMulti>(a, g, p0, p1, n, s);
+    if (plan) {
+      VertexChunk& vc = plan->chunks[c];
+      vc.p0 = p0;
+      vc.p1 = p1;
+      vc.n = n;
+      vc.rounds = rounds;
+      vc.rec_start = a.vs.rec_start;
+      vc.ent_start = a.vs.ent_start;
+      vc.starts = starts;
+      uint32_t tail[3] = {0, 0, 0};
+      cudaMemcpyAsync(plan->d_chunk_base + c * 2 * kVertexBases, a.vs.base, 2 * kVertexBases * sizeof(uint32_t),
+                      cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(&tail[0], a.vs.base + rounds, 4, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(&tail[1], a.vs.base + kVertexBases + rounds, 4, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(&tail[2], a.vs.overflow, 4, cudaMemcpyDeviceToHost, s);
       cudaStreamSynchronize(s);
+      vc.recs = tail[0] - vc.rec_start;
+      vc.ents = tail[1] - vc.ent_start;
+      vc.stored = a.vs.write && tail[2] == 0u;
+      if (vc.stored) {
+        rec_used = tail[0];
+        ent_used = tail[1];
+      } else {
+        room = false;   // the store is full: the later chunks are replayed
+      }
     }
     k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1); note_launch();
   }
 }
 
+}  // namespace
+
 void camera_gather(const FrameArgs& a, const std::vector<CameraRec>& views, uint32_t* d_view_start,
-                   cudaStream_t s) {
+                   cudaStream_t s, VertexPlan* plan) {
   if (a.total_pixels == 0 || views.empty()) return;
-  if (a.scenes.n > 1) camera_gather_impl<true>(a, views, d_view_start, s);
-  else camera_gather_impl<false>(a, views, d_view_start, s);
+  if (a.scenes.n > 1) camera_gather_impl<true>(a, views, d_view_start, s, plan);
+  else camera_gather_impl<false>(a, views, d_view_start, s, plan);
 }
 
 // ------------------------------------------------------------- adjoint
@@ -1362,6 +1487,129 @@ __device__ __forceinline__ AlphaGrad alpha_grad(const SurfelView& S, uint32_t k,
   g.su = k2 * u * (-u / su);
   g.sv = k2 * v * (-v / sv);
   return g;
+}
+
+// The gather estimator's sweep over the entries of one round (rounds are
+// swept last to first, so an entry finds the radiance behind its last
+// layer in the next round's entry).  A camera path composites its layers
+// front to back, I = sum_k T_k a_k Lo_k + T_end L_end with
+// T_{k+1} = T_k (1 - a_k), a_k = opacity alpha_geom(x_k) and
+// Lo_k = E(x_k) albedo alpha_r / pi; with Lb_k the radiance behind layer k
+// (composited back to front, Lb = a Lo + (1 - a) Lb), dI/da_k =
+// T_k (Lo_k - Lb_k).  The loss gradient of layer k, w = dL/dI . dI/da_k
+// over the view's passes, goes to the opacity as w alpha_geom, to beta,
+// position, tangents and scales as w d(a_k)/d(theta) (alpha_grad, the
+// derivatives of the hit's alpha_geom) and to the albedo as
+// dL/dI T_k a_k alpha_r E / pi per channel.  E(x_k) is the photon map's
+// and held; the transmittance T_k is recomputed from the entry's with the
+// forward's float operations.
+__global__ void __launch_bounds__(kBlock) k_vs_sweep(FrameArgs A, SweepArgs W, const uint32_t* __restrict__ base,
+                                                     uint32_t round) {
+  const uint32_t e1 = base[kVertexBases + round + 1];
+  const uint32_t e = base[kVertexBases + round] + blockIdx.x * kBlock + threadIdx.x;
+  if (e >= e1) return;
+  const float4 dT = A.vs.ent_d[e];
+  const uint4 b = A.vs.ent_b[e];
+  const uint32_t used = b.y & 0xFFu, first = b.x, path = b.w;
+  const uint32_t v = view_of_path(A, path);
+  const CameraRec& C = A.cams[v];
+  const SceneView& S = A.scenes.s[C.scene];
+  const SceneGrads& G = W.grads[C.scene];
+  const uint32_t npix = C.w * C.h;
+  const uint32_t gp = C.pixel_offset + (path - A.view_start[v]) % npix;
+  const V3 g = xyz(*reinterpret_cast<const float4*>(W.dldi + 4 * (size_t)gp));
+  const float inv = 1.0f / (float)C.passes;
+  V3 Lb = v3(0.f, 0.f, 0.f);
+  if (b.z != kInvalid) Lb = xyz(A.vs.ent_l[b.z]);
+  else if ((b.y >> 8) & 1u) Lb = xyz(A.vs.ent_l[e]);
+  float Ts[kGatherHits], as[kGatherHits];
+  int ns = 0;
+  float T = dT.w;
+#pragma unroll
+  for (int i = 0; i <= kGatherHits; ++i) {
+    if (i < (int)used) {
+      const float4 ew = A.vs.rec_ew[first + i];
+      const uint32_t word = __float_as_uint(ew.w);
+      const uint32_t kind = word >> 30, idx = word & kRecIndexMask;
+      if (kind == kRecSurfel && i < kGatherHits) {
+        const float ae = __ldg(&S.sf.n[idx]).w * A.vs.rec_xa[first + i].w;
+        Ts[i < kGatherHits ? i : 0] = T;
+        as[i < kGatherHits ? i : 0] = ae;
+        T *= (1.0f - ae);
+        ns = i + 1;
+      } else if (kind == kRecMesh) {
+        const float4 mat = __ldg(&S.mesh.materials[idx]);
+        Lb = mul(scale(xyz(mat), kInvPi), xyz(ew));
+      }
+    }
+  }
+  const V3 dd = normalize(xyz(dT));
+#pragma unroll
+  for (int i = kGatherHits - 1; i >= 0; --i) {
+    if (i < ns) {
+      const float4 xa = A.vs.rec_xa[first + i], ew = A.vs.rec_ew[first + i];
+      const uint32_t k = __float_as_uint(ew.w) & kRecIndexMask;
+      const float4 al = __ldg(&S.sf.alb[k]);
+      const V3 E = xyz(ew);
+      const V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
+      const float w = inv * dot(g, scale(Lo - Lb, Ts[i]));
+      if (w != 0.f) {
+        atomicAdd(&G.opacity[k], w * xa.w);
+        if (W.all_grads) {
+          const AlphaGrad ag = alpha_grad(S.sf, k, xyz(xa), dd);
+          atomicAdd(&G.all.beta[k], w * ag.beta);
+          atomicAdd(&G.all.position[3 * (size_t)k + 0], w * ag.pos.x);
+          atomicAdd(&G.all.position[3 * (size_t)k + 1], w * ag.pos.y);
+          atomicAdd(&G.all.position[3 * (size_t)k + 2], w * ag.pos.z);
+          atomicAdd(&G.all.tangent_u[3 * (size_t)k + 0], w * ag.tu.x);
+          atomicAdd(&G.all.tangent_u[3 * (size_t)k + 1], w * ag.tu.y);
+          atomicAdd(&G.all.tangent_u[3 * (size_t)k + 2], w * ag.tu.z);
+          atomicAdd(&G.all.tangent_v[3 * (size_t)k + 0], w * ag.tv.x);
+          atomicAdd(&G.all.tangent_v[3 * (size_t)k + 1], w * ag.tv.y);
+          atomicAdd(&G.all.tangent_v[3 * (size_t)k + 2], w * ag.tv.z);
+          atomicAdd(&G.all.scale[2 * (size_t)k + 0], w * ag.su);
+          atomicAdd(&G.all.scale[2 * (size_t)k + 1], w * ag.sv);
+        }
+      }
+      if (W.all_grads) {
+        const float ka = inv * Ts[i] * as[i] * al.w * kInvPi;
+        if (ka != 0.f) {
+          atomicAdd(&G.all.albedo[3 * (size_t)k + 0], g.x * ka * E.x);
+          atomicAdd(&G.all.albedo[3 * (size_t)k + 1], g.y * ka * E.y);
+          atomicAdd(&G.all.albedo[3 * (size_t)k + 2], g.z * ka * E.z);
+        }
+      }
+      Lb = scale(Lo, as[i]) + scale(Lb, 1.0f - as[i]);
+    }
+  }
+  A.vs.ent_l[e] = make_float4(Lb.x, Lb.y, Lb.z, 0.f);
+}
+
+void gather_backward(const FrameArgs& a0, const std::vector<CameraRec>& views, const VertexPlan& plan,
+                     const SweepArgs& w, const VertexStore& scratch, cudaStream_t s) {
+  const bool multi = a0.scenes.n > 1;
+  const GatherShape g = multi ? gather_shape<true>(a0) : gather_shape<false>(a0);
+  for (size_t c = 0; c < plan.chunks.size(); ++c) {
+    const VertexChunk& vc = plan.chunks[c];
+    FrameArgs a = a0;
+    cudaMemcpyAsync(const_cast<uint32_t*>(a.view_start), vc.starts.data(), vc.starts.size() * sizeof(uint32_t),
+                    cudaMemcpyHostToDevice, s);
+    const uint32_t* bases = plan.d_chunk_base + c * 2 * kVertexBases;
+    uint32_t rounds = vc.rounds;
+    if (!vc.stored) {
+      // replay: the chunk's rounds again, with the forward's seeds, into
+      // the scratch store from its first slot
+      a.vs = scratch;
+      a.vs.write = 1;
+      a.vs.rec_start = 0;
+      a.vs.ent_start = 0;
+      rounds = multi ? gather_rounds<true>(a, g, vc.p0, vc.p1, vc.n, s) : gather_rounds<false>(a, g, vc.p0, vc.p1, vc.n, s);
+      bases = a.vs.base;
+    }
+    for (uint32_t r = rounds; r-- > 0;) {
+      k_vs_sweep<<<blocks_for(vc.n), kBlock, 0, s>>>(a, w, bases, r); note_launch();
+    }
+  }
 }
 
 // launchAdjointTransportKernel (AdjointKernels.cpp:389-509).  A warp takes

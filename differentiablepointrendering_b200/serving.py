@@ -1,45 +1,55 @@
-"""Serving: resident scenes, continuous admission and merged forward requests.
+"""Serving: resident scenes and continuous batching of render requests.
 
-A :class:`Server` keeps every admitted scene's renderer resident on the GPU
-(surfels, LBVH, photon-map and queue buffers stay allocated between
-requests) and serves two kinds of request as they arrive:
+A :class:`Server` keeps every admitted scene resident on the GPU: its
+surfels, LBVH and photon map are built once when the scene is admitted and
+stay in HBM between requests (the photon map is traced once, at admission,
+as a scene that does not change needs no other).  Two kinds of request:
 
-* ``forward``: the LDR image of one camera;
+* ``forward``: the LDR image of one camera of a scene;
 * ``gradient``: the image, the L2 loss against a target image and the
-  per-surfel gradients of that loss (forward with the fused loss, then the
-  adjoint; the training loop's step 5-6 for one view).
+  per-surfel gradients of that loss (the training loop's forward with the
+  fused loss, then the adjoint, for one view).
 
-Each scene has a worker thread, and each renderer runs on its own CUDA
-stream, so requests for different scenes overlap on the device.  Within a
-scene the worker takes every queued request when it becomes free: the
-forward requests are merged into one render call over their cameras (one
-wavefront over all of them, each camera rendered once however many
-requests ask for it), then the gradient requests run one at a time (the
-adjoint accumulates into one gradient array per scene, so gradient requests
-cannot share a call).  Renderers are created with camera-keyed seeds
-(``camera_seeds="camera"``), so a camera's image does not depend on which
-other cameras share its call: a request gives the same result alone and in
-the mix (gradients up to the order of float atomic additions).
+Each request carries its own number of passes (samples per pixel, gather
+and adjoint) and adjoint bounces, up to the maxima its scene was created
+with; resolutions are the scene's cameras.
 
-Scenes are admitted against an HBM budget: ``add_scene`` measures the
-device memory the new renderer holds after one forward and adjoint pass and
-refuses the scene (:class:`AdmissionError`) if the admitted scenes would
-exceed the budget.  Request latency is measured from ``submit`` to the
-result being ready on the host.
+One dispatcher thread owns the GPU stream and serves requests in rounds.
+A round takes every queued request that fits (at most ``max_views`` views,
+``max_pixels`` camera pixels and, when set, ``max_paths`` camera paths of
+pixels x passes, which bounds a round's time; in arrival order) and renders them
+together: the views of all the round's requests, of any scenes, are ONE
+camera-gather wavefront (device.ViewBatch's entry point,
+``pale_render_views_loss_device``), and the round's gradient requests share
+ONE adjoint wavefront (``pale_render_views_backward_device``, up to eight
+requests per wavefront) in which every request's gradients go to arrays of
+its own.  Requests that arrive while a round runs are admitted to the next
+round, as view slots and memory free up: continuous batching at round
+granularity.
+
+Seeds are keyed by camera (``camera_seeds="camera"``) and the photon maps
+do not change, so a request's image and loss are the same alone and in any
+mix, bit for bit, and its gradients up to the order of float atomic
+additions.
+
+Admission: ``add_scene`` measures the device memory the scene's renderer
+holds (surfels, LBVH, photon map and grid, photon queues) and refuses the
+scene (:class:`AdmissionError`) when the admitted scenes would exceed the
+HBM budget.  The wavefront buffers shared by all rounds belong to a small
+executor renderer of the server, sized by ``max_pixels`` on the first round.
+Latency is measured from ``submit`` to the result being ready on the host.
 """
 from __future__ import annotations
 
-import ctypes as C
 import threading
 import time
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
-from . import _native as N
-from .pale import Renderer, _check
-from .scene import SceneArrays
+from .pale import Renderer
+from .scene import SceneArrays, make_box_scene
 
 
 class AdmissionError(RuntimeError):
@@ -52,12 +62,15 @@ class Request:
     camera: int
     kind: str = "forward"                  # "forward" or "gradient"
     target: Optional[np.ndarray] = None    # gradient: (H, W, 3) target image
+    passes: int = 0                        # samples per pixel (0: the scene's maximum)
+    depth: int = 0                         # adjoint bounces (0: the scene's maximum)
     # results, filled by the server
     image: Optional[np.ndarray] = None     # (H, W, 4) LDR
     loss: Optional[float] = None
     grads: Optional[Dict[str, np.ndarray]] = None   # BVH order
     error: Optional[str] = None
-    batch_views: int = 0                   # cameras in the forward call that served it
+    batch_views: int = 0                   # views in the round that served it
+    round: int = -1
     t_submit: float = 0.0
     t_done: float = 0.0
     done: threading.Event = field(default_factory=threading.Event, repr=False)
@@ -74,107 +87,92 @@ def _device_used() -> int:
     return int(total - free)
 
 
+@dataclass
 class _Scene:
-    def __init__(self, name: str, renderer: Renderer, footprint: int, max_views: int):
-        self.name = name
-        self.r = renderer
-        self.footprint = footprint
-        self.max_views = max_views
-        self.queue: List[Request] = []
-        self.cv = threading.Condition()
-        self.stop = False
-        self.batches: List[int] = []
-        self.thread = threading.Thread(target=self._run, name=f"pale-serve-{name}", daemon=True)
+    name: str
+    renderer: Renderer
+    footprint: int
+    max_passes: int
+    max_depth: int
 
-    # ------------------------------------------------------------ worker
-    def _run(self):
-        while True:
-            with self.cv:
-                while not self.queue and not self.stop:
-                    self.cv.wait()
-                if self.stop and not self.queue:
-                    return
-                reqs, self.queue = self.queue, []
-            fwd = [q for q in reqs if q.kind == "forward"]
-            grd = [q for q in reqs if q.kind == "gradient"]
-            while fwd:
-                cams = sorted({q.camera for q in fwd})[: self.max_views]
-                now = [q for q in fwd if q.camera in cams]
-                fwd = [q for q in fwd if q.camera not in cams]
-                self._forward(cams, now)
-            for q in grd:
-                self._gradient(q)
 
-    def _finish(self, q: Request):
-        q.t_done = time.perf_counter()
-        q.done.set()
-
-    def _forward(self, cams: List[int], reqs: List[Request]):
-        r = self.r
-        try:
-            pix = sum(r._sizes[i][0] * r._sizes[i][1] for i in cams)
-            ldr = np.empty(pix * 4, np.float32)
-            raw = np.empty(pix * 4, np.float32)
-            idx = N.cams_array(cams)
-            _check(r._lib, r._h, r._lib.pale_render_forward(r._h, len(cams), idx.ctypes.data_as(N.u32p),
-                                                            ldr.ctypes.data_as(N.f32p), raw.ctypes.data_as(N.f32p)),
-                   "serve forward")
-            images, off = {}, 0
-            for i in cams:
-                w, h = r._sizes[i]
-                images[i] = ldr[off:off + 4 * w * h].reshape(h, w, 4)
-                off += 4 * w * h
-            self.batches.append(len(cams))
-            for q in reqs:
-                q.image = images[q.camera].copy()
-                q.batch_views = len(cams)
-        except Exception as e:  # reported per request
-            for q in reqs:
-                q.error = str(e)
-        for q in reqs:
-            self._finish(q)
-
-    def _gradient(self, q: Request):
-        r = self.r
-        try:
-            name = r._names[q.camera]
-            images, dldi, loss = r.render_forward_loss({name: np.asarray(q.target, np.float32)})
-            grads, _ = r.render_backward(dldi)
-            q.image, q.loss, q.grads = images[name], loss[name], grads
-            q.batch_views = 1
-        except Exception as e:
-            q.error = str(e)
-        self._finish(q)
+def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], max_views: int,
+               max_pixels: int, max_paths: Optional[int] = None,
+               max_passes: Optional[Dict[str, int]] = None) -> Tuple[List[Request], List[Request]]:
+    """The requests of the next round: the queue's head in arrival order
+    while the round holds at most max_views views, max_pixels camera pixels
+    and (when given) max_paths camera paths, pixels x passes, a request's
+    passes 0 counting as its scene's max_passes (the first request always
+    goes); returns (taken, left)."""
+    taken, pix, paths = [], 0, 0
+    for i, q in enumerate(queue):
+        w, h = sizes[q.scene][q.camera]
+        n = w * h * (q.passes or (max_passes or {}).get(q.scene, 1))
+        if taken and (len(taken) + 1 > max_views or pix + w * h > max_pixels
+                      or (max_paths is not None and paths + n > max_paths)):
+            return taken, queue[i:]
+        taken.append(q)
+        pix += w * h
+        paths += n
+    return taken, []
 
 
 class Server:
-    """Resident scenes served by per-scene workers (see the module docs)."""
+    """Resident scenes served in rounds of batched wavefronts (see the
+    module docs)."""
 
-    def __init__(self, hbm_budget: int, max_views_per_call: int = 16):
+    GRADIENTS_PER_WAVEFRONT = 8
+
+    def __init__(self, hbm_budget: int, max_views: int = 64, max_pixels: int = 1 << 24,
+                 settings: Optional[dict] = None, device: Optional[int] = None,
+                 max_paths: Optional[int] = None):
+        import torch
+
         self.budget = int(hbm_budget)
-        self.max_views = int(max_views_per_call)
+        self.max_views = int(max_views)
+        self.max_pixels = int(max_pixels)
+        self.max_paths = None if max_paths is None else int(max_paths)
+        self.device = torch.device(f"cuda:{device if device is not None else torch.cuda.current_device()}")
         self.scenes: Dict[str, _Scene] = {}
         self.done: List[Request] = []
+        self.rounds: List[int] = []           # views per round
+        self._queue: List[Request] = []
+        self._cv = threading.Condition()
         self._lock = threading.Lock()
+        self._gpu = threading.Lock()          # the executor's buffers: one user at a time
+        self._stop = False
+        # the executor: a tiny scene whose renderer lends the wavefront
+        # buffers and the adjoint settings (rng mode, null weighting,
+        # gradient groups, batch sizes) of every round
+        st = {"gather_passes": 64, "adjoint_passes": 64, "adjoint_bounces": 8}
+        st.update(settings or {})
+        st.update(camera_seeds="camera", photons=1000, forward_passes=1)
+        self._exec_settings = st
+        self._exec = Renderer.from_scene(make_box_scene(8, cameras=1, resolution=8), st)
+        self._thread = threading.Thread(target=self._run, name="pale-serve", daemon=True)
+        self._thread.start()
 
+    # ------------------------------------------------------------ scenes
     @property
     def admitted_bytes(self) -> int:
         return sum(s.footprint for s in self.scenes.values())
 
     def add_scene(self, name: str, scene: SceneArrays, settings: Optional[dict] = None) -> int:
-        """Makes `scene` resident if it fits the budget; returns the bytes it holds."""
+        """Makes `scene` resident if it fits the budget (its photon map is
+        traced now); returns the bytes it holds.  settings' gather/adjoint
+        passes and adjoint bounces are the most a request may ask for."""
         if name in self.scenes:
             raise ValueError(f"scene '{name}' is already resident")
+        import torch
+
         st = dict(settings or {})
         st["camera_seeds"] = "camera"
+        torch.cuda.synchronize(self.device)
         before = _device_used()
         r = Renderer.from_scene(scene, st)
         try:
-            # one forward and adjoint pass allocates what later requests use
-            r.render_forward()
-            name0 = r.get_camera_names()[0]
-            w, h = r._sizes[0]
-            r.render_backward({name0: np.zeros((h, w, 3), np.float32)})
+            self._photon_map(r)
+            torch.cuda.synchronize(self.device)
             footprint = max(0, _device_used() - before)
         except Exception:
             r.close()
@@ -183,37 +181,139 @@ class Server:
             r.close()
             raise AdmissionError(f"scene '{name}' needs {footprint / 2**30:.2f} GiB; "
                                  f"{(self.budget - self.admitted_bytes) / 2**30:.2f} GiB of the budget left")
-        sc = _Scene(name, r, footprint, self.max_views)
-        self.scenes[name] = sc
-        sc.thread.start()
+        with self._cv:
+            self.scenes[name] = _Scene(name, r, footprint, min(int(r._settings.gather_passes),
+                                                               int(r._settings.adjoint_passes)),
+                                       int(r._settings.adjoint_bounces))
         return footprint
 
-    def remove_scene(self, name: str):
-        sc = self.scenes.pop(name)
-        with sc.cv:
-            sc.stop = True
-            sc.cv.notify()
-        sc.thread.join()
-        sc.r.close()
+    def _photon_map(self, r: Renderer):
+        """Traces the scene's photon map, which then stays resident."""
+        import ctypes as C
 
+        import torch
+
+        from .pale import _check
+
+        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        _check(r._lib, r._h, r._lib.pale_trace_photon_map(r._h, stream), "trace_photon_map")
+
+    def remove_scene(self, name: str):
+        with self._cv:
+            sc = self.scenes.pop(name)
+        sc.renderer.close()
+
+    # ---------------------------------------------------------- requests
     def submit(self, req: Request) -> Request:
         sc = self.scenes.get(req.scene)
         if sc is None:
             raise KeyError(f"scene '{req.scene}' is not resident")
         if req.kind not in ("forward", "gradient"):
             raise ValueError("kind must be 'forward' or 'gradient'")
-        if not 0 <= req.camera < len(sc.r._names):
+        if not 0 <= req.camera < len(sc.renderer._names):
             raise IndexError("camera index out of range")
         if req.kind == "gradient" and req.target is None:
             raise ValueError("a gradient request needs a target image")
+        if not 0 <= req.passes <= sc.max_passes:
+            raise ValueError(f"passes must be 0 .. {sc.max_passes}")
+        if not 0 <= req.depth <= sc.max_depth:
+            raise ValueError(f"depth must be 0 .. {sc.max_depth}")
         req.t_submit = time.perf_counter()
-        with sc.cv:
-            sc.queue.append(req)
-            sc.cv.notify()
+        with self._cv:
+            self._queue.append(req)
+            self._cv.notify()
         with self._lock:
             self.done.append(req)
         return req
 
+    # ------------------------------------------------------------ rounds
+    def _run(self):
+        import torch
+
+        torch.cuda.set_device(self.device)
+        while True:
+            with self._cv:
+                while not self._queue and not self._stop:
+                    self._cv.wait()
+                if self._stop and not self._queue:
+                    return
+                sizes = {n: s.renderer._sizes for n, s in self.scenes.items()}
+                spp = {n: s.max_passes for n, s in self.scenes.items()}
+                taken, self._queue = plan_round(self._queue, sizes, self.max_views, self.max_pixels,
+                                                self.max_paths, spp)
+            try:
+                with self._gpu:
+                    self._round(taken)
+            except Exception as e:  # reported per request
+                for q in taken:
+                    if not q.done.is_set():
+                        q.error = str(e)
+            now = time.perf_counter()
+            for q in taken:
+                if not q.done.is_set():
+                    q.t_done = now
+                    q.done.set()
+
+    def _round(self, reqs: List[Request]):
+        import torch
+
+        from .device import ViewBatch
+
+        n_round = len(self.rounds)
+        self.rounds.append(len(reqs))
+        names = sorted({q.scene for q in reqs})
+        entry = {n: k + 1 for k, n in enumerate(names)}     # entry 0: the executor
+        scenes = [self.scenes[n] for n in names]
+        renderers = [self._exec] + [s.renderer for s in scenes]
+
+        def passes(q):
+            return q.passes or self.scenes[q.scene].max_passes
+
+        views = [(entry[q.scene], q.camera, passes(q), q.depth) for q in reqs]
+        vb = ViewBatch(renderers, views, device=self.device)
+        vb.forward_loss(None, trace_photons=False)      # the resident photon maps
+        offs = np.cumsum([0] + [w * h for w, h in vb.sizes])
+        # the L2 loss and dL/dI of the gradient requests (compute_l2_loss /
+        # compute_l2_grad, python/losses.py:10-45, on the LDR image)
+        grad_idx = [i for i, q in enumerate(reqs) if q.kind == "gradient"]
+        dldi, loss = {}, {}
+        for i in grad_idx:
+            t = torch.from_numpy(np.ascontiguousarray(reqs[i].target, np.float32).reshape(-1, 3)).to(self.device)
+            ldr_i = vb.ldr[offs[i]:offs[i + 1], :3]
+            d = torch.zeros(int(offs[i + 1] - offs[i]), 4, dtype=torch.float32, device=self.device)
+            torch.sub(ldr_i, t, out=d[:, :3])
+            loss[i] = 0.5 * (d[:, :3].double() ** 2).mean()
+            d[:, :3].div_(float(3 * (offs[i + 1] - offs[i])))
+            dldi[i] = d
+        ldr = vb.ldr.cpu().numpy()
+        for i, q in enumerate(reqs):
+            w, h = vb.sizes[i]
+            q.image = ldr[offs[i]:offs[i + 1]].reshape(h, w, 4).copy()
+            q.batch_views = len(reqs)
+            q.round = n_round
+            if q.kind == "gradient":
+                q.loss = float(loss[i].item())
+            else:
+                q.t_done = time.perf_counter()
+                q.done.set()
+        per = self.GRADIENTS_PER_WAVEFRONT - 1     # entry 0 is the executor
+        for c0 in range(0, len(grad_idx), per):
+            chunk = grad_idx[c0:c0 + per]
+            # one scene entry per request, so each request keeps its own gradients
+            rs = [self._exec] + [self.scenes[reqs[i].scene].renderer for i in chunk]
+            gviews = [(k + 1, reqs[i].camera, passes(reqs[i]), reqs[i].depth) for k, i in enumerate(chunk)]
+            gb = ViewBatch(rs, gviews, device=self.device)
+            dl = torch.cat([dldi[i] for i in chunk]).contiguous()
+            grads = gb.backward(dl)
+            host = [{k: v.cpu().numpy() for k, v in grads[k + 1].items()} for k in range(len(chunk))]
+            now = time.perf_counter()
+            for k, i in enumerate(chunk):
+                q = reqs[i]
+                q.grads = host[k]
+                q.t_done = now
+                q.done.set()
+
+    # ----------------------------------------------------------- reports
     def latency(self, kind: Optional[str] = None) -> Dict[str, float]:
         """p50 / p99 / mean latency (ms) of the finished requests."""
         with self._lock:
@@ -224,6 +324,28 @@ class Server:
         return {"n": int(a.size), "p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)),
                 "mean": float(a.mean())}
 
+    def serve_one(self, req: Request) -> Request:
+        """The plain path: `req` rendered alone, right now, on the calling
+        thread, waiting for any round in flight (no batching: the
+        one-request-at-a-time baseline, and the check that a request's
+        result does not depend on its round)."""
+        req.t_submit = time.perf_counter()
+        with self._gpu:
+            saved = list(self.rounds)
+            try:
+                self._round([req])
+            finally:
+                self.rounds = saved
+        if not req.done.is_set():
+            req.t_done = time.perf_counter()
+            req.done.set()
+        return req
+
     def close(self):
+        with self._cv:
+            self._stop = True
+            self._cv.notify()
+        self._thread.join()
         for name in list(self.scenes):
             self.remove_scene(name)
+        self._exec.close()

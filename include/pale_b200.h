@@ -71,6 +71,32 @@ typedef struct pale_handle pale_handle;
 #define PALE_CAMERA_SEEDS_SELECTION 0u
 #define PALE_CAMERA_SEEDS_CAMERA 1u
 
+/* Which gradient the backward computes.  REFERENCE is the reference's
+ * adjoint (AdjointKernels.cpp): its own paths from the camera, events at
+ * their bounces, photon lookups at the events.  GATHER is the exact
+ * derivative of the forward's camera-gather image with the photon map
+ * held: the forward's camera paths (the same seeds) and their layers, each
+ * layer k of a path getting dI/d(alpha_k) = T_k (Lo_k - Lb_k), Lb_k the
+ * radiance composited behind it, chained to opacity, beta, position,
+ * tangents, scales (through alpha_geom) and albedo.  A GATHER backward
+ * differentiates the last forward render of the same views and fails with
+ * PALE_ERR_ARGUMENT for any other. */
+#define PALE_ESTIMATOR_REFERENCE 0u
+#define PALE_ESTIMATOR_GATHER 1u
+
+/* Where a GATHER backward finds the forward's path vertices (per layer its
+ * hit point, alpha_geom and irradiance; per path segment its direction,
+ * transmittance and links; 32 bytes per layer and 48 per segment).
+ * CHECKPOINT keeps them from the forward in a store grown to the last
+ * forward's need; REPLAY keeps none and the backward traces each chunk of
+ * camera paths again with the forward's seeds (deterministic, so the
+ * layers are the forward's) into a scratch store of one chunk; AUTO
+ * checkpoints while the store fits vertex_store_bytes (0: half the free
+ * device memory) and replays the chunks that do not fit. */
+#define PALE_VERTICES_AUTO 0u
+#define PALE_VERTICES_CHECKPOINT 1u
+#define PALE_VERTICES_REPLAY 2u
+
 typedef struct pale_settings {
     uint32_t photons_per_launch;   /* "photons"          (default 1e6)       */
     uint32_t max_bounces;          /* "bounces"          (6)                 */
@@ -102,6 +128,9 @@ typedef struct pale_settings {
                                       largest camera's pixels)               */
     uint32_t walk_block;           /* threads per block of the persistent
                                       BVH walks: 64, 128 or 256 (0 = 256)    */
+    uint32_t estimator;            /* PALE_ESTIMATOR_* ("estimator")          */
+    uint32_t vertex_store;         /* PALE_VERTICES_* ("vertices")            */
+    uint64_t vertex_store_bytes;   /* AUTO's budget (0 = half the free memory) */
 } pale_settings;
 
 /* Per-point parameter block (structure of arrays, float32).
@@ -172,6 +201,10 @@ typedef struct pale_stats {
                                        adjoint transport (CUDA events around
                                        each launch)                          */
     uint32_t timed_launches[4];     /* ... and their launch counts           */
+    uint64_t vertex_bytes;          /* vertex store + replay scratch held    */
+    uint32_t vertex_chunks_stored;  /* last GATHER backward: chunks swept
+                                       from the store ...                    */
+    uint32_t vertex_chunks_replayed;/* ... and chunks traced again           */
 } pale_stats;
 
 /* Fills *s with the reference's PathTracerSettings defaults. */
@@ -300,11 +333,23 @@ int pale_render_views_loss_device(uint32_t num_scenes, pale_handle *const *scene
                                   uint32_t channels, float *d_ldr, float *d_raw,
                                   float *d_dldi, double *d_loss, void *stream);
 
+/* The photon passes and the photon grid of the scene alone (the first half
+ * of render_forward, SyclBridge.cpp:82-138), enqueued on `stream` (NULL =
+ * the default stream) without waiting: the photon map that gather-only
+ * renders (pale_render_gather, or views rendered without trace_photons)
+ * then use, e.g. a server's resident scene. */
+int pale_trace_photon_map(pale_handle *h, void *stream);
+
 /* The adjoint pass of the same views as ONE wavefront of (view, pass) jobs:
- * dL/dI packed in view order (DEVICE).  Each scene's gradients accumulate
- * in its own arrays; d_grads is NULL or num_scenes entries of DEVICE
- * pointers that receive them (BVH order, as pale_render_backward_device).
- * The rng mode, null weighting and gradient groups are scenes[0]'s. */
+ * dL/dI packed in view order (DEVICE).  With d_grads NULL each scene's
+ * gradients accumulate in its own arrays (read them with a later
+ * pale_render_backward_device of no views, or through the renderer); else
+ * d_grads holds num_scenes entries of DEVICE arrays (BVH order, every field
+ * but shape non-null) that entry k's gradients accumulate in after they
+ * are zeroed, and one scene may then fill several entries, so that the
+ * views of different requests of one scene keep separate gradients in one
+ * wavefront.  The rng mode, null weighting and gradient groups are
+ * scenes[0]'s. */
 int pale_render_views_backward_device(uint32_t num_scenes, pale_handle *const *scenes,
                                       uint32_t num_views, const pale_view *views,
                                       const float *d_dldi, pale_points *d_grads,

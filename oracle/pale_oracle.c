@@ -1805,6 +1805,132 @@ int orc_render_backward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams,
     return render_backward_views(s, nsel, cams, passes, depths, dldi, grads, NULL);
 }
 
+/* ------------------------------------------ gather estimator (estimator 1)
+ * The exact derivative of the camera gather's image (gather_pixel) with the
+ * photon map held: a camera path composites its surfel layers front to back,
+ *   I = sum_k T_k a_k Lo_k + T_end L_end,  T_{k+1} = T_k (1 - a_k),
+ * with a_k = opacity_k alpha_geom_k, Lo_k = E(x_k) albedo_k alpha_r / pi and
+ * L_end the emitter (clamped) or the lit mesh that ends the path.  With Lb_k
+ * the radiance behind layer k, composited back to front
+ * (Lb = a Lo + (1 - a) Lb), dI/da_k = T_k (Lo_k - Lb_k); the opacity gets
+ * dI/da_k alpha_geom_k, the parameters of alpha_geom (beta, position,
+ * tangents, scales) dI/da_k d(a_k)/d(theta) (alpha_grad), the albedo
+ * T_k a_k alpha_r E(x_k) / pi per channel.  The irradiance E(x_k) is held:
+ * moving a surfel out of its plane also moves x_k against the photons,
+ * which this derivative does not follow.  Every pixel and pass replays the
+ * forward's camera path (same seeds), so the layers are the forward's. */
+typedef struct { uint32_t prim; v3 x, E; float a, T, ageom; } glayer_t;
+
+static void gather_pixel_grad(const orc_scene *s, uint32_t cam, uint64_t base, uint32_t pix, v3 g, float inv,
+                              glayer_t **buf, uint32_t *cap, float *gop, float *gall, int all) {
+    const uint32_t W = s->cam_size[2 * cam];
+    rng_t r = rng_make(orc_per_item_seed(base, pix));
+    float jx = rng_f(&r) - 0.5f, jy = rng_f(&r) - 0.5f;
+    v3 o, d;
+    primary_ray(s, cam, (float)(pix % W), (float)(pix / W), jx, jy, &o, &d);
+    float T = 1.0f;
+    uint32_t nl = 0;
+    v3 Lend = V3(0, 0, 0);
+    uint64_t dummy = 0;
+    trav_ctr ctr = {0, 0};
+    for (int layer = 0; layer < 65536; ++layer) {
+        hit_t h = intersect_scene(s, o, d, &ctr);
+        if (!h.hit) break;
+        if (h.inst >= (int)s->ninst) {
+            const point_t *sf = &s->pts[h.prim];
+            v3 n = vnorm(vcross(sf->tu, sf->tv));
+            if (vdot(n, vneg(d)) < 0.0f) n = vneg(n);
+            if (nl == *cap) {
+                *cap = *cap ? 2 * *cap : 64;
+                *buf = (glayer_t *)realloc(*buf, *cap * sizeof(glayer_t));
+            }
+            glayer_t *L = *buf + nl++;
+            L->prim = h.prim;
+            L->x = h.pos;
+            L->E = gather(s, h.pos, n, &dummy);
+            L->ageom = h.alpha;
+            L->a = sf->opacity * h.alpha;
+            L->T = T;
+            T *= (1.0f - L->a);
+            o = vadd(h.pos, vscale(d, 1e-4f));
+            continue;
+        }
+        const float *mat = s->mats + 4 * s->inst_mat[h.inst];
+        v3 base_c = V3(mat[0], mat[1], mat[2]);
+        if (mat[3] > 0.f) {
+            v3 Le = vscale(base_c, mat[3]);
+            Lend = V3(fminf(Le.x, 1.0f), fminf(Le.y, 1.0f), fminf(Le.z, 1.0f));
+        } else {
+            Lend = vmul(vscale(base_c, M_1_PIf_), gather(s, h.pos, h.normal, &dummy));
+        }
+        break;
+    }
+    const v3 dn = vnorm(d);
+    v3 Lb = Lend;
+    for (uint32_t k = nl; k-- > 0;) {
+        const glayer_t *L = *buf + k;
+        const point_t *sf = &s->pts[L->prim];
+        const v3 fr = vscale(vscale(sf->albedo, sf->alpha_r), M_1_PIf_);
+        const v3 Lo = vmul(L->E, fr);
+        const float w = inv * vdot(g, vscale(vsub(Lo, Lb), L->T));   /* dLoss / da_k */
+        float terms[16];
+        terms[0] = w * L->ageom;
+        int nt = 1;
+        if (all) {
+            float ag[12];
+            alpha_grad(sf, L->x, dn, ag);
+            for (int c = 0; c < 12; ++c) terms[1 + c] = w * ag[c];
+            const float ka = inv * L->T * L->a * sf->alpha_r * M_1_PIf_;
+            terms[13] = g.x * ka * L->E.x;
+            terms[14] = g.y * ka * L->E.y;
+            terms[15] = g.z * ka * L->E.z;
+            nt = 16;
+        }
+#pragma omp atomic
+        gop[L->prim] += terms[0];
+        for (int c = 1; c < nt; ++c) {
+#pragma omp atomic
+            gall[15 * (size_t)L->prim + c - 1] += terms[c];
+        }
+        Lb = vadd(vscale(Lo, L->a), vscale(Lb, 1.0f - L->a));
+    }
+}
+
+static void gather_backward(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
+                            const float *dldi, float *gop, float *gall, int all) {
+    mt64_t mt;
+    if (s->cam_mt_valid) mt = s->cam_mt;
+    else mt_seed(&mt, s->st.seed);
+    const uint32_t nseed = s->st.camera_seeds == 1 ? s->ncam : nsel;
+    uint32_t *cam_seed = (uint32_t *)malloc((nseed ? nseed : 1) * sizeof(uint32_t));
+    for (uint32_t k = 0; k < nseed; ++k) cam_seed[k] = (uint32_t)mt_next(&mt);
+    size_t off = 0;
+    for (uint32_t ci = 0; ci < nsel; ++ci) {
+        const uint32_t cam = cams[ci];
+        const uint32_t npix = s->cam_size[2 * cam] * s->cam_size[2 * cam + 1];
+        const uint64_t cseed = cam_seed[s->st.camera_seeds == 1 ? cam : ci];
+        const uint32_t npass = passes ? passes[ci] : s->st.gather_passes;
+        const float inv = 1.0f / (float)npass;
+        const float *img = dldi + off;
+        for (uint32_t pass = 0; pass < npass; ++pass) {
+            const uint64_t b = s->st.rng_mode == 1 ? orc_per_item_seed(cseed, pass) : cseed;
+#pragma omp parallel
+            {
+                glayer_t *buf = NULL;
+                uint32_t cap = 0;
+#pragma omp for schedule(dynamic, 64)
+                for (int64_t p = 0; p < (int64_t)npix; ++p) {
+                    const v3 g = V3(img[4 * p], img[4 * p + 1], img[4 * p + 2]);
+                    gather_pixel_grad(s, cam, b, (uint32_t)p, g, inv, &buf, &cap, gop, gall, all);
+                }
+                free(buf);
+            }
+        }
+        off += (size_t)npix * 4;
+    }
+    free(cam_seed);
+}
+
 /* passes / depths: per selected camera (a view's own passes and adjoint
  * bounces; depth 0 = the settings'), or NULL for the settings. */
 static int render_backward_views(orc_scene *s, uint32_t nsel, const uint32_t *cams, const uint32_t *passes,
@@ -1830,6 +1956,10 @@ static int render_backward_views(orc_scene *s, uint32_t nsel, const uint32_t *ca
     for (size_t k = 0; k < nseeds; ++k) seed_tab[k] = (uint32_t)mt_next(&mt);
     size_t off = 0;
 
+    if (st->estimator == 1) {
+        gather_backward(s, nsel, cams, passes, dldi, gop, gall, all);
+        nsel = 0;
+    }
     for (uint32_t ci = 0; ci < nsel; ++ci) {
         uint32_t cam = cams[ci];
         uint32_t W = s->cam_size[2 * cam], H = s->cam_size[2 * cam + 1], npix = W * H;

@@ -41,6 +41,10 @@ typedef struct orc_settings {
     uint32_t null_weight;   /* 0 reference, 1 unbiased (divide by q_null) */
     uint32_t gradients;     /* 0 opacity, 1 all seven groups */
     uint32_t camera_seeds;  /* 0 by position in the selection, 1 by camera index */
+    uint32_t gather_batch_paths, adjoint_batch_paths, walk_block;   /* GPU batching: unused here */
+    uint32_t estimator;     /* 0 the reference's adjoint (photon-path events),
+                               1 the derivative of the camera gather with the
+                               photon map held (render_backward) */
 } orc_settings;
 
 typedef struct orc_points {
