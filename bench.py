@@ -136,25 +136,38 @@ ADJ_COUNTERS = ("adjoint_segments", "node_visits", "surfel_tests", "gradient_eve
                 "photons_scanned")
 
 
-def kernel_bytes(sf: dict, sb: dict) -> dict:
+def kernel_bytes(sf: dict, sb: dict, estimator: str = "reference", all_grads: bool = False) -> dict:
     seg = lambda segs, nodes, tests: 80.0 * segs + 32.0 * nodes + 52.0 * tests
     look = lambda q, scanned: 36.0 * scanned + 8.0 * ROWS_PER_QUERY * q
     fwd_q = sf["gather_queries"]
     adj_q = sb["gather_queries"]
-    return {
+    out = {
         "k_cg_round": seg(sf["gather_segments"], sf["gather_node_visits"], sf["gather_surfel_tests"]),
         "k_cg_lookup": look(fwd_q, sf["gather_photons_scanned"]),
-        "k_adj_bounce": seg(sb["adjoint_segments"], sb["node_visits"], sb["surfel_tests"])
-        + (96.0 + 128.0) * sb["adjoint_segments"],
-        "k_transport": 72.0 * sb["gradient_events"] + look(adj_q, sb["photons_scanned"]),
     }
+    if estimator == "gather":
+        # the sweep: per path segment its direction, links, radiance (read
+        # and written) and dL/dI (96 B); per layer record its two float4s,
+        # read twice, the surfel's opacity and albedo, and the gradient
+        # atomics (opacity, or 16 terms with alpha_geom's surfel reads)
+        per_rec = 64.0 + 32.0 + (64.0 + 64.0 if all_grads else 4.0)
+        out["k_vs_sweep"] = 96.0 * sb["vertex_entries"] + per_rec * sb["vertex_records"]
+        return out
+    out["k_adj_bounce"] = seg(sb["adjoint_segments"], sb["node_visits"], sb["surfel_tests"]) \
+        + (96.0 + 128.0) * sb["adjoint_segments"]
+    out["k_transport"] = 72.0 * sb["gradient_events"] + look(adj_q, sb["photons_scanned"])
+    return out
 
 
-def kernel_times(sf: dict, sb: dict) -> dict:
-    return {"k_cg_round": (sf["trace_ms"], sf["trace_launches"]),
-            "k_cg_lookup": (sf["lookup_ms"], sf["lookup_launches"]),
-            "k_adj_bounce": (sb["adjoint_bounce_ms"], sb["adjoint_bounce_launches"]),
-            "k_transport": (sb["transport_ms"], sb["transport_launches"])}
+def kernel_times(sf: dict, sb: dict, estimator: str = "reference") -> dict:
+    out = {"k_cg_round": (sf["trace_ms"], sf["trace_launches"]),
+           "k_cg_lookup": (sf["lookup_ms"], sf["lookup_launches"])}
+    if estimator == "gather":
+        out["k_vs_sweep"] = (sb["transport_ms"], sb["transport_launches"])
+    else:
+        out["k_adj_bounce"] = (sb["adjoint_bounce_ms"], sb["adjoint_bounce_launches"])
+        out["k_transport"] = (sb["transport_ms"], sb["transport_launches"])
+    return out
 
 
 def read_peaks():
@@ -478,7 +491,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # weak scaling: one scene with cams x N cameras on the ring, split round
     # robin over the ranks (rank r renders cameras r, r + N, ...: cams each);
     # camera-keyed seeds make a camera's work independent of the split
-    st = dict(settings_for(w), camera_seeds="camera", gradients=args.gradients)
+    st = dict(settings_for(w), camera_seeds="camera", gradients=args.gradients, estimator=args.estimator)
     pts = make_surfels(w["n"], 1234)
     scene = make_box_scene(w["n"], cameras=w["cams"] * world, resolution=w["res"], points=pts)
     mine = shard_cameras(list(range(w["cams"] * world)), rank, world)
@@ -583,7 +596,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     hbm = peaks["hbm_gbs"] if peaks else 6650.0
     # per-kernel device time (events around every launch, stats step) and
     # algorithmic bytes; the roofline entry is the kernel with the most time
-    kb, kt = kernel_bytes(sf, sb), kernel_times(sf, sb)
+    kb = kernel_bytes(sf, sb, args.estimator, args.gradients == "all")
+    kt = kernel_times(sf, sb, args.estimator)
     kernels = {}
     for k in kb:
         ms, n = kt[k]
@@ -604,7 +618,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_for(args.workload, w),
-        "gradients": args.gradients,
+        "gradients": args.gradients, "estimator": args.estimator,
         "iters_per_s": round(1e3 / ms_per_step, 4), "rays_per_step_per_gpu": int(rays),
         "parallelism": f"{w['cams'] * world} ring cameras split round robin over {world} GPU(s), gradients all-reduced",
         "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
@@ -630,6 +644,85 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     print(json.dumps(line), flush=True)
     if args.skip_extra or world > 1:
         r.close()
+
+
+# ---------------------------------------------------------------- C3b
+C3B_MODES = (   # label, settings
+    ("reference adjoint", {"estimator": "reference"}),
+    ("gather, checkpoint", {"estimator": "gather", "vertices": "checkpoint"}),
+    ("gather, replay", {"estimator": "gather", "vertices": "replay"}),
+    ("gather, auto 32 GB", {"estimator": "gather", "vertices": "auto", "vertex_store_bytes": 32 * 10 ** 9}),
+)
+
+
+def run_c3b(args):
+    """The memory-bound case: box1m-32view's scene (1M surfels, 32 views of
+    800x800, depth 8) at --c3b-passes passes, one forward + backward per
+    iteration with all seven gradient groups, for the reference's adjoint
+    and for the gather estimator with its path vertices checkpointed,
+    replayed, or checkpointed within a 32 GB budget (the rest replayed).
+    Per mode: iterations/s over --steps timed iterations after --warmup
+    (the first iteration sizes the vertex store) and the device memory the
+    renderer and its frame hold afterwards.  One JSON line."""
+    import torch
+
+    from differentiablepointrendering_b200.build import build_library
+    from differentiablepointrendering_b200.device import DeviceFrame
+    from differentiablepointrendering_b200.pale import Renderer
+    from differentiablepointrendering_b200.scene import jitter_target, make_box_scene, make_surfels
+
+    build_library()
+    dev = torch.device("cuda:0")
+    w = dict(WORKLOADS["box1m-32view"], spp=args.c3b_passes, adjoint_spp=args.c3b_passes)
+    base = dict(settings_for(w), gradients="all")
+    pts = make_surfels(w["n"], 1234)
+    scene = make_box_scene(w["n"], cameras=w["cams"], resolution=w["res"], points=pts)
+    tr = Renderer.from_scene(scene.with_points(jitter_target(pts, 5678)), base)
+    tf = DeviceFrame(tr, device=dev)
+    tf.forward()
+    target = tf.ldr[:, :3].clone()
+    torch.cuda.synchronize()
+    del tf
+    tr.close()
+    torch.cuda.empty_cache()
+    stream = torch.cuda.current_stream(dev)
+    rows = []
+    for label, extra in C3B_MODES:
+        torch.cuda.synchronize()
+        free0, total = torch.cuda.mem_get_info()
+        r = Renderer.from_scene(scene, dict(base, **extra))
+        frame = DeviceFrame(r, device=dev)
+        for _ in range(max(1, args.warmup)):
+            frame.forward_loss(target)
+            frame.backward()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+        for k in range(args.steps):
+            ev[3 * k].record(stream)
+            frame.forward_loss(target)
+            ev[3 * k + 1].record(stream)
+            frame.backward()
+            ev[3 * k + 2].record(stream)
+        torch.cuda.synchronize()
+        fwd = sum(ev[3 * k].elapsed_time(ev[3 * k + 1]) for k in range(args.steps)) / args.steps
+        bwd = sum(ev[3 * k + 1].elapsed_time(ev[3 * k + 2]) for k in range(args.steps)) / args.steps
+        st = r.stats()
+        free1, _ = torch.cuda.mem_get_info()
+        grads = {k: float(v.double().norm()) for k, v in frame.grads.items() if k in ("opacity", "albedo")}
+        rows.append({"mode": label, "iters_per_s": round(1e3 / (fwd + bwd), 4), "forward_ms": round(fwd, 1),
+                     "backward_ms": round(bwd, 1), "device_bytes": int(free0 - free1),
+                     "vertex_bytes": int(st["vertex_bytes"]),
+                     "chunks_stored": int(st["vertex_chunks_stored"]),
+                     "chunks_replayed": int(st["vertex_chunks_replayed"]),
+                     "gather_segments": int(st["gather_segments"]), "grad_norms": grads})
+        del frame
+        r.close()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": "C3b iters/s and device memory, checkpointed vs replayed path vertices",
+                      "impl": "ours", "n_gpus": 1, "workload": dict(w, workload="box1m-32view"),
+                      "gradients": "all", "steps": args.steps, "warmup": max(1, args.warmup),
+                      "device_total_bytes": int(total), "modes": rows}), flush=True)
 
 
 # ---------------------------------------------------------------- serving
@@ -712,7 +805,8 @@ def run_serving(args):
     rng = np.random.default_rng(17)
     free, _ = torch.cuda.mem_get_info()
     budget = min(150 * 10 ** 9, int(free * 0.9))
-    srv = Server(hbm_budget=budget, max_views=64, max_pixels=1 << 24, max_paths=args.round_paths)
+    srv = Server(hbm_budget=budget, max_views=64, max_pixels=1 << 24, max_paths=args.round_paths,
+                 settings={"estimator": args.estimator})
     names = []
     t_admit = time.perf_counter()
     for k, n in enumerate(SERVING_SURFELS):
@@ -753,7 +847,7 @@ def run_serving(args):
     print(json.dumps({"metric": "serving latency p50/p99 (ms) and requests/s", "impl": "ours", "n_gpus": 1,
                       "scenes": [{"name": m, "surfels": n} for m, n in zip(names, SERVING_SURFELS)],
                       "scene_settings": SERVING_SETTINGS, "resolutions": SERVING_RES, "passes": SERVING_SPP,
-                      "depths": [4, 8], "round_paths": args.round_paths,
+                      "depths": [4, 8], "round_paths": args.round_paths, "estimator": args.estimator,
                       "mix": "70% forward (LDR image of one view), 30% gradient (L2 loss + adjoint of one view)",
                       "budget_bytes": budget, "admitted_bytes": admitted, "admit_s": round(t_admit, 2),
                       "runs": runs, "gradient_512": g512}), flush=True)
@@ -769,10 +863,14 @@ def main():
     ap.add_argument("--skip-cpu", dest="skip_cpu", action="store_true")
     ap.add_argument("--gradients", default="opacity", choices=("opacity", "all"),
                     help="gradient groups of the adjoint: the reference's opacity, or all seven")
+    ap.add_argument("--estimator", default="reference", choices=("reference", "gather"),
+                    help="backward: the reference's adjoint, or the gather estimator (checkpointed path vertices)")
     ap.add_argument("--skip-extra", dest="skip_extra", action="store_true",
                     help="skip the per-view and request-latency measurements")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true", help="C4 without the autotuner")
     ap.add_argument("--c4", action="store_true", help="only the C4 batched-vs-plain measurement")
+    ap.add_argument("--c3b", action="store_true", help="only the C3b checkpoint-vs-replay measurement")
+    ap.add_argument("--c3b-passes", dest="c3b_passes", type=int, default=2)
     ap.add_argument("--serving", action="store_true", help="serving benchmark (Poisson request stream)")
     ap.add_argument("--rates", type=float, nargs="*", default=[50.0, 200.0, 500.0, 2000.0])
     ap.add_argument("--seconds", type=float, default=4.0, help="serving: stream length per rate")
@@ -784,6 +882,9 @@ def main():
     args = ap.parse_args()
     if args.serving:
         run_serving(args)
+        return
+    if args.c3b:
+        run_c3b(args)
         return
     if args.c4:
         import torch

@@ -62,7 +62,8 @@ class PaleStats(C.Structure):
         "gather_surfel_tests", "gather_photons_scanned", "kernel_launches")] + \
         [(k, C.c_float) for k in ("forward_ms", "backward_ms", "photon_ms", "gather_ms")] + \
         [("timed_ms", C.c_float * 4), ("timed_launches", C.c_uint32 * 4), ("vertex_bytes", C.c_uint64),
-         ("vertex_chunks_stored", C.c_uint32), ("vertex_chunks_replayed", C.c_uint32)]
+         ("vertex_chunks_stored", C.c_uint32), ("vertex_chunks_replayed", C.c_uint32),
+         ("vertex_records", C.c_uint64), ("vertex_entries", C.c_uint64)]
 
     TIMED = ("trace", "lookup", "adjoint_bounce", "transport")
 
@@ -298,6 +299,9 @@ def load_library() -> C.CDLL:
         "pale_render_views_backward_device": (C.c_int, [C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
                                                         C.POINTER(PaleView), C.c_void_p, C.POINTER(PalePoints),
                                                         C.c_void_p]),
+        "pale_render_views_gradients_device": (C.c_int, [C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
+                                                         C.POINTER(PaleView), C.c_void_p, C.POINTER(PalePoints),
+                                                         C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -316,7 +320,7 @@ EXPORTED = ("pale_default_settings", "pale_version", "pale_last_error", "pale_cr
             "pale_optimizer_reset", "pale_render_forward_loss", "pale_render_forward_loss_device",
             "pale_prune_by_opacity", "pale_densify_long_axis_split", "pale_apply_points_device",
             "pale_lbvh_node_count", "pale_render_views_loss_device", "pale_render_views_backward_device",
-            "pale_trace_photon_map")
+            "pale_trace_photon_map", "pale_render_views_gradients_device")
 NOALLOC_MAX_SURFELS = 16384
 
 

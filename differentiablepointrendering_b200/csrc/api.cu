@@ -178,6 +178,7 @@ struct pale_handle {
   DBuf<float4> vs_rec_xa, vs_rec_ew, vs_ent_d, vs_ent_l, sc_rec_xa, sc_rec_ew, sc_ent_d, sc_ent_l;
   DBuf<uint4> vs_ent_b, sc_ent_b;
   DBuf<uint32_t> vs_base, vs_overflow, vs_chunk_base;
+  DBuf<SceneGrads> vs_view_grads;   // per view gradient arrays of a per-view backward
   uint64_t photon_gen = 0;     // photon maps traced or loaded so far
   uint64_t params_gen = 0;     // surfel parameter writes so far
   uint64_t bvh_gen = 0;        // BVH builds so far
@@ -919,11 +920,11 @@ FrameArgs frame_args(const std::vector<pale_handle*>& scenes, uint32_t nsel, uin
 constexpr uint64_t kRecSlotBytes = 2 * sizeof(float4), kEntSlotBytes = 2 * sizeof(float4) + sizeof(uint4);
 
 // Before a forward with the gather estimator: the store grows to hold every
-// chunk of the previous forward (with 1/16 to spare), when the vertex_store
-// mode is "checkpoint", or "auto" and the bytes fit the budget
-// (vertex_store_bytes; 0 = half the device memory free now).  A training
-// loop renders the same views every iteration, so from its second
-// iteration on every chunk is kept.
+// chunk of the previous forward (with 1/16 to spare) in the "checkpoint"
+// mode; in "auto" to that or to the budget (vertex_store_bytes; 0 = half
+// the device memory free now), whichever is smaller, which then holds the
+// first chunks.  A training loop renders the same views every iteration, so
+// from its second iteration on the chunks that fit are kept.
 void vertex_store_grow(pale_handle* h) {
   const pale_settings& st = h->st;
   if (st.vertex_store == PALE_VERTICES_REPLAY) return;
@@ -934,18 +935,24 @@ void vertex_store_grow(pale_handle* h) {
   }
   recs += recs / 16 + 1024;
   ents += ents / 16 + 1024;
-  if (recs <= h->vs_rec_xa.n && ents <= h->vs_ent_d.n) return;
-  if (recs >= (1ull << 32) || ents >= (1ull << 32)) return;   // slots are 32-bit: the chunks are replayed
-  const uint64_t bytes = recs * kRecSlotBytes + ents * kEntSlotBytes;
+  recs = std::min<uint64_t>(recs, 0xFFFFFFFFull);   // slots are 32-bit: the chunks past them are replayed
+  ents = std::min<uint64_t>(ents, 0xFFFFFFFFull);
   if (st.vertex_store == PALE_VERTICES_AUTO) {
+    // within the budget: as large a share of the need as it holds
     uint64_t budget = st.vertex_store_bytes;
     if (!budget) {
       size_t free_b = 0, total_b = 0;
       CK(cudaMemGetInfo(&free_b, &total_b));
       budget = free_b / 2 + h->vs_rec_xa.n * kRecSlotBytes + h->vs_ent_d.n * kEntSlotBytes;
     }
-    if (bytes > budget) return;
+    const uint64_t bytes = recs * kRecSlotBytes + ents * kEntSlotBytes;
+    if (bytes > budget) {
+      const double f = (double)budget / (double)bytes;
+      recs = (uint64_t)(recs * f);
+      ents = (uint64_t)(ents * f);
+    }
   }
+  if (recs <= h->vs_rec_xa.n && ents <= h->vs_ent_d.n) return;
   CK(cudaStreamSynchronize(h->stream));
   h->vs_rec_xa.alloc(recs); h->vs_rec_ew.alloc(recs);
   h->vs_ent_d.alloc(ents); h->vs_ent_b.alloc(ents); h->vs_ent_l.alloc(ents);
@@ -1066,7 +1073,7 @@ void zero_grads(pale_handle* h, cudaStream_t s) {
 // from the vertex store where its chunks were kept and replayed into the
 // scratch store where they were not.
 void gather_adjoint(const std::vector<pale_handle*>& scenes, const std::vector<CameraRec>& sel, uint32_t total,
-                    const float* d_dldi, const SceneGrads* grads, bool all) {
+                    const float* d_dldi, const SceneGrads* grads, bool all, const SceneGrads* d_view_grads = nullptr) {
   pale_handle* h = scenes[0];
   cudaStream_t s = h->stream;
   bool same = !h->vviews.empty() && h->vviews.size() == sel.size() && h->vscenes == scenes &&
@@ -1102,9 +1109,17 @@ void gather_adjoint(const std::vector<pale_handle*>& scenes, const std::vector<C
   W.dldi = d_dldi;
   for (size_t k = 0; k < scenes.size(); ++k) W.grads[k] = grads[k];
   W.all_grads = all ? 1 : 0;
+  W.view_grads = d_view_grads;
   gather_backward(F, sel, h->vplan, W, scratch, s);
   uint32_t stored = 0;
-  for (const VertexChunk& c : h->vplan.chunks) stored += c.stored ? 1u : 0u;
+  uint64_t recs_all = 0, ents_all = 0;
+  for (const VertexChunk& c : h->vplan.chunks) {
+    stored += c.stored ? 1u : 0u;
+    recs_all += c.recs;
+    ents_all += c.ents;
+  }
+  h->stats.vertex_records = recs_all;
+  h->stats.vertex_entries = ents_all;
   h->stats.vertex_chunks_stored = stored;
   h->stats.vertex_chunks_replayed = (uint32_t)h->vplan.chunks.size() - stored;
   h->stats.vertex_bytes = vertex_bytes(h);
@@ -1646,6 +1661,55 @@ int pale_render_views_backward_device(uint32_t num_scenes, pale_handle* const* s
     const cudaStream_t s = caller_stream(stream);
     for (pale_handle* sk : sc) use_stream(sk, s);
     adjoint_views(sc, vw, d_dldi, nullptr, false, d_grads);
+    return PALE_OK;
+  });
+}
+
+int pale_render_views_gradients_device(uint32_t num_scenes, pale_handle* const* scenes, uint32_t num_views,
+                                       const pale_view* views, const float* d_dldi, const pale_points* d_grads,
+                                       void* stream) {
+  if (!scenes || num_scenes == 0 || !scenes[0]) return fail(nullptr, PALE_ERR_ARGUMENT, "no scenes");
+  pale_handle* h = scenes[0];
+  return guarded(h, [&]() {
+    if (h->st.estimator != PALE_ESTIMATOR_GATHER)
+      throw ArgError("per-view gradients need the gather estimator (scenes[0]'s settings)");
+    std::vector<pale_handle*> sc = scene_list(num_scenes, scenes);
+    std::vector<ViewReq> vw = view_list(num_views, views);
+    if (num_views && (!d_dldi || !d_grads)) throw ArgError("dL/dI or the gradient outputs are null");
+    const cudaStream_t cs = caller_stream(stream);
+    for (pale_handle* sk : sc) use_stream(sk, cs);
+    cudaStream_t s = h->stream;
+    h->timer.used = 0;
+    const uint64_t launches0 = launches_issued();
+    check_views(sc, vw, false);
+    uint32_t total = 0, max_pix = 0;
+    std::vector<CameraRec> sel = view_records(sc, vw, total, max_pix);
+    std::vector<SceneGrads> vg(std::max<size_t>(1, vw.size()));
+    for (size_t i = 0; i < vw.size(); ++i) {
+      const pale_points& g = d_grads[i];
+      if (!g.opacity) continue;   // no gradients for this view
+      if (!g.position || !g.tangent_u || !g.tangent_v || !g.scale || !g.albedo || !g.beta)
+        throw ArgError("gradient outputs need every field but shape");
+      const size_t n = sc[vw[i].scene]->np;
+      for (float* f : {g.position, g.tangent_u, g.tangent_v, g.albedo}) CK(cudaMemsetAsync(f, 0, 12 * n, s));
+      CK(cudaMemsetAsync(g.scale, 0, 8 * n, s));
+      CK(cudaMemsetAsync(g.opacity, 0, 4 * n, s));
+      CK(cudaMemsetAsync(g.beta, 0, 4 * n, s));
+      if (g.shape) CK(cudaMemsetAsync(g.shape, 0, 4 * n, s));
+      vg[i] = SceneGrads{g.opacity, PointsDev{g.position, g.tangent_u, g.tangent_v, g.scale, g.albedo, g.opacity,
+                                              g.beta, g.shape}};
+    }
+    h->vs_view_grads.ensure(vg.size());
+    CK(cudaMemcpyAsync(h->vs_view_grads.p, vg.data(), vg.size() * sizeof(SceneGrads), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(h->run.p, 0, sizeof(RunState), s));
+    CK(cudaEventRecord(h->ev0, s));
+    SceneGrads none[kMaxScenes] = {};
+    gather_adjoint(sc, sel, total, d_dldi, none, h->st.gradients == PALE_GRADIENTS_ALL, h->vs_view_grads.p);
+    CK(cudaEventRecord(h->ev1, s));
+    CK(cudaGetLastError());
+    h->launches_last = launches_issued() - launches0;
+    h->timed = 2;
+    h->stats_pending = 1;
     return PALE_OK;
   });
 }

@@ -439,6 +439,9 @@ struct VertexPlan {
 struct SweepArgs {
   const float* dldi;
   SceneGrads grads[kMaxScenes];
+  // optional (device): per view the arrays its gradients go to instead of
+  // its scene's; a view whose opacity array is null is not swept
+  const SceneGrads* view_grads;
   int all_grads;
 };
 void gather_backward(const FrameArgs& a, const std::vector<CameraRec>& views, const VertexPlan& plan,

@@ -1503,28 +1503,66 @@ __device__ __forceinline__ AlphaGrad alpha_grad(const SurfelView& S, uint32_t k,
 // dL/dI T_k a_k alpha_r E / pi per channel.  E(x_k) is the photon map's
 // and held; the transmittance T_k is recomputed from the entry's with the
 // forward's float operations.
+__device__ __forceinline__ float* sweep_target(const SceneGrads& G, uint32_t k, int c) {
+  switch (c) {
+    case 0: return G.opacity + k;
+    case 1: return G.all.beta + k;
+    case 2: case 3: case 4: return G.all.position + 3 * (size_t)k + (c - 2);
+    case 5: case 6: case 7: return G.all.tangent_u + 3 * (size_t)k + (c - 5);
+    case 8: case 9: case 10: return G.all.tangent_v + 3 * (size_t)k + (c - 8);
+    case 11: case 12: return G.all.scale + 2 * (size_t)k + (c - 11);
+    default: return G.all.albedo + 3 * (size_t)k + (c - 13);
+  }
+}
+
+constexpr int kSweepTerms = 16;   // opacity, beta, position 3, tangent_u 3, tangent_v 3, scale 2, albedo 3
+
+// One thread per entry; the layers of a warp's entries are visited by layer
+// index, deepest first, and the terms of lanes whose layer at that index
+// is the same surfel are added up inside the warp (__match_any_sync on the
+// scene and surfel, the lowest lane sums in lane order from shared memory)
+// before one atomicAdd per component, the components spread over lanes.
+// Neighbouring camera paths cross the same front surfels, so the first
+// layers of a warp share targets.
 __global__ void __launch_bounds__(kBlock) k_vs_sweep(FrameArgs A, SweepArgs W, const uint32_t* __restrict__ base,
                                                      uint32_t round) {
+  __shared__ float s_val[kBlock / 32][kSweepTerms][33];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const uint32_t e1 = base[kVertexBases + round + 1];
   const uint32_t e = base[kVertexBases + round] + blockIdx.x * kBlock + threadIdx.x;
-  if (e >= e1) return;
-  const float4 dT = A.vs.ent_d[e];
-  const uint4 b = A.vs.ent_b[e];
-  const uint32_t used = b.y & 0xFFu, first = b.x, path = b.w;
-  const uint32_t v = view_of_path(A, path);
-  const CameraRec& C = A.cams[v];
-  const SceneView& S = A.scenes.s[C.scene];
-  const SceneGrads& G = W.grads[C.scene];
-  const uint32_t npix = C.w * C.h;
-  const uint32_t gp = C.pixel_offset + (path - A.view_start[v]) % npix;
-  const V3 g = xyz(*reinterpret_cast<const float4*>(W.dldi + 4 * (size_t)gp));
-  const float inv = 1.0f / (float)C.passes;
+  bool valid = e < e1;
+  if (!__any_sync(0xffffffffu, valid)) return;
+  const int nterms = W.all_grads ? kSweepTerms : 1;
+  float4 dT = make_float4(0.f, 0.f, 0.f, 1.f);
+  uint4 b = make_uint4(0u, 0u, kInvalid, 0u);
+  uint32_t sid = 0, route = 0, gp = 0;   // route: the gradient arrays' index (view or scene)
+  float inv = 0.f;
+  if (valid) {
+    b = A.vs.ent_b[e];
+    const uint32_t v = view_of_path(A, b.w);
+    const CameraRec& C = A.cams[v];
+    sid = C.scene;
+    route = W.view_grads ? v : sid;
+    if (W.view_grads && !W.view_grads[v].opacity) valid = false;   // a view without gradients
+    dT = A.vs.ent_d[e];
+    gp = C.pixel_offset + (b.w - A.view_start[v]) % (C.w * C.h);
+    inv = 1.0f / (float)C.passes;
+  }
+  if (!valid) b = make_uint4(0u, 0u, kInvalid, 0u);
+  const SceneView& S = A.scenes.s[sid];
+  const uint32_t used = b.y & 0xFFu, first = b.x;
+  const V3 g = valid ? xyz(*reinterpret_cast<const float4*>(W.dldi + 4 * (size_t)gp)) : v3(0.f, 0.f, 0.f);
   V3 Lb = v3(0.f, 0.f, 0.f);
-  if (b.z != kInvalid) Lb = xyz(A.vs.ent_l[b.z]);
-  else if ((b.y >> 8) & 1u) Lb = xyz(A.vs.ent_l[e]);
+  if (valid && b.z != kInvalid) Lb = xyz(A.vs.ent_l[b.z]);
+  else if (valid && ((b.y >> 8) & 1u)) Lb = xyz(A.vs.ent_l[e]);
   float Ts[kGatherHits], as[kGatherHits];
   int ns = 0;
   float T = dT.w;
+#pragma unroll
+  for (int i = 0; i <= kGatherHits; ++i) {
+    Ts[i < kGatherHits ? i : 0] = 0.f;
+    as[i < kGatherHits ? i : 0] = 0.f;
+  }
 #pragma unroll
   for (int i = 0; i <= kGatherHits; ++i) {
     if (i < (int)used) {
@@ -1544,45 +1582,62 @@ __global__ void __launch_bounds__(kBlock) k_vs_sweep(FrameArgs A, SweepArgs W, c
     }
   }
   const V3 dd = normalize(xyz(dT));
+  float (*val)[33] = s_val[wid];
 #pragma unroll
   for (int i = kGatherHits - 1; i >= 0; --i) {
+    if (!__any_sync(0xffffffffu, i < ns)) continue;
+    uint32_t k = kInvalid;
+    float t[kSweepTerms];
+#pragma unroll
+    for (int c = 0; c < kSweepTerms; ++c) t[c] = 0.f;
     if (i < ns) {
       const float4 xa = A.vs.rec_xa[first + i], ew = A.vs.rec_ew[first + i];
-      const uint32_t k = __float_as_uint(ew.w) & kRecIndexMask;
+      k = __float_as_uint(ew.w) & kRecIndexMask;
       const float4 al = __ldg(&S.sf.alb[k]);
       const V3 E = xyz(ew);
       const V3 Lo = mul(E, scale(scale(xyz(al), al.w), kInvPi));
       const float w = inv * dot(g, scale(Lo - Lb, Ts[i]));
-      if (w != 0.f) {
-        atomicAdd(&G.opacity[k], w * xa.w);
-        if (W.all_grads) {
-          const AlphaGrad ag = alpha_grad(S.sf, k, xyz(xa), dd);
-          atomicAdd(&G.all.beta[k], w * ag.beta);
-          atomicAdd(&G.all.position[3 * (size_t)k + 0], w * ag.pos.x);
-          atomicAdd(&G.all.position[3 * (size_t)k + 1], w * ag.pos.y);
-          atomicAdd(&G.all.position[3 * (size_t)k + 2], w * ag.pos.z);
-          atomicAdd(&G.all.tangent_u[3 * (size_t)k + 0], w * ag.tu.x);
-          atomicAdd(&G.all.tangent_u[3 * (size_t)k + 1], w * ag.tu.y);
-          atomicAdd(&G.all.tangent_u[3 * (size_t)k + 2], w * ag.tu.z);
-          atomicAdd(&G.all.tangent_v[3 * (size_t)k + 0], w * ag.tv.x);
-          atomicAdd(&G.all.tangent_v[3 * (size_t)k + 1], w * ag.tv.y);
-          atomicAdd(&G.all.tangent_v[3 * (size_t)k + 2], w * ag.tv.z);
-          atomicAdd(&G.all.scale[2 * (size_t)k + 0], w * ag.su);
-          atomicAdd(&G.all.scale[2 * (size_t)k + 1], w * ag.sv);
-        }
-      }
+      t[0] = w * xa.w;
       if (W.all_grads) {
-        const float ka = inv * Ts[i] * as[i] * al.w * kInvPi;
-        if (ka != 0.f) {
-          atomicAdd(&G.all.albedo[3 * (size_t)k + 0], g.x * ka * E.x);
-          atomicAdd(&G.all.albedo[3 * (size_t)k + 1], g.y * ka * E.y);
-          atomicAdd(&G.all.albedo[3 * (size_t)k + 2], g.z * ka * E.z);
+        if (w != 0.f) {
+          const AlphaGrad ag = alpha_grad(S.sf, k, xyz(xa), dd);
+          t[1] = w * ag.beta;
+          t[2] = w * ag.pos.x; t[3] = w * ag.pos.y; t[4] = w * ag.pos.z;
+          t[5] = w * ag.tu.x; t[6] = w * ag.tu.y; t[7] = w * ag.tu.z;
+          t[8] = w * ag.tv.x; t[9] = w * ag.tv.y; t[10] = w * ag.tv.z;
+          t[11] = w * ag.su; t[12] = w * ag.sv;
         }
+        const float ka = inv * Ts[i] * as[i] * al.w * kInvPi;
+        t[13] = g.x * ka * E.x;
+        t[14] = g.y * ka * E.y;
+        t[15] = g.z * ka * E.z;
       }
       Lb = scale(Lo, as[i]) + scale(Lb, 1.0f - as[i]);
     }
+    for (int c = 0; c < nterms; ++c) val[c][lane] = t[c];
+    __syncwarp();
+    const unsigned grp = __match_any_sync(0xffffffffu, ((unsigned long long)route << 32) | k);
+    const bool leader = k != kInvalid && lane == __ffs(grp) - 1;
+    if (leader && __popc(grp) > 1) {
+      for (int c = 0; c < nterms; ++c) {
+        float acc = 0.f;
+        for (unsigned r = grp; r; r &= r - 1u) acc += val[c][__ffs(r) - 1];
+        val[c][lane] = acc;
+      }
+    }
+    __syncwarp();
+    for (unsigned lm = __ballot_sync(0xffffffffu, leader); lm; lm &= lm - 1u) {
+      const int L = __ffs(lm) - 1;
+      const uint32_t kL = __shfl_sync(0xffffffffu, k, L);
+      const uint32_t rL = __shfl_sync(0xffffffffu, route, L);
+      if (lane < nterms) {
+        const float x = val[lane][L];
+        if (x != 0.f) atomicAdd(sweep_target(W.view_grads ? W.view_grads[rL] : W.grads[rL], kL, lane), x);
+      }
+    }
+    __syncwarp();
   }
-  A.vs.ent_l[e] = make_float4(Lb.x, Lb.y, Lb.z, 0.f);
+  if (valid) A.vs.ent_l[e] = make_float4(Lb.x, Lb.y, Lb.z, 0.f);
 }
 
 void gather_backward(const FrameArgs& a0, const std::vector<CameraRec>& views, const VertexPlan& plan,
@@ -1606,9 +1661,12 @@ void gather_backward(const FrameArgs& a0, const std::vector<CameraRec>& views, c
       rounds = multi ? gather_rounds<true>(a, g, vc.p0, vc.p1, vc.n, s) : gather_rounds<false>(a, g, vc.p0, vc.p1, vc.n, s);
       bases = a.vs.base;
     }
+    // timed as the adjoint's transport (this estimator has none)
+    if (a.timer) a.timer->begin(kTimeTransport, s);
     for (uint32_t r = rounds; r-- > 0;) {
       k_vs_sweep<<<blocks_for(vc.n), kBlock, 0, s>>>(a, w, bases, r); note_launch();
     }
+    if (a.timer) a.timer->end(s);
   }
 }
 

@@ -189,6 +189,29 @@ class ViewBatch:
         _check(L, self.renderers[0]._h, rc, "render_views_backward_device")
         return self.grads
 
+    def view_gradients(self, views: Sequence[int], dldi: Optional[torch.Tensor] = None) -> List[Dict[str, torch.Tensor]]:
+        """The gather estimator's backward of the last forward_loss (the
+        first renderer's estimator must be "gather") with gradients per
+        view: one gradient dict (BVH order of the view's scene) for each
+        view index in `views`; the other views are not swept."""
+        d = self.dldi if dldi is None else dldi.contiguous()
+        f = dict(dtype=torch.float32, device=self.device)
+        structs = (N.PalePoints * max(1, len(self.views)))()
+        out = []
+        for i in views:
+            s = self.views[i][0]
+            n = self.renderers[s].num_points
+            g = {key: torch.empty((n, POINT_WIDTH[key]) if POINT_WIDTH[key] > 1 else (n,), **f) for key in POINT_FIELDS}
+            out.append(g)
+            structs[i].count = n
+            for key in POINT_FIELDS:
+                setattr(structs[i], key, C.cast(C.c_void_p(g[key].data_ptr()), N.f32p))
+        L = self.renderers[0]._lib
+        rc = L.pale_render_views_gradients_device(len(self.renderers), self._scenes, len(self.views), self._views,
+                                                  C.c_void_p(d.data_ptr()), structs, self._stream())
+        _check(L, self.renderers[0]._h, rc, "render_views_gradients_device")
+        return out
+
     def split(self, packed: torch.Tensor) -> List[torch.Tensor]:
         """Packed (P, 4) -> list of (H, W, 4) views, one per view."""
         out, off = [], 0

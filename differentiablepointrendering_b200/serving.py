@@ -14,6 +14,13 @@ Each request carries its own number of passes (samples per pixel, gather
 and adjoint) and adjoint bounces, up to the maxima its scene was created
 with; resolutions are the scene's cameras.
 
+Gradients: with the server's settings' estimator "reference" (default) the
+round's gradient requests share adjoint wavefronts of the reference's
+adjoint; with "gather" each gets the exact derivative of its view of the
+round's forward (photon map held), swept from that forward's own path
+vertices into arrays of its own (``pale_render_views_gradients_device``),
+with no second wavefront.
+
 One dispatcher thread owns the GPU stream and serves requests in rounds.
 A round takes every queued request that fits (at most ``max_views`` views,
 ``max_pixels`` camera pixels and, when set, ``max_paths`` camera paths of
@@ -148,6 +155,7 @@ class Server:
         st.update(settings or {})
         st.update(camera_seeds="camera", photons=1000, forward_passes=1)
         self._exec_settings = st
+        self._gather = st.get("estimator", "reference") in ("gather", 1)
         self._exec = Renderer.from_scene(make_box_scene(8, cameras=1, resolution=8), st)
         self._thread = threading.Thread(target=self._run, name="pale-serve", daemon=True)
         self._thread.start()
@@ -296,6 +304,21 @@ class Server:
             else:
                 q.t_done = time.perf_counter()
                 q.done.set()
+        if grad_idx and self._gather:
+            # the gather estimator: one sweep over the round's own forward
+            # vertices, each gradient request's view into arrays of its own
+            dl = torch.zeros(max(1, int(offs[-1])), 4, dtype=torch.float32, device=self.device)
+            for i in grad_idx:
+                dl[offs[i]:offs[i + 1]] = dldi[i]
+            gl = vb.view_gradients(grad_idx, dl)
+            host = [{k: v.cpu().numpy() for k, v in g.items()} for g in gl]
+            now = time.perf_counter()
+            for k, i in enumerate(grad_idx):
+                q = reqs[i]
+                q.grads = host[k]
+                q.t_done = now
+                q.done.set()
+            return
         per = self.GRADIENTS_PER_WAVEFRONT - 1     # entry 0 is the executor
         for c0 in range(0, len(grad_idx), per):
             chunk = grad_idx[c0:c0 + per]

@@ -198,13 +198,16 @@ typedef struct pale_stats {
     float gather_ms;                /* camera gather part                    */
     float timed_ms[4];              /* device time of the hot kernels: camera
                                        trace, photon lookup, adjoint bounce,
-                                       adjoint transport (CUDA events around
-                                       each launch)                          */
+                                       adjoint transport or the gather
+                                       estimator's sweep (CUDA events around
+                                       each launch or group of launches)     */
     uint32_t timed_launches[4];     /* ... and their launch counts           */
     uint64_t vertex_bytes;          /* vertex store + replay scratch held    */
     uint32_t vertex_chunks_stored;  /* last GATHER backward: chunks swept
                                        from the store ...                    */
     uint32_t vertex_chunks_replayed;/* ... and chunks traced again           */
+    uint64_t vertex_records;        /* ... layer records and path segments   */
+    uint64_t vertex_entries;        /*     it swept                          */
 } pale_stats;
 
 /* Fills *s with the reference's PathTracerSettings defaults. */
@@ -342,8 +345,8 @@ int pale_trace_photon_map(pale_handle *h, void *stream);
 
 /* The adjoint pass of the same views as ONE wavefront of (view, pass) jobs:
  * dL/dI packed in view order (DEVICE).  With d_grads NULL each scene's
- * gradients accumulate in its own arrays (read them with a later
- * pale_render_backward_device of no views, or through the renderer); else
+ * gradients go to the scene's own gradient arrays (zeroed first), those
+ * that pale_optimizer_step with NULL gradients applies; else
  * d_grads holds num_scenes entries of DEVICE arrays (BVH order, every field
  * but shape non-null) that entry k's gradients accumulate in after they
  * are zeroed, and one scene may then fill several entries, so that the
@@ -354,6 +357,20 @@ int pale_render_views_backward_device(uint32_t num_scenes, pale_handle *const *s
                                       uint32_t num_views, const pale_view *views,
                                       const float *d_dldi, pale_points *d_grads,
                                       void *stream);
+
+/* The gather estimator's backward (scenes[0]'s estimator must be
+ * PALE_ESTIMATOR_GATHER) of the last pale_render_views_loss_device call
+ * with the same scenes and views, with gradients per VIEW: d_grads holds
+ * num_views entries of DEVICE arrays (BVH order of the view's scene, every
+ * field but shape non-null) that view i's gradients go to after they are
+ * zeroed; an entry whose opacity pointer is NULL gets none and its view is
+ * not swept.  dL/dI packed in view order (DEVICE).  So the requests of a
+ * server that share a scene keep separate gradients from one forward
+ * wavefront.  No reference counterpart (one camera per call there). */
+int pale_render_views_gradients_device(uint32_t num_scenes, pale_handle *const *scenes,
+                                       uint32_t num_views, const pale_view *views,
+                                       const float *d_dldi, const pale_points *d_grads,
+                                       void *stream);
 
 /* Current per-point parameters in BVH order (get_point_parameters,
  * pale_bindings.cpp:733-850). */

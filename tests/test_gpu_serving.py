@@ -1,9 +1,10 @@
 """The serving loop (serving.Server) on the GPU: resident scenes with
 their photon maps traced once, requests of several scenes, passes and
-depths batched into rounds (one camera-gather wavefront and a shared
-adjoint wavefront per round), and every result the same alone and in the
-mix: images and losses bit for bit, gradients up to the order of float
-atomic additions."""
+depths batched into rounds (one camera-gather wavefront per round, and for
+the gradient requests a shared adjoint wavefront of the reference's
+adjoint or a sweep of the gather estimator over the round's own path
+vertices), and every result the same alone and in the mix: images and
+losses bit for bit, gradients up to the order of float atomic additions."""
 import threading
 
 import numpy as np
@@ -23,13 +24,14 @@ def _scenes():
     return a, b
 
 
-def test_results_are_the_same_alone_and_in_the_mix(gpu):
+@pytest.mark.parametrize("estimator", ["reference", "gather"])
+def test_results_are_the_same_alone_and_in_the_mix(gpu, estimator):
     import torch
 
     from differentiablepointrendering_b200.serving import Request, Server
 
     free, _ = torch.cuda.mem_get_info()
-    srv = Server(hbm_budget=free, settings={"rng_mode": "decorrelated"})
+    srv = Server(hbm_budget=free, settings={"rng_mode": "decorrelated", "estimator": estimator})
     try:
         a, b = _scenes()
         srv.add_scene("a", a, SETTINGS)
