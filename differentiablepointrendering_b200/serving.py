@@ -147,6 +147,7 @@ class Server:
         self._cv = threading.Condition()
         self._lock = threading.Lock()
         self._gpu = threading.Lock()          # the executor's buffers: one user at a time
+        self._pin = None                      # pinned staging of the results
         self._stop = False
         # the executor: a tiny scene whose renderer lends the wavefront
         # buffers and the adjoint settings (rng mode, null weighting,
@@ -235,6 +236,19 @@ class Server:
         return req
 
     # ------------------------------------------------------------ rounds
+    def _host(self, t) -> np.ndarray:
+        """A host copy of device tensor `t` through a pinned staging buffer
+        (device-to-host copies from pinned memory run at several times the
+        rate of pageable ones)."""
+        import torch
+
+        n = t.numel()
+        if self._pin is None or self._pin.numel() < n:
+            self._pin = torch.empty(max(n, 1 << 20), dtype=torch.float32, pin_memory=True)
+        buf = self._pin[:n].view(t.shape)
+        buf.copy_(t)
+        return buf.numpy().copy()
+
     def _run(self):
         import torch
 
@@ -293,7 +307,7 @@ class Server:
             loss[i] = 0.5 * (d[:, :3].double() ** 2).mean()
             d[:, :3].div_(float(3 * (offs[i + 1] - offs[i])))
             dldi[i] = d
-        ldr = vb.ldr.cpu().numpy()
+        ldr = self._host(vb.ldr)
         for i, q in enumerate(reqs):
             w, h = vb.sizes[i]
             q.image = ldr[offs[i]:offs[i + 1]].reshape(h, w, 4).copy()
@@ -311,7 +325,7 @@ class Server:
             for i in grad_idx:
                 dl[offs[i]:offs[i + 1]] = dldi[i]
             gl = vb.view_gradients(grad_idx, dl)
-            host = [{k: v.cpu().numpy() for k, v in g.items()} for g in gl]
+            host = [{k: self._host(v) for k, v in g.items()} for g in gl]
             now = time.perf_counter()
             for k, i in enumerate(grad_idx):
                 q = reqs[i]
@@ -328,7 +342,7 @@ class Server:
             gb = ViewBatch(rs, gviews, device=self.device)
             dl = torch.cat([dldi[i] for i in chunk]).contiguous()
             grads = gb.backward(dl)
-            host = [{k: v.cpu().numpy() for k, v in grads[k + 1].items()} for k in range(len(chunk))]
+            host = [{k: self._host(v) for k, v in grads[k + 1].items()} for k in range(len(chunk))]
             now = time.perf_counter()
             for k, i in enumerate(chunk):
                 q = reqs[i]
