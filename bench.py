@@ -38,10 +38,10 @@ WORKLOADS = {
     # the memory-bound case: 1M surfels, 32 views of 800x800, 64 passes, depth 8
     "box1m-32view": dict(n=1000000, cams=32, res=800, photons=1000000, bounces=8, forward_passes=1, spp=64,
                          adjoint_bounces=8, adjoint_spp=64, radius=0.01),
-    # box200k's scene and photon map with one 256x256 view and 2 passes: the
-    # case the per-kernel profiles are captured on (a few hundred MB resident)
-    "box200k-1view": dict(n=200000, cams=1, res=256, photons=1000000, bounces=6, forward_passes=1, spp=2,
-                          adjoint_bounces=6, adjoint_spp=2, radius=0.01),
+    # box200k's scene and photon map with one 256x256 view and 8 passes: the
+    # case the per-kernel profiles are captured on (under 1 GB resident)
+    "box200k-1view": dict(n=200000, cams=1, res=256, photons=1000000, bounces=6, forward_passes=1, spp=8,
+                          adjoint_bounces=6, adjoint_spp=8, radius=0.01),
 }
 
 METRIC = "fwd+adjoint Mrays/s"
@@ -807,43 +807,45 @@ def run_serving(args):
     budget = min(150 * 10 ** 9, int(free * 0.9))
     srv = Server(hbm_budget=budget, max_views=64, max_pixels=1 << 24, max_paths=args.round_paths,
                  settings={"estimator": args.estimator})
-    names = []
-    t_admit = time.perf_counter()
-    for k, n in enumerate(SERVING_SURFELS):
-        name = f"box{n // 1000}k"
-        srv.add_scene(name, make_box_scene(n, cameras=2, resolutions=SERVING_RES,
-                                           points=make_surfels(n, 1234 + k)), SERVING_SETTINGS)
-        names.append(name)
-    t_admit = time.perf_counter() - t_admit
-    # warm-up: every scene once, both kinds, so the wavefront buffers exist
-    warm = [(0.0, serving_request(rng, names, kind, 1024, 1)) for kind in ("forward", "gradient")]
-    serve_stream(srv, warm)
-    runs = []
-    for rate in args.rates:
-        count = max(8, min(args.requests, int(rate * args.seconds)))
-        t, reqs = 0.0, []
-        for _ in range(count):
-            t += rng.exponential(1.0 / rate)
-            reqs.append((t, serving_request(rng, names)))
-        served, span, plain, clock, service = serve_stream(srv, reqs)
-        views = [q.batch_views for _, q in reqs]
-        runs.append({"rate_per_s": rate, "requests": count,
-                     "served": dict(_pcts(served), requests_per_s=round(count / span, 2),
-                                    mean_views_per_round=round(float(np.mean(views)), 2),
-                                    max_views_per_round=int(max(views))),
-                     "plain": dict(_pcts(plain), requests_per_s=round(count / clock, 2),
-                                   service=_pcts(service))})
-    g512 = []
-    for spp in (1, 4, 16):
-        t, reqs = 0.0, []
-        for _ in range(args.requests_512):
-            t += rng.exponential(1.0 / args.rate_512)
-            reqs.append((t, serving_request(rng, names, "gradient", 512, spp)))
-        served, span, plain, clock, service = serve_stream(srv, reqs)
-        g512.append({"passes": spp, "rate_per_s": args.rate_512, "requests": len(reqs),
-                     "served": _pcts(served), "plain": _pcts(plain), "service_alone": _pcts(service)})
-    admitted = srv.admitted_bytes
-    srv.close()
+    try:
+        names = []
+        t_admit = time.perf_counter()
+        for k, n in enumerate(SERVING_SURFELS):
+            name = f"box{n // 1000}k"
+            srv.add_scene(name, make_box_scene(n, cameras=2, resolutions=SERVING_RES,
+                                               points=make_surfels(n, 1234 + k)), SERVING_SETTINGS)
+            names.append(name)
+        t_admit = time.perf_counter() - t_admit
+        # warm-up: every scene once, both kinds, so the wavefront buffers exist
+        warm = [(0.0, serving_request(rng, names, kind, 1024, 1)) for kind in ("forward", "gradient")]
+        serve_stream(srv, warm)
+        runs = []
+        for rate in args.rates:
+            count = max(8, min(args.requests, int(rate * args.seconds)))
+            t, reqs = 0.0, []
+            for _ in range(count):
+                t += rng.exponential(1.0 / rate)
+                reqs.append((t, serving_request(rng, names)))
+            served, span, plain, clock, service = serve_stream(srv, reqs)
+            views = [q.batch_views for _, q in reqs]
+            runs.append({"rate_per_s": rate, "requests": count,
+                         "served": dict(_pcts(served), requests_per_s=round(count / span, 2),
+                                        mean_views_per_round=round(float(np.mean(views)), 2),
+                                        max_views_per_round=int(max(views))),
+                         "plain": dict(_pcts(plain), requests_per_s=round(count / clock, 2),
+                                       service=_pcts(service))})
+        g512 = []
+        for spp in (1, 4, 16):
+            t, reqs = 0.0, []
+            for _ in range(args.requests_512):
+                t += rng.exponential(1.0 / args.rate_512)
+                reqs.append((t, serving_request(rng, names, "gradient", 512, spp)))
+            served, span, plain, clock, service = serve_stream(srv, reqs)
+            g512.append({"passes": spp, "rate_per_s": args.rate_512, "requests": len(reqs),
+                         "served": _pcts(served), "plain": _pcts(plain), "service_alone": _pcts(service)})
+        admitted = srv.admitted_bytes
+    finally:
+        srv.close()
     print(json.dumps({"metric": "serving latency p50/p99 (ms) and requests/s", "impl": "ours", "n_gpus": 1,
                       "scenes": [{"name": m, "surfels": n} for m, n in zip(names, SERVING_SURFELS)],
                       "scene_settings": SERVING_SETTINGS, "resolutions": SERVING_RES, "passes": SERVING_SPP,

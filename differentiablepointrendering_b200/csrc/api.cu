@@ -1095,7 +1095,9 @@ void gather_adjoint(const std::vector<pale_handle*>& scenes, const std::vector<C
       recs = std::max<uint64_t>(recs, c.recs);
       ents = std::max<uint64_t>(ents, c.ents);
     }
-  if (recs) {
+  if (recs || ents) {
+    recs = std::max<uint64_t>(recs, 1);
+    ents = std::max<uint64_t>(ents, 1);
     h->sc_rec_xa.ensure(recs); h->sc_rec_ew.ensure(recs);
     h->sc_ent_d.ensure(ents); h->sc_ent_b.ensure(ents); h->sc_ent_l.ensure(ents);
   }

@@ -1531,6 +1531,10 @@ __global__ void __launch_bounds__(kBlock) k_vs_sweep(FrameArgs A, SweepArgs W, c
   const uint32_t e1 = base[kVertexBases + round + 1];
   const uint32_t e = base[kVertexBases + round] + blockIdx.x * kBlock + threadIdx.x;
   bool valid = e < e1;
+  if (valid && e >= A.vs.ent_cap) {   // slots past the store: never written
+    flag_error(A.st, kErrBounds);
+    valid = false;
+  }
   if (!__any_sync(0xffffffffu, valid)) return;
   const int nterms = W.all_grads ? kSweepTerms : 1;
   float4 dT = make_float4(0.f, 0.f, 0.f, 1.f);
@@ -1547,6 +1551,10 @@ __global__ void __launch_bounds__(kBlock) k_vs_sweep(FrameArgs A, SweepArgs W, c
     dT = A.vs.ent_d[e];
     gp = C.pixel_offset + (b.w - A.view_start[v]) % (C.w * C.h);
     inv = 1.0f / (float)C.passes;
+  }
+  if (valid && ((uint64_t)b.x + (b.y & 0xFFu) > A.vs.rec_cap || (b.z != kInvalid && b.z >= A.vs.ent_cap))) {
+    flag_error(A.st, kErrBounds);
+    valid = false;
   }
   if (!valid) b = make_uint4(0u, 0u, kInvalid, 0u);
   const SceneView& S = A.scenes.s[sid];

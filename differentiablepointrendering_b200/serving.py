@@ -103,24 +103,30 @@ class _Scene:
     max_depth: int
 
 
+MAX_ROUND_SCENES = 7   # a call's scene table holds 8 entries, the first the server's executor
+
+
 def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], max_views: int,
                max_pixels: int, max_paths: Optional[int] = None,
-               max_passes: Optional[Dict[str, int]] = None) -> Tuple[List[Request], List[Request]]:
+               max_passes: Optional[Dict[str, int]] = None,
+               max_scenes: int = MAX_ROUND_SCENES) -> Tuple[List[Request], List[Request]]:
     """The requests of the next round: the queue's head in arrival order
-    while the round holds at most max_views views, max_pixels camera pixels
-    and (when given) max_paths camera paths, pixels x passes, a request's
-    passes 0 counting as its scene's max_passes (the first request always
-    goes); returns (taken, left)."""
-    taken, pix, paths = [], 0, 0
+    while the round holds at most max_views views, max_pixels camera
+    pixels, max_scenes distinct scenes and (when given) max_paths camera
+    paths, pixels x passes, a request's passes 0 counting as its scene's
+    max_passes (the first request always goes); returns (taken, left)."""
+    taken, pix, paths, scenes = [], 0, 0, set()
     for i, q in enumerate(queue):
         w, h = sizes[q.scene][q.camera]
         n = w * h * (q.passes or (max_passes or {}).get(q.scene, 1))
         if taken and (len(taken) + 1 > max_views or pix + w * h > max_pixels
-                      or (max_paths is not None and paths + n > max_paths)):
+                      or (max_paths is not None and paths + n > max_paths)
+                      or (q.scene not in scenes and len(scenes) >= max_scenes)):
             return taken, queue[i:]
         taken.append(q)
         pix += w * h
         paths += n
+        scenes.add(q.scene)
     return taken, []
 
 
@@ -152,7 +158,9 @@ class Server:
         # the executor: a tiny scene whose renderer lends the wavefront
         # buffers and the adjoint settings (rng mode, null weighting,
         # gradient groups, batch sizes) of every round
-        st = {"gather_passes": 64, "adjoint_passes": 64, "adjoint_bounces": 8}
+        # (gather estimator: the round's path vertices are kept within 16 GB
+        # unless the settings say otherwise, the chunks past it replayed)
+        st = {"gather_passes": 64, "adjoint_passes": 64, "adjoint_bounces": 8, "vertex_store_bytes": 16 << 30}
         st.update(settings or {})
         st.update(camera_seeds="camera", photons=1000, forward_passes=1)
         self._exec_settings = st

@@ -61,6 +61,7 @@ def test_results_are_the_same_alone_and_in_the_mix(gpu, estimator):
             assert q.error is None, q.error
         assert max(q.batch_views for q in mix) > 1                 # some requests shared a round
         assert sum(1 for q in mix if q.kind == "gradient") >= 2
+        lit = 0
         for q in mix:
             alone = srv.serve_one(Request(q.scene, q.camera, q.kind, q.target, q.passes, q.depth))
             assert alone.error is None, alone.error
@@ -68,9 +69,12 @@ def test_results_are_the_same_alone_and_in_the_mix(gpu, estimator):
             np.testing.assert_array_equal(alone.image, q.image)
             if q.kind == "gradient":
                 assert alone.loss == q.loss
-                a_, b_ = alone.grads["opacity"].astype(np.float64), q.grads["opacity"].astype(np.float64)
-                assert np.linalg.norm(b_) > 0
-                assert np.linalg.norm(a_ - b_) <= 1e-4 * np.linalg.norm(b_)
+                for key in ("opacity", "albedo") if estimator == "gather" else ("opacity",):
+                    a_, b_ = alone.grads[key].astype(np.float64), q.grads[key].astype(np.float64)
+                    # a camera that looks at a closed wall of the box from outside sees no surfel
+                    assert np.linalg.norm(a_ - b_) <= 1e-4 * np.linalg.norm(b_), (key, q)
+                    lit += int(np.linalg.norm(b_) > 0)
+        assert lit >= 2
         lat = srv.latency()
         assert lat["n"] >= len(mix) and lat["p99"] >= lat["p50"] > 0
     finally:

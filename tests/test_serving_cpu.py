@@ -73,3 +73,12 @@ def test_round_respects_the_path_cap():
     assert taken == q and left == []
     taken, left = S.plan_round(q, _sizes(), 64, 10 ** 6, max_paths=10, max_passes=spp)
     assert taken == q[:1]
+
+
+def test_round_holds_at_most_seven_scenes():
+    sizes = {f"s{k}": [(4, 4)] for k in range(9)}
+    q = [S.Request(f"s{k}", 0) for k in range(9)] + [S.Request("s0", 0)]
+    taken, left = S.plan_round(q, sizes, 64, 10 ** 6)
+    assert [r.scene for r in taken] == [f"s{k}" for k in range(7)] and left == q[7:]
+    taken, left = S.plan_round(q, sizes, 64, 10 ** 6, max_scenes=2)
+    assert taken == q[:2]
