@@ -111,7 +111,7 @@ struct pale_handle {
   std::vector<CameraRec> cams;
   std::vector<std::string> cam_names;
   DBuf<CameraRec> d_cams;
-  DBuf<uint32_t> d_view_start;   // per view: first camera path of the current gather chunk
+  DBuf<uint32_t> d_view_start;   // the current gather chunk's view table (3 words per view)
   // surfels
   uint32_t np = 0;
   PointsBufs asset, collected, params;
@@ -981,7 +981,7 @@ uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector
   size_wavefronts(h, total, max_pix);
   const uint32_t nsel = (uint32_t)sel.size();
   h->d_cams.ensure(std::max<size_t>(1, nsel));
-  h->d_view_start.ensure(std::max<size_t>(1, nsel));
+  h->d_view_start.ensure(3 * std::max<size_t>(1, nsel));   // the gather chunks' view tables
   if (nsel) CK(cudaMemcpyAsync(h->d_cams.p, sel.data(), nsel * sizeof(CameraRec), cudaMemcpyHostToDevice, s));
   // photon maps of the scenes that some view renders (a scene of the list
   // without views, such as a handle that only lends its wavefront buffers,

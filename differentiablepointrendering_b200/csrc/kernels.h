@@ -226,9 +226,11 @@ struct FrameArgs {
   uint32_t total_pixels;
   float* raw;             // packed H*W*4 per camera
   float* ldr;
-  // paths of the current chunk: view v's passes [p0, min(p1, passes)) at
-  // paths view_start[v] + (pass - p0) * pixels + pixel; non-decreasing, a
-  // view without a pass in the chunk has an empty range
+  // the current chunk's view table (3 words per view): view_start[v], the
+  // first path of view v in the chunk (non-decreasing; a view without a
+  // pass in the chunk has an empty range), then view_start[ncams + v] and
+  // view_start[2 ncams + v], the view's passes [p0, p1) in the chunk, at
+  // paths view_start[v] + (pass - p0) * pixels + pixel
   const uint32_t* view_start;
   uint32_t walk_block;     // threads per block of the persistent walks (host side)
   uint32_t rng_mode;
@@ -404,23 +406,31 @@ void photon_bounce(const PhotonArgs& a, uint32_t parity, cudaStream_t s);
 void grid_build(const SceneView& sv, RunState* st, const PhotonStore& ps, const GridBufs& g, uint32_t cells,
                 int key_bits, cudaStream_t s);
 // The camera gather of the views `views` (host copy of a.cams; every view
-// passes >= 1); d_view_start holds views.size() words of device scratch.
+// passes >= 1); d_view_start holds 3 * views.size() words of device scratch
+// (the chunks' view tables).
 void camera_gather(const FrameArgs& a, const std::vector<CameraRec>& views, uint32_t* d_view_start,
                    cudaStream_t s, struct VertexPlan* plan = nullptr);
 
-// The chunks of a camera gather: runs of whole passes [p0, p1) whose paths
-// (every view's passes in the run) fit the path capacity, one pass at least.
-std::vector<std::pair<uint32_t, uint32_t>> gather_chunks(const std::vector<CameraRec>& views, uint32_t path_capacity);
+// One chunk of a camera gather: its paths and its view table (as
+// FrameArgs::view_start).  The (view, pass) jobs are packed in view order,
+// each view's passes in pass order, whole passes into a chunk while its
+// paths fit the path capacity (one pass at least), so that every chunk but
+// the last is full and a view's passes may span chunks.
+struct GatherChunk {
+  uint32_t n = 0;
+  std::vector<uint32_t> table;
+};
+std::vector<GatherChunk> gather_chunks(const std::vector<CameraRec>& views, uint32_t path_capacity);
 
 // Host record of a camera gather kept for the gather estimator: per chunk
-// its passes, paths, rounds, where its slots start and how many it used,
-// whether they were stored, and its view_start table; d_chunk_base holds
-// each chunk's 2 * kVertexBases bases.
+// its paths, rounds, where its slots start and how many it used, whether
+// they were stored, and its view table; d_chunk_base holds each chunk's
+// 2 * kVertexBases bases.
 struct VertexChunk {
-  uint32_t p0 = 0, p1 = 0, n = 0, rounds = 0;
+  uint32_t n = 0, rounds = 0;
   uint32_t rec_start = 0, ent_start = 0, recs = 0, ents = 0;
   bool stored = false;
-  std::vector<uint32_t> starts;
+  std::vector<uint32_t> table;   // the chunk's view table
 };
 
 struct VertexPlan {

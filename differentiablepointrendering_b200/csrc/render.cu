@@ -414,9 +414,9 @@ __device__ __forceinline__ uint32_t view_of_path(const FrameArgs& A, uint32_t pa
   return lo;
 }
 
-// Primary rays of the chunk of passes [p0, p1): view v's pass p at paths
-// view_start[v] + (p - p0) * pixels(v) + pixel.
-__global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1, uint32_t n) {
+// Primary rays of the chunk: view v's pass p at paths view_start[v] +
+// (p - p0(v)) * pixels(v) + pixel.
+__global__ void k_cg_init(FrameArgs A, uint32_t n) {
   const uint32_t path = blockIdx.x * kBlock + threadIdx.x;
   if (path == 0) A.counts[0] = n;
   if (path == 0 && A.vs.base) {
@@ -429,7 +429,7 @@ __global__ void k_cg_init(FrameArgs A, uint32_t p0, uint32_t p1, uint32_t n) {
   const CameraRec& C = A.cams[v];
   const uint32_t npix = C.w * C.h;
   const uint32_t local = path - A.view_start[v];
-  const uint32_t pass = p0 + local / npix, pix = local % npix;
+  const uint32_t pass = A.view_start[A.ncams + v] + local / npix, pix = local % npix;
   const SceneSeeds& SS = A.sseeds[C.scene];
   const uint64_t cseed = SS.seeds[*SS.cursor + C.seed_slot];
   const uint64_t base = A.rng_mode == 1 ? per_item_seed(cseed, pass) : cseed;
@@ -816,23 +816,23 @@ __global__ void k_cg_compose(FrameArgs A, uint32_t round) {
   }
 }
 
-// fb += res/passes over the view's passes of the chunk [p0, p1), in pass
-// order; the chunk that holds a view's last pass writes its RAW image and
-// the post-processed LDR image.
-__global__ void k_cg_finalize(FrameArgs A, uint32_t p0, uint32_t p1) {
+// fb += res/passes over the view's passes of the chunk [p0(v), p1(v)), in
+// pass order; the chunk that holds a view's last pass writes its RAW image
+// and the post-processed LDR image.
+__global__ void k_cg_finalize(FrameArgs A) {
   const uint32_t gp = blockIdx.x * kBlock + threadIdx.x;
   if (gp >= A.total_pixels) return;
   const uint32_t v = find_camera(A, gp);
   const CameraRec& C = A.cams[v];
   const uint32_t P = C.passes;
-  if (P == 0 || p0 >= P) return;                    // finished in an earlier chunk
+  const uint32_t p0 = A.view_start[A.ncams + v], p1 = A.view_start[2 * A.ncams + v];
+  if (P == 0 || p0 >= p1) return;                   // no pass of this view in the chunk
   const uint32_t npix = C.w * C.h, pix = gp - C.pixel_offset;
-  const uint32_t q1 = p1 < P ? p1 : P;
-  const bool last = q1 == P;
+  const bool last = p1 >= P;
   float4 f = p0 == 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : A.fb[gp];
   float fb[4] = {f.x, f.y, f.z, f.w};
   const float inv = 1.f / (float)P;
-  for (uint32_t p = p0; p < q1; ++p) {
+  for (uint32_t p = p0; p < p1; ++p) {
     const float4 a = A.res[(size_t)A.view_start[v] + (size_t)(p - p0) * npix + pix];
     float cur[4] = {a.x * inv, a.y * inv, a.z * inv, 1.0f * inv};
 #pragma unroll
@@ -908,41 +908,58 @@ void image_loss(const FrameArgs& a, double* partials, double* loss, cudaStream_t
   k_loss_final<<<(a.ncams + 63) / 64, 64, 0, s>>>(a, partials, kLossChunks, loss); note_launch();
 }
 
-std::vector<std::pair<uint32_t, uint32_t>> gather_chunks(const std::vector<CameraRec>& views, uint32_t path_capacity) {
-  uint32_t max_passes = 0;
-  for (const CameraRec& v : views) max_passes = std::max(max_passes, v.passes);
-  // paths of the chunk of passes [p0, p1): every view's passes in it
-  auto chunk_paths = [&](uint32_t p0, uint32_t p1) {
-    uint64_t n = 0;
-    for (const CameraRec& v : views) {
-      const uint32_t q1 = std::min(p1, v.passes);
-      if (q1 > p0) n += (uint64_t)v.w * v.h * (q1 - p0);
+std::vector<GatherChunk> gather_chunks(const std::vector<CameraRec>& views, uint32_t path_capacity) {
+  const size_t nv = views.size();
+  std::vector<GatherChunk> out;
+  GatherChunk cur;
+  std::vector<uint32_t> p0(nv, 0u), p1(nv, 0u);
+  std::vector<char> in(nv, 0);
+  uint64_t used = 0;
+  auto close = [&]() {
+    cur.n = (uint32_t)used;
+    cur.table.assign(3 * nv, 0u);
+    // paths in view order; a view absent from the chunk gets an empty
+    // range at the next view's start
+    uint64_t acc = 0;
+    for (size_t v = 0; v < nv; ++v) {
+      cur.table[v] = (uint32_t)acc;
+      if (in[v]) {
+        cur.table[nv + v] = p0[v];
+        cur.table[2 * nv + v] = p1[v];
+        acc += (uint64_t)views[v].w * views[v].h * (p1[v] - p0[v]);
+      }
     }
-    return n;
+    out.push_back(cur);
+    cur = GatherChunk{};
+    std::fill(in.begin(), in.end(), 0);
+    used = 0;
   };
-  std::vector<std::pair<uint32_t, uint32_t>> out;
-  for (uint32_t p0 = 0, p1 = 0; p0 < max_passes; p0 = p1) {
-    p1 = p0 + 1;
-    while (p1 < max_passes && chunk_paths(p0, p1 + 1) <= path_capacity) ++p1;
-    out.emplace_back(p0, p1);
+  for (size_t v = 0; v < nv; ++v) {
+    const uint64_t npix = (uint64_t)views[v].w * views[v].h;
+    uint32_t r = 0;
+    while (r < views[v].passes) {
+      uint64_t fit = used < path_capacity ? (path_capacity - used) / npix : 0;
+      if (fit == 0) {
+        if (used) {
+          close();
+          continue;
+        }
+        fit = 1;   // one pass of a view always goes
+      }
+      const uint32_t take = (uint32_t)std::min<uint64_t>(fit, views[v].passes - r);
+      in[v] = 1;
+      p0[v] = r;
+      p1[v] = r + take;
+      used += npix * take;
+      r += take;
+      if (r < views[v].passes) close();   // the chunk is full
+    }
   }
+  if (used) close();
   return out;
 }
 
 namespace {
-
-// view_start of the chunk [p0, p1): each view's first path in it
-std::vector<uint32_t> chunk_starts(const std::vector<CameraRec>& views, uint32_t p0, uint32_t p1, uint32_t& n) {
-  std::vector<uint32_t> starts(views.size());
-  uint64_t acc = 0;
-  for (size_t v = 0; v < views.size(); ++v) {
-    starts[v] = (uint32_t)acc;
-    const uint32_t q1 = std::min(p1, views[v].passes);
-    if (q1 > p0) acc += (uint64_t)views[v].w * views[v].h * (q1 - p0);
-  }
-  n = (uint32_t)acc;
-  return starts;
-}
 
 // The launch shapes of the camera gather's kernels.
 struct GatherShape {
@@ -970,10 +987,9 @@ GatherShape gather_shape(const FrameArgs& a) {
 // The rounds of one chunk of n paths (its view_start already on the
 // device); returns the rounds run.
 template <bool kMulti>
-uint32_t gather_rounds(const FrameArgs& a, const GatherShape& g, uint32_t p0, uint32_t p1, uint32_t n,
-                       cudaStream_t s) {
+uint32_t gather_rounds(const FrameArgs& a, const GatherShape& g, uint32_t n, cudaStream_t s) {
   cudaMemsetAsync(a.counts, 0, 2 * (kMaxLayers + 2) * sizeof(uint32_t), s);
-  k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, p0, p1, n); note_launch();
+  k_cg_init<<<blocks_for(n), kBlock, 0, s>>>(a, n); note_launch();
   // every round consumes at least one layer of each live path, so
   // kMaxLayers rounds bound the walk (the layer cap ends longer ones)
   uint32_t round = 0, live = n;
@@ -1010,10 +1026,9 @@ void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>& views
   uint32_t rec_used = 0, ent_used = 0;   // stored slots so far
   bool room = plan && plan->store;
   for (size_t c = 0; c < chunks.size(); ++c) {
-    const uint32_t p0 = chunks[c].first, p1 = chunks[c].second;
-    uint32_t n = 0;
-    std::vector<uint32_t> starts = chunk_starts(views, p0, p1, n);
-    cudaMemcpyAsync(d_view_start, starts.data(), starts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    const uint32_t n = chunks[c].n;
+    cudaMemcpyAsync(d_view_start, chunks[c].table.data(), chunks[c].table.size() * sizeof(uint32_t),
+                    cudaMemcpyHostToDevice, s);
     if (plan) {
       // write the chunk after the stored ones while the store has room;
       // otherwise only count its slots
@@ -1021,16 +1036,14 @@ void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>& views
       a.vs.rec_start = room ? rec_used : 0u;
       a.vs.ent_start = room ? ent_used : 0u;
     }
-    const uint32_t rounds = gather_rounds<kMulti>(a, g, p0, p1, n, s);
+    const uint32_t rounds = gather_rounds<kMulti>(a, g, n, s);
     if (plan) {
       VertexChunk& vc = plan->chunks[c];
-      vc.p0 = p0;
-      vc.p1 = p1;
       vc.n = n;
       vc.rounds = rounds;
       vc.rec_start = a.vs.rec_start;
       vc.ent_start = a.vs.ent_start;
-      vc.starts = starts;
+      vc.table = chunks[c].table;
       uint32_t tail[3] = {0, 0, 0};
       cudaMemcpyAsync(plan->d_chunk_base + c * 2 * kVertexBases, a.vs.base, 2 * kVertexBases * sizeof(uint32_t),
                       cudaMemcpyDeviceToDevice, s);
@@ -1048,7 +1061,7 @@ void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>& views
         room = false;   // the store is full: the later chunks are replayed
       }
     }
-    k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a, p0, p1); note_launch();
+    k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a); note_launch();
   }
 }
 
@@ -1655,7 +1668,7 @@ void gather_backward(const FrameArgs& a0, const std::vector<CameraRec>& views, c
   for (size_t c = 0; c < plan.chunks.size(); ++c) {
     const VertexChunk& vc = plan.chunks[c];
     FrameArgs a = a0;
-    cudaMemcpyAsync(const_cast<uint32_t*>(a.view_start), vc.starts.data(), vc.starts.size() * sizeof(uint32_t),
+    cudaMemcpyAsync(const_cast<uint32_t*>(a.view_start), vc.table.data(), vc.table.size() * sizeof(uint32_t),
                     cudaMemcpyHostToDevice, s);
     const uint32_t* bases = plan.d_chunk_base + c * 2 * kVertexBases;
     uint32_t rounds = vc.rounds;
@@ -1666,7 +1679,7 @@ void gather_backward(const FrameArgs& a0, const std::vector<CameraRec>& views, c
       a.vs.write = 1;
       a.vs.rec_start = 0;
       a.vs.ent_start = 0;
-      rounds = multi ? gather_rounds<true>(a, g, vc.p0, vc.p1, vc.n, s) : gather_rounds<false>(a, g, vc.p0, vc.p1, vc.n, s);
+      rounds = multi ? gather_rounds<true>(a, g, vc.n, s) : gather_rounds<false>(a, g, vc.n, s);
       bases = a.vs.base;
     }
     // timed as the adjoint's transport (this estimator has none)
