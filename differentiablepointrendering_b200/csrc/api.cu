@@ -854,13 +854,14 @@ void trace_photon_map(pale_handle* h) {
 SceneTable scene_table(const std::vector<pale_handle*>& scenes) {
   SceneTable T{};
   T.n = (uint32_t)scenes.size();
-  uint32_t staged = kTopNodes / T.n;
+  // each scene's slot: its top nodes up to kTopNodes, within 1024 nodes
+  // (32 KB of shared memory) for the whole table
+  const uint32_t slot = std::min<uint32_t>(kTopNodes, std::max<uint32_t>(32u, kStagedNodesPerCall / T.n));
   for (uint32_t k = 0; k < T.n; ++k) {
     T.s[k] = scenes[k]->view();
-    staged = std::min(staged, T.s[k].top_nodes);
+    T.s[k].top_nodes = std::min(T.s[k].top_nodes, slot);
   }
-  for (uint32_t k = 0; k < T.n; ++k) T.s[k].top_nodes = staged;
-  T.staged = staged;
+  T.staged = slot;
   return T;
 }
 

@@ -168,11 +168,12 @@ struct EventBufs {
 // The scenes of one render call.  A call renders views (a camera of a scene
 // and its number of passes); the views of every scene trace as one
 // wavefront, each path finding its scene's surfels, LBVH, meshes and photon
-// grid through the view's scene index.  The first `staged` LBVH nodes of
-// every scene are staged in shared memory by the traversal kernels, scene
-// k's at [k * staged, (k + 1) * staged), and each table entry's top_nodes
-// is that count.
+// grid through the view's scene index.  The traversal kernels stage each
+// scene's first top_nodes LBVH nodes in shared memory, scene k's in the
+// slot [k * staged, (k + 1) * staged) (top_nodes <= staged; a small scene
+// stages fewer), at most kStagedNodesPerCall nodes for the whole table.
 constexpr uint32_t kMaxScenes = 8;
+constexpr uint32_t kStagedNodesPerCall = 1024;
 
 struct SceneTable {
   SceneView s[kMaxScenes];

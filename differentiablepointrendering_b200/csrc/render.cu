@@ -27,12 +27,12 @@ __device__ __forceinline__ void stage_top_nodes(const SceneView& S, TravNode* sm
 }
 
 // The staged top nodes of every scene of a call: scene k's first
-// T.staged nodes at smem[k * T.staged].
+// T.s[k].top_nodes nodes at smem[k * T.staged].
 __device__ __forceinline__ void stage_top_nodes(const SceneTable& T, TravNode* smem) {
   const uint32_t total = T.n * T.staged;
   for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
-    const uint32_t k = i / T.staged;
-    smem[i] = T.s[k].nodes[i - k * T.staged];
+    const uint32_t k = i / T.staged, j = i - k * T.staged;
+    if (j < T.s[k].top_nodes) smem[i] = T.s[k].nodes[j];
   }
   __syncthreads();
 }
