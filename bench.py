@@ -780,6 +780,31 @@ def serve_stream(srv, reqs):
     return served, span, np.array(plain), clock, np.array(service)
 
 
+def plain_light_first(reqs, service_ms, starve_s: float = 2.0):
+    """The plain path with the server's light-first order: one request at a
+    time, the next one the lightest that has arrived (those waiting longer
+    than starve_s first), on a virtual clock of the measured service times;
+    returns the latencies (ms) and the end time (s)."""
+    import numpy as np
+
+    arr = np.array([at for at, _ in reqs])
+    svc = np.asarray(service_ms) / 1e3
+    left = set(range(len(reqs)))
+    lat = np.zeros(len(reqs))
+    clock = 0.0
+    while left:
+        ready = [i for i in left if arr[i] <= clock]
+        if not ready:
+            clock = min(arr[i] for i in left)
+            continue
+        old = [i for i in ready if clock - arr[i] > starve_s]
+        i = min(old, key=lambda j: arr[j]) if old else min(ready, key=lambda j: (svc[j], arr[j]))
+        clock += svc[i]
+        lat[i] = (clock - arr[i]) * 1e3
+        left.remove(i)
+    return lat, clock
+
+
 def _pcts(a):
     import numpy as np
 
@@ -806,7 +831,7 @@ def run_serving(args):
     free, _ = torch.cuda.mem_get_info()
     budget = min(150 * 10 ** 9, int(free * 0.9))
     srv = Server(hbm_budget=budget, max_views=64, max_pixels=1 << 24, max_paths=args.round_paths,
-                 settings={"estimator": args.estimator})
+                 settings={"estimator": args.estimator}, policy=args.policy)
     try:
         names = []
         t_admit = time.perf_counter()
@@ -827,13 +852,15 @@ def run_serving(args):
                 t += rng.exponential(1.0 / rate)
                 reqs.append((t, serving_request(rng, names)))
             served, span, plain, clock, service = serve_stream(srv, reqs)
+            lf, lf_clock = plain_light_first(reqs, service)
             views = [q.batch_views for _, q in reqs]
             runs.append({"rate_per_s": rate, "requests": count,
                          "served": dict(_pcts(served), requests_per_s=round(count / span, 2),
                                         mean_views_per_round=round(float(np.mean(views)), 2),
                                         max_views_per_round=int(max(views))),
                          "plain": dict(_pcts(plain), requests_per_s=round(count / clock, 2),
-                                       service=_pcts(service))})
+                                       service=_pcts(service)),
+                         "plain_light_first": dict(_pcts(lf), requests_per_s=round(count / lf_clock, 2))})
         g512 = []
         for spp in (1, 4, 16):
             t, reqs = 0.0, []
@@ -850,6 +877,7 @@ def run_serving(args):
                       "scenes": [{"name": m, "surfels": n} for m, n in zip(names, SERVING_SURFELS)],
                       "scene_settings": SERVING_SETTINGS, "resolutions": SERVING_RES, "passes": SERVING_SPP,
                       "depths": [4, 8], "round_paths": args.round_paths, "estimator": args.estimator,
+                      "policy": args.policy,
                       "mix": "70% forward (LDR image of one view), 30% gradient (L2 loss + adjoint of one view)",
                       "budget_bytes": budget, "admitted_bytes": admitted, "admit_s": round(t_admit, 2),
                       "runs": runs, "gradient_512": g512}), flush=True)
@@ -877,8 +905,10 @@ def main():
     ap.add_argument("--rates", type=float, nargs="*", default=[50.0, 200.0, 500.0, 2000.0])
     ap.add_argument("--seconds", type=float, default=4.0, help="serving: stream length per rate")
     ap.add_argument("--requests", type=int, default=200, help="serving: at most this many requests per rate")
-    ap.add_argument("--round-paths", dest="round_paths", type=int, default=1 << 26,
+    ap.add_argument("--round-paths", dest="round_paths", type=int, default=1 << 24,
                     help="serving: camera paths (pixels x passes) per round")
+    ap.add_argument("--policy", default="light_first", choices=("arrival", "light_first"),
+                    help="serving: the order in which a round takes queued requests")
     ap.add_argument("--rate-512", dest="rate_512", type=float, default=20.0)
     ap.add_argument("--requests-512", dest="requests_512", type=int, default=40)
     args = ap.parse_args()

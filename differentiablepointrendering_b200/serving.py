@@ -22,9 +22,11 @@ vertices into arrays of its own (``pale_render_views_gradients_device``),
 with no second wavefront.
 
 One dispatcher thread owns the GPU stream and serves requests in rounds.
-A round takes every queued request that fits (at most ``max_views`` views,
-``max_pixels`` camera pixels and, when set, ``max_paths`` camera paths of
-pixels x passes, which bounds a round's time; in arrival order) and renders them
+A round takes the queued requests that fit (at most ``max_views`` views,
+``max_pixels`` camera pixels, seven scenes and, when set, ``max_paths``
+camera paths of pixels x passes, which bounds a round's time), in arrival
+order or, with ``policy="light_first"``, the lightest first with requests
+waiting longer than ``starve_s`` ahead of them, and renders them
 together: the views of all the round's requests, of any scenes, are ONE
 camera-gather wavefront (device.ViewBatch's entry point,
 ``pale_render_views_loss_device``), and the round's gradient requests share
@@ -106,28 +108,55 @@ class _Scene:
 MAX_ROUND_SCENES = 7   # a call's scene table holds 8 entries, the first the server's executor
 
 
+def request_paths(q: Request, sizes: Dict[str, List[Tuple[int, int]]],
+                  max_passes: Optional[Dict[str, int]] = None) -> int:
+    """Camera paths of request q: its view's pixels x passes (passes 0: its
+    scene's max_passes)."""
+    w, h = sizes[q.scene][q.camera]
+    return w * h * (q.passes or (max_passes or {}).get(q.scene, 1))
+
+
 def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], max_views: int,
                max_pixels: int, max_paths: Optional[int] = None,
                max_passes: Optional[Dict[str, int]] = None,
-               max_scenes: int = MAX_ROUND_SCENES) -> Tuple[List[Request], List[Request]]:
-    """The requests of the next round: the queue's head in arrival order
-    while the round holds at most max_views views, max_pixels camera
-    pixels, max_scenes distinct scenes and (when given) max_paths camera
-    paths, pixels x passes, a request's passes 0 counting as its scene's
-    max_passes (the first request always goes); returns (taken, left)."""
+               max_scenes: int = MAX_ROUND_SCENES, policy: str = "arrival",
+               now: float = 0.0, starve_s: float = 2.0) -> Tuple[List[Request], List[Request]]:
+    """The requests of the next round, at most max_views views, max_pixels
+    camera pixels, max_scenes distinct scenes and (when given) max_paths
+    camera paths (request_paths); returns (taken, left), left in arrival
+    order.  policy "arrival": the queue's head in arrival order, up to the
+    first request that does not fit.  policy "light_first": requests that
+    have waited longer than starve_s first (in arrival order), then the
+    others by their work (paths, a gradient request's counted twice),
+    skipping those that do not fit, so that light requests are not held
+    behind heavy ones and a heavy one waits at most about starve_s plus a
+    round.  The first request considered always goes."""
+    def work(q):
+        return request_paths(q, sizes, max_passes) * (2 if q.kind == "gradient" else 1)
+
+    if policy == "arrival":
+        order = list(queue)
+    elif policy == "light_first":
+        old = [q for q in queue if now - q.t_submit > starve_s]
+        order = old + sorted((q for q in queue if not now - q.t_submit > starve_s), key=work)
+    else:
+        raise ValueError("policy must be 'arrival' or 'light_first'")
     taken, pix, paths, scenes = [], 0, 0, set()
-    for i, q in enumerate(queue):
+    for q in order:
         w, h = sizes[q.scene][q.camera]
-        n = w * h * (q.passes or (max_passes or {}).get(q.scene, 1))
+        n = request_paths(q, sizes, max_passes)
         if taken and (len(taken) + 1 > max_views or pix + w * h > max_pixels
                       or (max_paths is not None and paths + n > max_paths)
                       or (q.scene not in scenes and len(scenes) >= max_scenes)):
-            return taken, queue[i:]
+            if policy == "arrival":
+                break
+            continue
         taken.append(q)
         pix += w * h
         paths += n
         scenes.add(q.scene)
-    return taken, []
+    chosen = set(map(id, taken))
+    return taken, [q for q in queue if id(q) not in chosen]
 
 
 class Server:
@@ -138,13 +167,16 @@ class Server:
 
     def __init__(self, hbm_budget: int, max_views: int = 64, max_pixels: int = 1 << 24,
                  settings: Optional[dict] = None, device: Optional[int] = None,
-                 max_paths: Optional[int] = None):
+                 max_paths: Optional[int] = None, policy: str = "arrival", starve_s: float = 2.0):
         import torch
 
         self.budget = int(hbm_budget)
         self.max_views = int(max_views)
         self.max_pixels = int(max_pixels)
         self.max_paths = None if max_paths is None else int(max_paths)
+        if policy not in ("arrival", "light_first"):
+            raise ValueError("policy must be 'arrival' or 'light_first'")
+        self.policy, self.starve_s = policy, float(starve_s)
         self.device = torch.device(f"cuda:{device if device is not None else torch.cuda.current_device()}")
         self.scenes: Dict[str, _Scene] = {}
         self.done: List[Request] = []
@@ -166,6 +198,10 @@ class Server:
         self._exec_settings = st
         self._gather = st.get("estimator", "reference") in ("gather", 1)
         self._exec = Renderer.from_scene(make_box_scene(8, cameras=1, resolution=8), st)
+        # with the gather estimator, a second executor renders the forward-only
+        # requests without keeping path vertices
+        self._exec_plain = Renderer.from_scene(make_box_scene(8, cameras=1, resolution=8),
+                                               dict(st, estimator="reference")) if self._gather else None
         self._thread = threading.Thread(target=self._run, name="pale-serve", daemon=True)
         self._thread.start()
 
@@ -270,7 +306,8 @@ class Server:
                 sizes = {n: s.renderer._sizes for n, s in self.scenes.items()}
                 spp = {n: s.max_passes for n, s in self.scenes.items()}
                 taken, self._queue = plan_round(self._queue, sizes, self.max_views, self.max_pixels,
-                                                self.max_paths, spp)
+                                                self.max_paths, spp, policy=self.policy,
+                                                now=time.perf_counter(), starve_s=self.starve_s)
             try:
                 with self._gpu:
                     self._round(taken)
@@ -293,54 +330,66 @@ class Server:
         self.rounds.append(len(reqs))
         names = sorted({q.scene for q in reqs})
         entry = {n: k + 1 for k, n in enumerate(names)}     # entry 0: the executor
-        scenes = [self.scenes[n] for n in names]
-        renderers = [self._exec] + [s.renderer for s in scenes]
+        scene_renderers = [self.scenes[n].renderer for n in names]
 
         def passes(q):
             return q.passes or self.scenes[q.scene].max_passes
 
-        views = [(entry[q.scene], q.camera, passes(q), q.depth) for q in reqs]
-        vb = ViewBatch(renderers, views, device=self.device)
-        vb.forward_loss(None, trace_photons=False)      # the resident photon maps
-        offs = np.cumsum([0] + [w * h for w, h in vb.sizes])
-        # the L2 loss and dL/dI of the gradient requests (compute_l2_loss /
-        # compute_l2_grad, python/losses.py:10-45, on the LDR image)
-        grad_idx = [i for i, q in enumerate(reqs) if q.kind == "gradient"]
-        dldi, loss = {}, {}
-        for i in grad_idx:
-            t = torch.from_numpy(np.ascontiguousarray(reqs[i].target, np.float32).reshape(-1, 3)).to(self.device)
-            ldr_i = vb.ldr[offs[i]:offs[i + 1], :3]
-            d = torch.zeros(int(offs[i + 1] - offs[i]), 4, dtype=torch.float32, device=self.device)
-            torch.sub(ldr_i, t, out=d[:, :3])
-            loss[i] = 0.5 * (d[:, :3].double() ** 2).mean()
-            d[:, :3].div_(float(3 * (offs[i + 1] - offs[i])))
-            dldi[i] = d
-        ldr = self._host(vb.ldr)
-        for i, q in enumerate(reqs):
-            w, h = vb.sizes[i]
-            q.image = ldr[offs[i]:offs[i + 1]].reshape(h, w, 4).copy()
-            q.batch_views = len(reqs)
-            q.round = n_round
-            if q.kind == "gradient":
-                q.loss = float(loss[i].item())
-            else:
-                q.t_done = time.perf_counter()
-                q.done.set()
-        if grad_idx and self._gather:
-            # the gather estimator: one sweep over the round's own forward
-            # vertices, each gradient request's view into arrays of its own
-            dl = torch.zeros(max(1, int(offs[-1])), 4, dtype=torch.float32, device=self.device)
-            for i in grad_idx:
-                dl[offs[i]:offs[i + 1]] = dldi[i]
-            gl = vb.view_gradients(grad_idx, dl)
-            host = [{k: self._host(v) for k, v in g.items()} for g in gl]
-            now = time.perf_counter()
-            for k, i in enumerate(grad_idx):
+        def forward(idx, executor):
+            """One forward wavefront over requests idx: images to the host,
+            the L2 loss and dL/dI of its gradient requests (compute_l2_loss
+            / compute_l2_grad, python/losses.py:10-45, on the LDR image)."""
+            vb = ViewBatch([executor] + scene_renderers,
+                           [(entry[reqs[i].scene], reqs[i].camera, passes(reqs[i]), reqs[i].depth) for i in idx],
+                           device=self.device)
+            vb.forward_loss(None, trace_photons=False)      # the resident photon maps
+            offs = np.cumsum([0] + [w * h for w, h in vb.sizes])
+            dldi = {}
+            for k, i in enumerate(idx):
                 q = reqs[i]
-                q.grads = host[k]
-                q.t_done = now
-                q.done.set()
+                if q.kind != "gradient":
+                    continue
+                t = torch.from_numpy(np.ascontiguousarray(q.target, np.float32).reshape(-1, 3)).to(self.device)
+                d = torch.zeros(int(offs[k + 1] - offs[k]), 4, dtype=torch.float32, device=self.device)
+                torch.sub(vb.ldr[offs[k]:offs[k + 1], :3], t, out=d[:, :3])
+                q.loss = float((0.5 * (d[:, :3].double() ** 2).mean()).item())
+                d[:, :3].div_(float(3 * (offs[k + 1] - offs[k])))
+                dldi[i] = d
+            ldr = self._host(vb.ldr)
+            for k, i in enumerate(idx):
+                q = reqs[i]
+                w, h = vb.sizes[k]
+                q.image = ldr[offs[k]:offs[k + 1]].reshape(h, w, 4).copy()
+                q.batch_views = len(reqs)
+                q.round = n_round
+                if q.kind != "gradient":
+                    q.t_done = time.perf_counter()
+                    q.done.set()
+            return vb, offs, dldi
+
+        def finish(idx, host):
+            now = time.perf_counter()
+            for k, i in enumerate(idx):
+                reqs[i].grads = host[k]
+                reqs[i].t_done = now
+                reqs[i].done.set()
+
+        grad_idx = [i for i, q in enumerate(reqs) if q.kind == "gradient"]
+        plain_idx = [i for i, q in enumerate(reqs) if q.kind != "gradient"]
+        if self._gather:
+            # forward-only requests on the reference executor (no path
+            # vertices kept); the gradient requests' own forward on the
+            # gather executor, then one sweep over its vertices, each view
+            # into arrays of its own
+            if plain_idx:
+                forward(plain_idx, self._exec_plain)
+            if grad_idx:
+                vb, offs, dldi = forward(grad_idx, self._exec)
+                dl = torch.cat([dldi[i] for i in grad_idx]).contiguous()
+                gl = vb.view_gradients(list(range(len(grad_idx))), dl)
+                finish(grad_idx, [{k: self._host(v) for k, v in g.items()} for g in gl])
             return
+        vb, offs, dldi = forward(list(range(len(reqs))), self._exec)
         per = self.GRADIENTS_PER_WAVEFRONT - 1     # entry 0 is the executor
         for c0 in range(0, len(grad_idx), per):
             chunk = grad_idx[c0:c0 + per]
@@ -350,13 +399,7 @@ class Server:
             gb = ViewBatch(rs, gviews, device=self.device)
             dl = torch.cat([dldi[i] for i in chunk]).contiguous()
             grads = gb.backward(dl)
-            host = [{k: self._host(v) for k, v in grads[k + 1].items()} for k in range(len(chunk))]
-            now = time.perf_counter()
-            for k, i in enumerate(chunk):
-                q = reqs[i]
-                q.grads = host[k]
-                q.t_done = now
-                q.done.set()
+            finish(chunk, [{k: self._host(v) for k, v in grads[e + 1].items()} for e in range(len(chunk))])
 
     # ----------------------------------------------------------- reports
     def latency(self, kind: Optional[str] = None) -> Dict[str, float]:
@@ -394,3 +437,5 @@ class Server:
         for name in list(self.scenes):
             self.remove_scene(name)
         self._exec.close()
+        if self._exec_plain is not None:
+            self._exec_plain.close()

@@ -82,3 +82,22 @@ def test_round_holds_at_most_seven_scenes():
     assert [r.scene for r in taken] == [f"s{k}" for k in range(7)] and left == q[7:]
     taken, left = S.plan_round(q, sizes, 64, 10 ** 6, max_scenes=2)
     assert taken == q[:2]
+
+
+def test_light_first_takes_light_requests_past_a_heavy_one():
+    sizes = {"a": [(4, 4), (64, 64)]}
+    heavy = S.Request("a", 1, passes=8)                  # 32768 paths
+    light = [S.Request("a", 0, passes=1) for _ in range(3)]
+    grad = S.Request("a", 0, kind="gradient", passes=1)  # 16 paths, counted twice
+    for k, q in enumerate([heavy] + light + [grad]):
+        q.t_submit = 10.0 + k * 0.01
+    q = [heavy] + light + [grad]
+    taken, left = S.plan_round(q, sizes, 64, 10 ** 6, max_paths=1000, policy="light_first", now=10.5)
+    assert taken == light + [grad] and left == [heavy]
+    # the arrival order stops at the heavy head
+    taken, left = S.plan_round(q, sizes, 64, 10 ** 6, max_paths=1000, now=10.5)
+    assert taken == [heavy] and left == light + [grad]
+    # a request that waited past starve_s goes first
+    taken, left = S.plan_round(q, sizes, 64, 10 ** 6, max_paths=1000, policy="light_first", now=13.0,
+                               starve_s=2.0)
+    assert taken == [heavy] and left == light + [grad]
