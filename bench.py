@@ -177,12 +177,16 @@ def read_peaks():
         return None
 
 
-def read_traffic(kernel: str):
+def read_traffic(kernel: str, launch_ms: float):
+    """DRAM bytes of one launch of `kernel`: the DRAM rate of its ncu
+    capture on the small case (profiles/traffic.json) times the launch's
+    live device time; None without a capture."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
-        return json.load(open(p)).get(kernel)
+        rate = json.load(open(p))[kernel]["dram_bytes_per_s"]
     except Exception:
         return None
+    return int(rate * launch_ms / 1e3)
 
 
 def cpu_reference_run(w: dict, steps: int = 1, warmup: int = 0):
@@ -605,10 +609,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         ach = kb[k] / (ms / 1e3) / 1e9 if ms > 0 else 0.0
         kernels[k] = {"ms_per_step": round(ms, 3), "launches": n, "launch_ms": round(ms / n, 4),
                       "algorithmic_bytes_per_launch": int(kb[k] / n), "achieved_gbs": round(ach, 1),
-                      "frac": round(ach / hbm, 4)}
+                      "frac": round(ach / hbm, 4), "dram_bytes_per_launch": read_traffic(k, ms / n)}
     top = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
     achieved = kernels[top]["achieved_gbs"]
-    traffic = read_traffic(top)
+    traffic = read_traffic(top, kernels[top]["launch_ms"])
     if args.skip_cpu:
         cpu_val, cpu_desc, cpu_kind = None, "skipped", None
     else:
