@@ -285,6 +285,10 @@ static void launch_walk(KernelT kernel, int threads, const Args& a, uint32_t arg
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // the staged nodes of a call of several scenes and the shared stack reach
+  // 48 KB, and the kernel's own static shared memory comes on top: allow
+  // the dynamic part past the default limit
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   const uint64_t grid = std::min<uint64_t>((uint64_t)limit * (kBlock / threads),
                                            (uint64_t)std::max(1, sms * std::max(1, per_sm)));

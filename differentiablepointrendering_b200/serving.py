@@ -130,7 +130,9 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
     others by their work (paths, a gradient request's counted twice),
     skipping those that do not fit, so that light requests are not held
     behind heavy ones and a heavy one waits at most about starve_s plus a
-    round.  The first request considered always goes."""
+    round; the round's paths are then also capped at 8 times its first
+    request's (2^20 at least), so that requests of very different sizes
+    do not share a round.  The first request considered always goes."""
     def work(q):
         return request_paths(q, sizes, max_passes) * (2 if q.kind == "gradient" else 1)
 
@@ -142,15 +144,22 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
     else:
         raise ValueError("policy must be 'arrival' or 'light_first'")
     taken, pix, paths, scenes = [], 0, 0, set()
+    cap = max_paths
     for q in order:
         w, h = sizes[q.scene][q.camera]
         n = request_paths(q, sizes, max_passes)
         if taken and (len(taken) + 1 > max_views or pix + w * h > max_pixels
-                      or (max_paths is not None and paths + n > max_paths)
+                      or (cap is not None and paths + n > cap)
                       or (q.scene not in scenes and len(scenes) >= max_scenes)):
             if policy == "arrival":
                 break
             continue
+        if not taken and policy == "light_first":
+            # a round of light requests stays light: at most 8 times the
+            # work of its first request (2^20 paths at least), so that a
+            # light request does not wait for a heavy one in its own round
+            light = max(1 << 20, 8 * n)
+            cap = light if cap is None else min(cap, light)
         taken.append(q)
         pix += w * h
         paths += n

@@ -101,3 +101,16 @@ def test_light_first_takes_light_requests_past_a_heavy_one():
     taken, left = S.plan_round(q, sizes, 64, 10 ** 6, max_paths=1000, policy="light_first", now=13.0,
                                starve_s=2.0)
     assert taken == [heavy] and left == light + [grad]
+
+
+def test_light_first_round_stays_light():
+    sizes = {"a": [(4, 4), (1024, 1024)]}
+    light = S.Request("a", 0, passes=1)                   # 16 paths
+    medium = S.Request("a", 1, passes=2)                  # 2M paths
+    for k, q in enumerate([light, medium]):
+        q.t_submit = 1.0 + 0.01 * k
+    taken, left = S.plan_round([light, medium], sizes, 64, 1 << 24, max_paths=1 << 24,
+                               policy="light_first", now=1.1)
+    assert taken == [light] and left == [medium]         # 2M > max(2^20, 8 x 16)
+    taken, left = S.plan_round([medium], sizes, 64, 1 << 24, max_paths=1 << 24, policy="light_first", now=1.1)
+    assert taken == [medium]
