@@ -655,7 +655,7 @@ C3B_MODES = (   # label, settings
     ("reference adjoint", {"estimator": "reference"}),
     ("gather, checkpoint", {"estimator": "gather", "vertices": "checkpoint"}),
     ("gather, replay", {"estimator": "gather", "vertices": "replay"}),
-    ("gather, auto 32 GB", {"estimator": "gather", "vertices": "auto", "vertex_store_bytes": 32 * 10 ** 9}),
+    ("gather, auto 96 GB", {"estimator": "gather", "vertices": "auto", "vertex_store_bytes": 96 * 10 ** 9}),
 )
 
 
@@ -664,7 +664,8 @@ def run_c3b(args):
     800x800, depth 8) at --c3b-passes passes, one forward + backward per
     iteration with all seven gradient groups, for the reference's adjoint
     and for the gather estimator with its path vertices checkpointed,
-    replayed, or checkpointed within a 32 GB budget (the rest replayed).
+    replayed, or checkpointed within a 96 GB budget (the chunks past it
+    replayed).
     Per mode: iterations/s over --steps timed iterations after --warmup
     (the first iteration sizes the vertex store) and the device memory the
     renderer and its frame hold afterwards.  One JSON line."""
