@@ -655,7 +655,7 @@ C3B_MODES = (   # label, settings
     ("reference adjoint", {"estimator": "reference"}),
     ("gather, checkpoint", {"estimator": "gather", "vertices": "checkpoint"}),
     ("gather, replay", {"estimator": "gather", "vertices": "replay"}),
-    ("gather, auto 96 GB", {"estimator": "gather", "vertices": "auto", "vertex_store_bytes": 96 * 10 ** 9}),
+    ("gather, auto 48 GB", {"estimator": "gather", "vertices": "auto", "vertex_store_bytes": 48 * 10 ** 9}),
 )
 
 
@@ -664,8 +664,8 @@ def run_c3b(args):
     800x800, depth 8) at --c3b-passes passes, one forward + backward per
     iteration with all seven gradient groups, for the reference's adjoint
     and for the gather estimator with its path vertices checkpointed,
-    replayed, or checkpointed within a 96 GB budget (the chunks past it
-    replayed).
+    replayed, or checkpointed within a 48 GB budget (the chunks that do
+    not fit replayed).
     Per mode: iterations/s over --steps timed iterations after --warmup
     (the first iteration sizes the vertex store) and the device memory the
     renderer and its frame hold afterwards.  One JSON line."""
@@ -846,9 +846,14 @@ def run_serving(args):
                                                points=make_surfels(n, 1234 + k)), SERVING_SETTINGS)
             names.append(name)
         t_admit = time.perf_counter() - t_admit
-        # warm-up: every scene once, both kinds, so the wavefront buffers exist
-        warm = [(0.0, serving_request(rng, names, kind, 1024, 1)) for kind in ("forward", "gradient")]
-        serve_stream(srv, warm)
+        # warm-up: the largest request of each kind twice, so that the
+        # executors' wavefront buffers (and the gather estimator's vertex
+        # store, sized from the round before) reach their full size before
+        # the streams (a buffer that grows inside a stream costs a
+        # reallocation in some request's latency)
+        for _ in range(2):
+            warm = [(0.0, serving_request(rng, names, kind, 1024, SERVING_SPP[-1])) for kind in ("forward", "gradient")]
+            serve_stream(srv, warm)
         runs = []
         for rate in args.rates:
             count = max(8, min(args.requests, int(rate * args.seconds)))

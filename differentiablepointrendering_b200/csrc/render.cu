@@ -1061,9 +1061,9 @@ void camera_gather_impl(const FrameArgs& a0, const std::vector<CameraRec>& views
       if (vc.stored) {
         rec_used = tail[0];
         ent_used = tail[1];
-      } else {
-        room = false;   // the store is full: the later chunks are replayed
       }
+      // a chunk that did not fit leaves the store where it was: a later,
+      // smaller chunk may still fit (its slots overwrite the dropped ones)
     }
     k_cg_finalize<<<blocks_for(a.total_pixels), kBlock, 0, s>>>(a); note_launch();
   }
