@@ -1101,6 +1101,11 @@ void gather_adjoint(const std::vector<pale_handle*>& scenes, const std::vector<C
     ents = std::max<uint64_t>(ents, 1);
     h->sc_rec_xa.ensure(recs); h->sc_rec_ew.ensure(recs);
     h->sc_ent_d.ensure(ents); h->sc_ent_b.ensure(ents); h->sc_ent_l.ensure(ents);
+  } else if (h->sc_rec_xa.p) {
+    // every chunk is in the store: the scratch of an earlier replay goes
+    CK(cudaStreamSynchronize(s));
+    h->sc_rec_xa.free(); h->sc_rec_ew.free();
+    h->sc_ent_d.free(); h->sc_ent_b.free(); h->sc_ent_l.free();
   }
   h->vs_base.ensure(2 * kVertexBases);
   h->vs_overflow.ensure(1);
