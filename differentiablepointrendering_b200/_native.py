@@ -36,7 +36,8 @@ class PaleSettings(C.Structure):
 
 
 class PaleView(C.Structure):
-    _fields_ = [("scene", C.c_uint32), ("camera", C.c_uint32), ("passes", C.c_uint32), ("depth", C.c_uint32)]
+    _fields_ = [("scene", C.c_uint32), ("camera", C.c_uint32), ("passes", C.c_uint32), ("depth", C.c_uint32),
+                ("first_pass", C.c_uint32), ("pass_count", C.c_uint32)]
 
 
 class PalePoints(C.Structure):
@@ -295,7 +296,7 @@ def load_library() -> C.CDLL:
         "pale_trace_photon_map": (C.c_int, [C.c_void_p, C.c_void_p]),
         "pale_render_views_loss_device": (C.c_int, [C.c_uint32, C.POINTER(C.c_void_p), C.c_int, C.c_uint32,
                                                     C.POINTER(PaleView), C.c_void_p, C.c_uint32, C.c_void_p,
-                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "pale_render_views_backward_device": (C.c_int, [C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
                                                         C.POINTER(PaleView), C.c_void_p, C.POINTER(PalePoints),
                                                         C.c_void_p]),

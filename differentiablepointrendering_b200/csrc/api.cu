@@ -750,6 +750,7 @@ struct ViewReq {
   uint32_t cam;      // camera index in that scene
   uint32_t passes;
   uint32_t depth;
+  uint32_t first = 0, count = 0;   // forward slices: passes [first, first + count) (0, 0: all)
 };
 
 // The views of a one-scene call: the selected cameras with the scene's
@@ -757,7 +758,7 @@ struct ViewReq {
 std::vector<ViewReq> all_passes(pale_handle* h, uint32_t nsel, const uint32_t* idx, bool adjoint) {
   std::vector<ViewReq> v(nsel);
   const uint32_t passes = adjoint ? h->st.adjoint_passes : h->st.gather_passes;
-  for (uint32_t i = 0; i < nsel; ++i) v[i] = ViewReq{0u, idx[i], passes, h->st.adjoint_bounces};
+  for (uint32_t i = 0; i < nsel; ++i) v[i] = ViewReq{0u, idx[i], passes, h->st.adjoint_bounces, 0u, 0u};
   return v;
 }
 
@@ -781,6 +782,11 @@ void check_views(const std::vector<pale_handle*>& scenes, const std::vector<View
       throw ArgError(adjoint ? "view passes must be 1 .. the scene's adjoint_passes"
                              : "view passes must be 1 .. the scene's gather_passes");
     if (v.depth > h->st.adjoint_bounces) throw ArgError("view depth above the scene's adjoint bounces");
+    if (v.first || v.count) {
+      if (adjoint) throw ArgError("an adjoint call renders every pass of its views");
+      if (v.count == 0 || v.first >= v.passes || v.count > v.passes - v.first)
+        throw ArgError("view pass range outside its passes");
+    }
   }
 }
 
@@ -880,6 +886,8 @@ std::vector<CameraRec> view_records(const std::vector<pale_handle*>& scenes, con
     sel[i].passes = v.passes;
     sel[i].scene = v.scene;
     sel[i].depth = v.depth ? v.depth : scenes[v.scene]->st.adjoint_bounces;
+    sel[i].pass_begin = v.count ? v.first : 0u;
+    sel[i].pass_end = v.count ? v.first + v.count : v.passes;
     total += sel[i].w * sel[i].h;
     max_pix = std::max(max_pix, sel[i].w * sel[i].h);
   }
@@ -971,7 +979,7 @@ uint64_t vertex_bytes(const pale_handle* h) {
 // camera gather runs on the current photon maps (the last forward's or
 // loaded photons) with the camera seeds the last forward used.
 uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector<ViewReq>& views, float* d_raw,
-                      float* d_ldr, bool sync, bool trace_photons, const LossReq* lq) {
+                      float* d_ldr, bool sync, bool trace_photons, const LossReq* lq, float* d_partial = nullptr) {
   pale_handle* h = scenes[0];
   cudaStream_t s = h->stream;
   h->timer.used = 0;
@@ -1004,13 +1012,17 @@ uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector
   FrameArgs F = frame_args(scenes, nsel, total);
   F.raw = d_raw;
   F.ldr = d_ldr;
+  bool sliced = false;
+  for (const ViewReq& v : views) sliced = sliced || v.count != 0;
+  if (sliced && !d_partial) throw ArgError("views rendered in slices need the running sums (d_partial)");
+  if (d_partial) F.fb = reinterpret_cast<float4*>(d_partial);   // the caller's running sums
   if (lq) {
     F.target = lq->target;
     F.target_channels = lq->channels;
     F.dldi = lq->dldi;
   }
   VertexPlan* plan = nullptr;
-  if (h->st.estimator == PALE_ESTIMATOR_GATHER) {
+  if (h->st.estimator == PALE_ESTIMATOR_GATHER && !sliced) {
     // keep the path vertices: in the store while the chunks fit, else only
     // their counts (the backward replays those chunks)
     plan = &h->vplan;
@@ -1025,6 +1037,7 @@ uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector
                        h->vs_overflow.p, (uint32_t)h->vs_rec_xa.n, (uint32_t)h->vs_ent_d.n, 0u, 0u, 0};
     h->vviews.clear();   // valid again once the gather has run
   }
+  if (h->st.estimator == PALE_ESTIMATOR_GATHER && sliced) h->vviews.clear();   // nothing to differentiate
   camera_gather(F, sel, h->d_view_start.p, s, plan);
   if (plan) {
     h->vviews = sel;
@@ -1612,7 +1625,9 @@ std::vector<pale_handle*> scene_list(uint32_t n, pale_handle* const* scenes) {
 std::vector<ViewReq> view_list(uint32_t n, const pale_view* views) {
   if (n && !views) throw ArgError("view list is null");
   std::vector<ViewReq> v(n);
-  for (uint32_t i = 0; i < n; ++i) v[i] = ViewReq{views[i].scene, views[i].camera, views[i].passes, views[i].depth};
+  for (uint32_t i = 0; i < n; ++i)
+    v[i] = ViewReq{views[i].scene, views[i].camera, views[i].passes, views[i].depth, views[i].first_pass,
+                   views[i].pass_count};
   return v;
 }
 
@@ -1621,7 +1636,7 @@ std::vector<ViewReq> view_list(uint32_t n, const pale_view* views) {
 int pale_render_views_loss_device(uint32_t num_scenes, pale_handle* const* scenes, int trace_photons,
                                   uint32_t num_views, const pale_view* views, const float* d_target,
                                   uint32_t channels, float* d_ldr, float* d_raw, float* d_dldi, double* d_loss,
-                                  void* stream) {
+                                  float* d_partial, void* stream) {
   if (!scenes || num_scenes == 0 || !scenes[0]) return fail(nullptr, PALE_ERR_ARGUMENT, "no scenes");
   pale_handle* h = scenes[0];
   return guarded(h, [&]() {
@@ -1640,7 +1655,8 @@ int pale_render_views_loss_device(uint32_t num_scenes, pale_handle* const* scene
       d_ldr = h->img_ldr.p;
     }
     LossReq lq{d_target, channels, d_dldi, d_loss};
-    render_views(sc, vw, d_raw ? d_raw : h->img_raw.p, d_ldr, false, trace_photons != 0, d_target ? &lq : nullptr);
+    render_views(sc, vw, d_raw ? d_raw : h->img_raw.p, d_ldr, false, trace_photons != 0, d_target ? &lq : nullptr,
+                 d_partial);
     return PALE_OK;
   });
 }

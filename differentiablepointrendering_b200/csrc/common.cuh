@@ -255,7 +255,9 @@ struct CameraRec {
   uint32_t passes;         // gather / adjoint passes of this view
   uint32_t scene;          // index of the view's scene in the call's scene table
   uint32_t depth;          // adjoint bounces of this view
-  uint32_t pad[3];
+  uint32_t pass_begin;     // the passes [pass_begin, pass_end) of `passes` this call renders
+  uint32_t pass_end;       //   (a forward in slices keeps its running sums between calls)
+  uint32_t pad[1];
 };
 
 __device__ __forceinline__ void flag_error(RunState* st, uint32_t bit) { atomicOr(&st->error, bit); }

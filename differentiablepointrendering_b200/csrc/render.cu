@@ -940,8 +940,9 @@ std::vector<GatherChunk> gather_chunks(const std::vector<CameraRec>& views, uint
   };
   for (size_t v = 0; v < nv; ++v) {
     const uint64_t npix = (uint64_t)views[v].w * views[v].h;
-    uint32_t r = 0;
-    while (r < views[v].passes) {
+    const uint32_t end = views[v].pass_end;
+    uint32_t r = views[v].pass_begin;
+    while (r < end) {
       uint64_t fit = used < path_capacity ? (path_capacity - used) / npix : 0;
       if (fit == 0) {
         if (used) {
@@ -950,13 +951,13 @@ std::vector<GatherChunk> gather_chunks(const std::vector<CameraRec>& views, uint
         }
         fit = 1;   // one pass of a view always goes
       }
-      const uint32_t take = (uint32_t)std::min<uint64_t>(fit, views[v].passes - r);
+      const uint32_t take = (uint32_t)std::min<uint64_t>(fit, end - r);
       in[v] = 1;
       p0[v] = r;
       p1[v] = r + take;
       used += npix * take;
       r += take;
-      if (r < views[v].passes) close();   // the chunk is full
+      if (r < end) close();   // the chunk is full
     }
   }
   if (used) close();

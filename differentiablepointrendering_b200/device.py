@@ -120,7 +120,11 @@ class ViewBatch:
     1 to the scene's gather/adjoint passes, depth 0 (the scene's adjoint
     bounces) or fewer bounces.  Images, dL/dI and targets are packed in view
     order as DeviceFrame's; every call runs on the caller's CUDA stream with
-    the wavefront buffers of the first renderer."""
+    the wavefront buffers of the first renderer.  A view may carry a pass
+    range as fifth and sixth entries (first pass, pass count; forward only):
+    it then renders those passes of its passes, its running sums kept in
+    the `partial` tensor of forward_loss between calls (a request rendered
+    in slices over several batches)."""
 
     def __init__(self, renderers: Sequence[Renderer], views: Sequence[Sequence[int]], device=None):
         if not renderers:
@@ -129,17 +133,19 @@ class ViewBatch:
         self.device = torch.device(device or f"cuda:{torch.cuda.current_device()}")
         vs = []
         for v in views:
-            s, c, p, d = (list(v) + [0, 0, 0, 0])[:4]
-            vs.append((int(s), int(c), int(p), int(d)))
+            s, c, p, d, f, n = (list(v) + [0, 0, 0, 0, 0, 0])[:6]
+            vs.append((int(s), int(c), int(p), int(d), int(f), int(n)))
         self.views = vs
+        self.sliced = any(n for *_, n in vs)
         arr = (N.PaleView * max(1, len(vs)))()
-        for i, (s, c, p, d) in enumerate(vs):
+        for i, (s, c, p, d, f, n) in enumerate(vs):
             if not 0 <= s < len(self.renderers):
                 raise ValueError(f"view {i}: scene {s} outside the {len(self.renderers)} renderers")
             arr[i].scene, arr[i].camera, arr[i].passes, arr[i].depth = s, c, p, d
+            arr[i].first_pass, arr[i].pass_count = f, n
         self._views = arr
         self._scenes = (C.c_void_p * len(self.renderers))(*[r._h.value for r in self.renderers])
-        self.sizes = [self.renderers[s]._sizes[c] for s, c, _, _ in vs]
+        self.sizes = [self.renderers[v[0]]._sizes[v[1]] for v in vs]
         self.pixels = sum(w * h for w, h in self.sizes)
         f = dict(dtype=torch.float32, device=self.device)
         self.ldr = torch.zeros(max(1, self.pixels), 4, **f)
@@ -159,10 +165,13 @@ class ViewBatch:
     def _stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 
-    def forward_loss(self, target: Optional[torch.Tensor] = None, trace_photons: bool = True):
+    def forward_loss(self, target: Optional[torch.Tensor] = None, trace_photons: bool = True,
+                     partial: Optional[torch.Tensor] = None):
         """Forward render of every view (with the L2 loss against `target`,
         packed (P, 3) or (P, 4), when given); returns the per-view losses
-        (float64 device tensor) or None."""
+        (float64 device tensor) or None.  partial: packed (P, 4) running
+        sums of the views rendered in slices (read for a view whose range
+        starts after pass 0, written for a view not finished)."""
         L = self.renderers[0]._lib
         t = None
         if target is not None:
@@ -174,7 +183,8 @@ class ViewBatch:
             C.c_void_p(t.data_ptr()) if t is not None else None, t.shape[1] if t is not None else 0,
             C.c_void_p(self.ldr.data_ptr()), C.c_void_p(self.raw.data_ptr()),
             C.c_void_p(self.dldi.data_ptr()) if t is not None else None,
-            C.c_void_p(self.loss.data_ptr()) if t is not None else None, self._stream())
+            C.c_void_p(self.loss.data_ptr()) if t is not None else None,
+            C.c_void_p(partial.data_ptr()) if partial is not None else None, self._stream())
         _check(L, self.renderers[0]._h, rc, "render_views_loss_device")
         return self.loss if t is not None else None
 

@@ -80,9 +80,15 @@ class Request:
     error: Optional[str] = None
     batch_views: int = 0                   # views in the round that served it
     round: int = -1
+    slices: int = 0                        # rounds its passes were rendered in
     t_submit: float = 0.0
     t_done: float = 0.0
     done: threading.Event = field(default_factory=threading.Event, repr=False)
+    # server state: passes rendered so far, passes of the current round (0:
+    # all that remain), running sums of a forward rendered in slices
+    next_pass: int = field(default=0, repr=False)
+    round_passes: int = field(default=0, repr=False)
+    partial: object = field(default=None, repr=False)
 
     @property
     def latency_ms(self) -> float:
@@ -110,29 +116,39 @@ MAX_ROUND_SCENES = 7   # a call's scene table holds 8 entries, the first the ser
 
 def request_paths(q: Request, sizes: Dict[str, List[Tuple[int, int]]],
                   max_passes: Optional[Dict[str, int]] = None) -> int:
-    """Camera paths of request q: its view's pixels x passes (passes 0: its
-    scene's max_passes)."""
+    """Camera paths request q still has to render: its view's pixels x its
+    remaining passes (passes 0: its scene's max_passes)."""
     w, h = sizes[q.scene][q.camera]
-    return w * h * (q.passes or (max_passes or {}).get(q.scene, 1))
+    return w * h * (total_passes(q, max_passes) - q.next_pass)
+
+
+def total_passes(q: Request, max_passes: Optional[Dict[str, int]] = None) -> int:
+    return q.passes or (max_passes or {}).get(q.scene, 1)
 
 
 def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], max_views: int,
                max_pixels: int, max_paths: Optional[int] = None,
                max_passes: Optional[Dict[str, int]] = None,
                max_scenes: int = MAX_ROUND_SCENES, policy: str = "arrival",
-               now: float = 0.0, starve_s: float = 2.0) -> Tuple[List[Request], List[Request]]:
+               now: float = 0.0, starve_s: float = 2.0,
+               slices: bool = False) -> Tuple[List[Request], List[Request]]:
     """The requests of the next round, at most max_views views, max_pixels
     camera pixels, max_scenes distinct scenes and (when given) max_paths
     camera paths (request_paths); returns (taken, left), left in arrival
-    order.  policy "arrival": the queue's head in arrival order, up to the
-    first request that does not fit.  policy "light_first": requests that
-    have waited longer than starve_s first (in arrival order), then the
-    others by their work (paths, a gradient request's counted twice),
-    skipping those that do not fit, so that light requests are not held
-    behind heavy ones and a heavy one waits at most about starve_s plus a
-    round; the round's paths are then also capped at 8 times its first
-    request's (2^20 at least), so that requests of very different sizes
-    do not share a round.  The first request considered always goes."""
+    order, and sets each taken request's round_passes (the passes it renders
+    in the round, 0: all that remain).  policy "arrival": the queue's head
+    in arrival order, up to the first request that does not fit.  policy
+    "light_first": requests that have waited longer than starve_s first (in
+    arrival order), then the others by their work (paths, a gradient
+    request's counted twice), skipping those that do not fit, so that light
+    requests are not held behind heavy ones and a heavy one waits at most
+    about starve_s plus a round; the round's paths are then also capped at
+    8 times its first request's (2^20 at least), so that requests of very
+    different sizes do not share a round.  With slices (and a path cap) a
+    forward request that does not fit renders as many of its passes as do,
+    one at least, and goes back to the queue for the rest: a heavy request
+    advances in slices between which newly arrived requests get rounds.
+    The first request considered always goes."""
     def work(q):
         return request_paths(q, sizes, max_passes) * (2 if q.kind == "gradient" else 1)
 
@@ -148,21 +164,28 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
     for q in order:
         w, h = sizes[q.scene][q.camera]
         n = request_paths(q, sizes, max_passes)
-        if taken and (len(taken) + 1 > max_views or pix + w * h > max_pixels
-                      or (cap is not None and paths + n > cap)
+        k = 0                                  # all remaining passes
+        fits = not taken or cap is None or paths + n <= cap
+        if not fits and slices and q.kind == "forward" and cap is not None and paths + w * h <= cap:
+            k, fits = (cap - paths) // (w * h), True      # a slice of its passes
+        if not taken and slices and q.kind == "forward" and cap is not None and n > cap:
+            k = max(1, cap // (w * h))                      # a first request over the cap: a slice too
+        if taken and (not fits or len(taken) + 1 > max_views or pix + w * h > max_pixels
                       or (q.scene not in scenes and len(scenes) >= max_scenes)):
             if policy == "arrival":
                 break
             continue
+        q.round_passes = k
+        m = w * h * k if k else n
         if not taken and policy == "light_first":
             # a round of light requests stays light: at most 8 times the
             # work of its first request (2^20 paths at least), so that a
             # light request does not wait for a heavy one in its own round
-            light = max(1 << 20, 8 * n)
+            light = max(1 << 20, 8 * m)
             cap = light if cap is None else min(cap, light)
         taken.append(q)
         pix += w * h
-        paths += n
+        paths += m
         scenes.add(q.scene)
     chosen = set(map(id, taken))
     return taken, [q for q in queue if id(q) not in chosen]
@@ -176,7 +199,8 @@ class Server:
 
     def __init__(self, hbm_budget: int, max_views: int = 64, max_pixels: int = 1 << 24,
                  settings: Optional[dict] = None, device: Optional[int] = None,
-                 max_paths: Optional[int] = None, policy: str = "arrival", starve_s: float = 2.0):
+                 max_paths: Optional[int] = None, policy: str = "arrival", starve_s: float = 2.0,
+                 slices: bool = True):
         import torch
 
         self.budget = int(hbm_budget)
@@ -186,6 +210,7 @@ class Server:
         if policy not in ("arrival", "light_first"):
             raise ValueError("policy must be 'arrival' or 'light_first'")
         self.policy, self.starve_s = policy, float(starve_s)
+        self.slices = bool(slices) and self.max_paths is not None
         self.device = torch.device(f"cuda:{device if device is not None else torch.cuda.current_device()}")
         self.scenes: Dict[str, _Scene] = {}
         self.done: List[Request] = []
@@ -316,7 +341,8 @@ class Server:
                 spp = {n: s.max_passes for n, s in self.scenes.items()}
                 taken, self._queue = plan_round(self._queue, sizes, self.max_views, self.max_pixels,
                                                 self.max_paths, spp, policy=self.policy,
-                                                now=time.perf_counter(), starve_s=self.starve_s)
+                                                now=time.perf_counter(), starve_s=self.starve_s,
+                                                slices=self.slices)
             try:
                 with self._gpu:
                     self._round(taken)
@@ -325,10 +351,18 @@ class Server:
                     if not q.done.is_set():
                         q.error = str(e)
             now = time.perf_counter()
+            again = []
             for q in taken:
-                if not q.done.is_set():
-                    q.t_done = now
-                    q.done.set()
+                if q.done.is_set():
+                    continue
+                if q.error is None and q.partial is not None:
+                    again.append(q)          # a slice done, passes left: back to the queue
+                    continue
+                q.t_done = now
+                q.done.set()
+            if again:
+                with self._cv:
+                    self._queue = sorted(self._queue + again, key=lambda r: r.t_submit)
 
     def _round(self, reqs: List[Request]):
         import torch
@@ -347,12 +381,38 @@ class Server:
         def forward(idx, executor):
             """One forward wavefront over requests idx: images to the host,
             the L2 loss and dL/dI of its gradient requests (compute_l2_loss
-            / compute_l2_grad, python/losses.py:10-45, on the LDR image)."""
-            vb = ViewBatch([executor] + scene_renderers,
-                           [(entry[reqs[i].scene], reqs[i].camera, passes(reqs[i]), reqs[i].depth) for i in idx],
-                           device=self.device)
-            vb.forward_loss(None, trace_photons=False)      # the resident photon maps
+            / compute_l2_grad, python/losses.py:10-45, on the LDR image).  A
+            forward request with a slice renders those passes, its running
+            sums carried between rounds; it is finished (and its image read)
+            in the round of its last pass."""
+            views, ranges = [], []
+            for i in idx:
+                q = reqs[i]
+                P = passes(q)
+                k = q.round_passes or P - q.next_pass
+                rng = (q.next_pass, k) if (q.next_pass or k < P) else (0, 0)
+                ranges.append(rng)
+                views.append((entry[q.scene], q.camera, P, q.depth) + rng)
+            vb = ViewBatch([executor] + scene_renderers, views, device=self.device)
             offs = np.cumsum([0] + [w * h for w, h in vb.sizes])
+            partial = None
+            if vb.sliced:
+                partial = torch.zeros(max(1, int(offs[-1])), 4, dtype=torch.float32, device=self.device)
+                for k, i in enumerate(idx):
+                    if ranges[k][0] > 0:
+                        partial[offs[k]:offs[k + 1]].copy_(reqs[i].partial)
+            vb.forward_loss(None, trace_photons=False, partial=partial)   # the resident photon maps
+            finished = []
+            for k, i in enumerate(idx):
+                q = reqs[i]
+                first, count = ranges[k]
+                q.slices += 1
+                if count and first + count < passes(q):
+                    q.next_pass = first + count
+                    q.partial = partial[offs[k]:offs[k + 1]].clone()
+                else:
+                    q.next_pass, q.partial = passes(q), None
+                    finished.append(k)
             dldi = {}
             for k, i in enumerate(idx):
                 q = reqs[i]
@@ -365,8 +425,8 @@ class Server:
                 d[:, :3].div_(float(3 * (offs[k + 1] - offs[k])))
                 dldi[i] = d
             ldr = self._host(vb.ldr)
-            for k, i in enumerate(idx):
-                q = reqs[i]
+            for k in finished:
+                q = reqs[idx[k]]
                 w, h = vb.sizes[k]
                 q.image = ldr[offs[k]:offs[k + 1]].reshape(h, w, 4).copy()
                 q.batch_views = len(reqs)

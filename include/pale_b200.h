@@ -316,6 +316,11 @@ typedef struct pale_view {
                           adjoint_passes                                        */
     uint32_t depth;    /* adjoint bounces: 0 = the scene's adjoint_bounces, at
                           most that                                             */
+    uint32_t first_pass;  /* forward calls: render passes [first_pass,
+                          first_pass + pass_count) of `passes` (a view rendered
+                          in slices over several calls, its running sums kept
+                          in the caller's d_partial); 0 and 0: all of them       */
+    uint32_t pass_count;
 } pale_view;
 
 /* Batched forward render with the L2 loss: the views of up to 8 scenes of
@@ -329,12 +334,20 @@ typedef struct pale_view {
  * d_dldi and d_loss may be NULL.  Runs on `stream` (NULL = the default
  * stream) with the wavefront buffers of scenes[0], without waiting; a
  * camera's seeds follow the scenes' camera_seeds setting.  Errors are
- * reported through scenes[0] (pale_last_error). */
+ * reported through scenes[0] (pale_last_error).
+ * Slices: a view with a pass range (first_pass, pass_count) renders only
+ * those passes; d_partial (DEVICE, float4 per packed pixel, needed when any
+ * view has a range) holds the view's running sum of the passes before
+ * first_pass on entry (ignored for first_pass 0) and of the passes up to
+ * the range's end on return when the view is not finished; a view's images,
+ * dL/dI and loss are written by the call that renders its last pass, and
+ * are then the same, bit for bit, as those of one call over all passes. */
 int pale_render_views_loss_device(uint32_t num_scenes, pale_handle *const *scenes,
                                   int trace_photons, uint32_t num_views,
                                   const pale_view *views, const float *d_target,
                                   uint32_t channels, float *d_ldr, float *d_raw,
-                                  float *d_dldi, double *d_loss, void *stream);
+                                  float *d_dldi, double *d_loss, float *d_partial,
+                                  void *stream);
 
 /* The photon passes and the photon grid of the scene alone (the first half
  * of render_forward, SyclBridge.cpp:82-138), enqueued on `stream` (NULL =

@@ -92,3 +92,35 @@ def test_admission_refuses_scenes_beyond_the_budget(gpu):
         assert not srv.scenes
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("policy", ["arrival", "light_first"])
+def test_forward_requests_in_slices_equal_alone(gpu, policy):
+    """With a round cap of 4096 camera paths, a 64x64 request of 4 passes
+    renders in slices over several rounds (its running sums carried between
+    them) while other requests get rounds in between: its image is bit for
+    bit the one of the request rendered in one call."""
+    import torch
+
+    from differentiablepointrendering_b200.serving import Request, Server
+
+    free, _ = torch.cuda.mem_get_info()
+    srv = Server(hbm_budget=free, settings={"rng_mode": "decorrelated"}, max_paths=4096, policy=policy)
+    try:
+        a, b = _scenes()
+        srv.add_scene("a", a, SETTINGS)
+        srv.add_scene("b", b, SETTINGS)
+        mix = [Request("b", k % 3, "forward", None, 4, 0) for k in range(6)] + \
+              [Request("a", k % 4, "forward", None, 1 + k % 4, 0) for k in range(6)]
+        for q in mix:
+            srv.submit(q)
+        for q in mix:
+            assert q.done.wait(120), q
+            assert q.error is None, q.error
+        assert max(q.slices for q in mix) > 1
+        for q in mix:
+            alone = srv.serve_one(Request(q.scene, q.camera, q.kind, None, q.passes, q.depth))
+            assert alone.error is None and alone.slices == 1
+            np.testing.assert_array_equal(alone.image, q.image)
+    finally:
+        srv.close()

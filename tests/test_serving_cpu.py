@@ -114,3 +114,23 @@ def test_light_first_round_stays_light():
     assert taken == [light] and left == [medium]         # 2M > max(2^20, 8 x 16)
     taken, left = S.plan_round([medium], sizes, 64, 1 << 24, max_paths=1 << 24, policy="light_first", now=1.1)
     assert taken == [medium]
+
+
+def test_forward_requests_take_slices_of_their_passes():
+    sizes = {"a": [(64, 64), (4, 4)]}
+    big = S.Request("a", 0, passes=4)                    # 16384 paths
+    small = S.Request("a", 1, passes=2)                  # 32 paths
+    grad = S.Request("a", 0, kind="gradient", passes=4, target=None)
+    taken, left = S.plan_round([big, small], sizes, 64, 10 ** 6, max_paths=4096 + 32, slices=True)
+    assert taken == [big, small] and left == []
+    assert big.round_passes == 1 and small.round_passes == 0   # one pass of the big one, all of the small
+    big.next_pass = 3                                        # one pass left: fits whole
+    taken, _ = S.plan_round([big], sizes, 64, 10 ** 6, max_paths=4096, slices=True)
+    assert taken == [big] and big.round_passes == 0
+    # a gradient request is never sliced; as the first of a round it goes whole
+    taken, left = S.plan_round([grad, small], sizes, 64, 10 ** 6, max_paths=4096, slices=True)
+    assert taken == [grad] and grad.round_passes == 0 and left == [small]
+    # without slices the big request waits for a round of its own
+    big.next_pass = 0
+    taken, left = S.plan_round([small, big], sizes, 64, 10 ** 6, max_paths=4096)
+    assert taken == [small] and left == [big]
