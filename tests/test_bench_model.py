@@ -40,9 +40,13 @@ def test_every_timed_kernel_has_traffic_and_counters():
     with open(os.path.join(os.path.dirname(HERE), "profiles", "traffic.json")) as f:
         traffic = json.load(f)
     assert timed <= set(traffic), timed - set(traffic)
-    assert all(isinstance(v, int) and v > 0 for v in traffic.values())
+    rates = {k: v["dram_bytes_per_s"] for k, v in traffic.items() if not k.startswith("_")}
+    assert all(isinstance(v, int) and v > 0 for v in rates.values())
     for k in timed:
-        assert bench.read_traffic(k) == traffic[k]
+        # the DRAM rate of the small-case capture times the launch's time
+        assert bench.read_traffic(k, 2.0) == int(rates[k] * 2.0 / 1e3)
+    gather = set(bench.kernel_bytes(sf, dict(sb, vertex_entries=10, vertex_records=40), "gather"))
+    assert gather <= set(rates), gather - set(rates)
     # the model reads only counters the bench line reports
     assert {"gather_segments", "gather_node_visits", "gather_surfel_tests", "gather_queries",
             "gather_photons_scanned"} <= set(bench.FWD_COUNTERS)
