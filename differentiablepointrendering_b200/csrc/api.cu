@@ -985,6 +985,11 @@ uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector
   h->timer.used = 0;
   const uint64_t launches0 = launches_issued();
   check_views(scenes, views, false);
+  bool sliced = false;
+  for (const ViewReq& v : views) sliced = sliced || v.count != 0;
+  if (sliced && !d_partial) throw ArgError("views rendered in slices need the running sums (d_partial)");
+  if (sliced && trace_photons)
+    throw ArgError("views rendered in slices keep one photon map: trace it first, then render without trace_photons");
   uint32_t total = 0, max_pix = 0;
   std::vector<CameraRec> sel = view_records(scenes, views, total, max_pix);
   size_wavefronts(h, total, max_pix);
@@ -1012,9 +1017,6 @@ uint32_t render_views(const std::vector<pale_handle*>& scenes, const std::vector
   FrameArgs F = frame_args(scenes, nsel, total);
   F.raw = d_raw;
   F.ldr = d_ldr;
-  bool sliced = false;
-  for (const ViewReq& v : views) sliced = sliced || v.count != 0;
-  if (sliced && !d_partial) throw ArgError("views rendered in slices need the running sums (d_partial)");
   if (d_partial) F.fb = reinterpret_cast<float4*>(d_partial);   // the caller's running sums
   if (lq) {
     F.target = lq->target;

@@ -336,7 +336,8 @@ typedef struct pale_view {
  * camera's seeds follow the scenes' camera_seeds setting.  Errors are
  * reported through scenes[0] (pale_last_error).
  * Slices: a view with a pass range (first_pass, pass_count) renders only
- * those passes; d_partial (DEVICE, float4 per packed pixel, needed when any
+ * those passes (with trace_photons 0: every slice on one photon map);
+ * d_partial (DEVICE, float4 per packed pixel, needed when any
  * view has a range) holds the view's running sum of the passes before
  * first_pass on entry (ignored for first_pass 0) and of the passes up to
  * the range's end on return when the view is not finished; a view's images,
