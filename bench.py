@@ -785,7 +785,7 @@ def serve_stream(srv, reqs):
     return served, span, np.array(plain), clock, np.array(service)
 
 
-def plain_light_first(reqs, service_ms, starve_s: float = 2.0):
+def plain_light_first(reqs, service_ms, starve_s: float = 5.0):
     """The plain path with the server's light-first order: one request at a
     time, the next one the lightest that has arrived (those waiting longer
     than starve_s first), on a virtual clock of the measured service times;

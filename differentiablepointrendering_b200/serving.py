@@ -145,10 +145,11 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
     about starve_s plus a round; the round's paths are then also capped at
     8 times its first request's (2^20 at least), so that requests of very
     different sizes do not share a round.  With slices (and a path cap) a
-    forward request that does not fit renders as many of its passes as do,
-    one at least, and goes back to the queue for the rest: a heavy request
-    advances in slices between which newly arrived requests get rounds.
-    The first request considered always goes."""
+    forward request over the cap that comes first renders as many of its
+    passes as the cap holds, one at least, in a round of its own, and goes
+    back to the queue for the rest: a heavy request advances in slices
+    between which newly arrived requests get rounds.  The first request
+    considered always goes."""
     def work(q):
         return request_paths(q, sizes, max_passes) * (2 if q.kind == "gradient" else 1)
 
@@ -166,10 +167,8 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
         n = request_paths(q, sizes, max_passes)
         k = 0                                  # all remaining passes
         fits = not taken or cap is None or paths + n <= cap
-        if not fits and slices and q.kind == "forward" and cap is not None and paths + w * h <= cap:
-            k, fits = (cap - paths) // (w * h), True      # a slice of its passes
         if not taken and slices and q.kind == "forward" and cap is not None and n > cap:
-            k = max(1, cap // (w * h))                      # a first request over the cap: a slice too
+            k = max(1, cap // (w * h))         # a first request over the cap renders a slice
         if taken and (not fits or len(taken) + 1 > max_views or pix + w * h > max_pixels
                       or (q.scene not in scenes and len(scenes) >= max_scenes)):
             if policy == "arrival":
@@ -199,7 +198,7 @@ class Server:
 
     def __init__(self, hbm_budget: int, max_views: int = 64, max_pixels: int = 1 << 24,
                  settings: Optional[dict] = None, device: Optional[int] = None,
-                 max_paths: Optional[int] = None, policy: str = "arrival", starve_s: float = 2.0,
+                 max_paths: Optional[int] = None, policy: str = "arrival", starve_s: float = 5.0,
                  slices: bool = True):
         import torch
 

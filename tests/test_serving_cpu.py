@@ -124,6 +124,9 @@ def test_forward_requests_take_slices_of_their_passes():
     taken, left = S.plan_round([big, small], sizes, 64, 10 ** 6, max_paths=4096 + 32, slices=True)
     assert taken == [big, small] and left == []
     assert big.round_passes == 1 and small.round_passes == 0   # one pass of the big one, all of the small
+    # a request over the cap that does not come first waits (no slice in another's round)
+    taken, left = S.plan_round([small, big], sizes, 64, 10 ** 6, max_paths=4096, slices=True)
+    assert taken == [small] and left == [big]
     big.next_pass = 3                                        # one pass left: fits whole
     taken, _ = S.plan_round([big], sizes, 64, 10 ** 6, max_paths=4096, slices=True)
     assert taken == [big] and big.round_passes == 0
