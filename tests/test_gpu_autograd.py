@@ -13,14 +13,14 @@ SETTINGS = {"photons": 100000, "bounces": 3, "forward_passes": 1, "gather_passes
             "adjoint_passes": 2, "gather_radius": 0.03, "gradients": "all"}
 
 
-@pytest.mark.parametrize("output", ["raw", "ldr"])
-def test_backward_is_the_adjoint(gpu, output):
+@pytest.mark.parametrize("output,estimator", [("raw", "reference"), ("ldr", "reference"), ("raw", "gather")])
+def test_backward_is_the_adjoint(gpu, output, estimator):
     import torch
 
     from differentiablepointrendering_b200 import autograd as A
     from differentiablepointrendering_b200.device import DeviceFrame
 
-    r = Renderer.from_scene(make_box_scene(3000, cameras=2, resolution=32), SETTINGS)
+    r = Renderer.from_scene(make_box_scene(3000, cameras=2, resolution=32), dict(SETTINGS, estimator=estimator))
     try:
         f = DeviceFrame(r, device=torch.device("cuda:0"))
         params = A.parameters(r)
