@@ -280,6 +280,10 @@ constexpr uint32_t kTopNodes = PALE_TOP_NODES;
 #define PALE_GATHER_HITS 8
 #endif
 constexpr int kGatherHits = PALE_GATHER_HITS;
+// The camera walk's hit list in shared memory (1) or registers (0).
+#ifndef PALE_KHIT_SMEM
+#define PALE_KHIT_SMEM 0
+#endif
 // Words of a K-hit walk result: the count and K surfels, padded to uint4s.
 constexpr int kKHitWords = (kGatherHits + 4) / 4 * 4;
 // Resident blocks per SM the record kernels around the walks (camera

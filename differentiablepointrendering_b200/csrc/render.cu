@@ -532,7 +532,14 @@ __global__ void __launch_bounds__(kThreads, kRoundMinBlocks * (kBlock / kThreads
   const uint32_t n = A.counts[round];
   const int lane = threadIdx.x & 31;
   TravStack stk(s_top, A.scenes.n * A.scenes.staged);
+#if PALE_KHIT_SMEM
+  KHitWalkS<K> w;
+  // the hit lists after the staged nodes and the shared part of the stacks
+  w.bind(reinterpret_cast<uint2*>(s_top + A.scenes.n * A.scenes.staged) + (size_t)PALE_SMEM_STACK * kThreads +
+         threadIdx.x);
+#else
   KHitWalk<K> w;
+#endif
   TraceCounters ctr{0, 0};
   uint32_t sid = 0;          // scene of this lane's walk
   uint32_t cur = kInvalid;   // queue entry of this lane's walk
@@ -570,7 +577,11 @@ __global__ void __launch_bounds__(kThreads, kRoundMinBlocks * (kBlock / kThreads
       uint32_t rw[kKHitWords];
       rw[0] = w.count;
 #pragma unroll
+#if PALE_KHIT_SMEM
+      for (int k = 0; k < K; ++k) rw[1 + k] = w.prim(k);
+#else
       for (int k = 0; k < K; ++k) rw[1 + k] = w.prim_out[k];
+#endif
 #pragma unroll
       for (int k = K + 1; k < kKHitWords; ++k) rw[k] = 0u;
       uint4* dst = reinterpret_cast<uint4*>(A.khit + (size_t)kKHitWords * cur);
@@ -981,7 +992,7 @@ GatherShape gather_shape(const FrameArgs& a) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   g.wt = a.walk_block == 64 || a.walk_block == 128 ? (int)a.walk_block : kBlock;
-  g.smem = top_smem(a.scenes, g.wt);
+  g.smem = top_smem(a.scenes, g.wt) + (PALE_KHIT_SMEM ? (size_t)kGatherHits * g.wt * sizeof(uint2) : 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_cg_round<kGatherHits>, kBlock, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_cg_lookup<kMulti>, kBlock, 0);
   g.grid_r = (uint32_t)std::max(1, sms * std::max(1, per_sm_r));

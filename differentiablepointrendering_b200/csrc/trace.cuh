@@ -385,6 +385,45 @@ struct KHitWalk : WalkBase<KHitWalk<K>> {
   }
 };
 
+// The same walk with its sorted hit list in shared memory instead of
+// registers (entry q of a thread at hits[q * blockDim.x], (t, surfel)
+// pairs), which frees the registers of the list for one more resident
+// block; the list is read only when a surfel is hit.
+template <int K>
+struct KHitWalkS : WalkBase<KHitWalkS<K>> {
+  float best;   // the K-th distance once K hits are held
+  uint32_t count;
+  uint2* hits;  // this thread's first entry
+  __device__ __forceinline__ void bind(uint2* h) { hits = h; }
+  __device__ __forceinline__ void init(V3 o_, V3 d_, float tmin_, float limit) {
+    this->start(o_, d_, tmin_);
+    best = limit;
+    count = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) hits[(size_t)k * blockDim.x] = make_uint2(__float_as_uint(limit), 0u);
+  }
+  __device__ __forceinline__ void test(const SurfelView& sf, uint32_t i) {
+    float th, aa;
+    V3 xx;
+    if (surfel_hit(sf, i, this->o, this->d, this->tmin, best, th, xx, aa)) {
+      uint32_t pj = i;
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        const uint2 e = hits[(size_t)q * blockDim.x];
+        const float tq = __uint_as_float(e.x);
+        if (th < tq) {
+          hits[(size_t)q * blockDim.x] = make_uint2(__float_as_uint(th), pj);
+          th = tq;
+          pj = e.y;
+        }
+      }
+      count = count < (uint32_t)K ? count + 1 : count;
+      if (count == (uint32_t)K) best = __uint_as_float(hits[(size_t)(K - 1) * blockDim.x].x);
+    }
+  }
+  __device__ __forceinline__ uint32_t prim(int k) const { return hits[(size_t)k * blockDim.x].y; }
+};
+
 // One step of a persistent walk loop for the lanes of a warp: the lanes
 // whose walk stands at a leaf step together once at least kLeafBatch of
 // them (or all of the walking lanes) do, the other times the lanes at inner
