@@ -282,7 +282,7 @@ constexpr uint32_t kTopNodes = PALE_TOP_NODES;
 constexpr int kGatherHits = PALE_GATHER_HITS;
 // The camera walk's hit list in shared memory (1) or registers (0).
 #ifndef PALE_KHIT_SMEM
-#define PALE_KHIT_SMEM 0
+#define PALE_KHIT_SMEM 1
 #endif
 // Words of a K-hit walk result: the count and K surfels, padded to uint4s.
 constexpr int kKHitWords = (kGatherHits + 4) / 4 * 4;
@@ -293,10 +293,11 @@ constexpr int kKHitWords = (kGatherHits + 4) / 4 * 4;
 #define PALE_TRACE_MIN_BLOCKS 4
 #endif
 constexpr int kTraceMinBlocks = PALE_TRACE_MIN_BLOCKS;
-// The camera gather's 8-hit walk (its hit list needs the registers more
-// than it needs the fourth block).
+// The camera gather's 8-hit walk: 4 resident blocks with its hit list in
+// shared memory (3 with the list in registers, which need them more than
+// the fourth block).
 #ifndef PALE_ROUND_MIN_BLOCKS
-#define PALE_ROUND_MIN_BLOCKS 3
+#define PALE_ROUND_MIN_BLOCKS (PALE_KHIT_SMEM ? 4 : 3)
 #endif
 constexpr int kRoundMinBlocks = PALE_ROUND_MIN_BLOCKS;
 // The same for the warp-per-lookup kernels (camera lookups, transport).
