@@ -19,14 +19,18 @@ round's gradient requests share adjoint wavefronts of the reference's
 adjoint; with "gather" each gets the exact derivative of its view of the
 round's forward (photon map held), swept from that forward's own path
 vertices into arrays of its own (``pale_render_views_gradients_device``),
-with no second wavefront.
+with no second wavefront.  The server's settings' ``gradients`` picks the
+groups: opacity (default, as the reference's adjoint) or "all" seven; a
+request's ``grads`` holds those only.
 
 One dispatcher thread owns the GPU stream and serves requests in rounds.
 A round takes the queued requests that fit (at most ``max_views`` views,
 ``max_pixels`` camera pixels, seven scenes and, when set, ``max_paths``
 camera paths of pixels x passes, which bounds a round's time), in arrival
 order or, with ``policy="light_first"``, the lightest first with requests
-waiting longer than ``starve_s`` ahead of them, and renders them
+waiting longer than ``starve_s`` ahead of them (a request's weight: its
+camera paths times its view's surfel layers per path, measured for every
+camera when its scene is admitted), and renders them
 together: the views of all the round's requests, of any scenes, are ONE
 camera-gather wavefront (device.ViewBatch's entry point,
 ``pale_render_views_loss_device``), and the round's gradient requests share
@@ -58,7 +62,7 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 
 from .pale import Renderer
-from .scene import SceneArrays, make_box_scene
+from .scene import POINT_FIELDS, SceneArrays, make_box_scene
 
 
 class AdmissionError(RuntimeError):
@@ -76,7 +80,9 @@ class Request:
     # results, filled by the server
     image: Optional[np.ndarray] = None     # (H, W, 4) LDR
     loss: Optional[float] = None
-    grads: Optional[Dict[str, np.ndarray]] = None   # BVH order
+    # BVH order; the groups the server computes: opacity, or every field
+    # when its settings ask for gradients="all"
+    grads: Optional[Dict[str, np.ndarray]] = None
     error: Optional[str] = None
     batch_views: int = 0                   # views in the round that served it
     round: int = -1
@@ -109,6 +115,7 @@ class _Scene:
     footprint: int
     max_passes: int
     max_depth: int
+    layers: List[float] = field(default_factory=list)   # surfel layers per camera path, per camera
 
 
 MAX_ROUND_SCENES = 7   # a call's scene table holds 8 entries, the first the server's executor
@@ -126,12 +133,22 @@ def total_passes(q: Request, max_passes: Optional[Dict[str, int]] = None) -> int
     return q.passes or (max_passes or {}).get(q.scene, 1)
 
 
+def path_weight(q: Request, layers: Optional[Dict[str, List[float]]] = None) -> float:
+    """The cost of one camera path of q's view relative to a path that
+    ends at its first surface: the view's surfel layers per path (each a
+    walk step and a photon lookup), 1 when not measured."""
+    if not layers or q.scene not in layers or q.camera >= len(layers[q.scene]):
+        return 1.0
+    return max(1.0, float(layers[q.scene][q.camera]))
+
+
 def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], max_views: int,
                max_pixels: int, max_paths: Optional[int] = None,
                max_passes: Optional[Dict[str, int]] = None,
                max_scenes: int = MAX_ROUND_SCENES, policy: str = "arrival",
                now: float = 0.0, starve_s: float = 2.0,
-               slices: bool = False) -> Tuple[List[Request], List[Request]]:
+               slices: bool = False,
+               layers: Optional[Dict[str, List[float]]] = None) -> Tuple[List[Request], List[Request]]:
     """The requests of the next round, at most max_views views, max_pixels
     camera pixels, max_scenes distinct scenes and (when given) max_paths
     camera paths (request_paths); returns (taken, left), left in arrival
@@ -139,19 +156,20 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
     in the round, 0: all that remain).  policy "arrival": the queue's head
     in arrival order, up to the first request that does not fit.  policy
     "light_first": requests that have waited longer than starve_s first (in
-    arrival order), then the others by their work (paths, a gradient
-    request's counted twice), skipping those that do not fit, so that light
-    requests are not held behind heavy ones and a heavy one waits at most
-    about starve_s plus a round; the round's paths are then also capped at
-    8 times its first request's (2^20 at least), so that requests of very
-    different sizes do not share a round.  With slices (and a path cap) a
+    arrival order), then the others by their work (paths times the view's
+    surfel layers per path from `layers`, per scene and camera, 1 when not
+    given; a gradient request's counted twice), skipping those that do not
+    fit, so that light requests are not held behind heavy ones and a heavy
+    one waits at most about starve_s plus a round; the round's work is then
+    also capped at 8 times its first request's (2^20 paths at least), so
+    that requests of very different costs do not share a round.  With slices (and a path cap) a
     forward request over the cap that comes first renders as many of its
     passes as the cap holds, one at least, in a round of its own, and goes
     back to the queue for the rest: a heavy request advances in slices
     between which newly arrived requests get rounds.  The first request
     considered always goes."""
     def work(q):
-        return request_paths(q, sizes, max_passes) * (2 if q.kind == "gradient" else 1)
+        return request_paths(q, sizes, max_passes) * path_weight(q, layers) * (2 if q.kind == "gradient" else 1)
 
     if policy == "arrival":
         order = list(queue)
@@ -160,13 +178,15 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
         order = old + sorted((q for q in queue if not now - q.t_submit > starve_s), key=work)
     else:
         raise ValueError("policy must be 'arrival' or 'light_first'")
-    taken, pix, paths, scenes = [], 0, 0, set()
-    cap = max_paths
+    taken, pix, paths, cost, scenes = [], 0, 0, 0.0, set()
+    cap, cost_cap = max_paths, None
     for q in order:
         w, h = sizes[q.scene][q.camera]
         n = request_paths(q, sizes, max_passes)
+        pw = path_weight(q, layers)
         k = 0                                  # all remaining passes
-        fits = not taken or cap is None or paths + n <= cap
+        fits = not taken or ((cap is None or paths + n <= cap)
+                             and (cost_cap is None or cost + n * pw <= cost_cap))
         if not taken and slices and q.kind == "forward" and cap is not None and n > cap:
             k = max(1, cap // (w * h))         # a first request over the cap renders a slice
         if taken and (not fits or len(taken) + 1 > max_views or pix + w * h > max_pixels
@@ -180,11 +200,11 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
             # a round of light requests stays light: at most 8 times the
             # work of its first request (2^20 paths at least), so that a
             # light request does not wait for a heavy one in its own round
-            light = max(1 << 20, 8 * m)
-            cap = light if cap is None else min(cap, light)
+            cost_cap = max(float(1 << 20), 8.0 * m * pw)
         taken.append(q)
         pix += w * h
         paths += m
+        cost += m * pw
         scenes.add(q.scene)
     chosen = set(map(id, taken))
     return taken, [q for q in queue if id(q) not in chosen]
@@ -230,6 +250,9 @@ class Server:
         st.update(camera_seeds="camera", photons=1000, forward_passes=1)
         self._exec_settings = st
         self._gather = st.get("estimator", "reference") in ("gather", 1)
+        # the gradient groups the adjoint writes (the others stay zero and
+        # are not copied back)
+        self._grad_keys = tuple(POINT_FIELDS) if st.get("gradients") in ("all", 1) else ("opacity",)
         self._exec = Renderer.from_scene(make_box_scene(8, cameras=1, resolution=8), st)
         # with the gather estimator, a second executor renders the forward-only
         # requests without keeping path vertices
@@ -267,11 +290,32 @@ class Server:
             r.close()
             raise AdmissionError(f"scene '{name}' needs {footprint / 2**30:.2f} GiB; "
                                  f"{(self.budget - self.admitted_bytes) / 2**30:.2f} GiB of the budget left")
+        try:
+            layers = self._layers(r)
+        except Exception:
+            r.close()
+            raise
         with self._cv:
             self.scenes[name] = _Scene(name, r, footprint, min(int(r._settings.gather_passes),
                                                                int(r._settings.adjoint_passes)),
-                                       int(r._settings.adjoint_bounces))
+                                       int(r._settings.adjoint_bounces), layers)
         return footprint
+
+    def _layers(self, r: Renderer) -> List[float]:
+        """Surfel layers per camera path of each of r's cameras (gather
+        segments per path of one pass of the camera alone, on the executor
+        that keeps no path vertices): the planner's cost of a path of that
+        view.  A view into a dense cloud costs two orders of magnitude more
+        per path than one of a wall."""
+        from .device import ViewBatch
+
+        ex = self._exec_plain if self._exec_plain is not None else self._exec
+        out = []
+        with self._gpu:
+            for c, (w, h) in enumerate(r._sizes):
+                ViewBatch([ex, r], [(1, c, 1, 0)], device=self.device).forward_loss(None, trace_photons=False)
+                out.append(ex.stats()["gather_segments"] / float(max(1, w * h)))
+        return out
 
     def _photon_map(self, r: Renderer):
         """Traces the scene's photon map, which then stays resident."""
@@ -326,6 +370,25 @@ class Server:
         buf.copy_(t)
         return buf.numpy().copy()
 
+    def _host_grads(self, g) -> Dict[str, np.ndarray]:
+        """Host copies of the computed gradient groups of `g`, staged
+        through the pinned buffer with one synchronisation."""
+        import torch
+
+        keys = [k for k in self._grad_keys if k in g]
+        n = sum(g[k].numel() for k in keys)
+        if self._pin is None or self._pin.numel() < n:
+            self._pin = torch.empty(max(n, 1 << 20), dtype=torch.float32, pin_memory=True)
+        views, off = [], 0
+        for k in keys:
+            t = g[k]
+            buf = self._pin[off:off + t.numel()].view(t.shape)
+            buf.copy_(t, non_blocking=True)
+            views.append((k, buf))
+            off += t.numel()
+        torch.cuda.current_stream(self.device).synchronize()
+        return {k: buf.numpy().copy() for k, buf in views}
+
     def _run(self):
         import torch
 
@@ -338,10 +401,11 @@ class Server:
                     return
                 sizes = {n: s.renderer._sizes for n, s in self.scenes.items()}
                 spp = {n: s.max_passes for n, s in self.scenes.items()}
+                layers = {n: s.layers for n, s in self.scenes.items()}
                 taken, self._queue = plan_round(self._queue, sizes, self.max_views, self.max_pixels,
                                                 self.max_paths, spp, policy=self.policy,
                                                 now=time.perf_counter(), starve_s=self.starve_s,
-                                                slices=self.slices)
+                                                slices=self.slices, layers=layers)
             try:
                 with self._gpu:
                     self._round(taken)
@@ -455,7 +519,7 @@ class Server:
                 vb, offs, dldi = forward(grad_idx, self._exec)
                 dl = torch.cat([dldi[i] for i in grad_idx]).contiguous()
                 gl = vb.view_gradients(list(range(len(grad_idx))), dl)
-                finish(grad_idx, [{k: self._host(v) for k, v in g.items()} for g in gl])
+                finish(grad_idx, [self._host_grads(g) for g in gl])
             return
         vb, offs, dldi = forward(list(range(len(reqs))), self._exec)
         per = self.GRADIENTS_PER_WAVEFRONT - 1     # entry 0 is the executor
@@ -467,7 +531,7 @@ class Server:
             gb = ViewBatch(rs, gviews, device=self.device)
             dl = torch.cat([dldi[i] for i in chunk]).contiguous()
             grads = gb.backward(dl)
-            finish(chunk, [{k: self._host(v) for k, v in grads[e + 1].items()} for e in range(len(chunk))])
+            finish(chunk, [self._host_grads(grads[e + 1]) for e in range(len(chunk))])
 
     # ----------------------------------------------------------- reports
     def latency(self, kind: Optional[str] = None) -> Dict[str, float]:

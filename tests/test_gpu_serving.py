@@ -10,7 +10,7 @@ import threading
 import numpy as np
 import pytest
 
-from differentiablepointrendering_b200.scene import make_box_scene, make_surfels
+from differentiablepointrendering_b200.scene import POINT_FIELDS, make_box_scene, make_surfels
 
 pytestmark = pytest.mark.gpu
 
@@ -31,12 +31,19 @@ def test_results_are_the_same_alone_and_in_the_mix(gpu, estimator):
     from differentiablepointrendering_b200.serving import Request, Server
 
     free, _ = torch.cuda.mem_get_info()
-    srv = Server(hbm_budget=free, settings={"rng_mode": "decorrelated", "estimator": estimator})
+    # the gather variant computes every gradient group, the reference one opacity only
+    groups = "all" if estimator == "gather" else "opacity"
+    srv = Server(hbm_budget=free, settings={"rng_mode": "decorrelated", "estimator": estimator,
+                                            "gradients": groups})
     try:
         a, b = _scenes()
         srv.add_scene("a", a, SETTINGS)
         srv.add_scene("b", b, SETTINGS)
         sizes = {"a": a.camera_size, "b": b.camera_size}
+        # the planner's per-view cost: surfel layers per camera path, measured at admission
+        for name, sc in (("a", a), ("b", b)):
+            assert len(srv.scenes[name].layers) == len(sc.camera_size)
+            assert all(x > 0 for x in srv.scenes[name].layers)
         rng = np.random.default_rng(4)
         specs = []
         for _ in range(32):
@@ -69,6 +76,8 @@ def test_results_are_the_same_alone_and_in_the_mix(gpu, estimator):
             np.testing.assert_array_equal(alone.image, q.image)
             if q.kind == "gradient":
                 assert alone.loss == q.loss
+                # only the computed groups come back
+                assert set(q.grads) == ({"opacity"} if groups == "opacity" else set(POINT_FIELDS))
                 for key in ("opacity", "albedo") if estimator == "gather" else ("opacity",):
                     a_, b_ = alone.grads[key].astype(np.float64), q.grads[key].astype(np.float64)
                     # a camera that looks at a closed wall of the box from outside sees no surfel

@@ -116,6 +116,32 @@ def test_light_first_round_stays_light():
     assert taken == [medium]
 
 
+def test_light_first_weighs_paths_by_the_views_layers():
+    # two views of one size: camera 0 sees a wall (1 layer per path),
+    # camera 1 looks into a dense cloud (150 layers per path)
+    sizes = {"a": [(512, 512), (512, 512)]}
+    layers = {"a": [1.0, 150.0]}
+    dense = S.Request("a", 1, kind="gradient", passes=1)
+    walls = [S.Request("a", 0, kind="gradient", passes=1) for _ in range(3)]
+    for k, q in enumerate([dense] + walls):
+        q.t_submit = 1.0 + 0.01 * k
+    q = [dense] + walls
+    # by paths alone the four are equal: arrival order, one round
+    taken, left = S.plan_round(q, sizes, 64, 1 << 24, max_paths=1 << 24, policy="light_first", now=1.1)
+    assert taken == q and left == []
+    # by layers the wall views go first, and the dense view (150 x 262144
+    # > 8 x 262144) stays out of their round
+    taken, left = S.plan_round(q, sizes, 64, 1 << 24, max_paths=1 << 24, policy="light_first", now=1.1,
+                               layers=layers)
+    assert taken == walls and left == [dense]
+    taken, left = S.plan_round(left, sizes, 64, 1 << 24, max_paths=1 << 24, policy="light_first", now=1.1,
+                               layers=layers)
+    assert taken == [dense]
+    # unmeasured scenes and cameras weigh 1
+    assert S.path_weight(dense, None) == 1.0 and S.path_weight(S.Request("b", 0), layers) == 1.0
+    assert S.path_weight(dense, layers) == 150.0
+
+
 def test_forward_requests_take_slices_of_their_passes():
     sizes = {"a": [(64, 64), (4, 4)]}
     big = S.Request("a", 0, passes=4)                    # 16384 paths
