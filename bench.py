@@ -567,6 +567,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         off = sum(a * b for a, b in frame.sizes[:i])
         tgt_np[name] = target[off:off + ww * hh].view(hh, ww, 3).cpu().numpy()
     e2e_steps = max(1, min(args.steps, 3))
+    # one untimed step first: the host path's own buffers (the device images,
+    # the library's pinned staging of large copies) are allocated on first use
+    imgs, dl, losses = r.render_forward_loss(tgt_np)
+    r.render_backward(dl)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -626,7 +630,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "iters_per_s": round(1e3 / ms_per_step, 4), "rays_per_step_per_gpu": int(rays),
         "parallelism": f"{w['cams'] * world} ring cameras split round robin over {world} GPU(s), gradients all-reduced",
         "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "warmup": 1},
         "gpu_launches": launches * args.steps,
         "roofline": {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),

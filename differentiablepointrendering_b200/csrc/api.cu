@@ -8,10 +8,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pale_b200.h"
@@ -84,6 +86,77 @@ uint32_t next_pow2(uint32_t v) {
   uint32_t c = 1;
   while (c < v) c <<= 1;
   return c;
+}
+
+// Pinned host memory that stages the copies between a caller's (pageable)
+// host buffers and the device: the device side of a copy runs at the
+// pinned-memory rate and the host side is split over threads, where a
+// pageable cudaMemcpyAsync copies through the driver's staging on one.
+struct HostStage {
+  char* p = nullptr;
+  size_t n = 0;
+  bool in_flight = false;   // a host-to-device copy from it may still run
+  void ensure(size_t bytes, cudaStream_t s) {
+    if (bytes <= n && p) return;
+    if (in_flight) CK(cudaStreamSynchronize(s));
+    in_flight = false;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    CK(cudaMallocHost(&p, bytes));
+    n = bytes;
+  }
+  ~HostStage() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+// Copies of at least this many bytes in total go through the stage.
+constexpr size_t kStageMinBytes = 4u << 20;
+
+// Threads of a staged host copy: PALE_COPY_THREADS, else up to 8.
+unsigned copy_threads() {
+  static const unsigned t = [] {
+    const char* e = std::getenv("PALE_COPY_THREADS");
+    const long v = e ? std::strtol(e, nullptr, 10) : 0;
+    if (v > 0) return (unsigned)std::min<long>(v, 64);
+    return std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  }();
+  return t;
+}
+
+struct HostPiece {
+  char* dst;
+  const char* src;
+  size_t bytes;
+};
+
+// memcpy of every piece, the pieces' bytes split evenly over the threads
+// (each thread a contiguous range of the concatenated pieces).
+void host_copy(const std::vector<HostPiece>& pieces) {
+  size_t total = 0;
+  for (const HostPiece& q : pieces) total += q.bytes;
+  const unsigned nt = (unsigned)std::min<size_t>(copy_threads(), std::max<size_t>(1, total / (1u << 20)));
+  auto range = [&](size_t a, size_t b) {   // bytes [a, b) of the concatenation
+    size_t off = 0;
+    for (const HostPiece& q : pieces) {
+      const size_t lo = std::max(a, off), hi = std::min(b, off + q.bytes);
+      if (lo < hi) std::memcpy(q.dst + (lo - off), q.src + (lo - off), hi - lo);
+      off += q.bytes;
+    }
+  };
+  if (nt <= 1) {
+    range(0, total);
+    return;
+  }
+  const size_t per = (total + nt - 1) / nt;
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (unsigned t = 0; t < nt; ++t) {
+    const size_t a = std::min(total, (size_t)t * per), b = std::min(total, a + per);
+    if (a < b) th.emplace_back(range, a, b);
+  }
+  for (std::thread& x : th) x.join();
 }
 
 }  // namespace
@@ -191,6 +264,7 @@ struct pale_handle {
   // density control scratch
   DBuf<uint32_t> dc_keys, dc_vals, dc_keys_tmp, dc_vals_tmp, dc_sort_temp, dc_flags, dc_dst, dc_list, dc_word, dc_aux;
   PointsBufs dc_points;
+  HostStage stage;            // staging of large host copies
   pale_stats stats{};
   uint64_t launches_last = 0;  // kernels launched by the last render call
   int stats_pending = 0;   // a render ran without reading its run state yet
@@ -1305,19 +1379,70 @@ void backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, const float* d
   adjoint_views({h}, all_passes(h, nsel, idx, h->st.estimator != PALE_ESTIMATOR_GATHER), d_dldi, d_dbg, sync);
 }
 
-void download_points(pale_handle* h, const PointsBufs& src, pale_points* out) {
+// Host-to-device copy from a caller's buffer on the handle's stream,
+// staged when large.  The stage holds the data until the copy has run: a
+// later staged copy into the stage waits for it.
+void copy_in(pale_handle* h, void* dev, const void* host, size_t bytes) {
+  if (!bytes) return;
   cudaStream_t s = h->stream;
+  if (bytes < kStageMinBytes) {
+    CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s));
+    return;
+  }
+  if (h->stage.in_flight) {
+    CK(cudaStreamSynchronize(s));
+    h->stage.in_flight = false;
+  }
+  h->stage.ensure(bytes, s);
+  host_copy({HostPiece{h->stage.p, static_cast<const char*>(host), bytes}});
+  CK(cudaMemcpyAsync(dev, h->stage.p, bytes, cudaMemcpyHostToDevice, s));
+  h->stage.in_flight = true;
+}
+
+struct DeviceOut {
+  void* host;        // null: skipped
+  const void* dev;
+  size_t bytes;
+};
+
+// Device-to-host copies into callers' buffers: enqueued on the handle's
+// stream (through the stage when they add up to kStageMinBytes or more),
+// then the run state is read (with `stats`) and the stream synchronised.
+void copy_out(pale_handle* h, const std::vector<DeviceOut>& outs, bool stats) {
+  cudaStream_t s = h->stream;
+  auto slot = [](size_t b) { return (b + 255) & ~size_t(255); };
+  size_t total = 0;
+  for (const DeviceOut& o : outs)
+    if (o.host && o.bytes) total += slot(o.bytes);
+  const bool staged = total >= kStageMinBytes;
+  std::vector<HostPiece> pieces;
+  if (staged) {
+    h->stage.ensure(total, s);   // the copies into it run after any copy out of it
+    size_t off = 0;
+    for (const DeviceOut& o : outs) {
+      if (!o.host || !o.bytes) continue;
+      CK(cudaMemcpyAsync(h->stage.p + off, o.dev, o.bytes, cudaMemcpyDeviceToHost, s));
+      pieces.push_back(HostPiece{static_cast<char*>(o.host), h->stage.p + off, o.bytes});
+      off += slot(o.bytes);
+    }
+  } else {
+    for (const DeviceOut& o : outs)
+      if (o.host && o.bytes) CK(cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, s));
+  }
+  if (stats) copy_stats(h);
+  CK(cudaStreamSynchronize(s));
+  h->stage.in_flight = false;
+  if (staged) host_copy(pieces);
+}
+
+void download_points(pale_handle* h, const PointsBufs& src, pale_points* out) {
   const size_t n = h->np;
   if (!n) return;
-  if (out->position) CK(cudaMemcpyAsync(out->position, src.pos.p, 12 * n, cudaMemcpyDeviceToHost, s));
-  if (out->tangent_u) CK(cudaMemcpyAsync(out->tangent_u, src.tu.p, 12 * n, cudaMemcpyDeviceToHost, s));
-  if (out->tangent_v) CK(cudaMemcpyAsync(out->tangent_v, src.tv.p, 12 * n, cudaMemcpyDeviceToHost, s));
-  if (out->scale) CK(cudaMemcpyAsync(out->scale, src.sc.p, 8 * n, cudaMemcpyDeviceToHost, s));
-  if (out->albedo) CK(cudaMemcpyAsync(out->albedo, src.alb.p, 12 * n, cudaMemcpyDeviceToHost, s));
-  if (out->opacity) CK(cudaMemcpyAsync(out->opacity, src.op.p, 4 * n, cudaMemcpyDeviceToHost, s));
-  if (out->beta) CK(cudaMemcpyAsync(out->beta, src.beta.p, 4 * n, cudaMemcpyDeviceToHost, s));
-  if (out->shape) CK(cudaMemcpyAsync(out->shape, src.shape.p, 4 * n, cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  copy_out(h, {DeviceOut{out->position, src.pos.p, 12 * n}, DeviceOut{out->tangent_u, src.tu.p, 12 * n},
+               DeviceOut{out->tangent_v, src.tv.p, 12 * n}, DeviceOut{out->scale, src.sc.p, 8 * n},
+               DeviceOut{out->albedo, src.alb.p, 12 * n}, DeviceOut{out->opacity, src.op.p, 4 * n},
+               DeviceOut{out->beta, src.beta.p, 4 * n}, DeviceOut{out->shape, src.shape.p, 4 * n}},
+           false);
 }
 
 // dst := src for the current point count (device to device, enqueued).
@@ -1473,9 +1598,7 @@ int pale_render_forward(pale_handle* h, uint32_t nsel, const uint32_t* idx, floa
     h->img_raw.ensure(4 * std::max<size_t>(1, pix));
     h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
     forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, true);
-    if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
-    if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    copy_out(h, {DeviceOut{raw, h->img_raw.p, 16 * pix}, DeviceOut{ldr, h->img_ldr.p, 16 * pix}}, false);
     return PALE_OK;
   });
 }
@@ -1490,9 +1613,7 @@ int pale_render_gather(pale_handle* h, uint32_t nsel, const uint32_t* idx, float
     h->img_raw.ensure(4 * std::max<size_t>(1, pix));
     h->img_ldr.ensure(4 * std::max<size_t>(1, pix));
     forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, true, false);
-    if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
-    if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    copy_out(h, {DeviceOut{raw, h->img_raw.p, 16 * pix}, DeviceOut{ldr, h->img_ldr.p, 16 * pix}}, false);
     return PALE_OK;
   });
 }
@@ -1528,15 +1649,15 @@ int pale_render_forward_loss(pale_handle* h, uint32_t nsel, const uint32_t* idx,
     h->dldi.ensure(4 * p1);
     h->target.ensure(channels * p1);
     h->loss.ensure(std::max(1u, nsel));
-    if (pix) CK(cudaMemcpyAsync(h->target.p, target, 4 * channels * pix, cudaMemcpyHostToDevice, h->stream));
+    // the stage at the size of the call's largest staged copy, allocated once
+    const size_t out_bytes = (raw ? 16 * pix : 0) + (ldr ? 16 * pix : 0) + (dldi ? 16 * pix : 0) + 4096;
+    if (out_bytes >= kStageMinBytes) h->stage.ensure(std::max<size_t>(out_bytes, 4ull * channels * pix), h->stream);
+    copy_in(h, h->target.p, target, 4ull * channels * pix);
     LossReq lq{h->target.p, channels, h->dldi.p, h->loss.p};
     forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, false, true, &lq);
-    if (raw) CK(cudaMemcpyAsync(raw, h->img_raw.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
-    if (ldr) CK(cudaMemcpyAsync(ldr, h->img_ldr.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
-    if (dldi) CK(cudaMemcpyAsync(dldi, h->dldi.p, 16 * pix, cudaMemcpyDeviceToHost, h->stream));
-    if (loss && nsel) CK(cudaMemcpyAsync(loss, h->loss.p, 8ull * nsel, cudaMemcpyDeviceToHost, h->stream));
-    copy_stats(h);
-    CK(cudaStreamSynchronize(h->stream));
+    copy_out(h, {DeviceOut{raw, h->img_raw.p, 16 * pix}, DeviceOut{ldr, h->img_ldr.p, 16 * pix},
+                 DeviceOut{dldi, h->dldi.p, 16 * pix}, DeviceOut{nsel ? loss : nullptr, h->loss.p, 8ull * nsel}},
+             true);
     return PALE_OK;
   });
 }
@@ -1574,7 +1695,7 @@ int pale_render_backward(pale_handle* h, uint32_t nsel, const uint32_t* idx, con
     for (uint32_t i = 0; i < nsel; ++i) pix += (size_t)h->cams[idx[i]].w * h->cams[idx[i]].h;
     use_stream(h, h->own_stream);
     h->dldi.ensure(4 * std::max<size_t>(1, pix));
-    if (pix) CK(cudaMemcpyAsync(h->dldi.p, dldi, 16 * pix, cudaMemcpyHostToDevice, h->stream));
+    copy_in(h, h->dldi.p, dldi, 16 * pix);
     float* dbg = nullptr;
     if (debug_opacity && h->st.debug_images) {
       h->dbg.ensure(4 * std::max<size_t>(1, pix));

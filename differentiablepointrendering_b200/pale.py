@@ -41,6 +41,33 @@ def _split_rgba(buf: np.ndarray, sizes) -> list:
     return out
 
 
+def _packed_parent(rgbs):
+    """The packed float32 RGBA buffer whose consecutive (H, W, 4) images
+    the (H, W, 3) arrays `rgbs` are, in order, the RGB views of (as
+    render_forward_loss returns dL/dI), or None."""
+    if not rgbs:
+        return None
+
+    def root(a):
+        while isinstance(a.base, np.ndarray):
+            a = a.base
+        return a
+
+    r = root(rgbs[0])
+    if r.dtype != np.float32 or not r.flags.c_contiguous:
+        return None
+    p0, off = r.__array_interface__["data"][0], 0
+    for a in rgbs:
+        h, w, _ = a.shape
+        if (a.dtype != np.float32 or a.strides != (16 * w, 16, 4) or root(a) is not r
+                or a.__array_interface__["data"][0] != p0 + 16 * off):
+            return None
+        off += h * w
+    if r.size < 4 * off:
+        return None
+    return r.reshape(-1)[:4 * off]
+
+
 def _pack_rgba(rgbs) -> tuple:
     """One packed float32 buffer of (H, W, 3) images with alpha 1 (the
     layout the C-ABI reads), and its (H, W, 4) view per image; a 4-float
@@ -48,8 +75,17 @@ def _pack_rgba(rgbs) -> tuple:
     n = sum(a.shape[0] * a.shape[1] for a in rgbs) * 4
     if n == 0:
         return np.zeros(4, np.float32), []
+    sizes = [(a.shape[1], a.shape[0]) for a in rgbs]
+    buf = _packed_parent(rgbs)
+    if buf is not None:
+        # the RGB views of one packed buffer: passed in place (its alpha,
+        # which no view shows, set to 1)
+        views = _split_rgba(buf, sizes)
+        for v in views:
+            v[..., 3] = 1.0
+        return buf, views
     buf = np.empty(n, np.float32)
-    views = _split_rgba(buf, [(a.shape[1], a.shape[0]) for a in rgbs])
+    views = _split_rgba(buf, sizes)
     for v, a in zip(views, rgbs):
         v[..., :3] = a
         v[..., 3] = 1.0
@@ -184,7 +220,7 @@ class Renderer:
             name = self._names[i]
             images[name] = l4
             images[name + "_raw"] = r4
-            grads[name] = np.ascontiguousarray(d4[..., :3])
+            grads[name] = d4[..., :3]          # a view: render_backward takes it in place
             losses[name] = float(loss[k])
         return images, grads, losses
 
@@ -208,7 +244,7 @@ class Renderer:
                 raise RuntimeError(f"render_backward: resolution mismatch for camera '{name}': target image is "
                                    f"{w}x{h}, but sensor is {sw}x{sh}")
             idx.append(i)
-            imgs.append(np.ascontiguousarray(arr).view(np.float32).reshape(h, w, 3))
+            imgs.append(arr.view(np.float32).reshape(h, w, 3))
         # one packed RGBA buffer; the returned adjoint sources are its views
         dldi, imgs = _pack_rgba(imgs)
         n = self.num_points

@@ -73,3 +73,48 @@ def test_device_forward_loss_matches_host(gpu):
         torch.testing.assert_close(torch_dldi[:, :3], f.dldi[:, :3], rtol=2.4e-7, atol=0)
     finally:
         r.close()
+
+
+def test_large_host_copies_are_exact(gpu):
+    """Host calls whose copies go through the pinned stage (4 MB and more:
+    two 512x512 views, 80k surfels' gradients) return byte for byte what
+    the device-resident calls leave on the device, and the dL/dI views that
+    render_forward_loss returns go back to render_backward in place with the
+    same gradients as packed copies of them."""
+    import torch
+
+    from differentiablepointrendering_b200.device import DeviceFrame
+
+    sc = make_box_scene(80000, cameras=2, resolution=512)
+    r = Renderer.from_scene(sc, SETTINGS)
+    try:
+        names = r.get_camera_names()
+        rng = np.random.default_rng(11)
+        targets = {n: rng.uniform(0, 1, (512, 512, 3)).astype(np.float32) for n in names}
+        images, dldi, loss = r.render_forward_loss(targets)
+        f = DeviceFrame(r, device=torch.device("cuda:0"))
+        packed = torch.from_numpy(np.concatenate([targets[n].reshape(-1, 3) for n in names])).cuda()
+        dl = f.forward_loss(packed)
+        torch.cuda.synchronize()
+        for i, (n, l4, d4) in enumerate(zip(names, f.split(f.ldr), f.split(f.dldi))):
+            np.testing.assert_array_equal(l4.cpu().numpy(), images[n])
+            np.testing.assert_array_equal(d4[..., :3].cpu().numpy(), dldi[n])
+            assert float(dl[i]) == loss[n]
+            assert dldi[n].strides == (16 * 512, 16, 4)      # an RGB view of the packed buffer
+        g_inplace, src = r.render_backward(dldi)
+        g_copied, _ = r.render_backward({n: np.ascontiguousarray(v) for n, v in dldi.items()})
+        for n in names:
+            assert np.all(src["adjoint_source"][n][..., 3] == 1.0)
+            np.testing.assert_array_equal(src["adjoint_source"][n][..., :3], dldi[n])
+        for k in g_inplace:
+            a, b = g_inplace[k].astype(np.float64), g_copied[k].astype(np.float64)
+            # the same inputs; the adjoint adds its gradients with float atomics
+            assert np.linalg.norm(a - b) <= 1e-5 * max(np.linalg.norm(b), 1e-30), k
+        assert np.linalg.norm(g_inplace["opacity"]) > 0
+        # the staged gradient copy against the device-resident backward
+        f.backward()
+        torch.cuda.synchronize()
+        dev = f.grads["opacity"].cpu().numpy().astype(np.float64)
+        assert np.linalg.norm(dev - g_inplace["opacity"]) <= 1e-5 * np.linalg.norm(dev)
+    finally:
+        r.close()
