@@ -783,10 +783,12 @@ __global__ void __launch_bounds__(kBlock, kLookupMinBlocks) k_cg_lookup(FrameArg
     const uint32_t kind = word >> 30, idx = word & kRecIndexMask, sid = kMulti ? (word >> 27) & 7u : 0u;
     if (kind == kRecNone) continue;
     const SceneView& S = A.scenes.s[sid];
+    // the reflectance, loaded before the gather so that its latency overlaps it
+    float4 refl = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lane == 0) refl = kind == kRecSurfel ? __ldg(&S.sf.alb[idx]) : __ldg(&S.mesh.materials[idx]);
     uint32_t cnt = 0;
     const V3 E = gather_irradiance_warp<false>(S.grid, s_gc[sid], xyz(ra), xyz(rb), terms, cnt);
     if (lane == 0) {
-      const float4 refl = kind == kRecSurfel ? __ldg(&S.sf.alb[idx]) : __ldg(&S.mesh.materials[idx]);
       ++queries;
       scanned += cnt;
       V3 Lo;
