@@ -96,15 +96,22 @@ struct HostStage {
   char* p = nullptr;
   size_t n = 0;
   bool in_flight = false;   // a host-to-device copy from it may still run
-  void ensure(size_t bytes, cudaStream_t s) {
-    if (bytes <= n && p) return;
+  // At least `bytes` of pinned memory; false (and no stage) when the host
+  // cannot pin that much, and the copies then go through pageable memory.
+  bool ensure(size_t bytes, cudaStream_t s) {
+    if (bytes <= n && p) return true;
     if (in_flight) CK(cudaStreamSynchronize(s));
     in_flight = false;
     if (p) cudaFreeHost(p);
     p = nullptr;
     n = 0;
-    CK(cudaMallocHost(&p, bytes));
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();   // the failed allocation is not sticky; clear it
+      p = nullptr;
+      return false;
+    }
     n = bytes;
+    return true;
   }
   ~HostStage() {
     if (p) cudaFreeHost(p);
@@ -1393,7 +1400,10 @@ void copy_in(pale_handle* h, void* dev, const void* host, size_t bytes) {
     CK(cudaStreamSynchronize(s));
     h->stage.in_flight = false;
   }
-  h->stage.ensure(bytes, s);
+  if (!h->stage.ensure(bytes, s)) {
+    CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s));
+    return;
+  }
   host_copy({HostPiece{h->stage.p, static_cast<const char*>(host), bytes}});
   CK(cudaMemcpyAsync(dev, h->stage.p, bytes, cudaMemcpyHostToDevice, s));
   h->stage.in_flight = true;
@@ -1414,10 +1424,10 @@ void copy_out(pale_handle* h, const std::vector<DeviceOut>& outs, bool stats) {
   size_t total = 0;
   for (const DeviceOut& o : outs)
     if (o.host && o.bytes) total += slot(o.bytes);
-  const bool staged = total >= kStageMinBytes;
+  const bool staged = total >= kStageMinBytes && h->stage.ensure(total, s);
   std::vector<HostPiece> pieces;
   if (staged) {
-    h->stage.ensure(total, s);   // the copies into it run after any copy out of it
+    // (the copies into the stage run after any copy out of it: same stream)
     size_t off = 0;
     for (const DeviceOut& o : outs) {
       if (!o.host || !o.bytes) continue;
@@ -1651,7 +1661,7 @@ int pale_render_forward_loss(pale_handle* h, uint32_t nsel, const uint32_t* idx,
     h->loss.ensure(std::max(1u, nsel));
     // the stage at the size of the call's largest staged copy, allocated once
     const size_t out_bytes = (raw ? 16 * pix : 0) + (ldr ? 16 * pix : 0) + (dldi ? 16 * pix : 0) + 4096;
-    if (out_bytes >= kStageMinBytes) h->stage.ensure(std::max<size_t>(out_bytes, 4ull * channels * pix), h->stream);
+    if (out_bytes >= kStageMinBytes) (void)h->stage.ensure(std::max<size_t>(out_bytes, 4ull * channels * pix), h->stream);
     copy_in(h, h->target.p, target, 4ull * channels * pix);
     LossReq lq{h->target.p, channels, h->dldi.p, h->loss.p};
     forward(h, nsel, idx, h->img_raw.p, h->img_ldr.p, false, true, &lq);
