@@ -171,9 +171,14 @@ struct EventBufs {
 // grid through the view's scene index.  The traversal kernels stage each
 // scene's first top_nodes LBVH nodes in shared memory, scene k's in the
 // slot [k * staged, (k + 1) * staged) (top_nodes <= staged; a small scene
-// stages fewer), at most kStagedNodesPerCall nodes for the whole table.
+// stages fewer), at most kStagedNodesPerCall nodes for the whole table:
+// 16 KB, so that the camera walk (with its 16 KB stack and 16 KB hit list
+// per 256-thread block) keeps 4 resident blocks in a call of many scenes.
+#ifndef PALE_STAGED_NODES_PER_CALL
+#define PALE_STAGED_NODES_PER_CALL 512
+#endif
 constexpr uint32_t kMaxScenes = 8;
-constexpr uint32_t kStagedNodesPerCall = 1024;
+constexpr uint32_t kStagedNodesPerCall = PALE_STAGED_NODES_PER_CALL;
 
 struct SceneTable {
   SceneView s[kMaxScenes];
