@@ -114,3 +114,27 @@ def test_two_scenes_in_one_wavefront_equal_each_alone(gpu):
     finally:
         ra.close()
         rb.close()
+
+
+def test_five_scenes_in_one_wavefront_equal_each_alone(gpu):
+    """Five scenes in one call stage fewer top nodes each (the call's
+    staged-node budget split over its scenes) than a scene alone: the images
+    are still those of each scene rendered alone, bit for bit."""
+    import torch
+    from differentiablepointrendering_b200.device import DeviceFrame, ViewBatch
+
+    scenes = [_scene(2500 + 700 * k, 2, 32 + 8 * k, 40 + k) for k in range(5)]
+    rs = [Renderer.from_scene(sc, ST) for sc in scenes]
+    try:
+        views = [(k, c, 2 + k % 3, 0) for k in (4, 0, 3, 1, 2) for c in (1, 0)]
+        batch = ViewBatch(rs, views)
+        batch.forward_loss(None)
+        torch.cuda.synchronize()
+        for i, (s, c, p, _) in enumerate(views):
+            alone = ViewBatch([rs[s]], [(0, c, p, 0)])
+            alone.forward_loss(None)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(batch.split(batch.raw)[i].cpu().numpy(), alone.split(alone.raw)[0].cpu().numpy())
+    finally:
+        for r in rs:
+            r.close()
