@@ -15,6 +15,13 @@
  * pale_bindings.cpp:734-757) every per-point array that comes back
  * (parameters, gradients) is in BVH order; pale_get_order() gives the map
  * order[bvh_index] = asset_index.
+ *
+ * Host buffers: the render calls that take host pointers copy 4 MB and
+ * more at a time through pinned memory the handle holds (allocated at the
+ * size of the largest such copy; without it, when the host cannot pin that
+ * much, they copy from pageable memory), the host side of each copy split
+ * over threads: the environment variable PALE_COPY_THREADS, read once,
+ * sets how many (default: up to 8).
  */
 #ifndef PALE_B200_H
 #define PALE_B200_H
