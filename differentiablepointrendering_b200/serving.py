@@ -148,7 +148,8 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
                max_scenes: int = MAX_ROUND_SCENES, policy: str = "arrival",
                now: float = 0.0, starve_s: float = 2.0,
                slices: bool = False,
-               layers: Optional[Dict[str, List[float]]] = None) -> Tuple[List[Request], List[Request]]:
+               layers: Optional[Dict[str, List[float]]] = None,
+               slice_gradients: bool = False) -> Tuple[List[Request], List[Request]]:
     """The requests of the next round, at most max_views views, max_pixels
     camera pixels, max_scenes distinct scenes and (when given) max_paths
     camera paths (request_paths); returns (taken, left), left in arrival
@@ -162,11 +163,13 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
     fit, so that light requests are not held behind heavy ones and a heavy
     one waits at most about starve_s plus a round; the round's work is then
     also capped at 8 times its first request's (2^20 paths at least), so
-    that requests of very different costs do not share a round.  With slices (and a path cap) a
-    forward request over the cap that comes first renders as many of its
-    passes as the cap holds, one at least, in a round of its own, and goes
-    back to the queue for the rest: a heavy request advances in slices
-    between which newly arrived requests get rounds.  The first request
+    that requests of very different costs do not share a round.  With
+    slices (and a path cap) a forward request over the cap that comes first
+    renders as many of its passes as the cap holds, one at least, in a round
+    of its own, and goes back to the queue for the rest: a heavy request
+    advances in slices between which newly arrived requests get rounds; a
+    gradient request too with slice_gradients (its loss and adjoint then
+    run in the round of its last forward pass).  The first request
     considered always goes."""
     def work(q):
         return request_paths(q, sizes, max_passes) * path_weight(q, layers) * (2 if q.kind == "gradient" else 1)
@@ -187,7 +190,7 @@ def plan_round(queue: List[Request], sizes: Dict[str, List[Tuple[int, int]]], ma
         k = 0                                  # all remaining passes
         fits = not taken or ((cap is None or paths + n <= cap)
                              and (cost_cap is None or cost + n * pw <= cost_cap))
-        if not taken and slices and q.kind == "forward" and cap is not None and n > cap:
+        if not taken and slices and (q.kind == "forward" or slice_gradients) and cap is not None and n > cap:
             k = max(1, cap // (w * h))         # a first request over the cap renders a slice
         if taken and (not fits or len(taken) + 1 > max_views or pix + w * h > max_pixels
                       or (q.scene not in scenes and len(scenes) >= max_scenes)):
@@ -405,7 +408,8 @@ class Server:
                 taken, self._queue = plan_round(self._queue, sizes, self.max_views, self.max_pixels,
                                                 self.max_paths, spp, policy=self.policy,
                                                 now=time.perf_counter(), starve_s=self.starve_s,
-                                                slices=self.slices, layers=layers)
+                                                slices=self.slices, layers=layers,
+                                                slice_gradients=not self._gather)
             try:
                 with self._gpu:
                     self._round(taken)
@@ -477,10 +481,11 @@ class Server:
                     q.next_pass, q.partial = passes(q), None
                     finished.append(k)
             dldi = {}
+            done_now = set(finished)
             for k, i in enumerate(idx):
                 q = reqs[i]
-                if q.kind != "gradient":
-                    continue
+                if q.kind != "gradient" or k not in done_now:
+                    continue   # (a sliced gradient request's loss waits for its last slice)
                 t = torch.from_numpy(np.ascontiguousarray(q.target, np.float32).reshape(-1, 3)).to(self.device)
                 d = torch.zeros(int(offs[k + 1] - offs[k]), 4, dtype=torch.float32, device=self.device)
                 torch.sub(vb.ldr[offs[k]:offs[k + 1], :3], t, out=d[:, :3])
@@ -522,6 +527,7 @@ class Server:
                 finish(grad_idx, [self._host_grads(g) for g in gl])
             return
         vb, offs, dldi = forward(list(range(len(reqs))), self._exec)
+        grad_idx = [i for i in grad_idx if i in dldi]   # those whose image is finished
         per = self.GRADIENTS_PER_WAVEFRONT - 1     # entry 0 is the executor
         for c0 in range(0, len(grad_idx), per):
             chunk = grad_idx[c0:c0 + per]

@@ -133,3 +133,43 @@ def test_forward_requests_in_slices_equal_alone(gpu, policy):
             np.testing.assert_array_equal(alone.image, q.image)
     finally:
         srv.close()
+
+
+def test_gradient_requests_in_slices_equal_alone(gpu):
+    """With a round cap of 4096 camera paths, 64x64 gradient requests of 4
+    passes render their forward in slices over several rounds and their
+    adjoint in the round of the last slice: image and loss bit for bit those
+    of the request alone, gradients up to the order of float atomic
+    additions."""
+    import torch
+
+    from differentiablepointrendering_b200.serving import Request, Server
+
+    free, _ = torch.cuda.mem_get_info()
+    srv = Server(hbm_budget=free, settings={"rng_mode": "decorrelated"}, max_paths=4096, policy="light_first")
+    try:
+        a, b = _scenes()
+        srv.add_scene("a", a, SETTINGS)
+        srv.add_scene("b", b, SETTINGS)
+        rng = np.random.default_rng(6)
+        mix = [Request("b", k % 3, "gradient", rng.uniform(0, 1, (64, 64, 3)).astype(np.float32), 4, 2)
+               for k in range(4)] + [Request("a", k % 4, "forward", None, 1 + k % 4, 0) for k in range(6)]
+        for q in mix:
+            srv.submit(q)
+        for q in mix:
+            assert q.done.wait(120), q
+            assert q.error is None, q.error
+        grads = [q for q in mix if q.kind == "gradient"]
+        assert max(q.slices for q in grads) > 1
+        lit = 0
+        for q in grads:
+            alone = srv.serve_one(Request(q.scene, q.camera, q.kind, q.target, q.passes, q.depth))
+            assert alone.error is None and alone.slices == 1
+            np.testing.assert_array_equal(alone.image, q.image)
+            assert alone.loss == q.loss
+            a_, b_ = alone.grads["opacity"].astype(np.float64), q.grads["opacity"].astype(np.float64)
+            assert np.linalg.norm(a_ - b_) <= 1e-4 * np.linalg.norm(b_)
+            lit += int(np.linalg.norm(b_) > 0)
+        assert lit >= 1
+    finally:
+        srv.close()

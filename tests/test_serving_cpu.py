@@ -156,9 +156,13 @@ def test_forward_requests_take_slices_of_their_passes():
     big.next_pass = 3                                        # one pass left: fits whole
     taken, _ = S.plan_round([big], sizes, 64, 10 ** 6, max_paths=4096, slices=True)
     assert taken == [big] and big.round_passes == 0
-    # a gradient request is never sliced; as the first of a round it goes whole
+    # a gradient request is not sliced by default; as the first of a round it goes whole
     taken, left = S.plan_round([grad, small], sizes, 64, 10 ** 6, max_paths=4096, slices=True)
     assert taken == [grad] and grad.round_passes == 0 and left == [small]
+    # with slice_gradients its forward renders in slices like a forward request's
+    taken, left = S.plan_round([grad, small], sizes, 64, 10 ** 6, max_paths=4096, slices=True,
+                               slice_gradients=True)
+    assert taken == [grad] and grad.round_passes == 1
     # without slices the big request waits for a round of its own
     big.next_pass = 0
     taken, left = S.plan_round([small, big], sizes, 64, 10 ** 6, max_paths=4096)
